@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Benchmark of the D3Q27 cumulant time step (MLUPS and HBM-roofline fraction).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME] [--storage f32|f16|bf16]
+
+A "step" is one coarse time step (updateAllGrids) of the whole domain.
+One process per GPU (torchrun for N > 1); domains are independent replicas,
+so scaling is weak and there is no data-path collective.  Rank 0 prints one
+JSON line.  ``--impl reference`` times the reference algorithm's CPU
+implementation (the C oracle, all host threads) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+BYTES_PER_POP = {"f32": 4, "f16": 2, "bf16": 2}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- workloads
+def make_case(name: str, storage: str):
+    import lbm3_b200 as L
+    from lbm3_b200 import _abi as A
+    st = {"f32": A.LBM_STORE_F32, "f16": A.LBM_STORE_F16, "bf16": A.LBM_STORE_BF16}[storage]
+    if name == "box256x128x128":
+        # the 256x128x128 single-level grid of the flow-around-sphere
+        # configuration, fully periodic and without the obstacle
+        c = L.periodic_box(254, 126, 126, nu_lattice=0.0096, ux=0.04, storage=st)
+        desc = ("periodic box 256x128x128 cells incl. ghosts (sphere-config grid, no obstacle, "
+                "no open boundaries), nu=0.0096, u=0.04")
+        return c, desc, None
+    if name == "tgv64":
+        s = L.tgv_plain_method(storage=st)
+        return s.case, "Taylor-Green vortex 64^3 periodic (66^3 incl. ghosts), u0=0.05, nu=0.01", s
+    if name == "tgv128":
+        s = L.taylor_green(128, storage=st)
+        return s.case, "Taylor-Green vortex Re1600 Ma0.1 128^3 periodic (130^3 incl. ghosts)", s
+    raise SystemExit(f"unknown workload {name}")
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.file is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.file.flush()
+        rows = [l.split(",") for l in Path(self.file.name).read_text().splitlines() if l.strip()]
+        os.unlink(self.file.name)
+        if self.uuid:
+            rows = [r for r in rows if r[0].strip() == self.uuid] or rows
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for nme, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nme)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------- CPU legs
+def time_oracle(case, target_s: float, min_steps: int = 1):
+    """Time the C oracle (all host threads) on the same workload: returns
+    (MLUPS, steps, seconds, threads)."""
+    import oracle as O
+    g = O.OracleGrid(case)
+    cells = g.g.fluidUpdates
+    g.step(1)  # warm the pages
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        g.step(1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if steps >= min_steps and el >= target_s:
+            break
+    g.close()
+    return cells * steps / el / 1e6, steps, el, O.threads()
+
+
+def run_reference(args):
+    """CPU implementation of the reference algorithm (the C oracle, all host
+    threads) on the same workload.  Each timed step is a bounded slice of a
+    full step (a contiguous run of cells of the collide-stream), sized so the
+    whole --steps K run takes about --ref-seconds."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    case, desc, _ = make_case(args.workload, "f32")
+    import oracle as O
+    g = O.OracleGrid(case)
+    n = g.cell_count
+    # estimate the rate on a small slice, then size the per-step slice
+    probe = min(n, 200_000)
+    t0 = time.perf_counter()
+    g.collide_range(0, probe)
+    rate = probe / max(time.perf_counter() - t0, 1e-6)
+    per_step = int(min(n, max(1000, rate * args.ref_seconds / max(args.steps + args.warmup, 1))))
+    pos = 0
+
+    def one():
+        nonlocal pos
+        c0 = pos
+        c1 = min(n, c0 + per_step)
+        g.collide_range(c0, c1)
+        pos = 0 if c1 >= n else c1
+        return c1 - c0
+
+    for _ in range(args.warmup):
+        one()
+    done, t0 = 0, time.perf_counter()
+    for _ in range(args.steps):
+        done += one()
+    el = time.perf_counter() - t0
+    g.close()
+    mlups = done / el / 1e6
+    line = {
+        "impl": "reference", "metric": "MLUPS", "value": round(mlups, 3), "unit": "MLUPS",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * el / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": desc, "cells": n, "storage": "f32"},
+        "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": O.threads(), "kind": "port",
+                         "sample": f"each step = collide-stream of {per_step} consecutive cells of the "
+                                   f"{n}-cell grid (C restatement of the reference time step, OpenMP, "
+                                   f"{O.threads()} threads)"},
+        "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU leg
+def run_ours(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    import lbm3_b200 as L
+    case, desc, tgv = make_case(args.workload, args.storage)
+    stream = torch.cuda.Stream()
+    g = L.build_grids(case)
+    g.set_stream(stream.cuda_stream)
+    info = g.info()
+    updates = g.fluid_updates_per_iteration
+    with torch.cuda.stream(stream):
+        g.update_all_grids(args.warmup)
+    g.synchronize()
+
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(local).uuid)
+        uuid = "GPU-" + uuid if not uuid.startswith("GPU-") else uuid
+    except Exception:
+        pass
+
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(uuid) as clk:
+        ms = g.time_steps(args.steps)          # CUDA events on the grid stream
+    torch.cuda.synchronize()
+    kernel_ms, launches = g.last_kernel_time()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = updates * args.steps * world / (ms_max * 1e-3) / 1e6
+
+    # roofline of the dominant kernel (collide-stream): algorithmic bytes =
+    # 2 x 27 populations per fluid cell update at the storage width
+    bpp = BYTES_PER_POP[args.storage]
+    alg_bytes = updates * 2 * 27 * bpp
+    per_launch_ms = kernel_ms / max(launches, 1)
+    achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        tr = json.loads(tfile.read_text()).get(f"{args.workload}:{args.storage}")
+        if tr:
+            traffic = tr
+
+    # end to end through the public API: upload the initial state from pinned
+    # host memory, then run steps that each read the step's observable back
+    e2e_steps = max(10, min(args.steps // 10, 200))
+    f0 = g.populations()
+    pinned = torch.from_numpy(f0).pin_memory()
+    import numpy as np
+    f_np = pinned.numpy()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g.set_populations(f_np)
+    for _ in range(e2e_steps):
+        g.update_all_grids(1)
+        if tgv is not None:
+            g.kinetic_energy(tgv.u_initial_phys, tgv.domain_length)
+        else:
+            g.kinetic_energy(1.0, 1000.0)
+    g.synchronize()
+    e2e_s = time.perf_counter() - t0
+    t2 = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+    e2e_value = updates * e2e_steps * world / float(t2.item()) / 1e6
+    del np
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        mlups, steps, el, thr = time_oracle(case, target_s=args.cpu_seconds)
+        cpu = {"value": round(mlups, 3), "unit": "MLUPS", "cores": thr, "kind": "port",
+               "sample": f"{steps} full steps of the same workload ({el:.1f} s, FP32) by the C restatement "
+                         f"of the reference time step on the host cores (OpenMP)"}
+
+    clocks = clk.summary()
+    g.close()
+    if rank == 0:
+        line = {
+            "metric": "MLUPS", "value": round(value, 2), "unit": "MLUPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 5),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": args.storage if args.storage != "f32" else "f32", "data": "synthetic",
+            "config": {"workload": desc, "cells": info.cell_count, "fluid_updates_per_step": updates,
+                       "storage": args.storage, "compute": "f32",
+                       "l2": "inputs larger than L2 (populations %.0f MB > 126 MB)" % (alg_bytes / 2 / 1e6)
+                       if alg_bytes / 2 > 126e6 else "inputs smaller than L2",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
+                         "kernel": "collideStream", "kernel_ms_per_launch": round(per_launch_ms, 5),
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS",
+                    "h2d_bytes_per_step": int(f0.nbytes // e2e_steps), "d2h_bytes_per_step": 8,
+                    "steps": e2e_steps,
+                    "note": "initial populations uploaded from pinned host memory inside the timed "
+                            "region; every step reads its kinetic energy back (tracker period 1)"},
+            "gpu_launches": launches + (launches if info.periodic_count > 0 else 0),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="box256x128x128")
+    ap.add_argument("--storage", choices=["f32", "f16", "bf16"], default="f32")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-seconds", type=float, default=90.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

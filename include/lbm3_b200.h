@@ -1,0 +1,220 @@
+/*
+ * lbm3_b200.h — C ABI of the B200-native D3Q27 cumulant lattice-Boltzmann time step.
+ *
+ * Plain C types only (pointers, sizes, PODs); no C++ or torch types cross this
+ * boundary.  Every call returns an int status (LBM_OK == 0, negative on error)
+ * and leaves a human-readable message behind lbm_last_error().  Exceptions
+ * never cross the boundary.
+ *
+ * The reference (stepanmuller/LBM3) exposes a header-level C++ API whose case
+ * configuration is compile-time: constants such as RES_GLOBAL / NU_PHYS and
+ * four __cuda_callable__ hooks (getOpenBC, getLocalBC, getInitialCondition,
+ * getRefinementModifier) defined in the driver translation unit.  Here those
+ * become the runtime, table-driven `lbm_case` description below.  Each entry
+ * point names the reference function it replaces (path:line inside the
+ * reference project).
+ */
+#ifndef LBM3_B200_H
+#define LBM3_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define LBM_OK               0
+#define LBM_ERR_INVALID     -1  /* bad argument or inconsistent case            */
+#define LBM_ERR_CUDA        -2  /* a CUDA runtime call failed                   */
+#define LBM_ERR_OOM         -3  /* device allocation failed                     */
+#define LBM_ERR_BUILD       -4  /* setup failed (the reference throws
+                                   std::runtime_error at these points, e.g.
+                                   include/gridBuilderFunctions.h:1479,:1563) */
+#define LBM_ERR_UNSUPPORTED -5  /* feature not available in this build          */
+#define LBM_ERR_NO_DEVICE   -6  /* no CUDA device visible                       */
+
+/* ---- boundary kinds for a domain face (replaces the getOpenBC hook) ------ */
+#define LBM_BC_PERIODIC   0   /* BCStruct.periodic     (include/types.h:131-136) */
+#define LBM_BC_VELOCITY   1   /* BCStruct.dirichletU                             */
+#define LBM_BC_PRESSURE   2   /* BCStruct.dirichletRho                           */
+
+/* face order inside lbm_case.face[] */
+#define LBM_FACE_XMIN 0
+#define LBM_FACE_XMAX 1
+#define LBM_FACE_YMIN 2
+#define LBM_FACE_YMAX 3
+#define LBM_FACE_ZMIN 4
+#define LBM_FACE_ZMAX 5
+
+/* initial condition kinds (replaces the getInitialCondition hook) */
+#define LBM_IC_UNIFORM      0  /* dRho, ux, uy, uz constant                      */
+#define LBM_IC_TAYLOR_GREEN 1  /* cases/taylorGreenVortex/taylorGreenVortexMain.cu:66-87 */
+
+/* population storage precision (compute is always FP32) */
+#define LBM_STORE_F32  0
+#define LBM_STORE_F16  1      /* shifted populations f_i - w_i as IEEE half     */
+#define LBM_STORE_BF16 2      /* shifted populations f_i - w_i as bfloat16      */
+
+/* arrays that lbm_read_array can copy out (per level) */
+#define LBM_ARRAY_F            0  /* float  [27][cellCount] (always returned as FP32) */
+#define LBM_ARRAY_SHIFTER      1  /* int32  [cellCount]     IJKNBR.shifterArray   */
+#define LBM_ARRAY_ROW_I        2  /* int32  [rowCount]      IJKNBR.iArray         */
+#define LBM_ARRAY_ROW_J        3  /* int32  [rowCount]      IJKNBR.jArray         */
+#define LBM_ARRAY_ROW_K        4  /* int32  [rowCount]      IJKNBR.kArray         */
+#define LBM_ARRAY_ROW_JPLUS    5  /* int32  [rowCount]      IJKNBR.jPlusArray     */
+#define LBM_ARRAY_ROW_KPLUS    6  /* int32  [rowCount]      IJKNBR.kPlusArray     */
+#define LBM_ARRAY_ROW_JKPLUS   7  /* int32  [rowCount]      IJKNBR.jkPlusArray    */
+#define LBM_ARRAY_WALL_MAP     8  /* int32  [cellCount]     Wall.wallMapArray     */
+#define LBM_ARRAY_PERIODIC_INDEX  9  /* int32 [periodicCount] PeriodicBC.indexArray  */
+#define LBM_ARRAY_PERIODIC_SOURCE 10 /* int32 [periodicCount] PeriodicBC.sourceArray */
+#define LBM_ARRAY_MACRO        11 /* float  [4][cellCount]  dRho, ux, uy, uz of the
+                                     current pre-collision state (getDRhoUxUyUz)  */
+
+/* ---- case description -------------------------------------------------- */
+
+/* One domain face.  `priority` decides edge and corner cells: a boundary cell
+ * that touches several faces takes the description of the touching face with
+ * the highest priority (ties: lower face index).  This reproduces drivers
+ * such as cases/flowAroundSphere/flowAroundSphereMain.cu:103-135, where
+ * edges of the inlet/outlet faces belong to the side faces. */
+typedef struct lbm_face_bc {
+    int   kind;                 /* LBM_BC_*                                   */
+    int   open_bc_id;           /* BCStruct.openBCID                          */
+    int   priority;
+    int   non_reflective;       /* BCStruct.nonReflective                     */
+    float non_reflective_beta;  /* BCStruct.nonReflectiveBeta (default 7)     */
+    float dRho, ux, uy, uz;     /* target values                              */
+} lbm_face_bc;
+
+typedef struct lbm_case {
+    /* compile-time constants of a reference driver */
+    int   grid_level_count;     /* GRID_LEVEL_COUNT (1 in this build)          */
+    int   wall_refinement_count;/* WALL_REFINEMENT_COUNT                       */
+    float res_global;           /* RES_GLOBAL, mm                              */
+    float nu_phys;              /* NU_PHYS, m^2/s                              */
+    float rho_phys;             /* RHO_PHYS, kg/m^3                            */
+    float dt_phys_global;       /* DT_PHYS_GLOBAL, s                           */
+    float bounds[6];            /* BoundsStruct: xMin,yMin,zMin,xMax,yMax,zMax (mm) */
+    int   track_wall_force;     /* TRACK_WALL_FORCE                            */
+    int   track_open_boundaries;/* TRACK_OPEN_BOUNDARIES                       */
+
+    /* getOpenBC */
+    lbm_face_bc face[6];
+
+    /* getInitialCondition */
+    int   ic_kind;
+    float ic_dRho, ic_ux, ic_uy, ic_uz;   /* LBM_IC_UNIFORM                   */
+    float tgv_u0;               /* LBM_IC_TAYLOR_GREEN: lattice amplitude      */
+    float tgv_length;           /* X = x / tgv_length (x in mm)                */
+
+    /* getLocalBC (uniform over the domain) */
+    float collision_limiter;    /* BCStruct.collisionLimiter; <= 0 selects AllOne */
+    float nu_multiplier;        /* BCStruct.nuMultiplier                       */
+
+    /* storage */
+    int   storage;              /* LBM_STORE_*                                 */
+} lbm_case;
+
+/* Per-level summary (InfoStruct, include/types.h:120-129, plus table sizes). */
+typedef struct lbm_grid_info {
+    int   grid_id;
+    int   cell_count, cell_count_x, cell_count_y, cell_count_z;
+    int   row_count;            /* compressed IJKNBR rows                      */
+    int   wall_cell_count;      /* wallMap == -3                               */
+    int   wall_adjacent_count;  /* Wall.wallAdjacentCount                      */
+    int   periodic_count;       /* PeriodicBC.periodicBCCount                  */
+    int   open_bc_count;        /* total open-boundary cells over all IDs      */
+    int   esotwist_flipper;
+    int   iterations_finished;
+    int   storage;
+    float res, ox, oy, oz, nu, dt_phys;
+    unsigned long long grid_memory_bytes;
+} lbm_grid_info;
+
+typedef struct lbm_grids lbm_grids;   /* opaque: all levels of one domain */
+typedef struct lbm_plan lbm_plan;     /* opaque: host-side tables, no device memory */
+
+/* Last error message of the calling thread ("" when none). */
+const char* lbm_last_error(void);
+
+/* Number of visible CUDA devices, or a negative status. */
+int lbm_device_count(void);
+
+/* Run the grid construction on the host only: every table of every level
+ * and its device footprint, without touching a GPU.  Used for footprint
+ * admission before allocation and for table parity checks.
+ * Replaces the host-visible part of buildGrids (include/gridBuilderFunctions.h:1577-1649,
+ * including the per-level memory accounting printed at :1630-1663). */
+int lbm_plan_grids(const lbm_case* c, lbm_plan** out, long long* fluid_updates_per_iteration);
+void lbm_free_plan(lbm_plan* p);
+int lbm_plan_level_count(lbm_plan* p);
+int lbm_plan_info(lbm_plan* p, int level, lbm_grid_info* out);
+/* Same array ids as lbm_read_array except LBM_ARRAY_F and LBM_ARRAY_MACRO. */
+int lbm_plan_read_array(lbm_plan* p, int level, int which, void* host, size_t bytes);
+
+/* Build every grid level on the current CUDA device, allocate the populations
+ * and apply the initial condition.
+ * Replaces buildGrids (include/gridBuilderFunctions.h:1577-1670) together with
+ * applyInitialCondition (include/boundaryConditions/applyInitialCondition.h:8-84).
+ * `fluid_updates_per_iteration` receives Σ_level (cells − wall cells)·2^level
+ * (include/gridBuilderFunctions.h:1601-1608); it may be NULL. */
+int lbm_build_grids(const lbm_case* c, lbm_grids** out,
+                    long long* fluid_updates_per_iteration);
+
+/* Release all device and host memory of a domain. */
+void lbm_free_grids(lbm_grids* g);
+
+/* Launch subsequent work on this CUDA stream (cudaStream_t passed as void*,
+ * NULL = legacy default stream). */
+int lbm_set_stream(lbm_grids* g, void* stream);
+
+/* Advance `coarse_steps` coarse time steps (asynchronous on the grid stream).
+ * Replaces the driver loop `updateAllGrids(grids, 0)`
+ * (include/updateGrid.h:388-396, one call per coarse step). */
+int lbm_update_all_grids(lbm_grids* g, int coarse_steps);
+
+/* Block until the grid stream is idle; returns a pending CUDA error, if any. */
+int lbm_synchronize(lbm_grids* g);
+
+/* Time `steps` coarse steps with CUDA events on the grid stream; *ms receives
+ * the elapsed device time. */
+int lbm_time_steps(lbm_grids* g, int steps, float* ms);
+
+/* Device time of the collide-stream launches inside the most recent
+ * lbm_time_steps call, each bracketed by CUDA events on the grid stream:
+ * summed kernel milliseconds and the number of launches. */
+int lbm_last_kernel_time(lbm_grids* g, float* kernel_ms, int* launches);
+
+int lbm_level_count(lbm_grids* g);
+int lbm_get_grid_info(lbm_grids* g, int level, lbm_grid_info* out);
+
+/* Copy a device array of one level to host memory (replaces drivers reading
+ * GridStruct fields directly, e.g. cases/taylorGreenVortex/taylorGreenVortexMain.cu:123-156).
+ * `bytes` must equal the array size; see LBM_ARRAY_* for element types. */
+int lbm_read_array(lbm_grids* g, int level, int which, void* host, size_t bytes);
+
+/* Overwrite the populations of one level (float [27][cellCount], shifted
+ * f_i - w_i, in the current esotwist slot order). */
+int lbm_write_f(lbm_grids* g, int level, const float* host, size_t bytes);
+
+/* Normalised kinetic energy of the Taylor–Green driver
+ * (cases/taylorGreenVortex/taylorGreenVortexMain.cu:116-180), accumulated in
+ * FP64 on the device.  `u_ref_phys` is the physical reference velocity (m/s)
+ * and `domain_length` the physical periodic length (mm). */
+int lbm_kinetic_energy(lbm_grids* g, float u_ref_phys, float domain_length,
+                       double* out);
+
+/* Cell-wise collision on a device batch of shifted populations laid out as
+ * float [27][n] (structure of arrays), in place.
+ * Replaces applyCollision (include/applyCollision.h:17-491) applied per cell
+ * with a uniform BCStruct {gx,gy,gz, collisionLimiter, nuMultiplier}. */
+int lbm_apply_collision_batch(float* d_f, int n, float nu,
+                              float collision_limiter, float nu_multiplier,
+                              float gx, float gy, float gz, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBM3_B200_H */

@@ -1,0 +1,16 @@
+"""B200-native D3Q27 cumulant lattice-Boltzmann time step (drop-in for LBM3's hot path).
+
+The compute path is the in-tree CUDA library ``_lib/liblbm3_b200.so``
+(sm_100a), reached through the C ABI in ``include/lbm3_b200.h``.  This
+package is the host-side mirror of the reference driver API.
+"""
+from . import _abi
+from ._abi import LbmCase, LbmError, LbmFaceBC, LbmGridInfo, lib
+from .cases import periodic_box, taylor_green, tgv_plain_method
+from .grids import Grids, Plan, apply_collision_batch, build_grids
+
+__all__ = [
+    "LbmCase", "LbmError", "LbmFaceBC", "LbmGridInfo", "lib", "Grids", "Plan",
+    "build_grids", "apply_collision_batch", "taylor_green", "tgv_plain_method",
+    "periodic_box", "_abi",
+]

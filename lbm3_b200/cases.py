@@ -1,0 +1,130 @@
+"""Case descriptions: the runtime form of a reference driver's constants and hooks.
+
+A reference driver (``cases/*/…Main.cu``) fixes its configuration with
+``constexpr float`` constants and four ``__cuda_callable__`` hooks.  Here each
+driver becomes a function returning an :class:`LbmCase`; constants are
+evaluated in float32, operation by operation, so the grid geometry and the
+lattice viscosity are bit-identical to what the driver's compiler computes.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi as A
+
+f32 = np.float32
+
+
+def _face(kind, open_bc_id=0, priority=0, non_reflective=False, beta=7.0,
+          dRho=0.0, ux=0.0, uy=0.0, uz=0.0) -> A.LbmFaceBC:
+    return A.LbmFaceBC(kind, open_bc_id, priority, int(non_reflective), beta, dRho, ux, uy, uz)
+
+
+def _blank_case() -> A.LbmCase:
+    c = A.LbmCase()
+    c.grid_level_count = 1
+    c.wall_refinement_count = 0
+    c.rho_phys = 1.0
+    c.collision_limiter = 0.05   # BCStruct default (include/types.h:131-136)
+    c.nu_multiplier = 1.0
+    c.storage = A.LBM_STORE_F32
+    for f in range(6):
+        c.face[f] = _face(A.LBM_BC_PERIODIC)
+    return c
+
+
+@dataclass
+class TGVSetup:
+    """Numbers a Taylor–Green run needs next to its LbmCase."""
+    case: A.LbmCase
+    cells_per_domain: int
+    u_initial: float          # lattice amplitude u0
+    u_initial_phys: float     # m/s
+    domain_length: float      # mm, periodic length
+    reference_time: float     # s
+    dt: float                 # s per step
+    iteration_count: int      # steps to t* = end_time_star
+
+    def time_star(self, steps: int) -> float:
+        return steps * float(self.dt) / float(self.reference_time)
+
+
+def taylor_green(cells_per_domain: int = 128, reynolds: float = 1600.0, mach: float = 0.1,
+                 end_time_star: float = 20.0, storage: int = A.LBM_STORE_F32,
+                 u_lattice: float | None = None, nu_lattice: float | None = None) -> TGVSetup:
+    """Periodic Taylor–Green vortex (cases/taylorGreenVortex/taylorGreenVortexMain.cu:1-105, :187-204).
+
+    With the default arguments this is the reference driver (Re 1600, Ma 0.1,
+    one level).  ``u_lattice`` / ``nu_lattice`` override the Mach/Reynolds
+    derived values, which expresses the plain-method configuration
+    u0 = 0.05, nu = 0.01 on 64^3 in the same physical-unit framework.
+    """
+    PI = f32(3.14159265358979323846)
+    reference_length = f32(1000.0)          # mm
+    u_phys = f32(1.0)                       # m/s
+    domain = f32(f32(2.0) * PI) * reference_length
+    if u_lattice is None:
+        u0 = f32(f32(mach) * f32(0.5773502691896258))
+    else:
+        u0 = f32(u_lattice)
+    res = f32(domain / f32(cells_per_domain))
+    dt = f32(f32(u0 / u_phys) * f32(res / f32(1000.0)))
+    if nu_lattice is None:
+        nu_phys = f32(f32(u_phys * f32(reference_length / f32(1000.0))) / f32(reynolds))
+    else:
+        # choose NU_PHYS so that dt * NU_PHYS / (res/1000)^2 == nu_lattice
+        r = float(res) / 1000.0
+        nu_phys = f32(float(nu_lattice) * r * r / float(dt))
+    ref_time = f32(f32(reference_length / f32(1000.0)) / u_phys)
+    iters = int(f32(f32(f32(end_time_star) * ref_time) / dt) + f32(0.5))
+
+    c = _blank_case()
+    c.res_global = res
+    c.nu_phys = nu_phys
+    c.rho_phys = 1.0
+    c.dt_phys_global = dt
+    half = f32(f32(0.5) * domain)
+    eps = f32(f32(1e-6) * domain)
+    lo = f32(f32(-half - res) - eps)
+    hi = f32(f32(half + res) + eps)
+    for a in range(3):
+        c.bounds[a] = lo
+        c.bounds[a + 3] = hi
+    c.ic_kind = A.LBM_IC_TAYLOR_GREEN
+    c.tgv_u0 = u0
+    c.tgv_length = reference_length
+    c.storage = storage
+    return TGVSetup(c, cells_per_domain, float(u0), float(u_phys), float(domain),
+                    float(ref_time), float(dt), iters)
+
+
+def tgv_plain_method(storage: int = A.LBM_STORE_F32) -> TGVSetup:
+    """Plain-method Taylor–Green: periodic 64^3, u0 = 0.05, nu = 0.01, 1000 steps."""
+    s = taylor_green(64, u_lattice=0.05, nu_lattice=0.01, storage=storage)
+    s.iteration_count = 1000
+    return s
+
+
+def periodic_box(nx: int, ny: int, nz: int, nu_lattice: float = 0.01, ux: float = 0.0,
+                 uy: float = 0.0, uz: float = 0.0, storage: int = A.LBM_STORE_F32) -> A.LbmCase:
+    """Fully periodic box of nx*ny*nz active cells (one ghost layer per face)
+    with a uniform initial state.  nx, ny, nz must be even after adding the
+    two ghost layers, i.e. even themselves."""
+    if nx % 2 or ny % 2 or nz % 2:
+        raise ValueError("active cell counts must be even")
+    c = _blank_case()
+    res = f32(1.0)
+    c.res_global = res
+    c.dt_phys_global = f32(1e-3)
+    c.nu_phys = f32(float(nu_lattice) * 1e-6 / 1e-3)
+    eps = f32(1e-3)
+    for a, n in enumerate((nx, ny, nz)):
+        c.bounds[a] = f32(-0.5 * n - 1.0) - eps
+        c.bounds[a + 3] = f32(0.5 * n + 1.0) + eps
+    c.ic_kind = A.LBM_IC_UNIFORM
+    c.ic_ux, c.ic_uy, c.ic_uz = ux, uy, uz
+    c.storage = storage
+    return c

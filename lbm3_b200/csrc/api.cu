@@ -1,0 +1,537 @@
+// C ABI (include/lbm3_b200.h): owns device memory of every level, runs the
+// per-step schedule of updateAllGrids on one CUDA stream, and converts every
+// failure into a status code plus a thread-local message.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <exception>
+#include <functional>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/lbm3_b200.h"
+#include "builder.h"
+#include "step_launch.h"
+
+namespace {
+
+thread_local std::string gLastError;
+
+int fail(int code, const std::string& msg) {
+    gLastError = msg;
+    return code;
+}
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class T> T* devAlloc(size_t n) {
+    if (n == 0) return nullptr;
+    void* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        throw std::bad_alloc();
+    }
+    return static_cast<T*>(p);
+}
+
+template <class T> T* upload(const std::vector<T>& v, cudaStream_t s) {
+    T* p = devAlloc<T>(v.size());
+    if (p) ck(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), "upload");
+    return p;
+}
+
+size_t storageBytes(int storage) { return storage == LBM_STORE_F32 ? 4 : 2; }
+
+}  // namespace
+
+struct LevelState {
+    lbm::Info info;
+    int rowCount = 0;
+    int wallCellCount = 0;
+    int wallAdjacentCount = 0;
+    int openBCCount = 0;
+    unsigned long long memBytes = 0;
+    lbm::DevLevel dev{};
+    std::vector<void*> owned;
+};
+
+struct lbm_grids {
+    lbm_case c{};
+    std::vector<LevelState> levels;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double* scratch = nullptr;
+    float lastKernelMs = 0.f;
+    int lastLaunches = 0;
+    // event pairs bracketing collide-stream launches while lbm_time_steps runs
+    std::vector<cudaEvent_t> kernelEvents;
+    bool timingKernels = false;
+    int kernelEventsUsed = 0;
+
+    ~lbm_grids() {
+        for (cudaEvent_t e : kernelEvents) cudaEventDestroy(e);
+        for (auto& L : levels)
+            for (void* p : L.owned) cudaFree(p);
+        if (scratch) cudaFree(scratch);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+};
+
+struct lbm_plan {
+    lbm::HostDomain host;
+};
+
+namespace {
+
+// Device bytes of one level: populations at the storage width plus the index
+// tables, as the reference accounts them (gridBuilderFunctions.h:1630-1649).
+unsigned long long levelBytes(const lbm::HostLevel& H, int storage) {
+    const unsigned long long n = static_cast<unsigned long long>(H.info.cellCount);
+    unsigned long long b = 27ULL * n * storageBytes(storage);
+    b += 2ULL * n * 4;                       // shifter, wallMap
+    b += 6ULL * H.rowI.size() * 4;           // compressed rows
+    b += 2ULL * H.perIndex.size() * 4;       // periodic index/source
+    for (const auto& ob : H.openBCs) b += 4ULL * ob.index.size() * 4;
+    return b;
+}
+
+void fillInfo(const lbm::HostLevel& H, int storage, lbm_grid_info* out) {
+    std::memset(out, 0, sizeof(*out));
+    out->grid_id = H.info.gridID;
+    out->cell_count = H.info.cellCount;
+    out->cell_count_x = H.info.nx;
+    out->cell_count_y = H.info.ny;
+    out->cell_count_z = H.info.nz;
+    out->row_count = static_cast<int>(H.rowI.size());
+    out->wall_cell_count = H.wallCellCount;
+    out->wall_adjacent_count = H.wallAdjacentCount;
+    out->periodic_count = static_cast<int>(H.perIndex.size());
+    int ob = 0;
+    for (const auto& o : H.openBCs) ob += static_cast<int>(o.index.size());
+    out->open_bc_count = ob;
+    out->esotwist_flipper = H.info.esotwistFlipper ? 1 : 0;
+    out->iterations_finished = H.info.iterationsFinished;
+    out->storage = storage;
+    out->res = H.info.res;
+    out->ox = H.info.ox;
+    out->oy = H.info.oy;
+    out->oz = H.info.oz;
+    out->nu = H.info.nu;
+    out->dt_phys = H.info.dtPhys;
+    out->grid_memory_bytes = levelBytes(H, storage);
+}
+
+}  // namespace
+
+namespace {
+
+// updateSingleGrid (include/updateGrid.h:16-386): K1, flip, periodic copy.
+void updateSingleGrid(lbm_grids* g, LevelState& L) {
+    const bool flip = L.info.esotwistFlipper;
+    if (g->timingKernels) {
+        const size_t k = static_cast<size_t>(g->kernelEventsUsed);
+        ck(cudaEventRecord(g->kernelEvents[k], g->stream), "event");
+        lbm::launchCollideStream(L.dev, flip, g->stream);
+        ck(cudaEventRecord(g->kernelEvents[k + 1], g->stream), "event");
+        g->kernelEventsUsed += 2;
+    } else {
+        lbm::launchCollideStream(L.dev, flip, g->stream);
+    }
+    L.info.esotwistFlipper = !flip;  // applyStreaming
+    lbm::launchPeriodic(L.dev, L.info.esotwistFlipper, g->stream);
+    L.info.iterationsFinished++;
+}
+
+void updateAllGrids(lbm_grids* g, int level) {
+    updateSingleGrid(g, g->levels[level]);
+    // single-level build: no finer level to recurse into (updateGrid.h:391-395)
+}
+
+int guarded(const char* where, const std::function<void()>& body) {
+    try {
+        body();
+        gLastError.clear();
+        return LBM_OK;
+    } catch (const CudaError& e) {
+        return fail(LBM_ERR_CUDA, std::string(where) + ": " + e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(LBM_ERR_OOM, std::string(where) + ": device or host allocation failed");
+    } catch (const std::invalid_argument& e) {
+        return fail(LBM_ERR_INVALID, std::string(where) + ": " + e.what());
+    } catch (const std::runtime_error& e) {
+        return fail(LBM_ERR_BUILD, std::string(where) + ": " + e.what());
+    } catch (const std::exception& e) {
+        return fail(LBM_ERR_INVALID, std::string(where) + ": " + e.what());
+    }
+}
+}  // namespace
+
+extern "C" {
+
+const char* lbm_last_error(void) { return gLastError.c_str(); }
+
+int lbm_device_count(void) {
+    int n = 0;
+    const cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return 0;
+        return fail(LBM_ERR_CUDA, cudaGetErrorString(e));
+    }
+    return n;
+}
+
+int lbm_plan_grids(const lbm_case* c, lbm_plan** out, long long* fluidUpdates) {
+    if (!c || !out) return fail(LBM_ERR_INVALID, "lbm_plan_grids: null argument");
+    *out = nullptr;
+    lbm_plan* p = new lbm_plan();
+    const int rc = guarded("lbm_plan_grids", [&] {
+        lbm::buildDomain(*c, p->host);
+        if (fluidUpdates) *fluidUpdates = p->host.fluidUpdatesPerIteration;
+    });
+    if (rc != LBM_OK) {
+        delete p;
+        return rc;
+    }
+    *out = p;
+    return LBM_OK;
+}
+
+void lbm_free_plan(lbm_plan* p) { delete p; }
+
+int lbm_plan_level_count(lbm_plan* p) {
+    if (!p) return fail(LBM_ERR_INVALID, "lbm_plan_level_count: null plan");
+    return static_cast<int>(p->host.levels.size());
+}
+
+int lbm_plan_info(lbm_plan* p, int level, lbm_grid_info* out) {
+    if (!p || !out || level < 0 || level >= (int)p->host.levels.size())
+        return fail(LBM_ERR_INVALID, "lbm_plan_info: bad argument");
+    fillInfo(p->host.levels[level], p->host.c.storage, out);
+    return LBM_OK;
+}
+
+int lbm_plan_read_array(lbm_plan* p, int level, int which, void* host, size_t bytes) {
+    if (!p || !host || level < 0 || level >= (int)p->host.levels.size())
+        return fail(LBM_ERR_INVALID, "lbm_plan_read_array: bad argument");
+    const lbm::HostLevel& H = p->host.levels[level];
+    const std::vector<int>* v = nullptr;
+    switch (which) {
+        case LBM_ARRAY_SHIFTER: v = &H.shifter; break;
+        case LBM_ARRAY_ROW_I: v = &H.rowI; break;
+        case LBM_ARRAY_ROW_J: v = &H.rowJ; break;
+        case LBM_ARRAY_ROW_K: v = &H.rowK; break;
+        case LBM_ARRAY_ROW_JPLUS: v = &H.rowJP; break;
+        case LBM_ARRAY_ROW_KPLUS: v = &H.rowKP; break;
+        case LBM_ARRAY_ROW_JKPLUS: v = &H.rowJKP; break;
+        case LBM_ARRAY_WALL_MAP: v = &H.wallMap; break;
+        case LBM_ARRAY_PERIODIC_INDEX: v = &H.perIndex; break;
+        case LBM_ARRAY_PERIODIC_SOURCE: v = &H.perSource; break;
+        default: return fail(LBM_ERR_INVALID, "lbm_plan_read_array: array not available in a plan");
+    }
+    if (bytes != v->size() * sizeof(int))
+        return fail(LBM_ERR_INVALID, "lbm_plan_read_array: byte count does not match array size (expected " +
+                                         std::to_string(v->size() * sizeof(int)) + ")");
+    if (bytes) std::memcpy(host, v->data(), bytes);
+    return LBM_OK;
+}
+
+int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates) {
+    if (!c || !out) return fail(LBM_ERR_INVALID, "lbm_build_grids: null argument");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        (void)cudaGetLastError();
+        return fail(LBM_ERR_NO_DEVICE, "lbm_build_grids: no CUDA device visible");
+    }
+    lbm_grids* g = new lbm_grids();
+    const int rc = guarded("lbm_build_grids", [&] {
+        g->c = *c;
+        lbm::HostDomain host;
+        lbm::buildDomain(*c, host);
+        ck(cudaEventCreate(&g->ev0), "cudaEventCreate");
+        ck(cudaEventCreate(&g->ev1), "cudaEventCreate");
+        g->scratch = devAlloc<double>(8);
+        cudaStream_t s = g->stream;
+        g->levels.resize(host.levels.size());
+        for (size_t l = 0; l < host.levels.size(); ++l) {
+            const lbm::HostLevel& H = host.levels[l];
+            LevelState& L = g->levels[l];
+            L.info = H.info;
+            L.rowCount = static_cast<int>(H.rowI.size());
+            L.wallCellCount = H.wallCellCount;
+            L.wallAdjacentCount = H.wallAdjacentCount;
+            L.openBCCount = 0;
+            for (const auto& ob : H.openBCs) L.openBCCount += static_cast<int>(ob.index.size());
+            if (L.openBCCount > 0)
+                throw std::invalid_argument(
+                    "open (velocity/pressure) boundaries are not available in this build; "
+                    "use periodic faces");
+            const long long n = H.info.cellCount;
+            lbm::DevLevel& d = L.dev;
+            d.cellCount = H.info.cellCount;
+            d.stride = n;
+            d.storage = c->storage;
+            d.nx = H.info.nx; d.ny = H.info.ny; d.nz = H.info.nz;
+            d.res = H.info.res; d.ox = H.info.ox; d.oy = H.info.oy; d.oz = H.info.oz;
+            auto own = [&](auto* p) { if (p) L.owned.push_back(p); return p; };
+            d.f = own(devAlloc<unsigned char>(27ULL * n * storageBytes(c->storage)));
+            d.shifter = own(upload(H.shifter, s));
+            d.rowI = own(upload(H.rowI, s));
+            d.rowJ = own(upload(H.rowJ, s));
+            d.rowK = own(upload(H.rowK, s));
+            d.rowJP = own(upload(H.rowJP, s));
+            d.rowKP = own(upload(H.rowKP, s));
+            d.rowJKP = own(upload(H.rowJKP, s));
+            d.wallMap = own(upload(H.wallMap, s));
+            d.perIndex = own(upload(H.perIndex, s));
+            d.perSource = own(upload(H.perSource, s));
+            d.perCount = static_cast<int>(H.perIndex.size());
+            lbm::BC bc;
+            lbm::evalLocalBC(*c, bc);
+            d.coll = lbm::makeCollisionConsts(H.info.nu, bc.nuMultiplier, bc.collisionLimiter);
+            // memory accounting as the reference prints it (gridBuilderFunctions.h:1630-1649),
+            // scaled by the population storage size
+            L.memBytes = levelBytes(H, c->storage);
+
+            // initial condition: macroscopic fields from the host (exactly the
+            // getInitialCondition hook), equilibrium populations on the device
+            float4 uni = make_float4(c->ic_dRho, c->ic_ux, c->ic_uy, c->ic_uz);
+            float4* dm = nullptr;
+            if (c->ic_kind != LBM_IC_UNIFORM) {
+                std::vector<float4> macro(n);
+                for (long long q = 0; q < n; ++q) {
+                    const lbm::BC ic = lbm::evalInitialCondition(*c, H.info, H.I[q], H.J[q], H.K[q]);
+                    macro[q] = make_float4(ic.dRho, ic.ux, ic.uy, ic.uz);
+                }
+                dm = upload(macro, s);
+                lbm::launchInit(d, L.info.esotwistFlipper, s, dm, uni);
+                ck(cudaStreamSynchronize(s), "init");
+                cudaFree(dm);
+            } else {
+                lbm::launchInit(d, L.info.esotwistFlipper, s, nullptr, uni);
+            }
+            ck(cudaGetLastError(), "init launch");
+        }
+        ck(cudaStreamSynchronize(s), "build sync");
+        if (fluidUpdates) *fluidUpdates = host.fluidUpdatesPerIteration;
+    });
+    if (rc != LBM_OK) {
+        delete g;
+        return rc;
+    }
+    *out = g;
+    return LBM_OK;
+}
+
+void lbm_free_grids(lbm_grids* g) {
+    if (!g) return;
+    cudaStreamSynchronize(g->stream);
+    delete g;
+}
+
+int lbm_set_stream(lbm_grids* g, void* stream) {
+    if (!g) return fail(LBM_ERR_INVALID, "lbm_set_stream: null grids");
+    g->stream = static_cast<cudaStream_t>(stream);
+    return LBM_OK;
+}
+
+int lbm_update_all_grids(lbm_grids* g, int steps) {
+    if (!g || steps < 0) return fail(LBM_ERR_INVALID, "lbm_update_all_grids: bad argument");
+    return guarded("lbm_update_all_grids", [&] {
+        for (int s = 0; s < steps; ++s) updateAllGrids(g, 0);
+        ck(cudaGetLastError(), "step launch");
+    });
+}
+
+int lbm_synchronize(lbm_grids* g) {
+    if (!g) return fail(LBM_ERR_INVALID, "lbm_synchronize: null grids");
+    return guarded("lbm_synchronize", [&] { ck(cudaStreamSynchronize(g->stream), "sync"); });
+}
+
+int lbm_time_steps(lbm_grids* g, int steps, float* ms) {
+    if (!g || !ms || steps < 0) return fail(LBM_ERR_INVALID, "lbm_time_steps: bad argument");
+    return guarded("lbm_time_steps", [&] {
+        // one collide-stream launch per level substep: 2^level per coarse step
+        size_t launches = 0;
+        for (const LevelState& L : g->levels) launches += size_t(steps) << L.info.gridID;
+        while (g->kernelEvents.size() < 2 * launches) {
+            cudaEvent_t e;
+            ck(cudaEventCreate(&e), "cudaEventCreate");
+            g->kernelEvents.push_back(e);
+        }
+        g->kernelEventsUsed = 0;
+        g->timingKernels = true;
+        try {
+            ck(cudaEventRecord(g->ev0, g->stream), "event");
+            for (int s = 0; s < steps; ++s) updateAllGrids(g, 0);
+            ck(cudaEventRecord(g->ev1, g->stream), "event");
+        } catch (...) {
+            g->timingKernels = false;
+            throw;
+        }
+        g->timingKernels = false;
+        ck(cudaEventSynchronize(g->ev1), "event sync");
+        ck(cudaEventElapsedTime(ms, g->ev0, g->ev1), "elapsed");
+        float kernel = 0.f;
+        for (int k = 0; k + 1 < g->kernelEventsUsed; k += 2) {
+            float t = 0.f;
+            ck(cudaEventElapsedTime(&t, g->kernelEvents[k], g->kernelEvents[k + 1]), "elapsed");
+            kernel += t;
+        }
+        g->lastKernelMs = kernel;
+        g->lastLaunches = g->kernelEventsUsed / 2;
+    });
+}
+
+int lbm_last_kernel_time(lbm_grids* g, float* kernel_ms, int* launches) {
+    if (!g || !kernel_ms || !launches) return fail(LBM_ERR_INVALID, "lbm_last_kernel_time: bad argument");
+    *kernel_ms = g->lastKernelMs;
+    *launches = g->lastLaunches;
+    return LBM_OK;
+}
+
+int lbm_level_count(lbm_grids* g) {
+    if (!g) return fail(LBM_ERR_INVALID, "lbm_level_count: null grids");
+    return static_cast<int>(g->levels.size());
+}
+
+int lbm_get_grid_info(lbm_grids* g, int level, lbm_grid_info* out) {
+    if (!g || !out || level < 0 || level >= (int)g->levels.size())
+        return fail(LBM_ERR_INVALID, "lbm_get_grid_info: bad argument");
+    const LevelState& L = g->levels[level];
+    std::memset(out, 0, sizeof(*out));
+    out->grid_id = L.info.gridID;
+    out->cell_count = L.info.cellCount;
+    out->cell_count_x = L.info.nx;
+    out->cell_count_y = L.info.ny;
+    out->cell_count_z = L.info.nz;
+    out->row_count = L.rowCount;
+    out->wall_cell_count = L.wallCellCount;
+    out->wall_adjacent_count = L.wallAdjacentCount;
+    out->periodic_count = L.dev.perCount;
+    out->open_bc_count = L.openBCCount;
+    out->esotwist_flipper = L.info.esotwistFlipper ? 1 : 0;
+    out->iterations_finished = L.info.iterationsFinished;
+    out->storage = L.dev.storage;
+    out->res = L.info.res;
+    out->ox = L.info.ox;
+    out->oy = L.info.oy;
+    out->oz = L.info.oz;
+    out->nu = L.info.nu;
+    out->dt_phys = L.info.dtPhys;
+    out->grid_memory_bytes = L.memBytes;
+    return LBM_OK;
+}
+
+int lbm_read_array(lbm_grids* g, int level, int which, void* host, size_t bytes) {
+    if (!g || !host || level < 0 || level >= (int)g->levels.size())
+        return fail(LBM_ERR_INVALID, "lbm_read_array: bad argument");
+    LevelState& L = g->levels[level];
+    const lbm::DevLevel& d = L.dev;
+    const size_t n = static_cast<size_t>(d.cellCount);
+    const size_t r = static_cast<size_t>(L.rowCount);
+    const void* src = nullptr;
+    size_t need = 0;
+    switch (which) {
+        case LBM_ARRAY_SHIFTER: src = d.shifter; need = n * 4; break;
+        case LBM_ARRAY_ROW_I: src = d.rowI; need = r * 4; break;
+        case LBM_ARRAY_ROW_J: src = d.rowJ; need = r * 4; break;
+        case LBM_ARRAY_ROW_K: src = d.rowK; need = r * 4; break;
+        case LBM_ARRAY_ROW_JPLUS: src = d.rowJP; need = r * 4; break;
+        case LBM_ARRAY_ROW_KPLUS: src = d.rowKP; need = r * 4; break;
+        case LBM_ARRAY_ROW_JKPLUS: src = d.rowJKP; need = r * 4; break;
+        case LBM_ARRAY_WALL_MAP: src = d.wallMap; need = n * 4; break;
+        case LBM_ARRAY_PERIODIC_INDEX: src = d.perIndex; need = size_t(d.perCount) * 4; break;
+        case LBM_ARRAY_PERIODIC_SOURCE: src = d.perSource; need = size_t(d.perCount) * 4; break;
+        case LBM_ARRAY_F: need = 27 * n * 4; break;
+        case LBM_ARRAY_MACRO: need = 4 * n * 4; break;
+        default: return fail(LBM_ERR_INVALID, "lbm_read_array: unknown array id");
+    }
+    if (bytes != need)
+        return fail(LBM_ERR_INVALID, "lbm_read_array: byte count does not match array size (expected " +
+                                         std::to_string(need) + ")");
+    return guarded("lbm_read_array", [&] {
+        if (need == 0) return;
+        if (which == LBM_ARRAY_F || which == LBM_ARRAY_MACRO) {
+            float* tmp = devAlloc<float>(need / 4);
+            try {
+                if (which == LBM_ARRAY_F) lbm::launchGatherF(d, g->stream, tmp);
+                else lbm::launchMacro(d, L.info.esotwistFlipper, g->stream, tmp);
+                ck(cudaGetLastError(), "read launch");
+                ck(cudaMemcpyAsync(host, tmp, need, cudaMemcpyDeviceToHost, g->stream), "copy");
+                ck(cudaStreamSynchronize(g->stream), "sync");
+            } catch (...) {
+                cudaFree(tmp);
+                throw;
+            }
+            cudaFree(tmp);
+        } else {
+            ck(cudaMemcpyAsync(host, src, need, cudaMemcpyDeviceToHost, g->stream), "copy");
+            ck(cudaStreamSynchronize(g->stream), "sync");
+        }
+    });
+}
+
+int lbm_write_f(lbm_grids* g, int level, const float* host, size_t bytes) {
+    if (!g || !host || level < 0 || level >= (int)g->levels.size())
+        return fail(LBM_ERR_INVALID, "lbm_write_f: bad argument");
+    LevelState& L = g->levels[level];
+    const size_t need = 27ULL * L.dev.cellCount * 4;
+    if (bytes != need) return fail(LBM_ERR_INVALID, "lbm_write_f: byte count does not match");
+    return guarded("lbm_write_f", [&] {
+        float* tmp = devAlloc<float>(need / 4);
+        try {
+            ck(cudaMemcpyAsync(tmp, host, need, cudaMemcpyHostToDevice, g->stream), "copy");
+            lbm::launchScatterF(L.dev, g->stream, tmp);
+            ck(cudaGetLastError(), "write launch");
+            ck(cudaStreamSynchronize(g->stream), "sync");
+        } catch (...) {
+            cudaFree(tmp);
+            throw;
+        }
+        cudaFree(tmp);
+    });
+}
+
+int lbm_kinetic_energy(lbm_grids* g, float uRefPhys, float domainLength, double* out) {
+    if (!g || !out) return fail(LBM_ERR_INVALID, "lbm_kinetic_energy: bad argument");
+    return guarded("lbm_kinetic_energy", [&] {
+        double energy = 0.0;
+        for (LevelState& L : g->levels) {
+            ck(cudaMemsetAsync(g->scratch, 0, sizeof(double), g->stream), "memset");
+            lbm::launchKineticEnergy(L.dev, L.info.esotwistFlipper, g->stream, g->scratch);
+            ck(cudaGetLastError(), "energy launch");
+            double sum = 0.0;
+            ck(cudaMemcpyAsync(&sum, g->scratch, sizeof(double), cudaMemcpyDeviceToHost, g->stream), "copy");
+            ck(cudaStreamSynchronize(g->stream), "sync");
+            const double dx = double(L.info.res) / 1000.0;
+            const double vs = dx / (double(L.info.dtPhys) * uRefPhys);
+            energy += sum * dx * dx * dx * vs * vs;
+        }
+        const double len = double(domainLength) / 1000.0;
+        *out = energy / (len * len * len);
+    });
+}
+
+int lbm_apply_collision_batch(float* d_f, int n, float nu, float limiter, float nuMultiplier, float gx,
+                              float gy, float gz, void* stream) {
+    if (!d_f || n < 0) return fail(LBM_ERR_INVALID, "lbm_apply_collision_batch: bad argument");
+    return guarded("lbm_apply_collision_batch", [&] {
+        if (n == 0) return;
+        const lbm::CollisionConsts P = lbm::makeCollisionConsts(nu, nuMultiplier, limiter);
+        lbm::launchCollideBatch(d_f, n, P, gx, gy, gz, static_cast<cudaStream_t>(stream));
+        ck(cudaGetLastError(), "collision launch");
+    });
+}
+
+}  // extern "C"

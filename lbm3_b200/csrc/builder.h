@@ -1,0 +1,79 @@
+// Host-side grid construction for one domain (all levels).
+//
+// Produces the same tables as the reference's buildGrids pipeline
+// (include/gridBuilderFunctions.h:1577-1670): k-j-i sorted cell list,
+// compressed IJK/NBR rows, wallMap, periodic ghost lists and open-boundary
+// lists.  The kernels in step.cu consume exactly these tables.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/lbm3_b200.h"
+
+namespace lbm {
+
+// BCStruct (include/types.h:131-136) as produced by the table-driven hooks.
+struct BC {
+    float dRho = 0.f, ux = 0.f, uy = 0.f, uz = 0.f;
+    float gx = 0.f, gy = 0.f, gz = 0.f;
+    int wallID = -1, openBCID = 0;
+    bool useIBB = true, dirichletU = false, dirichletRho = false, periodic = false;
+    bool nonReflective = true;
+    float nonReflectiveBeta = 7.f, collisionLimiter = 0.05f, nuMultiplier = 1.f;
+};
+
+// InfoStruct (include/types.h:120-129), the fields the time step uses.
+struct Info {
+    int gridID = 0;
+    float res = 1.f, ox = 0.f, oy = 0.f, oz = 0.f;
+    float nu = 1.f, dtPhys = 1.f;
+    int nx = 0, ny = 0, nz = 0, cellCount = 0;
+    bool esotwistFlipper = false;
+    int iterationsFinished = 0;
+};
+
+// One open-boundary ID (OpenBCArrayStruct, include/types.h:223-226).
+struct OpenBCList {
+    int openBCID = 0;
+    std::vector<int> index, source;
+    int trackFlowCount = 0;
+};
+
+struct HostLevel {
+    Info info;
+    // builder view: sorted full IJK of the kept cells
+    std::vector<int> I, J, K;
+    std::vector<int> jPlus, kPlus;
+    std::vector<uint8_t> geomBits;
+    std::vector<uint8_t> wallMarker;
+    // compressed IJK/NBR (CompressedIJKNBRStruct, include/types.h:162-164)
+    std::vector<int> shifter, rowI, rowJ, rowK, rowJP, rowKP, rowJKP;
+    // Wall.wallMapArray: -3 wall, -2 no-track fluid, -1 fluid, >=0 wall-adjacent index
+    std::vector<int> wallMap;
+    // periodic ghost copies (PeriodicBCStruct)
+    std::vector<int> perIndex, perSource;
+    std::vector<OpenBCList> openBCs;
+    int wallCellCount = 0;
+    int wallAdjacentCount = 0;
+};
+
+struct HostDomain {
+    lbm_case c;
+    std::vector<HostLevel> levels;
+    long long fluidUpdatesPerIteration = 0;
+};
+
+// getOpenBC from the face table (see lbm_face_bc in include/lbm3_b200.h).
+BC evalOpenBC(const lbm_case& c, const Info& info, int i, int j, int k);
+// getLocalBC: uniform limiter / nuMultiplier.
+void evalLocalBC(const lbm_case& c, BC& bc);
+// getInitialCondition.
+BC evalInitialCondition(const lbm_case& c, const Info& info, int i, int j, int k);
+
+// Build all tables; throws std::runtime_error on an invalid case (the
+// reference's setup throws at the same points).
+void buildDomain(const lbm_case& c, HostDomain& out);
+
+}  // namespace lbm

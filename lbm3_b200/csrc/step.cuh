@@ -1,0 +1,147 @@
+// Device-side data of one grid level and the small helpers every kernel
+// shares: neighbour decode from the compressed rows, typed population access
+// and the esotwist slot maps.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cstdint>
+
+#include "cumulant.cuh"
+#include "lattice.h"
+
+namespace lbm {
+
+// Everything a kernel needs for one level, passed by value.
+struct DevLevel {
+    void* f;                 // populations [27][stride], element type per storage
+    long long stride;        // == cellCount
+    int cellCount;
+    int storage;             // LBM_STORE_*
+    const int* shifter;      // [cellCount]
+    const int* rowI;
+    const int* rowJ;
+    const int* rowK;
+    const int* rowJP;
+    const int* rowKP;
+    const int* rowJKP;       // [rowCount]
+    const int* wallMap;      // [cellCount]
+    const int* perIndex;     // [perCount]
+    const int* perSource;
+    int perCount;
+    int nx, ny, nz;
+    float res, ox, oy, oz;
+    CollisionConsts coll;
+};
+
+// Neighbour cells of `cell` in the order self, +i, +j, +ij, +k, +ik, +jk, +ijk
+// (bit 0 = i, bit 1 = j, bit 2 = k), from the compressed rows
+// (getCompressedIJKNBR, include/cellFunctions.h:21-49; finishNBRPlus,
+// include/NBRFunctions.h:5-11: +i neighbours are index + 1 with wrap).
+__device__ __forceinline__ void decodeNbr(const DevLevel& g, int cell, int (&nb)[8], int* ijk) {
+    const int shift = __ldg(g.shifter + cell);
+    int row, off;
+    if (shift >= 0) {
+        row = shift;
+        off = 0;
+    } else {
+        row = __ldg(g.shifter + cell + shift);
+        off = -shift;
+    }
+    const int jP = __ldg(g.rowJP + row) + off;
+    const int kP = __ldg(g.rowKP + row) + off;
+    const int jkP = __ldg(g.rowJKP + row) + off;
+    const int n = g.cellCount;
+    nb[0] = cell;
+    nb[1] = cell + 1 < n ? cell + 1 : 0;
+    nb[2] = jP;
+    nb[3] = jP + 1 < n ? jP + 1 : 0;
+    nb[4] = kP;
+    nb[5] = kP + 1 < n ? kP + 1 : 0;
+    nb[6] = jkP;
+    nb[7] = jkP + 1 < n ? jkP + 1 : 0;
+    if (ijk) {
+        ijk[0] = __ldg(g.rowI + row) + off;
+        ijk[1] = __ldg(g.rowJ + row);
+        ijk[2] = __ldg(g.rowK + row);
+    }
+}
+
+// Typed population storage.  Half and bfloat16 hold the shifted value
+// f_i - w_i directly (the reference already stores shifted FP32).
+template <class S> struct Store;
+template <> struct Store<float> {
+    static __device__ __forceinline__ float ld(const float* p) { return *p; }
+    static __device__ __forceinline__ void st(float* p, float v) { *p = v; }
+};
+template <> struct Store<__half> {
+    static __device__ __forceinline__ float ld(const __half* p) { return __half2float(*p); }
+    static __device__ __forceinline__ void st(__half* p, float v) { *p = __float2half_rn(v); }
+};
+template <> struct Store<__nv_bfloat16> {
+    static __device__ __forceinline__ float ld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+    static __device__ __forceinline__ void st(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+};
+
+// Esotwist: with flipper F, direction d is read from the cell offset by
+// max(0,-c_d) in slot (F ? inv(d) : d) and written after collision to the
+// cell offset by max(0,+c_d) in slot (F ? d : inv(d))
+// (include/esotwistStreamingFunctions.h:17-127).
+template <bool F> __device__ __forceinline__ constexpr int preSlot(int d) { return F ? inv(d) : d; }
+template <bool F> __device__ __forceinline__ constexpr int postSlot(int d) { return F ? d : inv(d); }
+
+template <bool F, class S>
+__device__ __forceinline__ void readPre(const DevLevel& g, const int (&nb)[8], float (&f)[27]) {
+    const S* base = static_cast<const S*>(g.f);
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        f[d] = Store<S>::ld(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
+}
+
+template <bool F, class S>
+__device__ __forceinline__ void writePost(const DevLevel& g, const int (&nb)[8], const float (&f)[27]) {
+    S* base = static_cast<S*>(g.f);
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        Store<S>::st(base + (long long)postSlot<F>(d) * g.stride + nb[postNbr(d)], f[d]);
+}
+
+// Write f as pre-collision values of the cell (used by initial condition and
+// periodic ghost copies, which both write with getPreCollisionIndex).
+template <bool F, class S>
+__device__ __forceinline__ void writePre(const DevLevel& g, const int (&nb)[8], const float (&f)[27]) {
+    S* base = static_cast<S*>(g.f);
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        Store<S>::st(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)], f[d]);
+}
+
+}  // namespace lbm
+
+namespace lbm {
+
+// Density deviation and velocity from shifted populations with the
+// reference's pairwise summation (getDRhoUxUyUz, include/cellFunctions.h:257-279).
+__host__ __device__ __forceinline__ void macroFromF(const float (&f)[27], float& dRho, float& ux,
+                                                    float& uy, float& uz) {
+    dRho = (((f[PPP] + f[MMM]) + (f[PMP] + f[MPM])) + ((f[PPM] + f[MMP]) + (f[PMM] + f[MPP]))) +
+           (((f[OPP] + f[OMM]) + (f[OPM] + f[OMP])) + ((f[POP] + f[MOM]) + (f[POM] + f[MOP])) +
+            ((f[PPO] + f[MMO]) + (f[PMO] + f[MPO]))) +
+           ((f[POO] + f[MOO]) + (f[OPO] + f[OMO]) + (f[OOP] + f[OOM])) + f[OOO];
+    const float rhoInv = 1.f / (dRho + 1.f);
+    const float a = f[PPP] - f[MMM], b = f[PMP] - f[MPM], c = f[PPM] - f[MMP], d = f[PMM] - f[MPP];
+    const float mx = (((a + b) + (c + d)) + (((f[POP] - f[MOM]) + (f[POM] - f[MOP])) +
+                                             ((f[PPO] - f[MMO]) + (f[PMO] - f[MPO])))) +
+                     (f[POO] - f[MOO]);
+    const float my = (((a - b) + (c - d)) + (((f[OPP] - f[OMM]) + (f[OPM] - f[OMP])) +
+                                             ((f[PPO] - f[MMO]) - (f[PMO] - f[MPO])))) +
+                     (f[OPO] - f[OMO]);
+    const float mz = (((a + b) - (c + d)) + (((f[OPP] - f[OMM]) - (f[OPM] - f[OMP])) +
+                                             ((f[POP] - f[MOM]) - (f[POM] - f[MOP])))) +
+                     (f[OOP] - f[OOM]);
+    ux = mx * rhoInv;
+    uy = my * rhoInv;
+    uz = mz * rhoInv;
+}
+
+}  // namespace lbm

@@ -1,0 +1,21 @@
+// Host-callable launchers of the level kernels (implemented in step.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/lbm3_b200.h"
+#include "step.cuh"
+
+namespace lbm {
+
+void launchCollideStream(const DevLevel& g, bool flip, cudaStream_t s);
+void launchPeriodic(const DevLevel& g, bool flip, cudaStream_t s);
+void launchInit(const DevLevel& g, bool flip, cudaStream_t s, const float4* macro, float4 uniform);
+void launchKineticEnergy(const DevLevel& g, bool flip, cudaStream_t s, double* out);
+void launchMacro(const DevLevel& g, bool flip, cudaStream_t s, float* out);
+void launchGatherF(const DevLevel& g, cudaStream_t s, float* out);
+void launchScatterF(const DevLevel& g, cudaStream_t s, const float* in);
+void launchCollideBatch(float* f, int n, const CollisionConsts& P, float gx, float gy, float gz,
+                        cudaStream_t s);
+
+}  // namespace lbm

@@ -1,0 +1,175 @@
+"""Host-side mirror of the reference driver API over the C ABI.
+
+``build_grids`` / ``Grids.update_all_grids`` correspond to the reference's
+``buildGrids`` and ``updateAllGrids`` (include/gridBuilderFunctions.h:1577,
+include/updateGrid.h:388); ``Plan`` exposes the host-only construction used
+for footprint admission and table parity.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi as A
+
+_INT_ARRAYS = {
+    "shifter": A.ARRAY_SHIFTER, "row_i": A.ARRAY_ROW_I, "row_j": A.ARRAY_ROW_J,
+    "row_k": A.ARRAY_ROW_K, "row_jplus": A.ARRAY_ROW_JPLUS, "row_kplus": A.ARRAY_ROW_KPLUS,
+    "row_jkplus": A.ARRAY_ROW_JKPLUS, "wall_map": A.ARRAY_WALL_MAP,
+    "periodic_index": A.ARRAY_PERIODIC_INDEX, "periodic_source": A.ARRAY_PERIODIC_SOURCE,
+}
+
+
+def _int_len(info: A.LbmGridInfo, which: int) -> int:
+    if which in (A.ARRAY_SHIFTER, A.ARRAY_WALL_MAP):
+        return info.cell_count
+    if which in (A.ARRAY_PERIODIC_INDEX, A.ARRAY_PERIODIC_SOURCE):
+        return info.periodic_count
+    return info.row_count
+
+
+class Plan:
+    """Host-only grid construction (no GPU needed)."""
+
+    def __init__(self, case: A.LbmCase):
+        lib = A.lib()
+        self._h = C.c_void_p()
+        fu = C.c_longlong()
+        A.check(lib.lbm_plan_grids(C.byref(case), C.byref(self._h), C.byref(fu)))
+        self.fluid_updates_per_iteration = fu.value
+
+    def close(self):
+        if self._h:
+            A.lib().lbm_free_plan(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def level_count(self) -> int:
+        return A.check(A.lib().lbm_plan_level_count(self._h))
+
+    def info(self, level: int = 0) -> A.LbmGridInfo:
+        out = A.LbmGridInfo()
+        A.check(A.lib().lbm_plan_info(self._h, level, C.byref(out)))
+        return out
+
+    def array(self, name: str, level: int = 0) -> np.ndarray:
+        which = _INT_ARRAYS[name]
+        n = _int_len(self.info(level), which)
+        out = np.empty(n, dtype=np.int32)
+        A.check(A.lib().lbm_plan_read_array(self._h, level, which,
+                                            out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+
+class Grids:
+    """All levels of one domain resident on the current CUDA device."""
+
+    def __init__(self, case: A.LbmCase):
+        lib = A.lib()
+        self._h = C.c_void_p()
+        fu = C.c_longlong()
+        A.check(lib.lbm_build_grids(C.byref(case), C.byref(self._h), C.byref(fu)))
+        self.fluid_updates_per_iteration = fu.value
+        self.case = case
+
+    # lifetime
+    def close(self):
+        if self._h:
+            A.lib().lbm_free_grids(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    # stepping
+    def set_stream(self, stream_ptr: int | None):
+        A.check(A.lib().lbm_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def update_all_grids(self, coarse_steps: int = 1):
+        A.check(A.lib().lbm_update_all_grids(self._h, int(coarse_steps)))
+
+    def synchronize(self):
+        A.check(A.lib().lbm_synchronize(self._h))
+
+    def time_steps(self, steps: int) -> float:
+        """Run `steps` coarse steps bracketed by CUDA events; returns device ms."""
+        ms = C.c_float()
+        A.check(A.lib().lbm_time_steps(self._h, int(steps), C.byref(ms)))
+        return ms.value
+
+    def last_kernel_time(self):
+        """(summed ms, launch count) of the collide-stream launches of the last time_steps."""
+        ms, n = C.c_float(), C.c_int()
+        A.check(A.lib().lbm_last_kernel_time(self._h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    # inspection
+    def level_count(self) -> int:
+        return A.check(A.lib().lbm_level_count(self._h))
+
+    def info(self, level: int = 0) -> A.LbmGridInfo:
+        out = A.LbmGridInfo()
+        A.check(A.lib().lbm_get_grid_info(self._h, level, C.byref(out)))
+        return out
+
+    def array(self, name: str, level: int = 0) -> np.ndarray:
+        which = _INT_ARRAYS[name]
+        n = _int_len(self.info(level), which)
+        out = np.empty(n, dtype=np.int32)
+        A.check(A.lib().lbm_read_array(self._h, level, which, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def populations(self, level: int = 0) -> np.ndarray:
+        """Raw slot array float32 [27][cellCount] (current esotwist slot order)."""
+        n = self.info(level).cell_count
+        out = np.empty((27, n), dtype=np.float32)
+        A.check(A.lib().lbm_read_array(self._h, level, A.ARRAY_F, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def set_populations(self, f: np.ndarray, level: int = 0):
+        f = np.ascontiguousarray(f, dtype=np.float32)
+        A.check(A.lib().lbm_write_f(self._h, level, f.ctypes.data_as(C.c_void_p), f.nbytes))
+
+    def macro(self, level: int = 0) -> np.ndarray:
+        """dRho, ux, uy, uz of every cell: float32 [4][cellCount]."""
+        n = self.info(level).cell_count
+        out = np.empty((4, n), dtype=np.float32)
+        A.check(A.lib().lbm_read_array(self._h, level, A.ARRAY_MACRO, out.ctypes.data_as(C.c_void_p),
+                                       out.nbytes))
+        return out
+
+    def kinetic_energy(self, u_ref_phys: float, domain_length: float) -> float:
+        out = C.c_double()
+        A.check(A.lib().lbm_kinetic_energy(self._h, u_ref_phys, domain_length, C.byref(out)))
+        return out.value
+
+
+def build_grids(case: A.LbmCase) -> Grids:
+    """buildGrids (include/gridBuilderFunctions.h:1577-1670) on the current device."""
+    return Grids(case)
+
+
+def apply_collision_batch(d_f_ptr: int, n: int, nu: float, limiter: float = 0.05,
+                          nu_multiplier: float = 1.0, g=(0.0, 0.0, 0.0), stream_ptr: int = 0):
+    """In-place cumulant collision of a device [27][n] float32 batch."""
+    A.check(A.lib().lbm_apply_collision_batch(C.c_void_p(d_f_ptr), int(n), nu, limiter, nu_multiplier,
+                                              g[0], g[1], g[2], C.c_void_p(stream_ptr)))

@@ -1,0 +1,187 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes loader for the CPU oracle (lbm_oracle.c).
+
+Only tests/, ``__graft_entry__.smoke`` and bench.py's CPU-baseline leg use
+this module, always as the checker or the timed CPU baseline, never as the
+product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+
+
+class OBC(C.Structure):
+    _fields_ = [
+        ("dRho", C.c_float), ("ux", C.c_float), ("uy", C.c_float), ("uz", C.c_float),
+        ("gx", C.c_float), ("gy", C.c_float), ("gz", C.c_float),
+        ("wallID", C.c_int), ("openBCID", C.c_int),
+        ("useIBB", C.c_int), ("dirichletU", C.c_int), ("dirichletRho", C.c_int),
+        ("periodic", C.c_int), ("nonReflective", C.c_int),
+        ("nonReflectiveBeta", C.c_float), ("collisionLimiter", C.c_float), ("nuMultiplier", C.c_float),
+    ]
+
+
+_IP = C.POINTER(C.c_int)
+
+
+class OGrid(C.Structure):
+    _fields_ = [
+        ("gridID", C.c_int), ("res", C.c_float), ("ox", C.c_float), ("oy", C.c_float), ("oz", C.c_float),
+        ("nu", C.c_float), ("dtPhys", C.c_float),
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("cellCount", C.c_int),
+        ("flip", C.c_int), ("iterationsFinished", C.c_int),
+        ("I", _IP), ("J", _IP), ("K", _IP), ("jPlus", _IP), ("kPlus", _IP),
+        ("geomBits", C.POINTER(C.c_ubyte)), ("wallMarker", C.POINTER(C.c_ubyte)),
+        ("shifter", _IP), ("rowCount", C.c_int),
+        ("rowI", _IP), ("rowJ", _IP), ("rowK", _IP), ("rowJP", _IP), ("rowKP", _IP), ("rowJKP", _IP),
+        ("wallMap", _IP), ("perCount", C.c_int), ("perIndex", _IP), ("perSource", _IP),
+        ("openBCCount", C.c_int), ("f", C.POINTER(C.c_float)), ("fluidUpdates", C.c_longlong),
+        ("limiter", C.c_float), ("nuMultiplier", C.c_float),
+    ]
+
+
+_lib = None
+
+
+def build() -> Path:
+    """Compile the oracle with its Makefile (no-op when up to date)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists() or LIB.stat().st_mtime < (HERE / "lbm_oracle.c").stat().st_mtime:
+            build()
+        h = C.CDLL(str(LIB))
+        h.oracle_default_bc.argtypes = [C.POINTER(OBC)]
+        h.oracle_apply_collision.argtypes = [C.POINTER(C.c_float), C.POINTER(OBC), C.c_float]
+        h.oracle_apply_collision_batch.argtypes = [C.POINTER(C.c_float), C.c_int, C.c_float, C.c_float,
+                                                   C.c_float, C.c_float, C.c_float, C.c_float]
+        h.oracle_get_feq.argtypes = [C.c_float] * 4 + [C.POINTER(C.c_float)]
+        h.oracle_get_drho_u.argtypes = [C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        h.oracle_build.argtypes = [C.c_void_p, C.POINTER(OGrid)]
+        h.oracle_build.restype = C.c_int
+        h.oracle_free.argtypes = [C.POINTER(OGrid)]
+        h.oracle_step.argtypes = [C.POINTER(OGrid), C.c_int]
+        h.oracle_kinetic_energy.argtypes = [C.POINTER(OGrid), C.c_float, C.c_float]
+        h.oracle_kinetic_energy.restype = C.c_double
+        h.oracle_macro.argtypes = [C.POINTER(OGrid), C.POINTER(C.c_float)]
+        h.oracle_threads.restype = C.c_int
+        h.oracle_collide_range.argtypes = [C.POINTER(OGrid), C.c_int, C.c_int]
+        _lib = h
+    return _lib
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def threads() -> int:
+    return lib().oracle_threads()
+
+
+def default_bc() -> OBC:
+    bc = OBC()
+    lib().oracle_default_bc(C.byref(bc))
+    return bc
+
+
+def apply_collision(f: np.ndarray, nu: float, limiter: float = 0.05, nu_multiplier: float = 1.0,
+                    g=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """Collide a single cell (27 shifted populations); returns a new array."""
+    v = np.ascontiguousarray(f, dtype=np.float32).copy()
+    bc = default_bc()
+    bc.collisionLimiter = limiter
+    bc.nuMultiplier = nu_multiplier
+    bc.gx, bc.gy, bc.gz = g
+    lib().oracle_apply_collision(_fp(v), C.byref(bc), nu)
+    return v
+
+
+def apply_collision_batch(f: np.ndarray, nu: float, limiter: float = 0.05, nu_multiplier: float = 1.0,
+                          g=(0.0, 0.0, 0.0)) -> np.ndarray:
+    v = np.ascontiguousarray(f, dtype=np.float32).copy()
+    n = v.shape[1]
+    lib().oracle_apply_collision_batch(_fp(v), n, nu, limiter, nu_multiplier, g[0], g[1], g[2])
+    return v
+
+
+def feq(dRho: float, ux: float, uy: float, uz: float) -> np.ndarray:
+    out = np.empty(27, dtype=np.float32)
+    lib().oracle_get_feq(dRho, ux, uy, uz, _fp(out))
+    return out
+
+
+def drho_u(f: np.ndarray) -> np.ndarray:
+    v = np.ascontiguousarray(f, dtype=np.float32)
+    out = np.empty(4, dtype=np.float32)
+    lib().oracle_get_drho_u(_fp(v), _fp(out))
+    return out
+
+
+class OracleGrid:
+    """Single-level box domain run by the oracle."""
+
+    def __init__(self, case):
+        self.g = OGrid()
+        rc = lib().oracle_build(C.cast(C.byref(case), C.c_void_p), C.byref(self.g))
+        if rc != 0:
+            raise RuntimeError(f"oracle_build failed with status {rc}")
+
+    def close(self):
+        if self.g.f:
+            lib().oracle_free(C.byref(self.g))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def cell_count(self) -> int:
+        return self.g.cellCount
+
+    def step(self, steps: int = 1):
+        lib().oracle_step(C.byref(self.g), int(steps))
+
+    def collide_range(self, c0: int, c1: int):
+        """Collide-stream of cells [c0, c1) of the current step (timing sample)."""
+        lib().oracle_collide_range(C.byref(self.g), int(c0), int(c1))
+
+    def kinetic_energy(self, u_ref_phys: float, domain_length: float) -> float:
+        return lib().oracle_kinetic_energy(C.byref(self.g), u_ref_phys, domain_length)
+
+    def macro(self) -> np.ndarray:
+        out = np.empty((4, self.g.cellCount), dtype=np.float32)
+        lib().oracle_macro(C.byref(self.g), _fp(out))
+        return out
+
+    def populations(self) -> np.ndarray:
+        n = self.g.cellCount
+        return np.ctypeslib.as_array(self.g.f, shape=(27 * n,)).reshape(27, n).copy()
+
+    def set_populations(self, f: np.ndarray):
+        n = self.g.cellCount
+        dst = np.ctypeslib.as_array(self.g.f, shape=(27 * n,))
+        dst[:] = np.ascontiguousarray(f, dtype=np.float32).reshape(-1)
+
+    def int_array(self, name: str) -> np.ndarray:
+        lengths = {"I": self.g.cellCount, "J": self.g.cellCount, "K": self.g.cellCount,
+                   "jPlus": self.g.cellCount, "kPlus": self.g.cellCount, "shifter": self.g.cellCount,
+                   "wallMap": self.g.cellCount, "rowI": self.g.rowCount, "rowJ": self.g.rowCount,
+                   "rowK": self.g.rowCount, "rowJP": self.g.rowCount, "rowKP": self.g.rowCount,
+                   "rowJKP": self.g.rowCount, "perIndex": self.g.perCount, "perSource": self.g.perCount}
+        n = lengths[name]
+        ptr = getattr(self.g, name)
+        if n == 0:
+            return np.empty(0, dtype=np.int32)
+        return np.ctypeslib.as_array(ptr, shape=(n,)).copy()

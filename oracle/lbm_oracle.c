@@ -1,0 +1,730 @@
+/*
+ * lbm_oracle.c — TEST INFRASTRUCTURE ONLY (see lbm_oracle.h).
+ *
+ * Scalar CPU restatement of the reference time step.  Built with
+ * -ffp-contract=off so that every float operation rounds exactly as written.
+ * Citations are path:line inside the reference project.
+ */
+#include "lbm_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ---- lattice (include/D3Q27Directions.h:8-54) --------------------------- */
+enum { OOO, POO, MOO, OOM, OOP, OMO, OPO, POM, MOP, POP, MOM, MMO, PPO, OPM,
+       OMP, MPO, PMO, OPP, OMM, MPM, PMP, MMP, PPM, PMM, MPP, MMM, PPP };
+static const int CX[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, -1, 1, 0, 0, -1, 1, 0, 0, -1, 1, -1, 1, 1, -1, -1, 1};
+static const int CY[27] = {0, 0, 0, 0, 0, -1, 1, 0, 0, 0, 0, -1, 1, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, -1, 1, -1, 1};
+static const int CZ[27] = {0, 0, 0, -1, 1, 0, 0, -1, 1, 1, -1, 0, 0, -1, 1, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, -1, 1};
+static const int INV[27] = {0, 2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13, 16, 15, 18, 17, 20, 19, 22, 21, 24, 23, 26, 25};
+static const float W[27] = {8.f / 27.f, 2.f / 27.f, 2.f / 27.f, 2.f / 27.f, 2.f / 27.f, 2.f / 27.f, 2.f / 27.f,
+                            1.f / 54.f, 1.f / 54.f, 1.f / 54.f, 1.f / 54.f, 1.f / 54.f, 1.f / 54.f, 1.f / 54.f,
+                            1.f / 54.f, 1.f / 54.f, 1.f / 54.f, 1.f / 54.f, 1.f / 54.f, 1.f / 216.f, 1.f / 216.f,
+                            1.f / 216.f, 1.f / 216.f, 1.f / 216.f, 1.f / 216.f, 1.f / 216.f, 1.f / 216.f};
+
+/* Neighbour slot used by the esotwist pre/post maps: 0 self, 1 iPlus, 2 jPlus,
+ * 3 ijPlus, 4 kPlus, 5 ikPlus, 6 jkPlus, 7 ijkPlus
+ * (include/esotwistStreamingFunctions.h:17-127). */
+static int pre_nbr(int d) { return (CX[d] < 0) | ((CY[d] < 0) << 1) | ((CZ[d] < 0) << 2); }
+static int post_nbr(int d) { return (CX[d] > 0) | ((CY[d] > 0) << 1) | ((CZ[d] > 0) << 2); }
+
+int oracle_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void oracle_default_bc(obc* bc) {
+    memset(bc, 0, sizeof(*bc));
+    bc->wallID = -1;
+    bc->useIBB = 1;
+    bc->nonReflective = 1;
+    bc->nonReflectiveBeta = 7.f;
+    bc->collisionLimiter = 0.05f;
+    bc->nuMultiplier = 1.f;
+}
+
+/* ---- getFeq / getDRhoUxUyUz -------------------------------------------- */
+void oracle_get_feq(float dRho, float ux, float uy, float uz, float feq[27]) {
+    const float ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;
+    for (int q = 0; q < 27; ++q) {
+        const float cx = (float)CX[q], cy = (float)CY[q], cz = (float)CZ[q];
+        const float dx = 3.f * cx * ux + (4.5f * cx * cx - 1.5f) * ux2;
+        const float dy = 3.f * cy * uy + (4.5f * cy * cy - 1.5f) * uy2;
+        const float dz = 3.f * cz * uz + (4.5f * cz * cz - 1.5f) * uz2;
+        const float xy = dx + dy + dx * dy;
+        const float corr = xy + dz + xy * dz;
+        feq[q] = W[q] * ((dRho + corr) + dRho * corr);
+    }
+}
+
+void oracle_get_drho_u(const float f[27], float out[4]) {
+    const float d = (((f[PPP] + f[MMM]) + (f[PMP] + f[MPM])) + ((f[PPM] + f[MMP]) + (f[PMM] + f[MPP]))) +
+                    (((f[OPP] + f[OMM]) + (f[OPM] + f[OMP])) + ((f[POP] + f[MOM]) + (f[POM] + f[MOP])) +
+                     ((f[PPO] + f[MMO]) + (f[PMO] + f[MPO]))) +
+                    ((f[POO] + f[MOO]) + (f[OPO] + f[OMO]) + (f[OOP] + f[OOM])) + f[OOO];
+    const float ri = 1.f / (d + 1.f);
+    const float mx = ((((f[PPP] - f[MMM]) + (f[PMP] - f[MPM])) + ((f[PPM] - f[MMP]) + (f[PMM] - f[MPP]))) +
+                      (((f[POP] - f[MOM]) + (f[POM] - f[MOP])) + ((f[PPO] - f[MMO]) + (f[PMO] - f[MPO]))) +
+                      (f[POO] - f[MOO]));
+    const float my = ((((f[PPP] - f[MMM]) - (f[PMP] - f[MPM])) + ((f[PPM] - f[MMP]) - (f[PMM] - f[MPP]))) +
+                      (((f[OPP] - f[OMM]) + (f[OPM] - f[OMP])) + ((f[PPO] - f[MMO]) - (f[PMO] - f[MPO]))) +
+                      (f[OPO] - f[OMO]));
+    const float mz = ((((f[PPP] - f[MMM]) + (f[PMP] - f[MPM])) - ((f[PPM] - f[MMP]) + (f[PMM] - f[MPP]))) +
+                      (((f[OPP] - f[OMM]) - (f[OPM] - f[OMP])) + ((f[POP] - f[MOM]) - (f[POM] - f[MOP]))) +
+                      (f[OOP] - f[OOM]));
+    out[0] = d;
+    out[1] = mx * ri;
+    out[2] = my * ri;
+    out[3] = mz * ri;
+}
+
+/* ---- applyCollision ------------------------------------------------------
+ * Variables are named after their (x,y,z) index; population lines use
+ * a/b/c for -1/0/+1 and moments use 0/1/2 for the order, as in Geier 2017. */
+
+/* population index of (x,y,z) in {0,1,2}^3 meaning {-1,0,+1} */
+static const int PIDX[3][3][3] = {{{25, 11, 21}, {10, 2, 8}, {19, 15, 24}},
+                                  {{18, 5, 14}, {3, 0, 4}, {13, 6, 17}},
+                                  {{23, 16, 20}, {7, 1, 9}, {22, 12, 26}}};
+#define pidx(x, y, z) PIDX[x][y][z]
+
+/* weight moments (include/applyCollision.h:24-38) */
+static float kw_z(int x, int y) {
+    static const float t[3][3] = {{1.f / 36.f, 1.f / 9.f, 1.f / 36.f},
+                                  {1.f / 9.f, 4.f / 9.f, 1.f / 9.f},
+                                  {1.f / 36.f, 1.f / 9.f, 1.f / 36.f}};
+    return t[x][y];
+}
+static float kw_y(int x, int zord) {
+    if (zord == 1) return 0.f;
+    if (zord == 0) return x == 1 ? 2.f / 3.f : 1.f / 6.f;
+    return x == 1 ? 2.f / 9.f : 1.f / 18.f;
+}
+
+void oracle_apply_collision(float f[27], const obc* bc, float nu) {
+    const float gx = bc->gx, gy = bc->gy, gz = bc->gz;
+    float A0[3][3]; /* zeroth z moment of line (x,y): k_xy0 */
+    for (int x = 0; x < 3; ++x)
+        for (int y = 0; y < 3; ++y)
+            A0[x][y] = (f[pidx(x, y, 2)] + f[pidx(x, y, 0)]) + f[pidx(x, y, 1)];
+
+    /* :49-56 */
+    const float dRho = ((A0[0][0] + A0[0][1]) + A0[0][2]) + ((A0[1][0] + A0[1][1]) + A0[1][2]) +
+                       ((A0[2][0] + A0[2][1]) + A0[2][2]);
+    const float rho = 1.f + dRho;
+    const float rhoInv = 1.f / rho;
+    /* :59-65 */
+    const float momX = ((A0[2][0] + A0[2][1]) + A0[2][2]) - ((A0[0][0] + A0[0][1]) + A0[0][2]);
+    const float momY = ((A0[0][2] + A0[1][2]) + A0[2][2]) - ((A0[0][0] + A0[1][0]) + A0[2][0]);
+    const float momZ = (((f[MMP] - f[MMM]) + (f[MOP] - f[MOM])) + ((f[MPP] - f[MPM]) + (f[OMP] - f[OMM]))) +
+                       (((f[OOP] - f[OOM]) + (f[OPP] - f[OPM])) + ((f[PMP] - f[PMM]) + (f[POP] - f[POM]))) +
+                       (f[PPP] - f[PPM]);
+    /* :70-72 */
+    const float ux = (momX + 0.5f * gx) * rhoInv;
+    const float uy = (momY + 0.5f * gy) * rhoInv;
+    const float uz = (momZ + 0.5f * gz) * rhoInv;
+    const float ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;
+
+    /* z transform (:82-100): Z[x][y][order] */
+    float Z[3][3][3];
+    for (int x = 0; x < 3; ++x)
+        for (int y = 0; y < 3; ++y) {
+            const float p = f[pidx(x, y, 2)], m = f[pidx(x, y, 0)];
+            const float K = kw_z(x, y);
+            Z[x][y][0] = A0[x][y];
+            Z[x][y][1] = (p - m) - uz * (A0[x][y] + K);
+            Z[x][y][2] = (p + m) - 2.f * uz * (p - m) + uz2 * (A0[x][y] + K);
+        }
+    /* y transform (:102-130): Y[x][order y][order z] */
+    float Y[3][3][3];
+    for (int x = 0; x < 3; ++x)
+        for (int n = 0; n < 3; ++n) {
+            const float a = Z[x][0][n], b = Z[x][1][n], c = Z[x][2][n];
+            const float K = kw_y(x, n);
+            const float s0 = (c + a) + b;
+            Y[x][0][n] = s0;
+            if (n == 1) {
+                Y[x][1][n] = (c - a) - uy * s0;
+                Y[x][2][n] = (c + a) - 2.f * uy * (c - a) + uy2 * s0;
+            } else {
+                Y[x][1][n] = (c - a) - uy * (s0 + K);
+                Y[x][2][n] = (c + a) - 2.f * uy * (c - a) + uy2 * (s0 + K);
+            }
+        }
+    /* x transform (:134-159): k[order x][order y][order z] */
+    float k[3][3][3];
+    memset(k, 0, sizeof(k));
+    for (int m = 0; m < 3; ++m)
+        for (int n = 0; n < 3; ++n) {
+            const float a = Y[0][m][n], b = Y[1][m][n], c = Y[2][m][n];
+            const float s0 = (m == 0 && n == 0) ? dRho : (c + a) + b;
+            k[0][m][n] = s0;
+            float K = 0.f;
+            int hasK = 0;
+            if (m == 0 && n == 0) { K = 1.f; hasK = 1; }
+            else if ((m == 0 && n == 2) || (m == 2 && n == 0)) { K = 1.f / 3.f; hasK = 1; }
+            else if (m == 2 && n == 2) { K = 1.f / 9.f; hasK = 1; }
+            if (hasK) {
+                k[1][m][n] = (c - a) - ux * (s0 + K);
+                k[2][m][n] = (c + a) - 2.f * ux * (c - a) + ux2 * (s0 + K);
+            } else {
+                k[1][m][n] = (c - a) - ux * s0;
+                k[2][m][n] = (c + a) - 2.f * ux * (c - a) + ux2 * s0;
+            }
+        }
+
+    /* cumulants (:164-187) */
+    const float C110 = k[1][1][0], C101 = k[1][0][1], C011 = k[0][1][1];
+    const float C200 = k[2][0][0], C020 = k[0][2][0], C002 = k[0][0][2];
+    const float C111 = k[1][1][1];
+    const float C120 = k[1][2][0], C102 = k[1][0][2], C210 = k[2][1][0];
+    const float C012 = k[0][1][2], C201 = k[2][0][1], C021 = k[0][2][1];
+    const float C211 = k[2][1][1] - ((k[2][0][0] + 1.f / 3.f) * k[0][1][1] + 2.f * k[1][0][1] * k[1][1][0]) * rhoInv;
+    const float C121 = k[1][2][1] - ((k[0][2][0] + 1.f / 3.f) * k[1][0][1] + 2.f * k[1][1][0] * k[0][1][1]) * rhoInv;
+    const float C112 = k[1][1][2] - ((k[0][0][2] + 1.f / 3.f) * k[1][1][0] + 2.f * k[0][1][1] * k[1][0][1]) * rhoInv;
+    const float C220 = k[2][2][0] - ((k[0][2][0] * k[2][0][0] + 2.f * k[1][1][0] * k[1][1][0] +
+                                      (k[2][0][0] + k[0][2][0]) / 3.f) * rhoInv - dRho * rhoInv / 9.f);
+    const float C022 = k[0][2][2] - ((k[0][0][2] * k[0][2][0] + 2.f * k[0][1][1] * k[0][1][1] +
+                                      (k[0][0][2] + k[0][2][0]) / 3.f) * rhoInv - dRho * rhoInv / 9.f);
+    const float C202 = k[2][0][2] - ((k[2][0][0] * k[0][0][2] + 2.f * k[1][0][1] * k[1][0][1] +
+                                      (k[2][0][0] + k[0][0][2]) / 3.f) * rhoInv - dRho * rhoInv / 9.f);
+    const float k000 = dRho;
+
+    /* relaxation (:193-342) */
+    const float w1 = 1.f / (3.f * (nu * bc->nuMultiplier) + 0.5f);
+    const float w2 = 1.f;
+    const float Dxu = -w1 * 0.5f * rhoInv * (2.f * C200 - C020 - C002) - w2 * 0.5f * rhoInv * (C200 + C020 + C002 - k000);
+    const float Dyv = Dxu + 1.5f * w1 * rhoInv * (C200 - C020);
+    const float Dzw = Dxu + 1.5f * w1 * rhoInv * (C200 - C002);
+    const float DxvDyu = -3.f * w1 * rhoInv * C110;
+    const float DxwDzu = -3.f * w1 * rhoInv * C101;
+    const float DywDzv = -3.f * w1 * rhoInv * C011;
+    const float S110 = (1.f - w1) * C110, S101 = (1.f - w1) * C101, S011 = (1.f - w1) * C011;
+    const float r33 = (1.f - w1) * (C200 - C020) - 3.f * rho * (1.f - 0.5f * w1) * (ux2 * Dxu - uy2 * Dyv);
+    const float r34 = (1.f - w1) * (C200 - C002) - 3.f * rho * (1.f - 0.5f * w1) * (ux2 * Dxu - uz2 * Dzw);
+    const float r35 = k000 * w2 + (1.f - w2) * (C200 + C020 + C002) -
+                      3.f * rho * (1.f - 0.5f * w2) * (ux2 * Dxu + uy2 * Dyv + uz2 * Dzw);
+    const float S200 = (r33 + r34 + r35) / 3.f;
+    const float S020 = (r34 - 2.f * r33 + r35) / 3.f;
+    const float S002 = (r33 - 2.f * r34 + r35) / 3.f;
+
+    float S120 = 0.f, S102 = 0.f, S210 = 0.f, S012 = 0.f, S201 = 0.f, S021 = 0.f, S111 = 0.f;
+    float S220 = 0.f, S202 = 0.f, S022 = 0.f, S211 = 0.f, S121 = 0.f, S112 = 0.f;
+    const float w6 = 1.f, w7 = 1.f, w8 = 1.f;
+    if (bc->collisionLimiter > 0.f && bc->nuMultiplier <= 1.f) {
+        const float w3 = 8.f * (w1 - 2.f) * (w2 * (3.f * w1 - 1.f) - 5.f * w1) /
+                         (8.f * (5.f - 2.f * w1) * w1 + w2 * (8.f + w1 * (9.f * w1 - 26.f)));
+        const float w4 = 8.f * (w1 - 2.f) * (w1 + w2 * (3.f * w1 - 7.f)) /
+                         (w2 * (56.f - 42.f * w1 + 9.f * w1 * w1) - 8.f * w1);
+        const float w5 = 24.f * (w1 - 2.f) *
+                         (4.f * w1 * w1 + w1 * w2 * (18.f - 13.f * w1) + w2 * w2 * (2.f + w1 * (6.f * w1 - 11.f))) /
+                         (16.f * w1 * w1 * (w1 - 6.f) - 2.f * w1 * w2 * (216.f + 5.f * w1 * (9.f * w1 - 46.f)) +
+                          w2 * w2 * (w1 * (3.f * w1 - 10.f) * (15.f * w1 - 28.f) - 48.f));
+        const float A = (4.f * w1 * w1 + 2.f * w1 * w2 * (w1 - 6.f) + w2 * w2 * (w1 * (10.f - 3.f * w1) - 4.f)) /
+                        ((w1 - w2) * (w2 * (2.f + 3.f * w1) - 8.f * w1));
+        const float B = (4.f * w1 * w2 * (9.f * w1 - 16.f) - 4.f * w1 * w1 - 2.f * w2 * w2 * (2.f + 9.f * w1 * (w1 - 2.f))) /
+                        (3.f * (w1 - w2) * (w2 * (2.f + 3.f * w1) - 8.f * w1));
+        const float lam = bc->collisionLimiter;
+        const float P1 = C120 + C102, P2 = C210 + C012, P3 = C201 + C021;
+        const float M1 = C120 - C102, M2 = C210 - C012, M3 = C201 - C021;
+        const float aP1 = fabsf(P1), aP2 = fabsf(P2), aP3 = fabsf(P3);
+        const float aM1 = fabsf(M1), aM2 = fabsf(M2), aM3 = fabsf(M3), a111 = fabsf(C111);
+        const float oP1 = w3 + (1.f - w3) * aP1 / (lam + aP1);
+        const float oP2 = w3 + (1.f - w3) * aP2 / (lam + aP2);
+        const float oP3 = w3 + (1.f - w3) * aP3 / (lam + aP3);
+        const float oM1 = w4 + (1.f - w4) * aM1 / (lam + aM1);
+        const float oM2 = w4 + (1.f - w4) * aM2 / (lam + aM2);
+        const float oM3 = w4 + (1.f - w4) * aM3 / (lam + aM3);
+        const float o111 = w5 + (1.f - w5) * a111 / (lam + a111);
+        const float e117 = (1.f - oP1) * P1, e118 = (1.f - oP2) * P2, e119 = (1.f - oP3) * P3;
+        const float e120 = (1.f - oM1) * M1, e121 = (1.f - oM2) * M2, e122 = (1.f - oM3) * M3;
+        S120 = 0.5f * (e120 + e117);
+        S102 = 0.5f * (-e120 + e117);
+        S210 = 0.5f * (e121 + e118);
+        S012 = 0.5f * (-e121 + e118);
+        S201 = 0.5f * (e122 + e119);
+        S021 = 0.5f * (-e122 + e119);
+        S111 = (1.f - o111) * C111;
+        const float e43 = (2.f / 3.f) * (1.f / w1 - 0.5f) * w6 * A * rho * (Dxu - 2.f * Dyv + Dzw) +
+                          (1.f - w6) * (C220 - 2.f * C202 + C022);
+        const float e44 = (2.f / 3.f) * (1.f / w1 - 0.5f) * w6 * A * rho * (-2.f * Dxu + Dyv + Dzw) +
+                          (1.f - w6) * (C220 + C202 - 2.f * C022);
+        const float e45 = -(4.f / 3.f) * (1.f / w1 - 0.5f) * w7 * A * rho * (Dxu + Dyv + Dzw) +
+                          (1.f - w7) * (C220 + C202 + C022);
+        S220 = (e43 + e44 + e45) / 3.f;
+        S202 = (-e43 + e45) / 3.f;
+        S022 = (-e44 + e45) / 3.f;
+        S211 = -(1.f / 3.f) * (1.f / w1 - 0.5f) * w8 * B * rho * DywDzv + (1.f - w8) * C211;
+        S121 = -(1.f / 3.f) * (1.f / w1 - 0.5f) * w8 * B * rho * DxwDzu + (1.f - w8) * C121;
+        S112 = -(1.f / 3.f) * (1.f / w1 - 0.5f) * w8 * B * rho * DxvDyu + (1.f - w8) * C112;
+    }
+
+    /* cumulants -> central moments (:348-384) */
+    float s[3][3][3];
+    s[0][1][1] = S011; s[1][0][1] = S101; s[1][1][0] = S110; s[1][1][1] = S111;
+    s[0][0][2] = S002; s[0][2][0] = S020; s[2][0][0] = S200;
+    s[0][1][2] = S012; s[0][2][1] = S021; s[1][0][2] = S102; s[2][0][1] = S201;
+    s[1][2][0] = S120; s[2][1][0] = S210;
+    s[2][1][1] = S211 + ((S200 + 1.f / 3.f) * S011 + 2.f * S101 * S110) * rhoInv;
+    s[1][2][1] = S121 + ((S020 + 1.f / 3.f) * S101 + 2.f * S110 * S011) * rhoInv;
+    s[1][1][2] = S112 + ((S002 + 1.f / 3.f) * S110 + 2.f * S011 * S101) * rhoInv;
+    s[2][2][0] = S220 + ((S020 * S200 + 2.f * S110 * S110 + (S200 + S020) / 3.f) * rhoInv - dRho * rhoInv / 9.f);
+    s[0][2][2] = S022 + ((S002 * S020 + 2.f * S011 * S011 + (S002 + S020) / 3.f) * rhoInv - dRho * rhoInv / 9.f);
+    s[2][0][2] = S202 + ((S200 * S002 + 2.f * S101 * S101 + (S200 + S002) / 3.f) * rhoInv - dRho * rhoInv / 9.f);
+    s[1][2][2] = (S020 * S102 + S002 * S120 + 4.f * S011 * S111 + 2.f * (S110 * S012 + S101 * S021) +
+                  (S120 + S102) / 3.f) * rhoInv;
+    s[2][1][2] = (S002 * S210 + S200 * S012 + 4.f * S101 * S111 + 2.f * (S011 * S201 + S110 * S102) +
+                  (S210 + S012) / 3.f) * rhoInv;
+    s[2][2][1] = (S200 * S021 + S020 * S201 + 4.f * S110 * S111 + 2.f * (S101 * S120 + S011 * S210) +
+                  (S021 + S201) / 3.f) * rhoInv;
+    s[2][2][2] = (4.f * S111 * S111 + S200 * s[0][2][2] + S020 * s[2][0][2] + S002 * s[2][2][0] +
+                  4.f * (S011 * s[2][1][1] + S101 * s[1][2][1] + S110 * s[1][1][2]) +
+                  2.f * (S120 * S102 + S210 * S012 + S201 * S021)) * rhoInv -
+                 (16.f * S110 * S101 * S011 + 4.f * (S101 * S101 * S020 + S011 * S011 * S200 + S110 * S110 * S002) +
+                  2.f * S200 * S020 * S002) * rhoInv * rhoInv +
+                 (3.f * (s[0][2][2] + s[2][0][2] + s[2][2][0]) + (S200 + S020 + S002)) * rhoInv / 9.f -
+                 (2.f / 3.f) * (2.f * (S101 * S101 + S011 * S011 + S110 * S110) + (S002 * S020 + S002 * S200 + S020 * S200) +
+                                (S002 + S020 + S200) / 3.f) * rhoInv * rhoInv -
+                 (dRho * dRho - dRho) * rhoInv * rhoInv / 27.f;
+    s[0][0][0] = k000;
+    s[1][0][0] = -k[1][0][0];
+    s[0][1][0] = -k[0][1][0];
+    s[0][0][1] = -k[0][0][1];
+
+    /* back transform x (:390-418): X[x line][order y][order z] */
+    float X[3][3][3];
+    for (int m = 0; m < 3; ++m)
+        for (int n = 0; n < 3; ++n) {
+            const float s0 = s[0][m][n], s1 = s[1][m][n], s2 = s[2][m][n];
+            float K = 0.f, centre = s0 * (1.f - ux2) - 2.f * ux * s1 - s2;
+            if (m == 0 && n == 0) { K = 1.f; centre = centre - ux2; }
+            else if ((m == 0 && n == 2) || (m == 2 && n == 0)) { K = 1.f / 3.f; centre = centre - ux2 / 3.f; }
+            else if (m == 2 && n == 2) { K = 1.f / 9.f; centre = centre - ux2 / 9.f; }
+            X[1][m][n] = centre;
+            if (K != 0.f) {
+                X[0][m][n] = ((s0 + K) * (ux2 - ux) + s1 * (2.f * ux - 1.f) + s2) * 0.5f;
+                X[2][m][n] = ((s0 + K) * (ux2 + ux) + s1 * (2.f * ux + 1.f) + s2) * 0.5f;
+            } else {
+                X[0][m][n] = (s0 * (ux2 - ux) + s1 * (2.f * ux - 1.f) + s2) * 0.5f;
+                X[2][m][n] = (s0 * (ux2 + ux) + s1 * (2.f * ux + 1.f) + s2) * 0.5f;
+            }
+        }
+    /* back transform y (:420-448): V[x line][y line][order z] */
+    float V[3][3][3];
+    for (int x = 0; x < 3; ++x)
+        for (int n = 0; n < 3; ++n) {
+            const float s0 = X[x][0][n], s1 = X[x][1][n], s2 = X[x][2][n];
+            if (n == 1) {
+                V[x][1][n] = s0 * (1.f - uy2) - 2.f * uy * s1 - s2;
+                V[x][0][n] = (s0 * (uy2 - uy) + s1 * (2.f * uy - 1.f) + s2) * 0.5f;
+                V[x][2][n] = (s0 * (uy2 + uy) + s1 * (2.f * uy + 1.f) + s2) * 0.5f;
+            } else {
+                const float K = kw_y(x, n);
+                V[x][1][n] = s0 * (1.f - uy2) - 2.f * uy * s1 - s2 - K * uy2;
+                V[x][0][n] = ((s0 + K) * (uy2 - uy) + s1 * (2.f * uy - 1.f) + s2) * 0.5f;
+                V[x][2][n] = ((s0 + K) * (uy2 + uy) + s1 * (2.f * uy + 1.f) + s2) * 0.5f;
+            }
+        }
+    /* back transform z (:450-490) */
+    for (int x = 0; x < 3; ++x)
+        for (int y = 0; y < 3; ++y) {
+            const float s0 = V[x][y][0], s1 = V[x][y][1], s2 = V[x][y][2];
+            const float K = kw_z(x, y);
+            f[pidx(x, y, 1)] = s0 * (1.f - uz2) - 2.f * uz * s1 - s2 - K * uz2;
+            f[pidx(x, y, 0)] = ((s0 + K) * (uz2 - uz) + s1 * (2.f * uz - 1.f) + s2) * 0.5f;
+            f[pidx(x, y, 2)] = ((s0 + K) * (uz2 + uz) + s1 * (2.f * uz + 1.f) + s2) * 0.5f;
+        }
+}
+
+void oracle_apply_collision_batch(float* f, int n, float nu, float limiter, float nuMultiplier, float gx,
+                                  float gy, float gz) {
+    obc bc;
+    oracle_default_bc(&bc);
+    bc.collisionLimiter = limiter;
+    bc.nuMultiplier = nuMultiplier;
+    bc.gx = gx; bc.gy = gy; bc.gz = gz;
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < n; ++c) {
+        float v[27];
+        for (int d = 0; d < 27; ++d) v[d] = f[(long long)d * n + c];
+        oracle_apply_collision(v, &bc, nu);
+        for (int d = 0; d < 27; ++d) f[(long long)d * n + c] = v[d];
+    }
+}
+
+/* ---- grid construction (include/gridBuilderFunctions.h) ------------------ */
+
+static obc open_bc(const lbm_case* c, const ogrid* g, int i, int j, int k) {
+    /* getOpenBC as the face table defines it (include/lbm3_b200.h) */
+    obc bc;
+    oracle_default_bc(&bc);
+    const int touch[6] = {i == 0, i == g->nx - 1, j == 0, j == g->ny - 1, k == 0, k == g->nz - 1};
+    int best = -1;
+    for (int f = 0; f < 6; ++f)
+        if (touch[f] && (best < 0 || c->face[f].priority > c->face[best].priority)) best = f;
+    if (best < 0) return bc;
+    const lbm_face_bc* fb = &c->face[best];
+    bc.openBCID = fb->open_bc_id;
+    bc.nonReflective = fb->non_reflective;
+    bc.nonReflectiveBeta = fb->non_reflective_beta;
+    if (fb->kind == LBM_BC_PERIODIC) bc.periodic = 1;
+    else if (fb->kind == LBM_BC_VELOCITY) { bc.dirichletU = 1; bc.ux = fb->ux; bc.uy = fb->uy; bc.uz = fb->uz; }
+    else if (fb->kind == LBM_BC_PRESSURE) { bc.dirichletRho = 1; bc.dRho = fb->dRho; }
+    return bc;
+}
+
+static int cmp_kji(const void* a, const void* b) {
+    const int* x = (const int*)a;
+    const int* y = (const int*)b;
+    if (x[2] != y[2]) return x[2] < y[2] ? -1 : 1;
+    if (x[1] != y[1]) return x[1] < y[1] ? -1 : 1;
+    if (x[0] != y[0]) return x[0] < y[0] ? -1 : 1;
+    return 0;
+}
+
+/* connectNBRInRows (include/NBRFunctions.h:44-80) for rows keyed by `key` */
+static void connect_rows(int n, const int* key, int keyCount, int* nbr) {
+    int* counter = (int*)calloc((size_t)keyCount + 1, sizeof(int));
+    int* temp = (int*)calloc((size_t)keyCount + 1, sizeof(int));
+    int* rowMap = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    for (int c = 0; c < n; ++c) counter[key[c]]++;
+    /* exclusive scan */
+    int run = 0;
+    for (int r = 0; r <= keyCount; ++r) { const int v = counter[r]; counter[r] = run; run += v; }
+    for (int c = 0; c < n; ++c) rowMap[counter[key[c]] + temp[key[c]]++] = c;
+    for (int r = 0; r < keyCount; ++r) {
+        const int start = counter[r], cnt = counter[r + 1] - start;
+        if (cnt == 0) continue;
+        for (int layer = 1; layer < cnt; ++layer) { /* insertion sort */
+            const int v = rowMap[start + layer];
+            int s = layer - 1;
+            while (s >= 0 && rowMap[start + s] > v) { rowMap[start + s + 1] = rowMap[start + s]; --s; }
+            rowMap[start + s + 1] = v;
+        }
+        for (int layer = 0; layer < cnt - 1; ++layer) nbr[rowMap[start + layer]] = rowMap[start + layer + 1];
+        nbr[rowMap[start + cnt - 1]] = rowMap[start];
+    }
+    free(counter); free(temp); free(rowMap);
+}
+
+static int find_cell(const ogrid* g, int i, int j, int k) {
+    int lo = 0, hi = g->cellCount;
+    while (lo < hi) {
+        const int mid = lo + (hi - lo) / 2;
+        if (g->I[mid] == i && g->J[mid] == j && g->K[mid] == k) return mid;
+        const int before = g->K[mid] < k || (g->K[mid] == k && g->J[mid] < j) ||
+                           (g->K[mid] == k && g->J[mid] == j && g->I[mid] < i);
+        if (before) lo = mid + 1; else hi = mid;
+    }
+    return -1;
+}
+
+static void get_nbr(const ogrid* g, int cell, int nb[8]);
+
+int oracle_build(const lbm_case* c, ogrid* g) {
+    memset(g, 0, sizeof(*g));
+    if (c->grid_level_count != 1) return LBM_ERR_UNSUPPORTED;
+    /* initializeGridInfo (:9-64), level 0 */
+    const float* b = c->bounds;
+    g->res = c->res_global;
+    const float sres = g->res * 2.f;
+    const int snx = (int)((b[3] - b[0]) / sres), sny = (int)((b[4] - b[1]) / sres), snz = (int)((b[5] - b[2]) / sres);
+    if (snx < 1 || sny < 1 || snz < 1) return LBM_ERR_INVALID;
+    const float sox = b[0] + ((b[3] - b[0]) - (snx * sres) + sres) / 2.0f;
+    const float soy = b[1] + ((b[4] - b[1]) - (sny * sres) + sres) / 2.0f;
+    const float soz = b[2] + ((b[5] - b[2]) - (snz * sres) + sres) / 2.0f;
+    g->nx = snx * 2; g->ny = sny * 2; g->nz = snz * 2;
+    g->ox = sox - g->res * 0.5f; g->oy = soy - g->res * 0.5f; g->oz = soz - g->res * 0.5f;
+    g->dtPhys = c->dt_phys_global;
+    g->nu = (g->dtPhys * c->nu_phys) / ((g->res / 1000.f) * (g->res / 1000.f));
+    g->limiter = c->collision_limiter;
+    g->nuMultiplier = c->nu_multiplier;
+
+    /* buildFinerGridBuilder from the skeleton (:66-132): every skeleton cell
+     * is kept without geometry; 8 children each, then sortIJK (:204-234) */
+    const int n = 8 * snx * sny * snz;
+    int* ijk = (int*)malloc(sizeof(int) * 3 * (size_t)n);
+    int cf = 0;
+    for (int sc = 0; sc < snx * sny * snz; ++sc) {
+        const int ks = sc / (snx * sny), rem = sc % (snx * sny), js = rem / snx, is = rem % snx;
+        for (int ka = 0; ka < 2; ++ka)
+            for (int ja = 0; ja < 2; ++ja)
+                for (int ia = 0; ia < 2; ++ia) {
+                    ijk[3 * cf] = 2 * is + ia;
+                    ijk[3 * cf + 1] = 2 * js + ja;
+                    ijk[3 * cf + 2] = 2 * ks + ka;
+                    ++cf;
+                }
+    }
+    qsort(ijk, (size_t)n, 3 * sizeof(int), cmp_kji);
+    g->cellCount = n;
+    g->I = (int*)malloc(sizeof(int) * n); g->J = (int*)malloc(sizeof(int) * n); g->K = (int*)malloc(sizeof(int) * n);
+    for (int q = 0; q < n; ++q) { g->I[q] = ijk[3 * q]; g->J[q] = ijk[3 * q + 1]; g->K[q] = ijk[3 * q + 2]; }
+    free(ijk);
+
+    /* buildNBRPlus (include/NBRFunctions.h:82-152) */
+    g->jPlus = (int*)malloc(sizeof(int) * n);
+    g->kPlus = (int*)malloc(sizeof(int) * n);
+    int* key = (int*)malloc(sizeof(int) * n);
+    for (int q = 0; q < n; ++q) key[q] = g->K[q] * g->nx + g->I[q];
+    connect_rows(n, key, g->nx * g->nz, g->jPlus);
+    for (int q = 0; q < n; ++q) key[q] = g->J[q] * g->nx + g->I[q];
+    connect_rows(n, key, g->nx * g->ny, g->kPlus);
+    free(key);
+    /* markGeometricNBRPlus (:154-194) */
+    g->geomBits = (unsigned char*)calloc((size_t)n, 1);
+    for (int q = 0; q < n; ++q) {
+        const int iP = q + 1 < n ? q + 1 : 0, jP = g->jPlus[q], ijP = jP + 1 < n ? jP + 1 : 0;
+        const int kP = g->kPlus[q], ikP = kP + 1 < n ? kP + 1 : 0, jkP = g->jPlus[kP];
+        const int ijkP = jkP + 1 < n ? jkP + 1 : 0;
+        const int i = g->I[q], j = g->J[q], k = g->K[q];
+        unsigned char bits = 0;
+        if (g->I[iP] == i + 1 && g->J[iP] == j && g->K[iP] == k) bits |= 1;
+        if (g->I[jP] == i && g->J[jP] == j + 1 && g->K[jP] == k) bits |= 2;
+        if (g->I[ijP] == i + 1 && g->J[ijP] == j + 1 && g->K[ijP] == k) bits |= 4;
+        if (g->I[kP] == i && g->J[kP] == j && g->K[kP] == k + 1) bits |= 8;
+        if (g->I[ikP] == i + 1 && g->J[ikP] == j && g->K[ikP] == k + 1) bits |= 16;
+        if (g->I[jkP] == i && g->J[jkP] == j + 1 && g->K[jkP] == k + 1) bits |= 32;
+        if (g->I[ijkP] == i + 1 && g->J[ijkP] == j + 1 && g->K[ijkP] == k + 1) bits |= 64;
+        g->geomBits[q] = bits;
+    }
+    g->wallMarker = (unsigned char*)calloc((size_t)n, 1);
+
+    /* gridBuilderToGrid (:1032-1126): first-in-row marks, inclusive max scan,
+     * exclusive sum scan, compressed arrays */
+    int* firstInRow = (int*)malloc(sizeof(int) * n);
+    int* scan = (int*)malloc(sizeof(int) * n);
+    for (int q = 0; q < n; ++q) {
+        if (q == 0) { firstInRow[q] = 0; scan[q] = 1; continue; }
+        const int jk = g->jPlus[g->kPlus[q]], jkPrev = g->jPlus[g->kPlus[q - 1]];
+        const int brk = g->I[q] != g->I[q - 1] + 1 || g->J[q] != g->J[q - 1] || g->K[q] != g->K[q - 1] ||
+                        g->jPlus[q] != g->jPlus[q - 1] + 1 || g->kPlus[q] != g->kPlus[q - 1] + 1 ||
+                        jk != jkPrev + 1;
+        firstInRow[q] = brk ? q : 0;
+        scan[q] = brk ? 1 : 0;
+    }
+    for (int q = 1; q < n; ++q) if (firstInRow[q] < firstInRow[q - 1]) firstInRow[q] = firstInRow[q - 1];
+    int rows = 0;
+    for (int q = 0; q < n; ++q) { const int v = scan[q]; scan[q] = rows; rows += v; }
+    g->rowCount = rows;
+    g->shifter = (int*)malloc(sizeof(int) * n);
+    g->rowI = (int*)malloc(sizeof(int) * rows); g->rowJ = (int*)malloc(sizeof(int) * rows);
+    g->rowK = (int*)malloc(sizeof(int) * rows); g->rowJP = (int*)malloc(sizeof(int) * rows);
+    g->rowKP = (int*)malloc(sizeof(int) * rows); g->rowJKP = (int*)malloc(sizeof(int) * rows);
+    for (int q = 0; q < n; ++q) {
+        if (q == firstInRow[q]) {
+            const int r = scan[q];
+            g->shifter[q] = r;
+            g->rowI[r] = g->I[q]; g->rowJ[r] = g->J[q]; g->rowK[r] = g->K[q];
+            g->rowJP[r] = g->jPlus[q]; g->rowKP[r] = g->kPlus[q]; g->rowJKP[r] = g->jPlus[g->kPlus[q]];
+        } else {
+            g->shifter[q] = firstInRow[q] - q;
+        }
+    }
+    free(firstInRow); free(scan);
+
+    /* wallMap (:1128-1149) and the periodic overlap (:1232-1274) */
+    g->wallMap = (int*)malloc(sizeof(int) * n);
+    for (int q = 0; q < n; ++q) g->wallMap[q] = g->wallMarker[q] ? -3 : -1;
+    const int layers = 1 << g->gridID;
+    for (int q = 0; q < n; ++q) {
+        if (g->wallMarker[q]) continue;
+        const int i = g->I[q], j = g->J[q], k = g->K[q];
+        int ov = 0;
+        if (i < layers || i >= g->nx - layers) ov |= open_bc(c, g, i < layers ? 0 : g->nx - 1, j, k).periodic;
+        if (j < layers || j >= g->ny - layers) ov |= open_bc(c, g, i, j < layers ? 0 : g->ny - 1, k).periodic;
+        if (k < layers || k >= g->nz - layers) ov |= open_bc(c, g, i, j, k < layers ? 0 : g->nz - 1).periodic;
+        if (ov && g->wallMap[q] == -1) g->wallMap[q] = -2;
+    }
+    /* open boundaries are not restated in this oracle build */
+    g->openBCCount = 0;
+    for (int q = 0; q < n; ++q) {
+        const int i = g->I[q], j = g->J[q], k = g->K[q];
+        if (i == 0 || i == g->nx - 1 || j == 0 || j == g->ny - 1 || k == 0 || k == g->nz - 1)
+            if (!open_bc(c, g, i, j, k).periodic) g->openBCCount++;
+    }
+    if (g->openBCCount > 0) { oracle_free(g); return LBM_ERR_UNSUPPORTED; }
+
+    /* periodic lists (:1486-1564) */
+    g->perIndex = (int*)malloc(sizeof(int) * n);
+    g->perSource = (int*)malloc(sizeof(int) * n);
+    g->perCount = 0;
+    const int per = (int)lround(pow(2.0, g->gridID));
+    for (int q = 0; q < n; ++q) {
+        int i = g->I[q], j = g->J[q], k = g->K[q];
+        if (!(i == 0 || i == g->nx - 1 || j == 0 || j == g->ny - 1 || k == 0 || k == g->nz - 1)) continue;
+        if (!open_bc(c, g, i, j, k).periodic) continue;
+        if (i == 0) i = g->nx - 2 * per; else if (i == g->nx - 1) i = 2 * per - 1;
+        if (j == 0) j = g->ny - 2 * per; else if (j == g->ny - 1) j = 2 * per - 1;
+        if (k == 0) k = g->nz - 2 * per; else if (k == g->nz - 1) k = 2 * per - 1;
+        const int src = find_cell(g, i, j, k);
+        if (src < 0) { oracle_free(g); return LBM_ERR_BUILD; }
+        g->perIndex[g->perCount] = q;
+        g->perSource[g->perCount] = src;
+        g->perCount++;
+    }
+    g->fluidUpdates = (long long)n;
+
+    /* allocateFArray + applyInitialCondition (applyInitialCondition.h:8-41) */
+    g->f = (float*)malloc(sizeof(float) * 27 * (size_t)n);
+#pragma omp parallel for schedule(static)
+    for (int q = 0; q < n; ++q) {
+        obc bc;
+        oracle_default_bc(&bc);
+        if (c->ic_kind == LBM_IC_TAYLOR_GREEN) {
+            const float x = g->I[q] * g->res + g->ox, y = g->J[q] * g->res + g->oy, z = g->K[q] * g->res + g->oz;
+            const float X = x / c->tgv_length, Y = y / c->tgv_length, Z = z / c->tgv_length;
+            const float u0 = c->tgv_u0;
+            bc.ux = u0 * sinf(X) * cosf(Y) * cosf(Z);
+            bc.uy = -u0 * cosf(X) * sinf(Y) * cosf(Z);
+            bc.uz = 0.f;
+            bc.dRho = (3.f * u0 * u0 / 16.f) * (cosf(2.f * X) + cosf(2.f * Y)) * (2.f + cosf(2.f * Z));
+        } else {
+            bc.dRho = c->ic_dRho; bc.ux = c->ic_ux; bc.uy = c->ic_uy; bc.uz = c->ic_uz;
+        }
+        float feq[27];
+        oracle_get_feq(bc.dRho, bc.ux, bc.uy, bc.uz, feq);
+        int nb[8];
+        get_nbr(g, q, nb);
+        for (int d = 0; d < 27; ++d) {
+            const int slot = g->flip ? INV[d] : d;
+            g->f[(size_t)slot * n + nb[pre_nbr(d)]] = feq[d];
+        }
+    }
+    return 0;
+}
+
+void oracle_free(ogrid* g) {
+    free(g->I); free(g->J); free(g->K); free(g->jPlus); free(g->kPlus); free(g->geomBits);
+    free(g->wallMarker); free(g->shifter); free(g->rowI); free(g->rowJ); free(g->rowK);
+    free(g->rowJP); free(g->rowKP); free(g->rowJKP); free(g->wallMap); free(g->perIndex);
+    free(g->perSource); free(g->f);
+    memset(g, 0, sizeof(*g));
+}
+
+/* getCompressedNBR + finishNBRPlus (include/cellFunctions.h:74-94,
+ * include/NBRFunctions.h:5-11) */
+static void get_nbr(const ogrid* g, int cell, int nb[8]) {
+    const int shift = g->shifter[cell];
+    int jP, kP, jkP;
+    if (shift >= 0) {
+        jP = g->rowJP[shift]; kP = g->rowKP[shift]; jkP = g->rowJKP[shift];
+    } else {
+        const int ci = g->shifter[cell + shift];
+        jP = g->rowJP[ci] - shift; kP = g->rowKP[ci] - shift; jkP = g->rowJKP[ci] - shift;
+    }
+    const int n = g->cellCount;
+    nb[0] = cell;
+    nb[1] = cell + 1 >= n ? 0 : cell + 1;
+    nb[2] = jP;
+    nb[3] = jP + 1 >= n ? 0 : jP + 1;
+    nb[4] = kP;
+    nb[5] = kP + 1 >= n ? 0 : kP + 1;
+    nb[6] = jkP;
+    nb[7] = jkP + 1 >= n ? 0 : jkP + 1;
+}
+
+/* ---- updateSingleGrid (include/updateGrid.h:16-386) --------------------- */
+void oracle_step(ogrid* g, int steps) {
+    const long long n = g->cellCount;
+    for (int s = 0; s < steps; ++s) {
+        const int flip = g->flip;
+        /* K1: cell lambda (:51-177) */
+#pragma omp parallel for schedule(static)
+        for (int cell = 0; cell < g->cellCount; ++cell) {
+            if (g->wallMap[cell] == -3) continue;
+            int nb[8];
+            get_nbr(g, cell, nb);
+            float f[27];
+            for (int d = 0; d < 27; ++d) f[d] = g->f[(size_t)(flip ? INV[d] : d) * n + nb[pre_nbr(d)]];
+            obc bc;
+            oracle_default_bc(&bc);
+            float m[4];
+            oracle_get_drho_u(f, m);
+            bc.dRho = m[0]; bc.ux = m[1]; bc.uy = m[2]; bc.uz = m[3];
+            bc.collisionLimiter = g->limiter;
+            bc.nuMultiplier = g->nuMultiplier;
+            oracle_apply_collision(f, &bc, g->nu);
+            for (int d = 0; d < 27; ++d) g->f[(size_t)(flip ? d : INV[d]) * n + nb[post_nbr(d)]] = f[d];
+        }
+        /* applyStreaming (esotwistStreamingFunctions.h:6-9) */
+        g->flip = !flip;
+        /* K3: periodic copy (:358-382) */
+#pragma omp parallel for schedule(static)
+        for (int p = 0; p < g->perCount; ++p) {
+            int nb[8];
+            float f[27];
+            get_nbr(g, g->perSource[p], nb);
+            for (int d = 0; d < 27; ++d) f[d] = g->f[(size_t)(g->flip ? INV[d] : d) * n + nb[pre_nbr(d)]];
+            get_nbr(g, g->perIndex[p], nb);
+            for (int d = 0; d < 27; ++d) g->f[(size_t)(g->flip ? INV[d] : d) * n + nb[pre_nbr(d)]] = f[d];
+        }
+        g->iterationsFinished++;
+    }
+}
+
+/* K1 over cells [c0, c1) only, without the flip: a bounded slice of one step
+ * for timing the CPU implementation on large grids. */
+void oracle_collide_range(ogrid* g, int c0, int c1) {
+    const long long n = g->cellCount;
+    const int flip = g->flip;
+    if (c0 < 0) c0 = 0;
+    if (c1 > g->cellCount) c1 = g->cellCount;
+#pragma omp parallel for schedule(static)
+    for (int cell = c0; cell < c1; ++cell) {
+        if (g->wallMap[cell] == -3) continue;
+        int nb[8];
+        get_nbr(g, cell, nb);
+        float f[27];
+        for (int d = 0; d < 27; ++d) f[d] = g->f[(size_t)(flip ? INV[d] : d) * n + nb[pre_nbr(d)]];
+        obc bc;
+        oracle_default_bc(&bc);
+        float m[4];
+        oracle_get_drho_u(f, m);
+        bc.dRho = m[0]; bc.ux = m[1]; bc.uy = m[2]; bc.uz = m[3];
+        bc.collisionLimiter = g->limiter;
+        bc.nuMultiplier = g->nuMultiplier;
+        oracle_apply_collision(f, &bc, g->nu);
+        for (int d = 0; d < 27; ++d) g->f[(size_t)(flip ? d : INV[d]) * n + nb[post_nbr(d)]] = f[d];
+    }
+}
+
+double oracle_kinetic_energy(const ogrid* g, float uRefPhys, float domainLength) {
+    const long long n = g->cellCount;
+    double sum = 0.0;
+#pragma omp parallel for reduction(+ : sum) schedule(static)
+    for (int cell = 0; cell < g->cellCount; ++cell) {
+        const int wm = g->wallMap[cell];
+        if (wm == -3 || wm == -2) continue;
+        int nb[8];
+        get_nbr(g, cell, nb);
+        float f[27], m[4];
+        for (int d = 0; d < 27; ++d) f[d] = g->f[(size_t)(g->flip ? INV[d] : d) * n + nb[pre_nbr(d)]];
+        oracle_get_drho_u(f, m);
+        sum += 0.5 * (1.0 + (double)m[0]) * ((double)m[1] * m[1] + (double)m[2] * m[2] + (double)m[3] * m[3]);
+    }
+    const double dx = (double)g->res / 1000.0;
+    const double vs = dx / ((double)g->dtPhys * uRefPhys);
+    const double len = (double)domainLength / 1000.0;
+    return sum * dx * dx * dx * vs * vs / (len * len * len);
+}
+
+void oracle_macro(const ogrid* g, float* out) {
+    const long long n = g->cellCount;
+#pragma omp parallel for schedule(static)
+    for (int cell = 0; cell < g->cellCount; ++cell) {
+        int nb[8];
+        get_nbr(g, cell, nb);
+        float f[27], m[4];
+        for (int d = 0; d < 27; ++d) f[d] = g->f[(size_t)(g->flip ? INV[d] : d) * n + nb[pre_nbr(d)]];
+        oracle_get_drho_u(f, m);
+        for (int q = 0; q < 4; ++q) out[q * n + cell] = m[q];
+    }
+}

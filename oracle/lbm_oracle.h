@@ -1,0 +1,95 @@
+/*
+ * lbm_oracle.h — TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU restatement of the reference's D3Q27 cumulant time step
+ * (stepanmuller/LBM3, include/updateGrid.h and the headers it uses), in
+ * plain C with no floating-point contraction.  Only tests/, the smoke check
+ * and bench.py's CPU-baseline leg may load it; the product never does.
+ *
+ * Parity pin: the reference itself needs the absent TNL library, so it is
+ * unbuildable here.  The restatement is pinned against the reference's own
+ * stored Taylor–Green kinetic-energy curves
+ * (cases/taylorGreenVortex/results/COARSE_kineticEnergy.txt and its siblings), committed as
+ * fixtures under tests/golden/.
+ */
+#ifndef LBM_ORACLE_H
+#define LBM_ORACLE_H
+
+#include "../include/lbm3_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* BCStruct (include/types.h:131-136) */
+typedef struct obc {
+    float dRho, ux, uy, uz, gx, gy, gz;
+    int wallID, openBCID;
+    int useIBB, dirichletU, dirichletRho, periodic, nonReflective;
+    float nonReflectiveBeta, collisionLimiter, nuMultiplier;
+} obc;
+
+void oracle_default_bc(obc* bc);
+
+/* applyCollision, include/applyCollision.h:17-491 */
+void oracle_apply_collision(float f[27], const obc* bc, float nu);
+/* the same over a [27][n] batch (OpenMP) */
+void oracle_apply_collision_batch(float* f, int n, float nu, float limiter, float nuMultiplier,
+                                  float gx, float gy, float gz);
+/* getFeq, include/cellFunctions.h:125-148 */
+void oracle_get_feq(float dRho, float ux, float uy, float uz, float feq[27]);
+/* getDRhoUxUyUz, include/cellFunctions.h:257-279; out = {dRho, ux, uy, uz} */
+void oracle_get_drho_u(const float f[27], float out[4]);
+
+/* One grid level: InfoStruct + the tables updateSingleGrid reads. */
+typedef struct ogrid {
+    /* Info */
+    int gridID;
+    float res, ox, oy, oz, nu, dtPhys;
+    int nx, ny, nz, cellCount;
+    int flip;
+    int iterationsFinished;
+    /* builder arrays (sorted full IJK, NBR plus) */
+    int *I, *J, *K, *jPlus, *kPlus;
+    unsigned char* geomBits;
+    unsigned char* wallMarker;
+    /* compressed IJK/NBR */
+    int* shifter;
+    int rowCount;
+    int *rowI, *rowJ, *rowK, *rowJP, *rowKP, *rowJKP;
+    int* wallMap;
+    int perCount;
+    int *perIndex, *perSource;
+    int openBCCount;
+    /* populations [27][cellCount] */
+    float* f;
+    long long fluidUpdates;
+    /* uniform getLocalBC */
+    float limiter, nuMultiplier;
+} ogrid;
+
+/* buildGrids for a box domain without geometry, single level, followed by
+ * applyInitialCondition.  Returns 0 or a negative LBM_ERR_* code. */
+int oracle_build(const lbm_case* c, ogrid* g);
+void oracle_free(ogrid* g);
+
+/* updateSingleGrid (include/updateGrid.h:16-386) `steps` times. */
+void oracle_step(ogrid* g, int steps);
+
+/* the collide-stream of cells [c0, c1) of one step, flipper unchanged
+ * (bounded CPU timing sample) */
+void oracle_collide_range(ogrid* g, int c0, int c1);
+
+/* getKineticEnergy (cases/taylorGreenVortex/taylorGreenVortexMain.cu:116-180). */
+double oracle_kinetic_energy(const ogrid* g, float uRefPhys, float domainLength);
+
+/* dRho,ux,uy,uz of every cell: out[4][cellCount]. */
+void oracle_macro(const ogrid* g, float* out);
+
+/* number of OpenMP threads the oracle uses */
+int oracle_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

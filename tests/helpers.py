@@ -1,0 +1,20 @@
+"""Shared test helpers: tolerances and comparisons."""
+import numpy as np
+
+# FP32 field parity bar for the collide-stream path (relative L2 of
+# dRho, ux, uy, uz against the oracle after N steps).
+FIELD_REL_L2 = 1e-5
+
+
+def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    den = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (den if den > 0 else 1.0))
+
+
+def load_golden(name: str):
+    from pathlib import Path
+    path = Path(__file__).resolve().parent / "golden" / name
+    rows = [l.split(";") for l in path.read_text().splitlines() if l and not l.startswith("#")]
+    return np.array([[float(a), float(b)] for a, b in rows])

@@ -1,0 +1,61 @@
+"""The C-ABI library loads and exports every entry point include/lbm3_b200.h declares."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+from lbm3_b200 import _abi as A
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADER = ROOT / "include" / "lbm3_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"^\s*[A-Za-z_][\w\s\*]*?\b(lbm_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared_functions()
+    assert len(names) >= 15
+    lib = A.lib()
+    for n in names:
+        assert hasattr(lib, n), n
+    assert {s[0] for s in A.SIGNATURES} == set(names)
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    src = tmp_path / "sizes.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "lbm3_b200.h"\n'
+                   'int main(void){printf("%zu %zu %zu %zu %zu\\n", sizeof(lbm_case), sizeof(lbm_face_bc),'
+                   ' sizeof(lbm_grid_info), offsetof(lbm_case, storage), offsetof(lbm_grid_info, grid_memory_bytes));'
+                   'return 0;}\n')
+    exe = tmp_path / "sizes"
+    subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    assert int(out[0]) == C.sizeof(A.LbmCase)
+    assert int(out[1]) == C.sizeof(A.LbmFaceBC)
+    assert int(out[2]) == C.sizeof(A.LbmGridInfo)
+    assert int(out[3]) == A.LbmCase.storage.offset
+    assert int(out[4]) == A.LbmGridInfo.grid_memory_bytes.offset
+
+
+def test_null_arguments_are_rejected_without_a_device():
+    lib = A.lib()
+    assert lib.lbm_plan_grids(None, None, None) == A.LBM_ERR_INVALID
+    assert b"null" in lib.lbm_last_error()
+    assert lib.lbm_update_all_grids(None, 1) == A.LBM_ERR_INVALID
+    assert lib.lbm_read_array(None, 0, 0, None, 0) == A.LBM_ERR_INVALID
+
+
+def test_build_without_device_fails_loudly():
+    lib = A.lib()
+    if lib.lbm_device_count() > 0:
+        pytest.skip("a CUDA device is visible")
+    import lbm3_b200 as L
+    with pytest.raises(A.LbmError) as e:
+        L.build_grids(L.tgv_plain_method().case)
+    assert e.value.code == A.LBM_ERR_NO_DEVICE
