@@ -21,6 +21,17 @@ struct CollisionConsts {
     float tauTerm;     // 1/omega1 - 1/2
     float lambda;      // collision limiter (K17 when > 0 and nuMultiplier <= 1)
     int useK17;
+    // products of the above that every cell needs, formed in the order the
+    // reference multiplies them so the per-cell result rounds the same way
+    float mHalfW1;     // -omega1 * 0.5
+    float w1x15;       // 1.5 * omega1
+    float mW1x3;       // -3 * omega1
+    float oneMinusW1;  // 1 - omega1
+    float halfW1c;     // 1 - 0.5 * omega1
+    float oneMinusW3, oneMinusW4, oneMinusW5;
+    float c43;         // (2/3) * tauTerm * A
+    float c45;         // -(4/3) * tauTerm * A
+    float cB;          // -(1/3) * tauTerm * B
 };
 
 // Host-side evaluation of the per-grid constants, with the reference's
@@ -49,10 +60,35 @@ inline CollisionConsts makeCollisionConsts(float nu, float nuMultiplier, float l
     k.tauTerm = 1.f / omega1 - 0.5f;
     k.lambda = limiter;
     k.useK17 = (limiter > 0.f) && (nuMultiplier <= 1.f);
+    k.mHalfW1 = -omega1 * 0.5f;
+    k.w1x15 = 1.5f * omega1;
+    k.mW1x3 = -3.f * omega1;
+    k.oneMinusW1 = 1.f - omega1;
+    k.halfW1c = 1.f - 0.5f * omega1;
+    k.oneMinusW3 = 1.f - k.omega3;
+    k.oneMinusW4 = 1.f - k.omega4;
+    k.oneMinusW5 = 1.f - k.omega5;
+    k.c43 = (2.f / 3.f) * k.tauTerm * k.A;
+    k.c45 = -(4.f / 3.f) * k.tauTerm * k.A;
+    k.cB = -(1.f / 3.f) * k.tauTerm * k.B;
     return k;
 }
 
 namespace detail {
+
+constexpr float kThird = 1.f / 3.f;
+constexpr float kNinth = 1.f / 9.f;
+constexpr float k27th = 1.f / 27.f;
+
+// a / b for the limiter weights: the hardware reciprocal on the device
+// (two ulp), an exact division on the host.
+LBM_HD float limDiv(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fdividef(a, b);
+#else
+    return a / b;
+#endif
+}
 
 // Weight moments of the shifted transform, as the literal fractions the
 // reference uses (K_aa0 ... K_c02, include/applyCollision.h:24-38).
@@ -162,79 +198,68 @@ LBM_HD void collideCumulant(float (&f)[27], const CollisionConsts& P, float lamb
     const float C111 = k[1][1][1];
     const float C120 = k[1][2][0], C102 = k[1][0][2], C210 = k[2][1][0];
     const float C012 = k[0][1][2], C201 = k[2][0][1], C021 = k[0][2][1];
-    const float third = 1.f / 3.f;
-    const float C211 = k[2][1][1] - ((k[2][0][0] + third) * k[0][1][1] + 2.f * k[1][0][1] * k[1][1][0]) * rhoInv;
-    const float C121 = k[1][2][1] - ((k[0][2][0] + third) * k[1][0][1] + 2.f * k[1][1][0] * k[0][1][1]) * rhoInv;
-    const float C112 = k[1][1][2] - ((k[0][0][2] + third) * k[1][1][0] + 2.f * k[0][1][1] * k[1][0][1]) * rhoInv;
-    const float C220 = k[2][2][0] - ((k[0][2][0] * k[2][0][0] + 2.f * k[1][1][0] * k[1][1][0] +
-                                      (k[2][0][0] + k[0][2][0]) / 3.f) * rhoInv - dRho * rhoInv / 9.f);
-    const float C022 = k[0][2][2] - ((k[0][0][2] * k[0][2][0] + 2.f * k[0][1][1] * k[0][1][1] +
-                                      (k[0][0][2] + k[0][2][0]) / 3.f) * rhoInv - dRho * rhoInv / 9.f);
-    const float C202 = k[2][0][2] - ((k[2][0][0] * k[0][0][2] + 2.f * k[1][0][1] * k[1][0][1] +
-                                      (k[2][0][0] + k[0][0][2]) / 3.f) * rhoInv - dRho * rhoInv / 9.f);
+    const float third = kThird;
+    const float dRhoNinth = dRho * rhoInv * kNinth;
+    // C211, C121, C112, C220, C022, C202 (:170-187) only enter the reference's
+    // relaxation multiplied by (1 - omega6..8) = 0, so they are not formed.
     const float k000 = dRho;
 
-    // ---- relaxation (:193-342) ----
-    const float omega1 = P.omega1;
-    const float omega2 = 1.f;
-    const float Dxu = -omega1 * 0.5f * rhoInv * (2.f * C200 - C020 - C002) -
-                      omega2 * 0.5f * rhoInv * (C200 + C020 + C002 - k000);
-    const float Dyv = Dxu + 1.5f * omega1 * rhoInv * (C200 - C020);
-    const float Dzw = Dxu + 1.5f * omega1 * rhoInv * (C200 - C002);
-    const float DxvDyu = -3.f * omega1 * rhoInv * C110;
-    const float DxwDzu = -3.f * omega1 * rhoInv * C101;
-    const float DywDzv = -3.f * omega1 * rhoInv * C011;
+    // ---- relaxation (:193-342); omega2 = omega6 = omega7 = omega8 = 1, so
+    // the (1 - omega) terms of those rates vanish and are not evaluated ----
+    const float Dxu = P.mHalfW1 * rhoInv * (2.f * C200 - C020 - C002) -
+                      0.5f * rhoInv * (C200 + C020 + C002 - k000);
+    const float Dyv = Dxu + P.w1x15 * rhoInv * (C200 - C020);
+    const float Dzw = Dxu + P.w1x15 * rhoInv * (C200 - C002);
+    const float DxvDyu = P.mW1x3 * rhoInv * C110;
+    const float DxwDzu = P.mW1x3 * rhoInv * C101;
+    const float DywDzv = P.mW1x3 * rhoInv * C011;
 
-    const float Cs110 = (1.f - omega1) * C110;
-    const float Cs101 = (1.f - omega1) * C101;
-    const float Cs011 = (1.f - omega1) * C011;
-    const float e33 = (1.f - omega1) * (C200 - C020) -
-                      3.f * rho * (1.f - 0.5f * omega1) * (ux2 * Dxu - uy2 * Dyv);
-    const float e34 = (1.f - omega1) * (C200 - C002) -
-                      3.f * rho * (1.f - 0.5f * omega1) * (ux2 * Dxu - uz2 * Dzw);
-    const float e35 = k000 * omega2 + (1.f - omega2) * (C200 + C020 + C002) -
-                      3.f * rho * (1.f - 0.5f * omega2) * (ux2 * Dxu + uy2 * Dyv + uz2 * Dzw);
-    const float Cs200 = (e33 + e34 + e35) / 3.f;
-    const float Cs020 = (e34 - 2.f * e33 + e35) / 3.f;
-    const float Cs002 = (e33 - 2.f * e34 + e35) / 3.f;
+    const float Cs110 = P.oneMinusW1 * C110;
+    const float Cs101 = P.oneMinusW1 * C101;
+    const float Cs011 = P.oneMinusW1 * C011;
+    const float r3 = 3.f * rho * P.halfW1c;
+    const float e33 = P.oneMinusW1 * (C200 - C020) - r3 * (ux2 * Dxu - uy2 * Dyv);
+    const float e34 = P.oneMinusW1 * (C200 - C002) - r3 * (ux2 * Dxu - uz2 * Dzw);
+    const float e35 = k000 - 3.f * rho * 0.5f * (ux2 * Dxu + uy2 * Dyv + uz2 * Dzw);
+    const float Cs200 = (e33 + e34 + e35) * kThird;
+    const float Cs020 = (e34 - 2.f * e33 + e35) * kThird;
+    const float Cs002 = (e33 - 2.f * e34 + e35) * kThird;
 
     float Cs120 = 0.f, Cs102 = 0.f, Cs210 = 0.f, Cs012 = 0.f, Cs201 = 0.f, Cs021 = 0.f;
     float Cs111 = 0.f, Cs220 = 0.f, Cs202 = 0.f, Cs022 = 0.f, Cs211 = 0.f, Cs121 = 0.f, Cs112 = 0.f;
     if (P.useK17 && lambda > 0.f) {
-        // K17 with limiter: third order relaxed by omega3..5 pushed towards 1
+        // K17 with limiter: third-order rates pushed from omega3..5 towards 1
+        // where the cumulant is large compared with lambda (:270-306)
         const float p1 = C120 + C102, p2 = C210 + C012, p3 = C201 + C021;
         const float q1 = C120 - C102, q2 = C210 - C012, q3 = C201 - C021;
-        auto lim = [&](float om, float v) {
-            const float av = v < 0.f ? -v : v;
-            return om + (1.f - om) * av / (lambda + av);
+        // 1 - (om + (1 - om) |v| / (lambda + |v|)) applied to v
+        auto relax = [&](float om, float oneMinusOm, float v) {
+            const float av = fabsf(v);
+            return (1.f - (om + limDiv(oneMinusOm * av, lambda + av))) * v;
         };
-        const float e117 = (1.f - lim(P.omega3, p1)) * p1;
-        const float e118 = (1.f - lim(P.omega3, p2)) * p2;
-        const float e119 = (1.f - lim(P.omega3, p3)) * p3;
-        const float e120 = (1.f - lim(P.omega4, q1)) * q1;
-        const float e121 = (1.f - lim(P.omega4, q2)) * q2;
-        const float e122 = (1.f - lim(P.omega4, q3)) * q3;
+        const float e117 = relax(P.omega3, P.oneMinusW3, p1);
+        const float e118 = relax(P.omega3, P.oneMinusW3, p2);
+        const float e119 = relax(P.omega3, P.oneMinusW3, p3);
+        const float e120 = relax(P.omega4, P.oneMinusW4, q1);
+        const float e121 = relax(P.omega4, P.oneMinusW4, q2);
+        const float e122 = relax(P.omega4, P.oneMinusW4, q3);
         Cs120 = 0.5f * (e120 + e117);
         Cs102 = 0.5f * (-e120 + e117);
         Cs210 = 0.5f * (e121 + e118);
         Cs012 = 0.5f * (-e121 + e118);
         Cs201 = 0.5f * (e122 + e119);
         Cs021 = 0.5f * (-e122 + e119);
-        Cs111 = (1.f - lim(P.omega5, C111)) * C111;
-        // fourth order: omega6 = omega7 = omega8 = 1 (:226-228, :316-323)
-        const float t = P.tauTerm;
-        const float e43 = (2.f / 3.f) * t * 1.f * P.A * rho * (Dxu - 2.f * Dyv + Dzw) +
-                          (1.f - 1.f) * (C220 - 2.f * C202 + C022);
-        const float e44 = (2.f / 3.f) * t * 1.f * P.A * rho * (-2.f * Dxu + Dyv + Dzw) +
-                          (1.f - 1.f) * (C220 + C202 - 2.f * C022);
-        const float e45 = -(4.f / 3.f) * t * 1.f * P.A * rho * (Dxu + Dyv + Dzw) +
-                          (1.f - 1.f) * (C220 + C202 + C022);
-        Cs220 = (e43 + e44 + e45) / 3.f;
-        Cs202 = (-e43 + e45) / 3.f;
-        Cs022 = (-e44 + e45) / 3.f;
-        Cs211 = -(1.f / 3.f) * t * 1.f * P.B * rho * DywDzv + (1.f - 1.f) * C211;
-        Cs121 = -(1.f / 3.f) * t * 1.f * P.B * rho * DxwDzu + (1.f - 1.f) * C121;
-        Cs112 = -(1.f / 3.f) * t * 1.f * P.B * rho * DxvDyu + (1.f - 1.f) * C112;
+        Cs111 = relax(P.omega5, P.oneMinusW5, C111);
+        // fourth order (:310-323)
+        const float e43 = P.c43 * rho * (Dxu - 2.f * Dyv + Dzw);
+        const float e44 = P.c43 * rho * (-2.f * Dxu + Dyv + Dzw);
+        const float e45 = P.c45 * rho * (Dxu + Dyv + Dzw);
+        Cs220 = (e43 + e44 + e45) * kThird;
+        Cs202 = (-e43 + e45) * kThird;
+        Cs022 = (-e44 + e45) * kThird;
+        Cs211 = P.cB * rho * DywDzv;
+        Cs121 = P.cB * rho * DxwDzu;
+        Cs112 = P.cB * rho * DxvDyu;
     }
 
     // ---- cumulants -> central moments (:348-384) ----
@@ -246,18 +271,15 @@ LBM_HD void collideCumulant(float (&f)[27], const CollisionConsts& P, float lamb
     s[2][1][1] = Cs211 + ((Cs200 + third) * Cs011 + 2.f * Cs101 * Cs110) * rhoInv;
     s[1][2][1] = Cs121 + ((Cs020 + third) * Cs101 + 2.f * Cs110 * Cs011) * rhoInv;
     s[1][1][2] = Cs112 + ((Cs002 + third) * Cs110 + 2.f * Cs011 * Cs101) * rhoInv;
-    s[2][2][0] = Cs220 + ((Cs020 * Cs200 + 2.f * Cs110 * Cs110 + (Cs200 + Cs020) / 3.f) * rhoInv -
-                          dRho * rhoInv / 9.f);
-    s[0][2][2] = Cs022 + ((Cs002 * Cs020 + 2.f * Cs011 * Cs011 + (Cs002 + Cs020) / 3.f) * rhoInv -
-                          dRho * rhoInv / 9.f);
-    s[2][0][2] = Cs202 + ((Cs200 * Cs002 + 2.f * Cs101 * Cs101 + (Cs200 + Cs002) / 3.f) * rhoInv -
-                          dRho * rhoInv / 9.f);
+    s[2][2][0] = Cs220 + ((Cs020 * Cs200 + 2.f * Cs110 * Cs110 + (Cs200 + Cs020) * kThird) * rhoInv - dRhoNinth);
+    s[0][2][2] = Cs022 + ((Cs002 * Cs020 + 2.f * Cs011 * Cs011 + (Cs002 + Cs020) * kThird) * rhoInv - dRhoNinth);
+    s[2][0][2] = Cs202 + ((Cs200 * Cs002 + 2.f * Cs101 * Cs101 + (Cs200 + Cs002) * kThird) * rhoInv - dRhoNinth);
     s[1][2][2] = (Cs020 * Cs102 + Cs002 * Cs120 + 4.f * Cs011 * Cs111 +
-                  2.f * (Cs110 * Cs012 + Cs101 * Cs021) + (Cs120 + Cs102) / 3.f) * rhoInv;
+                  2.f * (Cs110 * Cs012 + Cs101 * Cs021) + (Cs120 + Cs102) * kThird) * rhoInv;
     s[2][1][2] = (Cs002 * Cs210 + Cs200 * Cs012 + 4.f * Cs101 * Cs111 +
-                  2.f * (Cs011 * Cs201 + Cs110 * Cs102) + (Cs210 + Cs012) / 3.f) * rhoInv;
+                  2.f * (Cs011 * Cs201 + Cs110 * Cs102) + (Cs210 + Cs012) * kThird) * rhoInv;
     s[2][2][1] = (Cs200 * Cs021 + Cs020 * Cs201 + 4.f * Cs110 * Cs111 +
-                  2.f * (Cs101 * Cs120 + Cs011 * Cs210) + (Cs021 + Cs201) / 3.f) * rhoInv;
+                  2.f * (Cs101 * Cs120 + Cs011 * Cs210) + (Cs021 + Cs201) * kThird) * rhoInv;
     {
         const float a200 = Cs200, a020 = Cs020, a002 = Cs002;
         const float a110 = Cs110, a101 = Cs101, a011 = Cs011, a111 = Cs111;
@@ -268,12 +290,12 @@ LBM_HD void collideCumulant(float (&f)[27], const CollisionConsts& P, float lamb
             (16.f * a110 * a101 * a011 +
              4.f * (a101 * a101 * a020 + a011 * a011 * a200 + a110 * a110 * a002) +
              2.f * a200 * a020 * a002) * rhoInv * rhoInv +
-            (3.f * (s[0][2][2] + s[2][0][2] + s[2][2][0]) + (a200 + a020 + a002)) * rhoInv / 9.f -
+            (3.f * (s[0][2][2] + s[2][0][2] + s[2][2][0]) + (a200 + a020 + a002)) * rhoInv * kNinth -
             (2.f / 3.f) *
                 (2.f * (a101 * a101 + a011 * a011 + a110 * a110) +
-                 (a002 * a020 + a002 * a200 + a020 * a200) + (a002 + a020 + a200) / 3.f) *
+                 (a002 * a020 + a002 * a200 + a020 * a200) + (a002 + a020 + a200) * kThird) *
                 rhoInv * rhoInv -
-            (dRho * dRho - dRho) * rhoInv * rhoInv / 27.f;
+            (dRho * dRho - dRho) * rhoInv * rhoInv * k27th;
     }
     s[0][0][0] = k000;
     s[1][0][0] = -k[1][0][0];
@@ -293,7 +315,7 @@ LBM_HD void collideCumulant(float (&f)[27], const CollisionConsts& P, float lamb
                                                : 1.f / 3.f;
             const float div = (b == 0 && n == 0) ? 1.f : (b == 2 && n == 2) ? 9.f : 3.f;
             float mid = s0 * (1.f - ux2) - 2.f * ux * s1 - s2;
-            if (hasK) mid = mid - ((b == 0 && n == 0) ? ux2 : ux2 / div);
+            if (hasK) mid = mid - ((b == 0 && n == 0) ? ux2 : ux2 * (1.f / div));
             m[1][b][n] = mid;
             m[0][b][n] = ((s0 + K) * (ux2 - ux) + s1 * (2.f * ux - 1.f) + s2) * 0.5f;
             m[2][b][n] = ((s0 + K) * (ux2 + ux) + s1 * (2.f * ux + 1.f) + s2) * 0.5f;

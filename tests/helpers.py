@@ -18,3 +18,10 @@ def load_golden(name: str):
     path = Path(__file__).resolve().parent / "golden" / name
     rows = [l.split(";") for l in path.read_text().splitlines() if l and not l.startswith("#")]
     return np.array([[float(a), float(b)] for a, b in rows])
+
+
+def field_errors(got: np.ndarray, ref: np.ndarray):
+    """(rel L2 of dRho, rel L2 of the velocity vector field) for [4][n] macro arrays."""
+    e_rho = rel_l2(got[0], ref[0])
+    e_u = rel_l2(got[1:4].reshape(-1), ref[1:4].reshape(-1))
+    return e_rho, e_u
