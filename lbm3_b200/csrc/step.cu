@@ -18,6 +18,11 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstdlib>
+#include <string>
+#include <type_traits>
+
 namespace lbm {
 
 namespace {
@@ -36,6 +41,66 @@ __global__ void __launch_bounds__(kBlock) collideStream(DevLevel g) {
     readPre<F, S>(g, nb, f);
     collideCumulant(f, g.coll, g.coll.lambda, 0.f, 0.f, 0.f);
     writePost<F, S>(g, nb, f);
+}
+
+// ---- pipelined collide-stream (FP32 storage) --------------------------------
+// Persistent CTAs walk tiles of kPipeBlock consecutive cells.  While a tile is
+// collided from registers, the 27 gathers of the thread's next cell are already
+// in flight as cp.async copies into shared memory (two stages).  Each thread
+// reads back only the stage slots its own copies filled, so no block-level
+// barrier is needed; in-place esotwist streaming keeps every global slot owned
+// by exactly one cell, so the prefetch never reads a value this step writes.
+constexpr int kPipeBlock = 128;
+
+__device__ __forceinline__ void cpAsync4(float* smem, const float* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncWaitPrev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Decode the tile's cell for this thread and start its 27 gathers into stage `buf`.
+template <bool F>
+__device__ __forceinline__ bool issueTile(const DevLevel& g, int tile, float* stage, int (&nb)[8]) {
+    const int cell = tile * kPipeBlock + threadIdx.x;
+    if (cell >= g.cellCount) return false;
+    if (__ldg(g.wallMap + cell) == -3) return false;
+    decodeNbr(g, cell, nb, nullptr);
+    const float* base = static_cast<const float*>(g.f);
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        cpAsync4(stage + d * kPipeBlock + threadIdx.x,
+                 base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
+    return true;
+}
+
+template <bool F>
+__global__ void __launch_bounds__(kPipeBlock) collideStreamPipelined(DevLevel g, int tiles) {
+    extern __shared__ float stages[];  // [2][27][kPipeBlock]
+    float* stage[2] = {stages, stages + 27 * kPipeBlock};
+    int tile = blockIdx.x;
+    int nbCur[8];
+    bool cur = tile < tiles && issueTile<F>(g, tile, stage[0], nbCur);
+    cpAsyncCommit();
+    int b = 0;
+    for (; tile < tiles; tile += gridDim.x) {
+        const int next = tile + gridDim.x;
+        int nbNext[8];
+        const bool nxt = next < tiles && issueTile<F>(g, next, stage[b ^ 1], nbNext);
+        cpAsyncCommit();
+        cpAsyncWaitPrev();  // this thread's copies of the current tile have landed
+        if (cur) {
+            float f[27];
+#pragma unroll
+            for (int d = 0; d < 27; ++d) f[d] = stage[b][d * kPipeBlock + threadIdx.x];
+            collideCumulant(f, g.coll, g.coll.lambda, 0.f, 0.f, 0.f);
+            writePost<F, float>(g, nbCur, f);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) nbCur[q] = nbNext[q];
+        cur = nxt;
+        b ^= 1;
+    }
 }
 
 // F is the flipper after streaming, i.e. the state the ghosts are read in.
@@ -183,9 +248,39 @@ void dispatch(const DevLevel& g, bool flip, A&&... args) {
     }
 }
 
+int pipelineGrid() {
+    static int grid = 0;
+    if (grid == 0) {
+        int dev = 0, sms = 0, perSm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int smem = 2 * 27 * kPipeBlock * sizeof(float);
+        cudaFuncSetAttribute(collideStreamPipelined<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(collideStreamPipelined<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, collideStreamPipelined<false>, kPipeBlock, smem);
+        grid = sms * (perSm > 0 ? perSm : 1);
+    }
+    return grid;
+}
+
+bool usePipelined() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("LBM3_COLLIDE_KERNEL");
+        v = (e && std::string(e) == "simple") ? 0 : 1;
+    }
+    return v == 1;
+}
+
 template <bool F, class S> struct RunCollide {
     static void run(const DevLevel& g, cudaStream_t s) {
-        collideStream<F, S><<<blocksFor(g.cellCount), kBlock, 0, s>>>(g);
+        if (std::is_same<S, float>::value && usePipelined()) {
+            const int tiles = (g.cellCount + kPipeBlock - 1) / kPipeBlock;
+            const int grid = std::min(pipelineGrid(), tiles);
+            collideStreamPipelined<F><<<grid, kPipeBlock, 2 * 27 * kPipeBlock * sizeof(float), s>>>(g, tiles);
+        } else {
+            collideStream<F, S><<<blocksFor(g.cellCount), kBlock, 0, s>>>(g);
+        }
     }
 };
 template <bool F, class S> struct RunPeriodic {
