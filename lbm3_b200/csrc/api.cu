@@ -296,6 +296,16 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
             d.perIndex = own(upload(H.perIndex, s));
             d.perSource = own(upload(H.perSource, s));
             d.perCount = static_cast<int>(H.perIndex.size());
+            {
+                std::vector<int4> seg(H.segCell.size());
+                for (size_t q = 0; q < seg.size(); ++q)
+                    seg[q] = make_int4(H.segCell[q], H.segJP[q], H.segKP[q], H.segJKP[q]);
+                d.seg = own(upload(seg, s));
+                d.segLen = own(upload(H.segLen, s));
+                d.segCount = static_cast<int>(seg.size());
+                d.special = own(upload(H.specialCells, s));
+                d.specialCount = static_cast<int>(H.specialCells.size());
+            }
             lbm::BC bc;
             lbm::evalLocalBC(*c, bc);
             d.coll = lbm::makeCollisionConsts(H.info.nu, bc.nuMultiplier, bc.collisionLimiter);

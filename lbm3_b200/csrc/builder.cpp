@@ -346,6 +346,34 @@ void buildBoundaryLists(const lbm_case& c, HostLevel& L) {
 
 }  // namespace
 
+void buildSegments(HostLevel& L) {
+    L.segCell.clear(); L.segJP.clear(); L.segKP.clear(); L.segJKP.clear(); L.segLen.clear();
+    L.specialCells.clear();
+    const int n = L.info.cellCount;
+    int c = 0;
+    while (c < n) {
+        // extent of the compressed row starting at c
+        int end = c + 1;
+        while (end < n && L.shifter[end] < 0) ++end;
+        const int row = L.shifter[c];
+        for (int q = c; q < end;) {
+            const int wm = L.wallMap[q];
+            if (wm >= 0) { L.specialCells.push_back(q); ++q; continue; }
+            if (wm == -3) { ++q; continue; }
+            int r = q;
+            while (r < end && r - q < kSegmentCells && (L.wallMap[r] == -1 || L.wallMap[r] == -2)) ++r;
+            const int off = q - c;
+            L.segCell.push_back(q);
+            L.segJP.push_back(L.rowJP[row] + off);
+            L.segKP.push_back(L.rowKP[row] + off);
+            L.segJKP.push_back(L.rowJKP[row] + off);
+            L.segLen.push_back(r - q);
+            q = r;
+        }
+        c = end;
+    }
+}
+
 void buildDomain(const lbm_case& c, HostDomain& out) {
     validateCase(c);
     out.c = c;
@@ -362,6 +390,7 @@ void buildDomain(const lbm_case& c, HostDomain& out) {
     L.wallMarker.assign(L.info.cellCount, 0);
     compressRows(L);
     buildBoundaryLists(c, L);
+    buildSegments(L);
 
     out.fluidUpdatesPerIteration = 0;
     for (const HostLevel& lv : out.levels)

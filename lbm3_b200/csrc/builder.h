@@ -57,7 +57,16 @@ struct HostLevel {
     std::vector<OpenBCList> openBCs;
     int wallCellCount = 0;
     int wallAdjacentCount = 0;
+    // Bulk segments: runs of at most kSegmentCells plain-fluid cells (wallMap
+    // -1 or -2) inside one compressed row.  Inside such a run every neighbour
+    // index is the run's base plus the lane offset, so the bulk kernel needs
+    // one descriptor per tile and no per-cell metadata.
+    std::vector<int> segCell, segJP, segKP, segJKP, segLen;
+    // cells outside the bulk segments that still collide (wall-adjacent)
+    std::vector<int> specialCells;
 };
+
+constexpr int kSegmentCells = 128;
 
 struct HostDomain {
     lbm_case c;
@@ -71,6 +80,9 @@ BC evalOpenBC(const lbm_case& c, const Info& info, int i, int j, int k);
 void evalLocalBC(const lbm_case& c, BC& bc);
 // getInitialCondition.
 BC evalInitialCondition(const lbm_case& c, const Info& info, int i, int j, int k);
+
+// Split the compressed rows into bulk segments (needs wallMap).
+void buildSegments(HostLevel& L);
 
 // Build all tables; throws std::runtime_error on an invalid case (the
 // reference's setup throws at the same points).

@@ -14,6 +14,7 @@
 // most one cell).  The esotwist scheme makes every slot read and written by
 // exactly one thread per step, so the kernel needs no second buffer and no
 // synchronisation between cells.
+#include "builder.h"
 #include "step_launch.h"
 
 #include <cuda_runtime.h>
@@ -43,64 +44,137 @@ __global__ void __launch_bounds__(kBlock) collideStream(DevLevel g) {
     writePost<F, S>(g, nb, f);
 }
 
-// ---- pipelined collide-stream (FP32 storage) --------------------------------
-// Persistent CTAs walk tiles of kPipeBlock consecutive cells.  While a tile is
-// collided from registers, the 27 gathers of the thread's next cell are already
-// in flight as cp.async copies into shared memory (two stages).  Each thread
-// reads back only the stage slots its own copies filled, so no block-level
-// barrier is needed; in-place esotwist streaming keeps every global slot owned
-// by exactly one cell, so the prefetch never reads a value this step writes.
-constexpr int kPipeBlock = 128;
+// ---- bulk collide-stream ---------------------------------------------------
+// Persistent CTAs walk the bulk segments (runs of up to kSegmentCells plain
+// fluid cells inside one compressed row; one segment per CTA iteration, one
+// cell per thread).  Inside a segment the 8 esotwist neighbours of lane t are
+// the segment's base indices + t, so no per-cell metadata is loaded: a CTA
+// reads one 20-byte descriptor per tile, two tiles ahead.  The 27 gathers of
+// the next tile are issued as cp.async copies into shared memory before the
+// current tile is collided, so HBM traffic overlaps the cumulant arithmetic.
+// A thread reads back only the stage slots its own copies filled, hence no
+// block barrier; esotwist gives every global slot a single owning cell, so
+// prefetching the next tile never reads a value the current tile writes.
+// 16-bit storage stages the aligned 32-bit word that holds the element.
+constexpr int kTile = 128;  // == kSegmentCells
+static_assert(kTile == kSegmentCells, "tile and segment length differ");
 
-__device__ __forceinline__ void cpAsync4(float* smem, const float* gmem) {
+__device__ __forceinline__ void cpAsync4(void* smem, const void* gmem) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cpAsyncWaitPrev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
-// Decode the tile's cell for this thread and start its 27 gathers into stage `buf`.
-template <bool F>
-__device__ __forceinline__ bool issueTile(const DevLevel& g, int tile, float* stage, int (&nb)[8]) {
-    const int cell = tile * kPipeBlock + threadIdx.x;
-    if (cell >= g.cellCount) return false;
-    if (__ldg(g.wallMap + cell) == -3) return false;
-    decodeNbr(g, cell, nb, nullptr);
-    const float* base = static_cast<const float*>(g.f);
-#pragma unroll
-    for (int d = 0; d < 27; ++d)
-        cpAsync4(stage + d * kPipeBlock + threadIdx.x,
-                 base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
-    return true;
+__device__ __forceinline__ void segNbr(const DevLevel& g, const int4& d, int t, int (&nb)[8]) {
+    const int n = g.cellCount;
+    nb[0] = d.x + t;
+    nb[2] = d.y + t;
+    nb[4] = d.z + t;
+    nb[6] = d.w + t;
+    nb[1] = nb[0] + 1 < n ? nb[0] + 1 : 0;
+    nb[3] = nb[2] + 1 < n ? nb[2] + 1 : 0;
+    nb[5] = nb[4] + 1 < n ? nb[4] + 1 : 0;
+    nb[7] = nb[6] + 1 < n ? nb[6] + 1 : 0;
 }
 
-template <bool F>
-__global__ void __launch_bounds__(kPipeBlock) collideStreamPipelined(DevLevel g, int tiles) {
-    extern __shared__ float stages[];  // [2][27][kPipeBlock]
-    float* stage[2] = {stages, stages + 27 * kPipeBlock};
+template <class S> __device__ __forceinline__ float fromWord(unsigned w, const S* p);
+template <> __device__ __forceinline__ float fromWord<float>(unsigned w, const float*) {
+    return __uint_as_float(w);
+}
+template <> __device__ __forceinline__ float fromWord<__half>(unsigned w, const __half* p) {
+    const unsigned short h = (reinterpret_cast<uintptr_t>(p) & 2) ? (w >> 16) : (w & 0xffffu);
+    return __half2float(__ushort_as_half(h));
+}
+template <> __device__ __forceinline__ float fromWord<__nv_bfloat16>(unsigned w, const __nv_bfloat16* p) {
+    const unsigned short h = (reinterpret_cast<uintptr_t>(p) & 2) ? (w >> 16) : (w & 0xffffu);
+    return __bfloat162float(__ushort_as_bfloat16(h));
+}
+
+template <bool F, class S>
+__device__ __forceinline__ const S* preAddr(const DevLevel& g, const int (&nb)[8], int d) {
+    return static_cast<const S*>(g.f) + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)];
+}
+
+template <bool F, class S>
+__device__ __forceinline__ void issueGathers(const DevLevel& g, const int (&nb)[8], unsigned* stage) {
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        const S* p = preAddr<F, S>(g, nb, d);
+        const void* w = reinterpret_cast<const void*>(reinterpret_cast<uintptr_t>(p) & ~uintptr_t(3));
+        cpAsync4(stage + d * kTile + threadIdx.x, w);
+    }
+}
+
+// resident CTAs per SM the register allocation is sized for
+#ifndef LBM3_BULK_MIN_BLOCKS
+#define LBM3_BULK_MIN_BLOCKS 6
+#endif
+
+template <bool F, class S>
+__global__ void __launch_bounds__(kTile, LBM3_BULK_MIN_BLOCKS) collideBulk(DevLevel g) {
+    extern __shared__ unsigned stages[];  // [2][27][kTile] words
+    const int T = g.segCount;
+    const int G = gridDim.x;
+    const int t = threadIdx.x;
     int tile = blockIdx.x;
+    int4 dCur = make_int4(0, 0, 0, 0), dNext = dCur;
+    int lCur = 0, lNext = 0;
+    if (tile < T) {
+        dCur = __ldg(g.seg + tile);
+        lCur = __ldg(g.segLen + tile);
+    }
+    if (tile + G < T) {
+        dNext = __ldg(g.seg + tile + G);
+        lNext = __ldg(g.segLen + tile + G);
+    }
     int nbCur[8];
-    bool cur = tile < tiles && issueTile<F>(g, tile, stage[0], nbCur);
+    segNbr(g, dCur, t, nbCur);
+    if (t < lCur) issueGathers<F, S>(g, nbCur, stages);
     cpAsyncCommit();
     int b = 0;
-    for (; tile < tiles; tile += gridDim.x) {
-        const int next = tile + gridDim.x;
+    for (; tile < T; tile += G) {
+        // descriptor two tiles ahead: consumed by the next iteration's issue
+        int4 dAfter = make_int4(0, 0, 0, 0);
+        int lAfter = 0;
+        if (tile + 2 * G < T) {
+            dAfter = __ldg(g.seg + tile + 2 * G);
+            lAfter = __ldg(g.segLen + tile + 2 * G);
+        }
         int nbNext[8];
-        const bool nxt = next < tiles && issueTile<F>(g, next, stage[b ^ 1], nbNext);
+        segNbr(g, dNext, t, nbNext);
+        if (t < lNext) issueGathers<F, S>(g, nbNext, stages + (b ^ 1) * 27 * kTile);
         cpAsyncCommit();
-        cpAsyncWaitPrev();  // this thread's copies of the current tile have landed
-        if (cur) {
+        cpAsyncWaitPrev();  // this thread's copies for the current tile have landed
+        if (t < lCur) {
             float f[27];
 #pragma unroll
-            for (int d = 0; d < 27; ++d) f[d] = stage[b][d * kPipeBlock + threadIdx.x];
+            for (int d = 0; d < 27; ++d)
+                f[d] = fromWord<S>(stages[(b * 27 + d) * kTile + t], preAddr<F, S>(g, nbCur, d));
             collideCumulant(f, g.coll, g.coll.lambda, 0.f, 0.f, 0.f);
-            writePost<F, float>(g, nbCur, f);
+            writePost<F, S>(g, nbCur, f);
         }
 #pragma unroll
         for (int q = 0; q < 8; ++q) nbCur[q] = nbNext[q];
-        cur = nxt;
+        lCur = lNext;
+        dNext = dAfter;
+        lNext = lAfter;
         b ^= 1;
     }
+}
+
+// Cells outside the bulk segments (wall-adjacent), one thread per listed cell.
+template <bool F, class S>
+__global__ void __launch_bounds__(kBlock) collideList(DevLevel g) {
+    const int idx = blockIdx.x * kBlock + threadIdx.x;
+    if (idx >= g.specialCount) return;
+    const int cell = __ldg(g.special + idx);
+    int nb[8];
+    decodeNbr(g, cell, nb, nullptr);
+    float f[27];
+    readPre<F, S>(g, nb, f);
+    collideCumulant(f, g.coll, g.coll.lambda, 0.f, 0.f, 0.f);
+    writePost<F, S>(g, nb, f);
 }
 
 // F is the flipper after streaming, i.e. the state the ghosts are read in.
@@ -248,22 +322,23 @@ void dispatch(const DevLevel& g, bool flip, A&&... args) {
     }
 }
 
-int pipelineGrid() {
+constexpr int kStageBytes = 2 * 27 * kTile * 4;
+
+template <class S> int bulkGrid() {
     static int grid = 0;
     if (grid == 0) {
         int dev = 0, sms = 0, perSm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const int smem = 2 * 27 * kPipeBlock * sizeof(float);
-        cudaFuncSetAttribute(collideStreamPipelined<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(collideStreamPipelined<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, collideStreamPipelined<false>, kPipeBlock, smem);
+        cudaFuncSetAttribute(collideBulk<false, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
+        cudaFuncSetAttribute(collideBulk<true, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, collideBulk<false, S>, kTile, kStageBytes);
         grid = sms * (perSm > 0 ? perSm : 1);
     }
     return grid;
 }
 
-bool usePipelined() {
+bool useBulk() {
     static int v = -1;
     if (v < 0) {
         const char* e = std::getenv("LBM3_COLLIDE_KERNEL");
@@ -274,15 +349,18 @@ bool usePipelined() {
 
 template <bool F, class S> struct RunCollide {
     static void run(const DevLevel& g, cudaStream_t s) {
-        if (std::is_same<S, float>::value && usePipelined()) {
-            const int tiles = (g.cellCount + kPipeBlock - 1) / kPipeBlock;
-            const int grid = std::min(pipelineGrid(), tiles);
-            collideStreamPipelined<F><<<grid, kPipeBlock, 2 * 27 * kPipeBlock * sizeof(float), s>>>(g, tiles);
+        if (useBulk()) {
+            if (g.segCount > 0) {
+                const int grid = std::min(bulkGrid<S>(), g.segCount);
+                collideBulk<F, S><<<grid, kTile, kStageBytes, s>>>(g);
+            }
+            if (g.specialCount > 0) collideList<F, S><<<blocksFor(g.specialCount), kBlock, 0, s>>>(g);
         } else {
             collideStream<F, S><<<blocksFor(g.cellCount), kBlock, 0, s>>>(g);
         }
     }
 };
+
 template <bool F, class S> struct RunPeriodic {
     static void run(const DevLevel& g, cudaStream_t s) {
         if (g.perCount > 0) periodicCopy<F, S><<<blocksFor(g.perCount), kBlock, 0, s>>>(g);

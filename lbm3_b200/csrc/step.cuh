@@ -29,6 +29,13 @@ struct DevLevel {
     const int* perIndex;     // [perCount]
     const int* perSource;
     int perCount;
+    // bulk segments: {first cell, its jPlus, kPlus, jkPlus} and length
+    const int4* seg;
+    const int* segLen;
+    int segCount;
+    // cells collided outside the bulk segments (wall-adjacent)
+    const int* special;
+    int specialCount;
     int nx, ny, nz;
     float res, ox, oy, oz;
     CollisionConsts coll;
