@@ -34,6 +34,8 @@ extern "C" {
                                    include/gridBuilderFunctions.h:1479,:1563) */
 #define LBM_ERR_UNSUPPORTED -5  /* feature not available in this build          */
 #define LBM_ERR_NO_DEVICE   -6  /* no CUDA device visible                       */
+#define LBM_ERR_DEVICE_WAIT -7  /* a bounded wait inside a kernel gave up; the
+                                   step that reported it is not trustworthy */
 
 /* ---- boundary kinds for a domain face (replaces the getOpenBC hook) ------ */
 #define LBM_BC_PERIODIC   0   /* BCStruct.periodic     (include/types.h:131-136) */

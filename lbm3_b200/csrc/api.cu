@@ -3,6 +3,7 @@
 // failure into a status code plus a thread-local message.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <cstring>
 #include <exception>
 #include <functional>
@@ -50,6 +51,19 @@ template <class T> T* upload(const std::vector<T>& v, cudaStream_t s) {
 
 size_t storageBytes(int storage) { return storage == LBM_STORE_F32 ? 4 : 2; }
 
+// Distance between consecutive population planes, in elements.  Planes start
+// on 128-byte boundaries and are an odd number of 128-byte granules apart, so
+// the 27 read and 27 write streams of a step do not all map onto the same
+// DRAM channels when the cell count is a power of two.  LBM3_PLANE_PAD_LINES
+// adds further 128-byte granules (tuning).
+long long planeStride(long long n, int storage) {
+    const long long perLine = 128 / static_cast<long long>(storageBytes(storage));
+    long long lines = (n + perLine - 1) / perLine;
+    if (lines % 2 == 0) ++lines;
+    if (const char* e = std::getenv("LBM3_PLANE_PAD_LINES")) lines += std::atoll(e);
+    return lines * perLine;
+}
+
 }  // namespace
 
 struct LevelState {
@@ -69,6 +83,7 @@ struct lbm_grids {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double* scratch = nullptr;
+    int* errorFlag = nullptr;  // device word the kernels set when a bounded wait gives up
     float lastKernelMs = 0.f;
     int lastLaunches = 0;
     // event pairs bracketing collide-stream launches while lbm_time_steps runs
@@ -81,6 +96,7 @@ struct lbm_grids {
         for (auto& L : levels)
             for (void* p : L.owned) cudaFree(p);
         if (scratch) cudaFree(scratch);
+        if (errorFlag) cudaFree(errorFlag);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
     }
@@ -96,7 +112,7 @@ namespace {
 // tables, as the reference accounts them (gridBuilderFunctions.h:1630-1649).
 unsigned long long levelBytes(const lbm::HostLevel& H, int storage) {
     const unsigned long long n = static_cast<unsigned long long>(H.info.cellCount);
-    unsigned long long b = 27ULL * n * storageBytes(storage);
+    unsigned long long b = 27ULL * planeStride(static_cast<long long>(n), storage) * storageBytes(storage);
     b += 2ULL * n * 4;                       // shifter, wallMap
     b += 6ULL * H.rowI.size() * 4;           // compressed rows
     b += 2ULL * H.perIndex.size() * 4;       // periodic index/source
@@ -156,6 +172,22 @@ void updateAllGrids(lbm_grids* g, int level) {
     // single-level build: no finer level to recurse into (updateGrid.h:391-395)
 }
 
+struct DeviceWaitError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+// After the stream is idle: report (and clear) a bounded device wait that gave up.
+void checkDeviceFlag(lbm_grids* g) {
+    int flag = 0;
+    ck(cudaMemcpyAsync(&flag, g->errorFlag, sizeof(int), cudaMemcpyDeviceToHost, g->stream), "flag copy");
+    ck(cudaStreamSynchronize(g->stream), "flag sync");
+    if (flag) {
+        ck(cudaMemsetAsync(g->errorFlag, 0, sizeof(int), g->stream), "flag reset");
+        ck(cudaStreamSynchronize(g->stream), "flag sync");
+        throw DeviceWaitError("a bounded device wait in the collide-stream kernel gave up");
+    }
+}
+
 int guarded(const char* where, const std::function<void()>& body) {
     try {
         body();
@@ -163,6 +195,8 @@ int guarded(const char* where, const std::function<void()>& body) {
         return LBM_OK;
     } catch (const CudaError& e) {
         return fail(LBM_ERR_CUDA, std::string(where) + ": " + e.what());
+    } catch (const DeviceWaitError& e) {
+        return fail(LBM_ERR_DEVICE_WAIT, std::string(where) + ": " + e.what());
     } catch (const std::bad_alloc&) {
         return fail(LBM_ERR_OOM, std::string(where) + ": device or host allocation failed");
     } catch (const std::invalid_argument& e) {
@@ -261,7 +295,9 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
         ck(cudaEventCreate(&g->ev0), "cudaEventCreate");
         ck(cudaEventCreate(&g->ev1), "cudaEventCreate");
         g->scratch = devAlloc<double>(8);
+        g->errorFlag = devAlloc<int>(1);
         cudaStream_t s = g->stream;
+        ck(cudaMemsetAsync(g->errorFlag, 0, sizeof(int), s), "memset");
         g->levels.resize(host.levels.size());
         for (size_t l = 0; l < host.levels.size(); ++l) {
             const lbm::HostLevel& H = host.levels[l];
@@ -279,12 +315,14 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
             const long long n = H.info.cellCount;
             lbm::DevLevel& d = L.dev;
             d.cellCount = H.info.cellCount;
-            d.stride = n;
+            d.stride = planeStride(n, c->storage);
             d.storage = c->storage;
             d.nx = H.info.nx; d.ny = H.info.ny; d.nz = H.info.nz;
             d.res = H.info.res; d.ox = H.info.ox; d.oy = H.info.oy; d.oz = H.info.oz;
             auto own = [&](auto* p) { if (p) L.owned.push_back(p); return p; };
-            d.f = own(devAlloc<unsigned char>(27ULL * n * storageBytes(c->storage)));
+            // 256 bytes of tail so bulk copies rounded up to 16 bytes stay inside
+            d.f = own(devAlloc<unsigned char>(27ULL * d.stride * storageBytes(c->storage) + 256));
+            d.errorFlag = g->errorFlag;
             d.shifter = own(upload(H.shifter, s));
             d.rowI = own(upload(H.rowI, s));
             d.rowJ = own(upload(H.rowJ, s));
@@ -365,7 +403,10 @@ int lbm_update_all_grids(lbm_grids* g, int steps) {
 
 int lbm_synchronize(lbm_grids* g) {
     if (!g) return fail(LBM_ERR_INVALID, "lbm_synchronize: null grids");
-    return guarded("lbm_synchronize", [&] { ck(cudaStreamSynchronize(g->stream), "sync"); });
+    return guarded("lbm_synchronize", [&] {
+        ck(cudaStreamSynchronize(g->stream), "sync");
+        checkDeviceFlag(g);
+    });
 }
 
 int lbm_time_steps(lbm_grids* g, int steps, float* ms) {
@@ -391,6 +432,7 @@ int lbm_time_steps(lbm_grids* g, int steps, float* ms) {
         }
         g->timingKernels = false;
         ck(cudaEventSynchronize(g->ev1), "event sync");
+        checkDeviceFlag(g);
         ck(cudaEventElapsedTime(ms, g->ev0, g->ev1), "elapsed");
         float kernel = 0.f;
         for (int k = 0; k + 1 < g->kernelEventsUsed; k += 2) {

@@ -356,17 +356,29 @@ void buildSegments(HostLevel& L) {
         int end = c + 1;
         while (end < n && L.shifter[end] < 0) ++end;
         const int row = L.shifter[c];
+        // neighbours of the cell at offset `off` in this row
+        auto jP = [&](int off) { return L.rowJP[row] + off; };
+        auto kP = [&](int off) { return L.rowKP[row] + off; };
+        auto jkP = [&](int off) { return L.rowJKP[row] + off; };
+        // a +1 neighbour that wraps to cell 0 (finishNBRPlus) breaks the
+        // linear run, so such a cell is collided from the special list
+        auto wraps = [&](int q) {
+            const int off = q - c;
+            return q + 1 >= n || jP(off) + 1 >= n || kP(off) + 1 >= n || jkP(off) + 1 >= n;
+        };
+        auto bulk = [&](int q) {
+            return (L.wallMap[q] == -1 || L.wallMap[q] == -2) && !wraps(q);
+        };
         for (int q = c; q < end;) {
-            const int wm = L.wallMap[q];
-            if (wm >= 0) { L.specialCells.push_back(q); ++q; continue; }
-            if (wm == -3) { ++q; continue; }
+            if (L.wallMap[q] == -3) { ++q; continue; }
+            if (!bulk(q)) { L.specialCells.push_back(q); ++q; continue; }
             int r = q;
-            while (r < end && r - q < kSegmentCells && (L.wallMap[r] == -1 || L.wallMap[r] == -2)) ++r;
+            while (r < end && r - q < kSegmentCells && bulk(r)) ++r;
             const int off = q - c;
             L.segCell.push_back(q);
-            L.segJP.push_back(L.rowJP[row] + off);
-            L.segKP.push_back(L.rowKP[row] + off);
-            L.segJKP.push_back(L.rowJKP[row] + off);
+            L.segJP.push_back(jP(off));
+            L.segKP.push_back(kP(off));
+            L.segJKP.push_back(jkP(off));
             L.segLen.push_back(r - q);
             q = r;
         }

@@ -62,7 +62,8 @@ struct HostLevel {
     // index is the run's base plus the lane offset, so the bulk kernel needs
     // one descriptor per tile and no per-cell metadata.
     std::vector<int> segCell, segJP, segKP, segJKP, segLen;
-    // cells outside the bulk segments that still collide (wall-adjacent)
+    // cells outside the bulk segments that still collide (wall-adjacent, or
+    // whose +1 neighbour wraps around the end of the cell list)
     std::vector<int> specialCells;
 };
 

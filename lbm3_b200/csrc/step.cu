@@ -45,121 +45,256 @@ __global__ void __launch_bounds__(kBlock) collideStream(DevLevel g) {
 }
 
 // ---- bulk collide-stream ---------------------------------------------------
-// Persistent CTAs walk the bulk segments (runs of up to kSegmentCells plain
-// fluid cells inside one compressed row; one segment per CTA iteration, one
-// cell per thread).  Inside a segment the 8 esotwist neighbours of lane t are
-// the segment's base indices + t, so no per-cell metadata is loaded: a CTA
-// reads one 20-byte descriptor per tile, two tiles ahead.  The 27 gathers of
-// the next tile are issued as cp.async copies into shared memory before the
-// current tile is collided, so HBM traffic overlaps the cumulant arithmetic.
-// A thread reads back only the stage slots its own copies filled, hence no
-// block barrier; esotwist gives every global slot a single owning cell, so
-// prefetching the next tile never reads a value the current tile writes.
-// 16-bit storage stages the aligned 32-bit word that holds the element.
+// Persistent CTAs walk the bulk segments: runs of up to kSegmentCells plain
+// fluid cells inside one compressed row, one segment per CTA iteration, one
+// cell per thread.  Inside a segment the 8 esotwist neighbours of lane t are
+// the segment's base indices + t, so a CTA reads one 20-byte descriptor per
+// tile and no per-cell metadata.  For every direction q the tile's 27
+// pre-collision values form one contiguous run of a population plane.
+//
+// collideBulkTma: one elected thread copies those 27 runs with
+// cp.async.bulk (the TMA engine, global -> shared, completion counted on an
+// mbarrier) into a ring of kStages tiles, kStages-1 tiles ahead of the tile
+// being collided.  The copies bypass L1 and hold no registers, so many tiles
+// stay in flight per SM while the cumulant arithmetic runs.  Runs are copied
+// from the 16-byte boundary below their first element; the lane offset of a
+// run inside its stage slot is that misalignment.
+// collidePrefetch: the same walk with the next tile's gathers held in
+// registers (no shared memory); kept as the fallback variant.
 constexpr int kTile = 128;  // == kSegmentCells
 static_assert(kTile == kSegmentCells, "tile and segment length differ");
 
-__device__ __forceinline__ void cpAsync4(void* smem, const void* gmem) {
-    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cpAsyncWaitPrev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+#ifndef LBM3_TMA_STAGES
+#define LBM3_TMA_STAGES 4
+#endif
+#ifndef LBM3_TMA_MIN_BLOCKS
+#define LBM3_TMA_MIN_BLOCKS 3
+#endif
+#ifndef LBM3_PREFETCH_MIN_BLOCKS
+#define LBM3_PREFETCH_MIN_BLOCKS 4
+#endif
+constexpr int kStages = LBM3_TMA_STAGES;
+// bytes of one run slot: kTile elements plus the 16-byte alignment slack
+template <class S> constexpr int runBytes() { return kTile * int(sizeof(S)) + 16; }
+template <class S> constexpr int stageBytes() { return 27 * runBytes<S>(); }
+template <class S> constexpr int tmaSmemBytes() { return kStages * stageBytes<S>() + kStages * 8; }
+// bound on mbarrier polls before a wait is declared lost (~0.1 s)
+constexpr int kWaitPolls = 1 << 22;
 
 __device__ __forceinline__ void segNbr(const DevLevel& g, const int4& d, int t, int (&nb)[8]) {
-    const int n = g.cellCount;
+    // segments never contain a lane whose +1 neighbour wraps (the builder
+    // sends those cells to the special list), so +1 is plain addition
     nb[0] = d.x + t;
+    nb[1] = d.x + t + 1;
     nb[2] = d.y + t;
+    nb[3] = d.y + t + 1;
     nb[4] = d.z + t;
+    nb[5] = d.z + t + 1;
     nb[6] = d.w + t;
-    nb[1] = nb[0] + 1 < n ? nb[0] + 1 : 0;
-    nb[3] = nb[2] + 1 < n ? nb[2] + 1 : 0;
-    nb[5] = nb[4] + 1 < n ? nb[4] + 1 : 0;
-    nb[7] = nb[6] + 1 < n ? nb[6] + 1 : 0;
+    nb[7] = d.w + t + 1;
 }
 
-template <class S> __device__ __forceinline__ float fromWord(unsigned w, const S* p);
-template <> __device__ __forceinline__ float fromWord<float>(unsigned w, const float*) {
-    return __uint_as_float(w);
-}
-template <> __device__ __forceinline__ float fromWord<__half>(unsigned w, const __half* p) {
-    const unsigned short h = (reinterpret_cast<uintptr_t>(p) & 2) ? (w >> 16) : (w & 0xffffu);
-    return __half2float(__ushort_as_half(h));
-}
-template <> __device__ __forceinline__ float fromWord<__nv_bfloat16>(unsigned w, const __nv_bfloat16* p) {
-    const unsigned short h = (reinterpret_cast<uintptr_t>(p) & 2) ? (w >> 16) : (w & 0xffffu);
-    return __bfloat162float(__ushort_as_bfloat16(h));
-}
-
-template <bool F, class S>
-__device__ __forceinline__ const S* preAddr(const DevLevel& g, const int (&nb)[8], int d) {
-    return static_cast<const S*>(g.f) + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)];
-}
-
-template <bool F, class S>
-__device__ __forceinline__ void issueGathers(const DevLevel& g, const int (&nb)[8], unsigned* stage) {
-#pragma unroll
-    for (int d = 0; d < 27; ++d) {
-        const S* p = preAddr<F, S>(g, nb, d);
-        const void* w = reinterpret_cast<const void*>(reinterpret_cast<uintptr_t>(p) & ~uintptr_t(3));
-        cpAsync4(stage + d * kTile + threadIdx.x, w);
+__device__ __forceinline__ void loadDesc(const DevLevel& g, int tile, int4& d, int& l) {
+    if (tile < g.segCount) {
+        d = __ldg(g.seg + tile);
+        l = __ldg(g.segLen + tile);
+    } else {
+        d = make_int4(0, 0, 0, 0);
+        l = 0;
     }
 }
 
-// resident CTAs per SM the register allocation is sized for
-#ifndef LBM3_BULK_MIN_BLOCKS
-#define LBM3_BULK_MIN_BLOCKS 6
-#endif
+__device__ __forceinline__ unsigned smemAddr(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbarInit(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smemAddr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbarArriveExpectTx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;\n" ::"r"(smemAddr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbarTestWait(uint64_t* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smemAddr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase with the given parity to complete.
+__device__ __forceinline__ bool mbarWait(uint64_t* bar, unsigned parity) {
+    for (int i = 0; i < kWaitPolls; ++i) {
+        if (mbarTestWait(bar, parity)) return true;
+        if (i > 64) __nanosleep(20);
+    }
+    return false;
+}
+
+__device__ __forceinline__ void bulkLoad(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+            smemAddr(dst)),
+        "l"(src), "r"(bytes), "r"(smemAddr(bar))
+        : "memory");
+}
+
+// Plane base index of direction q's run for a tile starting at descriptor d.
+template <bool F>
+__device__ __forceinline__ long long runStart(const DevLevel& g, const int4& d, int q) {
+    const int k = preNbr(q);
+    const int b = (k >> 1) == 0 ? d.x : (k >> 1) == 1 ? d.y : (k >> 1) == 2 ? d.z : d.w;
+    return (long long)preSlot<F>(q) * g.stride + b + (k & 1);
+}
+
+// Elected thread: start the 27 run copies of a tile into `stage`.
+template <bool F, class S>
+__device__ __forceinline__ void produceTile(const DevLevel& g, const int4& d, int len, unsigned char* stage,
+                                            uint64_t* bar) {
+    const char* base = static_cast<const char*>(g.f);
+    unsigned total = 0;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const uintptr_t a = reinterpret_cast<uintptr_t>(base + runStart<F>(g, d, q) * (long long)sizeof(S));
+        const uintptr_t a0 = a & ~uintptr_t(15);
+        const uintptr_t a1 = (a + uintptr_t(len) * sizeof(S) + 15) & ~uintptr_t(15);
+        total += static_cast<unsigned>(a1 - a0);
+    }
+    mbarArriveExpectTx(bar, total);
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const uintptr_t a = reinterpret_cast<uintptr_t>(base + runStart<F>(g, d, q) * (long long)sizeof(S));
+        const uintptr_t a0 = a & ~uintptr_t(15);
+        const uintptr_t a1 = (a + uintptr_t(len) * sizeof(S) + 15) & ~uintptr_t(15);
+        bulkLoad(stage + q * runBytes<S>(), reinterpret_cast<const void*>(a0), static_cast<unsigned>(a1 - a0),
+                 bar);
+    }
+}
 
 template <bool F, class S>
-__global__ void __launch_bounds__(kTile, LBM3_BULK_MIN_BLOCKS) collideBulk(DevLevel g) {
-    extern __shared__ unsigned stages[];  // [2][27][kTile] words
+__global__ void __launch_bounds__(kTile, LBM3_TMA_MIN_BLOCKS) collideBulkTma(DevLevel g) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kStages * stageBytes<S>());
+    const int T = g.segCount;
+    const int G = gridDim.x;
+    const int t = threadIdx.x;
+    if (t == 0) {
+#pragma unroll
+        for (int k = 0; k < kStages; ++k) mbarInit(&bar[k], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+
+    int4 d[kStages];
+    int l[kStages];
+    unsigned parity = 0;   // bit k: parity of the next phase of stage k
+    unsigned pending = 0;  // bit k: copies issued into stage k not yet consumed
+#pragma unroll
+    for (int k = 0; k < kStages - 1; ++k) {
+        loadDesc(g, blockIdx.x + k * G, d[k], l[k]);
+        if (t == 0 && l[k] > 0) produceTile<F, S>(g, d[k], l[k], smem + k * stageBytes<S>(), &bar[k]);
+        if (l[k] > 0) pending |= 1u << k;
+    }
+    int4 dNext;
+    int lNext;
+    loadDesc(g, blockIdx.x + (kStages - 1) * G, dNext, lNext);
+    bool lost = false;
+    for (int base = blockIdx.x; base < T; base += kStages * G) {
+        bool stop = false;
+#pragma unroll
+        for (int k = 0; k < kStages; ++k) {
+            const int tile = base + k * G;
+            // every thread is done with the stage consumed last iteration, and
+            // a lost wait anywhere in the CTA stops all of it
+            if (__syncthreads_or(lost) || tile >= T) {
+                stop = true;
+                break;
+            }
+            const int ks = (k + kStages - 1) % kStages;
+            d[ks] = dNext;
+            l[ks] = lNext;
+            if (l[ks] > 0) {
+                if (t == 0) produceTile<F, S>(g, d[ks], l[ks], smem + ks * stageBytes<S>(), &bar[ks]);
+                pending |= 1u << ks;
+            }
+            loadDesc(g, tile + kStages * G, dNext, lNext);
+            if (l[k] > 0) {
+                if (!mbarWait(&bar[k], (parity >> k) & 1u)) {
+                    lost = true;
+                    continue;
+                }
+                parity ^= 1u << k;
+                pending &= ~(1u << k);
+            }
+            if (t < l[k]) {
+                int nb[8];
+                segNbr(g, d[k], t, nb);
+                const unsigned char* st = smem + k * stageBytes<S>();
+                float f[27];
+#pragma unroll
+                for (int q = 0; q < 27; ++q) {
+                    const int off = static_cast<int>((runStart<F>(g, d[k], q) * (long long)sizeof(S)) & 15) /
+                                    int(sizeof(S));
+                    f[q] = Store<S>::ld(reinterpret_cast<const S*>(st + q * runBytes<S>()) + off + t);
+                }
+                collideCumulant(f, g.coll, g.coll.lambda, 0.f, 0.f, 0.f);
+                writePost<F, S>(g, nb, f);
+            }
+        }
+        if (stop) break;
+    }
+    if (lost) {
+        if (t == 0) {
+            atomicExch(g.errorFlag, 1);
+            // let copies still in flight land before the CTA's shared memory goes away
+#pragma unroll
+            for (int k = 0; k < kStages; ++k)
+                if ((pending >> k) & 1u) mbarWait(&bar[k], (parity >> k) & 1u);
+        }
+        __syncthreads();
+    }
+}
+
+template <bool F, class S>
+__global__ void __launch_bounds__(kTile, LBM3_PREFETCH_MIN_BLOCKS) collidePrefetch(DevLevel g) {
     const int T = g.segCount;
     const int G = gridDim.x;
     const int t = threadIdx.x;
     int tile = blockIdx.x;
-    int4 dCur = make_int4(0, 0, 0, 0), dNext = dCur;
-    int lCur = 0, lNext = 0;
-    if (tile < T) {
-        dCur = __ldg(g.seg + tile);
-        lCur = __ldg(g.segLen + tile);
-    }
-    if (tile + G < T) {
-        dNext = __ldg(g.seg + tile + G);
-        lNext = __ldg(g.segLen + tile + G);
-    }
-    int nbCur[8];
-    segNbr(g, dCur, t, nbCur);
-    if (t < lCur) issueGathers<F, S>(g, nbCur, stages);
-    cpAsyncCommit();
-    int b = 0;
+    int4 dCur, dNext;
+    int lCur, lNext;
+    loadDesc(g, tile, dCur, lCur);
+    loadDesc(g, tile + G, dNext, lNext);
+    int nb[8];
+    segNbr(g, dCur, t, nb);
+    float fn[27];
+    if (t < lCur) readPre<F, S>(g, nb, fn);
     for (; tile < T; tile += G) {
-        // descriptor two tiles ahead: consumed by the next iteration's issue
-        int4 dAfter = make_int4(0, 0, 0, 0);
-        int lAfter = 0;
-        if (tile + 2 * G < T) {
-            dAfter = __ldg(g.seg + tile + 2 * G);
-            lAfter = __ldg(g.segLen + tile + 2 * G);
-        }
-        int nbNext[8];
-        segNbr(g, dNext, t, nbNext);
-        if (t < lNext) issueGathers<F, S>(g, nbNext, stages + (b ^ 1) * 27 * kTile);
-        cpAsyncCommit();
-        cpAsyncWaitPrev();  // this thread's copies for the current tile have landed
+        int4 dAfter;
+        int lAfter;
+        loadDesc(g, tile + 2 * G, dAfter, lAfter);
+        float f[27];
+#pragma unroll
+        for (int q = 0; q < 27; ++q) f[q] = fn[q];
+        int nbn[8];
+        segNbr(g, dNext, t, nbn);
+        if (t < lNext) readPre<F, S>(g, nbn, fn);
         if (t < lCur) {
-            float f[27];
-#pragma unroll
-            for (int d = 0; d < 27; ++d)
-                f[d] = fromWord<S>(stages[(b * 27 + d) * kTile + t], preAddr<F, S>(g, nbCur, d));
             collideCumulant(f, g.coll, g.coll.lambda, 0.f, 0.f, 0.f);
-            writePost<F, S>(g, nbCur, f);
+            writePost<F, S>(g, nb, f);
         }
 #pragma unroll
-        for (int q = 0; q < 8; ++q) nbCur[q] = nbNext[q];
+        for (int q = 0; q < 8; ++q) nb[q] = nbn[q];
         lCur = lNext;
         dNext = dAfter;
         lNext = lAfter;
-        b ^= 1;
     }
 }
 
@@ -278,19 +413,22 @@ __global__ void __launch_bounds__(kBlock) macroFields(DevLevel g, float* out) {
 
 template <bool F, class S>
 __global__ void __launch_bounds__(kBlock) gatherF(DevLevel g, float* out) {
-    // raw slot copy: out[slot][cell] = f[slot][cell] as FP32
+    // raw slot copy: out[slot][cell] = f[slot][cell] as FP32 (planes are
+    // stride apart on the device, cellCount apart in the output)
     const long long i = (long long)blockIdx.x * kBlock + threadIdx.x;
-    const long long total = 27LL * g.stride;
-    if (i >= total) return;
-    out[i] = Store<S>::ld(static_cast<const S*>(g.f) + i);
+    const long long n = g.cellCount;
+    if (i >= 27 * n) return;
+    const long long slot = i / n, cell = i - slot * n;
+    out[i] = Store<S>::ld(static_cast<const S*>(g.f) + slot * g.stride + cell);
 }
 
 template <class S>
 __global__ void __launch_bounds__(kBlock) scatterF(DevLevel g, const float* in) {
     const long long i = (long long)blockIdx.x * kBlock + threadIdx.x;
-    const long long total = 27LL * g.stride;
-    if (i >= total) return;
-    Store<S>::st(static_cast<S*>(g.f) + i, in[i]);
+    const long long n = g.cellCount;
+    if (i >= 27 * n) return;
+    const long long slot = i / n, cell = i - slot * n;
+    Store<S>::st(static_cast<S*>(g.f) + slot * g.stride + cell, in[i]);
 }
 
 __global__ void __launch_bounds__(kBlock) collideBatch(float* f, int n, CollisionConsts P,
@@ -322,42 +460,50 @@ void dispatch(const DevLevel& g, bool flip, A&&... args) {
     }
 }
 
-constexpr int kStageBytes = 2 * 27 * kTile * 4;
-
-template <class S> int bulkGrid() {
-    static int grid = 0;
-    if (grid == 0) {
-        int dev = 0, sms = 0, perSm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaFuncSetAttribute(collideBulk<false, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
-        cudaFuncSetAttribute(collideBulk<true, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, collideBulk<false, S>, kTile, kStageBytes);
-        grid = sms * (perSm > 0 ? perSm : 1);
-    }
-    return grid;
+// Persistent grid size: SMs x resident CTAs of the kernel.
+template <class K> int persistentGrid(K kernel, int smem) {
+    int dev = 0, sms = 0, perSm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (smem > 0) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, kTile, smem);
+    return sms * (perSm > 0 ? perSm : 1);
 }
 
-bool useBulk() {
+enum class CollideVariant { Tma, Prefetch, Simple };
+
+CollideVariant collideVariant() {
     static int v = -1;
     if (v < 0) {
         const char* e = std::getenv("LBM3_COLLIDE_KERNEL");
-        v = (e && std::string(e) == "simple") ? 0 : 1;
+        const std::string s = e ? e : "";
+        v = s == "simple" ? 2 : s == "prefetch" ? 1 : 0;
     }
-    return v == 1;
+    return static_cast<CollideVariant>(v);
 }
 
 template <bool F, class S> struct RunCollide {
     static void run(const DevLevel& g, cudaStream_t s) {
-        if (useBulk()) {
-            if (g.segCount > 0) {
-                const int grid = std::min(bulkGrid<S>(), g.segCount);
-                collideBulk<F, S><<<grid, kTile, kStageBytes, s>>>(g);
-            }
-            if (g.specialCount > 0) collideList<F, S><<<blocksFor(g.specialCount), kBlock, 0, s>>>(g);
-        } else {
+        const CollideVariant v = collideVariant();
+        if (v == CollideVariant::Simple) {
             collideStream<F, S><<<blocksFor(g.cellCount), kBlock, 0, s>>>(g);
+            return;
         }
+        if (g.segCount > 0) {
+            if (v == CollideVariant::Tma) {
+                static int grid = 0;
+                if (grid == 0) {
+                    grid = persistentGrid(collideBulkTma<F, S>, tmaSmemBytes<S>());
+                    persistentGrid(collideBulkTma<!F, S>, tmaSmemBytes<S>());
+                }
+                collideBulkTma<F, S><<<std::min(grid, g.segCount), kTile, tmaSmemBytes<S>(), s>>>(g);
+            } else {
+                static int grid = 0;
+                if (grid == 0) grid = persistentGrid(collidePrefetch<F, S>, 0);
+                collidePrefetch<F, S><<<std::min(grid, g.segCount), kTile, 0, s>>>(g);
+            }
+        }
+        if (g.specialCount > 0) collideList<F, S><<<blocksFor(g.specialCount), kBlock, 0, s>>>(g);
     }
 };
 
@@ -383,12 +529,12 @@ template <bool F, class S> struct RunMacro {
 };
 template <bool F, class S> struct RunGather {
     static void run(const DevLevel& g, cudaStream_t s, float* out) {
-        gatherF<F, S><<<blocksFor(27LL * g.stride), kBlock, 0, s>>>(g, out);
+        gatherF<F, S><<<blocksFor(27LL * g.cellCount), kBlock, 0, s>>>(g, out);
     }
 };
 template <bool F, class S> struct RunScatter {
     static void run(const DevLevel& g, cudaStream_t s, const float* in) {
-        scatterF<S><<<blocksFor(27LL * g.stride), kBlock, 0, s>>>(g, in);
+        scatterF<S><<<blocksFor(27LL * g.cellCount), kBlock, 0, s>>>(g, in);
     }
 };
 

@@ -36,6 +36,7 @@ struct DevLevel {
     // cells collided outside the bulk segments (wall-adjacent)
     const int* special;
     int specialCount;
+    int* errorFlag;          // set to nonzero when a bounded device wait gives up
     int nx, ny, nz;
     float res, ox, oy, oz;
     CollisionConsts coll;
