@@ -52,15 +52,17 @@ __global__ void __launch_bounds__(kBlock) collideStream(DevLevel g) {
 // tile and no per-cell metadata.  For every direction q the tile's 27
 // pre-collision values form one contiguous run of a population plane.
 //
-// collideBulkTma: one elected thread copies those 27 runs with
+// collidePrefetch (default): the next tile's 27 gathers are issued into
+// registers before the current tile is collided.
+// collideBulkTma (LBM3_COLLIDE_KERNEL=tma): one elected thread copies those 27 runs with
 // cp.async.bulk (the TMA engine, global -> shared, completion counted on an
 // mbarrier) into a ring of kStages tiles, kStages-1 tiles ahead of the tile
 // being collided.  The copies bypass L1 and hold no registers, so many tiles
 // stay in flight per SM while the cumulant arithmetic runs.  Runs are copied
 // from the 16-byte boundary below their first element; the lane offset of a
 // run inside its stage slot is that misalignment.
-// collidePrefetch: the same walk with the next tile's gathers held in
-// registers (no shared memory); kept as the fallback variant.
+// On B200 the small (about 0.5 KB) bulk copies of 128-cell tiles make the TMA
+// variant slower than register prefetch, which is therefore the default.
 constexpr int kTile = 128;  // == kSegmentCells
 static_assert(kTile == kSegmentCells, "tile and segment length differ");
 
@@ -477,7 +479,7 @@ CollideVariant collideVariant() {
     if (v < 0) {
         const char* e = std::getenv("LBM3_COLLIDE_KERNEL");
         const std::string s = e ? e : "";
-        v = s == "simple" ? 2 : s == "prefetch" ? 1 : 0;
+        v = s == "simple" ? 2 : s == "tma" ? 0 : 1;
     }
     return static_cast<CollideVariant>(v);
 }
