@@ -73,6 +73,13 @@ extern "C" {
 #define LBM_ARRAY_PERIODIC_SOURCE 10 /* int32 [periodicCount] PeriodicBC.sourceArray */
 #define LBM_ARRAY_MACRO        11 /* float  [4][cellCount]  dRho, ux, uy, uz of the
                                      current pre-collision state (getDRhoUxUyUz)  */
+#define LBM_ARRAY_WALL_INDEX   12 /* int32  [wallAdjacentCount] Wall.indexArray    */
+#define LBM_ARRAY_WALL_DATA    13 /* uint32 [wallAdjacentCount] Wall.wallDataArray */
+#define LBM_ARRAY_LINK_LENGTH  14 /* uint32 [7][wallAdjacentCount] Wall.linkLengthArray */
+#define LBM_ARRAY_WALL_FORCE   15 /* float  [3][wallAdjacentCount] Wall.gx/gy/gzArray
+                                     accumulated since the last tracker reset   */
+#define LBM_ARRAY_WALL_VELOCITY 16 /* float [3][wallAdjacentCount] wall velocity the
+                                     body motion gives each wall-adjacent cell   */
 
 /* ---- case description -------------------------------------------------- */
 
@@ -89,6 +96,24 @@ typedef struct lbm_face_bc {
     float non_reflective_beta;  /* BCStruct.nonReflectiveBeta (default 7)     */
     float dRho, ux, uy, uz;     /* target values                              */
 } lbm_face_bc;
+
+/* wall motion of a static body (replaces the per-wallID branch of getLocalBC,
+ * e.g. cases/torqueTest/torqueTestMain.cu:100-122) */
+#define LBM_WALL_STATIC   0   /* u_wall = 0                                   */
+#define LBM_WALL_ROTATING 1   /* rigid rotation about an axis parallel to x/y/z */
+
+#define LBM_MAX_BODIES 16     /* wallID is packed into 5 bits of wallData      */
+
+/* One static body: a triangle soup in mm (the reference's gridStaticSTLs
+ * entry; its index is the body's wallID). */
+typedef struct lbm_body {
+    const float* triangles;     /* [triangle_count][9]: ax ay az bx by bz cx cy cz */
+    int   triangle_count;
+    int   motion;               /* LBM_WALL_*                                  */
+    int   axis;                 /* 0, 1, 2: rotation axis parallel to x, y, z  */
+    float origin[3];            /* a point on the rotation axis, mm            */
+    float radians_per_second;   /* signed angular speed                        */
+} lbm_body;
 
 typedef struct lbm_case {
     /* compile-time constants of a reference driver */
@@ -114,6 +139,12 @@ typedef struct lbm_case {
     /* getLocalBC (uniform over the domain) */
     float collision_limiter;    /* BCStruct.collisionLimiter; <= 0 selects AllOne */
     float nu_multiplier;        /* BCStruct.nuMultiplier                       */
+    float gx, gy, gz;           /* BCStruct.gx/gy/gz body force, lattice units */
+    int   use_ibb;              /* BCStruct.useIBB: 1 interpolated, 0 gamma=1/2 */
+
+    /* gridStaticSTLs */
+    int      body_count;
+    lbm_body body[LBM_MAX_BODIES];
 
     /* storage */
     int   storage;              /* LBM_STORE_*                                 */
@@ -207,6 +238,13 @@ int lbm_write_f(lbm_grids* g, int level, const float* host, size_t bytes);
  * and `domain_length` the physical periodic length (mm). */
 int lbm_kinetic_energy(lbm_grids* g, float u_ref_phys, float domain_length,
                        double* out);
+
+/* Momentum-exchange force and torque on one body (wallID), accumulated in
+ * FP64 on the device over the wall-adjacent cells and averaged over the
+ * steps since the last reset: out = {Fx, Fy, Fz [N], Tx, Ty, Tz [N m]} about
+ * the coordinate origin.  `reset` != 0 zeroes the accumulators afterwards.
+ * Replaces the wall branch of updateTracker (include/trackerFunctions.h:366-497). */
+int lbm_wall_force(lbm_grids* g, int wall_id, int reset, double* out);
 
 /* Cell-wise collision on a device batch of shifted populations laid out as
  * float [27][n] (structure of arrays), in place.

@@ -62,6 +62,24 @@ class LbmFaceBC(C.Structure):
     ]
 
 
+LBM_WALL_STATIC = 0
+LBM_WALL_ROTATING = 1
+LBM_MAX_BODIES = 16
+ARRAY_WALL_INDEX = 12
+ARRAY_WALL_DATA = 13
+ARRAY_LINK_LENGTH = 14
+ARRAY_WALL_FORCE = 15
+ARRAY_WALL_VELOCITY = 16
+LBM_ERR_DEVICE_WAIT = -7
+
+
+class LbmBody(C.Structure):
+    _fields_ = [
+        ("triangles", C.POINTER(C.c_float)), ("triangle_count", C.c_int), ("motion", C.c_int),
+        ("axis", C.c_int), ("origin", C.c_float * 3), ("radians_per_second", C.c_float),
+    ]
+
+
 class LbmCase(C.Structure):
     _fields_ = [
         ("grid_level_count", C.c_int), ("wall_refinement_count", C.c_int),
@@ -73,6 +91,8 @@ class LbmCase(C.Structure):
         ("ic_uy", C.c_float), ("ic_uz", C.c_float),
         ("tgv_u0", C.c_float), ("tgv_length", C.c_float),
         ("collision_limiter", C.c_float), ("nu_multiplier", C.c_float),
+        ("gx", C.c_float), ("gy", C.c_float), ("gz", C.c_float), ("use_ibb", C.c_int),
+        ("body_count", C.c_int), ("body", LbmBody * LBM_MAX_BODIES),
         ("storage", C.c_int),
     ]
 
@@ -114,6 +134,7 @@ SIGNATURES = [
     ("lbm_read_array", C.c_int, [_P, C.c_int, C.c_int, _P, C.c_size_t]),
     ("lbm_write_f", C.c_int, [_P, C.c_int, _P, C.c_size_t]),
     ("lbm_kinetic_energy", C.c_int, [_P, C.c_float, C.c_float, C.POINTER(C.c_double)]),
+    ("lbm_wall_force", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     ("lbm_apply_collision_batch", C.c_int,
      [_P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, _P]),
 ]

@@ -30,6 +30,7 @@ def _blank_case() -> A.LbmCase:
     c.rho_phys = 1.0
     c.collision_limiter = 0.05   # BCStruct default (include/types.h:131-136)
     c.nu_multiplier = 1.0
+    c.use_ibb = 1                # BCStruct.useIBB default
     c.storage = A.LBM_STORE_F32
     for f in range(6):
         c.face[f] = _face(A.LBM_BC_PERIODIC)

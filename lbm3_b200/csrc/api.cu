@@ -68,6 +68,7 @@ long long planeStride(long long n, int storage) {
 
 struct LevelState {
     lbm::Info info;
+    int iterationsSinceTrackerReset = 0;
     int rowCount = 0;
     int wallCellCount = 0;
     int wallAdjacentCount = 0;
@@ -165,6 +166,7 @@ void updateSingleGrid(lbm_grids* g, LevelState& L) {
     L.info.esotwistFlipper = !flip;  // applyStreaming
     lbm::launchPeriodic(L.dev, L.info.esotwistFlipper, g->stream);
     L.info.iterationsFinished++;
+    L.iterationsSinceTrackerReset++;
 }
 
 void updateAllGrids(lbm_grids* g, int level) {
@@ -259,6 +261,13 @@ int lbm_plan_read_array(lbm_plan* p, int level, int which, void* host, size_t by
         return fail(LBM_ERR_INVALID, "lbm_plan_read_array: bad argument");
     const lbm::HostLevel& H = p->host.levels[level];
     const std::vector<int>* v = nullptr;
+    const std::vector<uint32_t>* u = nullptr;
+    if (which == LBM_ARRAY_WALL_VELOCITY) {
+        const size_t need = H.wallVelocity.size() * sizeof(float);
+        if (bytes != need) return fail(LBM_ERR_INVALID, "lbm_plan_read_array: byte count does not match array size");
+        if (bytes) std::memcpy(host, H.wallVelocity.data(), bytes);
+        return LBM_OK;
+    }
     switch (which) {
         case LBM_ARRAY_SHIFTER: v = &H.shifter; break;
         case LBM_ARRAY_ROW_I: v = &H.rowI; break;
@@ -270,7 +279,17 @@ int lbm_plan_read_array(lbm_plan* p, int level, int which, void* host, size_t by
         case LBM_ARRAY_WALL_MAP: v = &H.wallMap; break;
         case LBM_ARRAY_PERIODIC_INDEX: v = &H.perIndex; break;
         case LBM_ARRAY_PERIODIC_SOURCE: v = &H.perSource; break;
+        case LBM_ARRAY_WALL_INDEX: v = &H.wallIndex; break;
+        case LBM_ARRAY_WALL_DATA: u = &H.wallData; break;
+        case LBM_ARRAY_LINK_LENGTH: u = &H.linkLength; break;
         default: return fail(LBM_ERR_INVALID, "lbm_plan_read_array: array not available in a plan");
+    }
+    if (u) {
+        if (bytes != u->size() * sizeof(uint32_t))
+            return fail(LBM_ERR_INVALID, "lbm_plan_read_array: byte count does not match array size (expected " +
+                                             std::to_string(u->size() * sizeof(uint32_t)) + ")");
+        if (bytes) std::memcpy(host, u->data(), bytes);
+        return LBM_OK;
     }
     if (bytes != v->size() * sizeof(int))
         return fail(LBM_ERR_INVALID, "lbm_plan_read_array: byte count does not match array size (expected " +
@@ -344,6 +363,18 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
                 d.special = own(upload(H.specialCells, s));
                 d.specialCount = static_cast<int>(H.specialCells.size());
             }
+            d.wallCount = static_cast<int>(H.wallIndex.size());
+            d.wallIndex = own(upload(H.wallIndex, s));
+            d.wallData = own(upload(H.wallData, s));
+            d.linkLength = own(upload(H.linkLength, s));
+            d.wallVel = own(upload(H.wallVelocity, s));
+            d.wallForce = own(devAlloc<float>(3 * H.wallIndex.size()));
+            if (d.wallForce) ck(cudaMemsetAsync(d.wallForce, 0, 3 * H.wallIndex.size() * sizeof(float), s), "memset");
+            d.trackWallForce = c->track_wall_force ? 1 : 0;
+            d.useIBB = c->use_ibb ? 1 : 0;
+            d.gx = c->gx;
+            d.gy = c->gy;
+            d.gz = c->gz;
             lbm::BC bc;
             lbm::evalLocalBC(*c, bc);
             d.coll = lbm::makeCollisionConsts(H.info.nu, bc.nuMultiplier, bc.collisionLimiter);
@@ -505,6 +536,11 @@ int lbm_read_array(lbm_grids* g, int level, int which, void* host, size_t bytes)
         case LBM_ARRAY_WALL_MAP: src = d.wallMap; need = n * 4; break;
         case LBM_ARRAY_PERIODIC_INDEX: src = d.perIndex; need = size_t(d.perCount) * 4; break;
         case LBM_ARRAY_PERIODIC_SOURCE: src = d.perSource; need = size_t(d.perCount) * 4; break;
+        case LBM_ARRAY_WALL_INDEX: src = d.wallIndex; need = size_t(d.wallCount) * 4; break;
+        case LBM_ARRAY_WALL_DATA: src = d.wallData; need = size_t(d.wallCount) * 4; break;
+        case LBM_ARRAY_LINK_LENGTH: src = d.linkLength; need = size_t(d.wallCount) * 7 * 4; break;
+        case LBM_ARRAY_WALL_FORCE: src = d.wallForce; need = size_t(d.wallCount) * 3 * 4; break;
+        case LBM_ARRAY_WALL_VELOCITY: src = d.wallVel; need = size_t(d.wallCount) * 3 * 4; break;
         case LBM_ARRAY_F: need = 27 * n * 4; break;
         case LBM_ARRAY_MACRO: need = 4 * n * 4; break;
         default: return fail(LBM_ERR_INVALID, "lbm_read_array: unknown array id");
@@ -572,6 +608,36 @@ int lbm_kinetic_energy(lbm_grids* g, float uRefPhys, float domainLength, double*
         }
         const double len = double(domainLength) / 1000.0;
         *out = energy / (len * len * len);
+    });
+}
+
+int lbm_wall_force(lbm_grids* g, int wallID, int reset, double* out) {
+    if (!g || !out || wallID < 0 || wallID >= LBM_MAX_BODIES)
+        return fail(LBM_ERR_INVALID, "lbm_wall_force: bad argument");
+    return guarded("lbm_wall_force", [&] {
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        for (LevelState& L : g->levels) {
+            ck(cudaMemsetAsync(g->scratch, 0, 6 * sizeof(double), g->stream), "memset");
+            lbm::launchWallForce(L.dev, wallID, g->stream, g->scratch);
+            ck(cudaGetLastError(), "force launch");
+            double r[6];
+            ck(cudaMemcpyAsync(r, g->scratch, sizeof(r), cudaMemcpyDeviceToHost, g->stream), "copy");
+            ck(cudaStreamSynchronize(g->stream), "sync");
+            const double span = L.iterationsSinceTrackerReset > 0 ? L.iterationsSinceTrackerReset : 1;
+            // convertToPhysicalForce (include/cellFunctions.h:296-301); torque from N mm to N m
+            const double rm = double(L.info.res) / 1000.0;
+            const double conv = double(g->c.rho_phys) * rm * rm * rm * rm / (double(L.info.dtPhys) * L.info.dtPhys);
+            for (int q = 0; q < 3; ++q) acc[q] += r[q] / span * conv;
+            for (int q = 3; q < 6; ++q) acc[q] += r[q] / span * conv * 0.001;
+            if (reset) {
+                if (L.dev.wallForce)
+                    ck(cudaMemsetAsync(L.dev.wallForce, 0, 3 * size_t(L.dev.wallCount) * sizeof(float), g->stream),
+                       "memset");
+                L.iterationsSinceTrackerReset = 0;
+            }
+        }
+        if (reset) ck(cudaStreamSynchronize(g->stream), "sync");
+        for (int q = 0; q < 6; ++q) out[q] = acc[q];
     });
 }
 

@@ -9,6 +9,8 @@
 // column instead of bin + insertion sort.  The resulting tables are the same
 // as the reference's (the oracle checks them element by element).
 #include "builder.h"
+#include "geometry.h"
+#include "lattice.h"
 
 #include <algorithm>
 #include <cmath>
@@ -101,6 +103,17 @@ void validateCase(const lbm_case& c) {
     }
     if (c.storage != LBM_STORE_F32 && c.storage != LBM_STORE_F16 && c.storage != LBM_STORE_BF16)
         throw std::runtime_error("unknown storage precision");
+    if (c.body_count < 0 || c.body_count > LBM_MAX_BODIES)
+        throw std::runtime_error("body_count must be in [0, LBM_MAX_BODIES]");
+    for (int b = 0; b < c.body_count; ++b) {
+        const lbm_body& bd = c.body[b];
+        if (bd.triangle_count <= 0 || !bd.triangles)
+            throw std::runtime_error("voxelizeSTL failed: the passed STL has 0 triangles.");
+        if (bd.motion != LBM_WALL_STATIC && bd.motion != LBM_WALL_ROTATING)
+            throw std::runtime_error("unknown wall motion");
+        if (bd.motion == LBM_WALL_ROTATING && (bd.axis < 0 || bd.axis > 2))
+            throw std::runtime_error("rotation axis must be 0, 1 or 2");
+    }
 }
 
 // initializeGridInfo, level 0 (include/gridBuilderFunctions.h:9-64): the
@@ -175,6 +188,13 @@ void buildCellsAndNBR(HostLevel& L, const std::vector<uint8_t>& keepFull) {
             }
             if (prev >= 0) L.kPlus[prev] = first;
         }
+    // NBR minus as the inverse of the plus permutations (gridBuilderFunctions.h:565-575)
+    L.jMinus.assign(n, 0);
+    L.kMinus.assign(n, 0);
+    for (int cidx = 0; cidx < n; ++cidx) {
+        L.jMinus[L.jPlus[cidx]] = cidx;
+        L.kMinus[L.kPlus[cidx]] = cidx;
+    }
     // geometric-validity bits (markGeometricNBRPlus, include/NBRFunctions.h:154-194)
     L.geomBits.assign(n, 0);
     auto wrap = [n](int v) { return v + 1 < n ? v + 1 : 0; };
@@ -245,7 +265,8 @@ void buildBoundaryLists(const lbm_case& c, HostLevel& L) {
     L.wallCellCount = 0;
     for (int cidx = 0; cidx < n; ++cidx)
         if (L.wallMarker[cidx]) { L.wallMap[cidx] = -3; ++L.wallCellCount; }
-    L.wallAdjacentCount = 0;
+    L.wallAdjacentCount = static_cast<int>(L.wallIndex.size());
+    for (int w = 0; w < L.wallAdjacentCount; ++w) L.wallMap[L.wallIndex[w]] = w;
 
     // Periodic overlap: no force/flow tracking in the ghost layers
     // (include/gridBuilderFunctions.h:1232-1274).
@@ -260,7 +281,9 @@ void buildBoundaryLists(const lbm_case& c, HostLevel& L) {
             overlap |= evalOpenBC(c, in, i, j < layers ? 0 : in.ny - 1, k).periodic;
         if (k < layers || k >= in.nz - layers)
             overlap |= evalOpenBC(c, in, i, j, k < layers ? 0 : in.nz - 1).periodic;
-        if (overlap && L.wallMap[cidx] == -1) L.wallMap[cidx] = -2;
+        if (!overlap) continue;
+        if (L.wallMap[cidx] >= 0) L.wallData[L.wallMap[cidx]] |= 1u;
+        else if (L.wallMap[cidx] == -1) L.wallMap[cidx] = -2;
     }
 
     // Open boundaries: one list per openBCID (:1276-1484).
@@ -346,6 +369,270 @@ void buildBoundaryLists(const lbm_case& c, HostLevel& L) {
 
 }  // namespace
 
+namespace {
+
+// The 7 plus neighbours of a cell (iPlus, jPlus, ijPlus, kPlus, ikPlus,
+// jkPlus, ijkPlus) with the +1 wrap of finishNBRPlus.
+void plusNbrs(const HostLevel& L, int c, int (&nb)[7]) {
+    const int n = L.info.cellCount;
+    auto wrap = [n](int v) { return v + 1 < n ? v + 1 : 0; };
+    nb[0] = wrap(c);
+    nb[1] = L.jPlus[c];
+    nb[2] = wrap(nb[1]);
+    nb[3] = L.kPlus[c];
+    nb[4] = wrap(nb[3]);
+    nb[5] = L.jPlus[nb[3]];
+    nb[6] = wrap(nb[5]);
+}
+
+// spreadMarkers over the cell list (include/markerFunctions.h:344-399): a cell
+// is marked when it or a geometric plus neighbour is; a marked cell also marks
+// all its geometric plus neighbours.
+std::vector<uint8_t> spreadCells(const HostLevel& L, const std::vector<uint8_t>& src) {
+    std::vector<uint8_t> out = src;
+    const int n = L.info.cellCount;
+    for (int c = 0; c < n; ++c) {
+        int nb[7];
+        plusNbrs(L, c, nb);
+        const uint8_t bits = L.geomBits[c];
+        bool marker = src[c] != 0;
+        for (int q = 0; q < 7 && !marker; ++q)
+            if (((bits >> q) & 1u) && src[nb[q]]) marker = true;
+        if (!marker) continue;
+        out[c] = 1;
+        for (int q = 0; q < 7; ++q)
+            if ((bits >> q) & 1u) out[nb[q]] = 1;
+    }
+    return out;
+}
+
+// spreadMarkers on the dense skeleton (include/markerFunctions.h:290-342): 26 neighbours.
+std::vector<uint8_t> spreadDense(const std::vector<uint8_t>& src, int nx, int ny, int nz) {
+    std::vector<uint8_t> out = src;
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const size_t c = (static_cast<size_t>(k) * ny + j) * nx + i;
+                if (src[c]) continue;
+                bool hit = false;
+                for (int dk = -1; dk <= 1 && !hit; ++dk)
+                    for (int dj = -1; dj <= 1 && !hit; ++dj)
+                        for (int di = -1; di <= 1 && !hit; ++di) {
+                            if (!dk && !dj && !di) continue;
+                            const int a = i + di, b = j + dj, e = k + dk;
+                            if (a < 0 || a >= nx || b < 0 || b >= ny || e < 0 || e >= nz) continue;
+                            if (src[(static_cast<size_t>(e) * ny + b) * nx + a]) hit = true;
+                        }
+                if (hit) out[c] = 1;
+            }
+    return out;
+}
+
+// Full 26-neighbour list of a cell reached through the plus/minus chains, as
+// buildLinkExistenceMarkerArray forms it (interpolatedBouncebackFunctions.h:227-260).
+void fullNbrList(const HostLevel& L, int c, int (&nb)[27]) {
+    const int n = L.info.cellCount;
+    const auto& jP = L.jPlus;
+    const auto& kP = L.kPlus;
+    const auto& jM = L.jMinus;
+    const auto& kM = L.kMinus;
+    const int iPlus = c + 1 >= n ? 0 : c + 1;
+    const int iMinus = c - 1 < 0 ? n - 1 : c - 1;
+    nb[OOO] = c;
+    nb[POO] = iPlus;
+    nb[MOO] = iMinus;
+    nb[OOM] = kM[c];
+    nb[OOP] = kP[c];
+    nb[OMO] = jM[c];
+    nb[OPO] = jP[c];
+    nb[POM] = kM[iPlus];
+    nb[MOP] = kP[iMinus];
+    nb[POP] = kP[iPlus];
+    nb[MOM] = kM[iMinus];
+    nb[MMO] = jM[iMinus];
+    nb[PPO] = jP[iPlus];
+    nb[OPM] = kM[jP[c]];
+    nb[OMP] = kP[jM[c]];
+    nb[MPO] = jP[iMinus];
+    nb[PMO] = jM[iPlus];
+    nb[OPP] = jP[kP[c]];
+    nb[OMM] = kM[jM[c]];
+    nb[MPM] = kM[jP[iMinus]];
+    nb[PMP] = kP[jM[iPlus]];
+    nb[MMP] = kP[jM[iMinus]];
+    nb[PPM] = kM[jP[iPlus]];
+    nb[PMM] = kM[jM[iPlus]];
+    nb[MPP] = jP[kP[iMinus]];
+    nb[MMM] = kM[jM[iMinus]];
+    nb[PPP] = jP[kP[iPlus]];
+}
+
+// Links of one wall-adjacent cell (buildLinkExistenceMarkerArray,
+// interpolatedBouncebackFunctions.h:181-398, single level: no interface links).
+uint32_t linkBits(const HostLevel& L, int c) {
+    const Info& in = L.info;
+    int nb[27];
+    fullNbrList(L, c, nb);
+    const int i = L.I[c], j = L.J[c], k = L.K[c];
+    bool geom[27];
+    bool all = true, ip = true, jp = true, kp = true, im = true, jm = true, km = true;
+    for (int d = 1; d < 27; ++d) {
+        geom[d] = true;
+        const int ie = i + cx(d), je = j + cy(d), ke = k + cz(d);
+        const int q = nb[d];
+        if (L.I[q] == ie && L.J[q] == je && L.K[q] == ke) continue;
+        geom[d] = false;
+        if (ie < 0 || ie >= in.nx || je < 0 || je >= in.ny || ke < 0 || ke >= in.nz) continue;
+        all = false;
+        if (cx(d) > 0) ip = false;
+        if (cy(d) > 0) jp = false;
+        if (cz(d) > 0) kp = false;
+        if (cx(d) < 0) im = false;
+        if (cy(d) < 0) jm = false;
+        if (cz(d) < 0) km = false;
+    }
+    uint32_t bits = 0;
+    const bool interior = i != 0 && i != in.nx - 1 && j != 0 && j != in.ny - 1 && k != 0 && k != in.nz - 1;
+    if (interior) {
+        if (!all) return 0;
+        for (int d = 1; d < 27; ++d)
+            if (L.wallMarker[nb[d]]) bits |= 1u << d;
+        return bits;
+    }
+    for (int d = 1; d < 27; ++d) {
+        if (!geom[d] || !L.wallMarker[nb[d]]) continue;
+        if ((cx(d) > 0 && !ip) || (cy(d) > 0 && !jp) || (cz(d) > 0 && !kp)) continue;
+        if ((cx(d) < 0 && !im) || (cy(d) < 0 && !jm) || (cz(d) < 0 && !km)) continue;
+        bits |= 1u << d;
+    }
+    return bits;
+}
+
+// Wall markers, wall IDs, wall-adjacent list, link existence and link lengths
+// (buildWallMarkers, include/gridBuilderFunctions.h:590-739, and
+// buildLinkLengthArray, interpolatedBouncebackFunctions.h:482-660), then the
+// packed wallData / linkLength words (packWallData, :662-695).
+void buildWalls(const lbm_case& c, HostLevel& L, const std::vector<Triangles>& bodies,
+                const std::vector<RayMap>& maps, const RayMap& total) {
+    const Info& in = L.info;
+    const int n = in.cellCount;
+    L.wallMarker.assign(n, 0);
+    for (int q = 0; q < n; ++q) L.wallMarker[q] = isSolid(total, L.I[q], L.J[q], L.K[q]) ? 1 : 0;
+    std::vector<int> wallID(n, -1);
+    for (size_t b = 0; b < maps.size(); ++b) {
+        std::vector<uint8_t> body(n, 0);
+        for (int q = 0; q < n; ++q) body[q] = isSolid(maps[b], L.I[q], L.J[q], L.K[q]) ? 1 : 0;
+        body = spreadCells(L, body);
+        for (int q = 0; q < n; ++q)
+            if (body[q] && !L.wallMarker[q]) wallID[q] = static_cast<int>(b);  // last body wins
+    }
+    L.wallIndex.clear();
+    std::vector<int> ids;
+    for (int q = 0; q < n; ++q)
+        if (wallID[q] >= 0) {
+            L.wallIndex.push_back(q);
+            ids.push_back(wallID[q]);
+        }
+    const int nw = static_cast<int>(L.wallIndex.size());
+    std::vector<uint32_t> links(nw, 0);
+    for (int w = 0; w < nw; ++w) links[w] = linkBits(L, L.wallIndex[w]);
+
+    // link lengths: nearest triangle crossing of each link, per body bins
+    std::vector<float> len(static_cast<size_t>(nw) * 27, 2.f);
+    const float edgeTol = 0.1f * in.res;
+    const float qTol = 0.2f;
+    for (const Triangles& t : bodies) {
+        const int bxy = t.binCountX * t.binCountY;
+        for (int w = 0; w < nw; ++w) {
+            if (!links[w]) continue;
+            const int cell = L.wallIndex[w];
+            const float x = L.I[cell] * in.res + in.ox;
+            const float y = L.J[cell] * in.res + in.oy;
+            const float z = L.K[cell] * in.res + in.oz;
+            const int ib = static_cast<int>((x - t.oxBin) / t.binSize);
+            const int jb = static_cast<int>((y - t.oyBin) / t.binSize);
+            const int kb = static_cast<int>((z - t.ozBin) / t.binSize);
+            if (ib < 0 || ib >= t.binCountX || jb < 0 || jb >= t.binCountY || kb < 0 || kb >= t.binCountZ)
+                continue;
+            const int bin = bxy * kb + t.binCountX * jb + ib;
+            for (int r = t.firstInBin[bin]; r < t.firstInBin[bin + 1]; ++r) {
+                const int tri = t.bin[r];
+                const float ax = t.ax[tri] - x, ay = t.ay[tri] - y, az = t.az[tri] - z;
+                const float bx = t.bx[tri] - x, by = t.by[tri] - y, bz = t.bz[tri] - z;
+                const float cxv = t.cx[tri] - x, cyv = t.cy[tri] - y, czv = t.cz[tri] - z;
+                for (int d = 1; d < 27; ++d) {
+                    if (!((links[w] >> d) & 1u)) continue;
+                    float tHit;
+                    if (!intersectRayTriangle(ax, ay, az, bx, by, bz, cxv, cyv, czv, float(cx(d)), float(cy(d)),
+                                              float(cz(d)), edgeTol, tHit))
+                        continue;
+                    float q = tHit / in.res;
+                    float& slot = len[static_cast<size_t>(w) * 27 + d];
+                    if (q > 0 && q <= 1.f) {  // accurate crossing
+                        q = std::clamp(q, 0.00001f, 1.f);
+                        if (slot < 0.f || q < slot) slot = q;
+                    } else if (q > -qTol && q <= 1.f + qTol) {  // near miss, kept as negative
+                        q = std::clamp(q, 0.00001f, 1.f);
+                        if (slot < 0.f) {
+                            if (q < -slot) slot = -q;
+                        } else if (slot > 1.f) {
+                            slot = -q;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    L.linksTotal = 0;
+    L.linksNotFound = 0;
+    for (int w = 0; w < nw; ++w)
+        for (int d = 1; d < 27; ++d) {
+            if (!((links[w] >> d) & 1u)) continue;
+            ++L.linksTotal;
+            float& slot = len[static_cast<size_t>(w) * 27 + d];
+            if (slot > 1.f) {
+                slot = 0.5f;  // no crossing found: safe fallback
+                ++L.linksNotFound;
+            } else if (slot < 0.f) {
+                slot = -slot;
+            }
+        }
+
+    // pack
+    L.wallData.assign(nw, 0);
+    L.linkLength.assign(static_cast<size_t>(7) * nw, 0);
+    L.wallVelocity.assign(static_cast<size_t>(3) * nw, 0.f);
+    for (int w = 0; w < nw; ++w) {
+        uint32_t data = static_cast<uint32_t>(ids[w]) << 27;
+        int li = 0;
+        for (int d = 1; d < 27; ++d) {
+            if (!((links[w] >> d) & 1u)) continue;
+            data |= 1u << d;
+            const float q = std::clamp(len[static_cast<size_t>(w) * 27 + d], 0.f, 1.f);
+            const uint32_t code = static_cast<uint32_t>(q * 254.f + 0.5f);
+            L.linkLength[static_cast<size_t>(li / 4) * nw + w] |= code << (8 * (li % 4));
+            ++li;
+        }
+        L.wallData[w] = data;
+        // getLocalBC wall velocity of the body (evaluated at the fluid cell centre)
+        const lbm_body& body = c.body[ids[w]];
+        if (body.motion == LBM_WALL_ROTATING) {
+            const int cell = L.wallIndex[w];
+            const float x = L.I[cell] * in.res + in.ox - body.origin[0];
+            const float y = L.J[cell] * in.res + in.oy - body.origin[1];
+            const float z = L.K[cell] * in.res + in.oz - body.origin[2];
+            const float s = body.radians_per_second * in.dtPhys / in.res;
+            float u[3] = {0.f, 0.f, 0.f};
+            if (body.axis == 2) { u[0] = -s * y; u[1] = s * x; }
+            else if (body.axis == 0) { u[1] = -s * z; u[2] = s * y; }
+            else { u[2] = -s * x; u[0] = s * z; }
+            for (int a = 0; a < 3; ++a) L.wallVelocity[static_cast<size_t>(a) * nw + w] = u[a];
+        }
+    }
+}
+
+}  // namespace
+
 void buildSegments(HostLevel& L) {
     L.segCell.clear(); L.segJP.clear(); L.segKP.clear(); L.segJKP.clear(); L.segLen.clear();
     L.specialCells.clear();
@@ -389,17 +676,68 @@ void buildSegments(HostLevel& L) {
 void buildDomain(const lbm_case& c, HostDomain& out) {
     validateCase(c);
     out.c = c;
+    out.c.body_count = 0;  // triangle pointers are not kept past this call
     out.levels.assign(1, HostLevel{});
     HostLevel& L = out.levels[0];
     Info skel;
     initLevel0(c, L.info, skel);
+    const Info& in = L.info;
 
-    // Without static geometry every skeleton cell is kept (markKeepCells,
-    // include/markerFunctions.h:401-409, over an empty ray map).
-    const size_t full = static_cast<size_t>(L.info.nx) * L.info.ny * L.info.nz;
-    std::vector<uint8_t> keep(full, 1);
+    // bodies: triangles, bins and one ray map each, plus their union
+    // (readSTL/sortSTLToBins, initializeVoxelizers: voxelizerFunctions.h:692-728)
+    std::vector<Triangles> bodies(c.body_count);
+    std::vector<RayMap> maps(c.body_count);
+    RayMap total;
+    total.nx = in.nx;
+    total.ny = in.ny;
+    total.scan.assign(static_cast<size_t>(in.nx) * in.ny + 1, 0);
+    for (int b = 0; b < c.body_count; ++b) {
+        loadTriangles(c.body[b].triangles, c.body[b].triangle_count, bodies[b]);
+        sortToBins(bodies[b], c.res_global);
+        voxelize(bodies[b], in.ox, in.oy, in.oz, in.res, in.nx, in.ny, maps[b]);
+        if (b == 0) total = maps[0];
+        else unionRayMaps(total, maps[b]);
+    }
+
+    // markKeepCells on the skeleton: keep a skeleton cell that covers fluid,
+    // plus one layer (markerFunctions.h:401-409)
+    const int snx = skel.nx, sny = skel.ny, snz = skel.nz;
+    std::vector<uint8_t> keepSkel(static_cast<size_t>(snx) * sny * snz, 1);
+    if (c.body_count > 0) {
+        for (int k = 0; k < snz; ++k)
+            for (int j = 0; j < sny; ++j)
+                for (int i = 0; i < snx; ++i)
+                    keepSkel[(static_cast<size_t>(k) * sny + j) * snx + i] = coarseHasFluid(total, 2, i, j, k) ? 1 : 0;
+        keepSkel = spreadDense(keepSkel, snx, sny, snz);
+    }
+    const size_t full = static_cast<size_t>(in.nx) * in.ny * in.nz;
+    std::vector<uint8_t> keep(full, 0);
+    for (int k = 0; k < in.nz; ++k)
+        for (int j = 0; j < in.ny; ++j)
+            for (int i = 0; i < in.nx; ++i)
+                keep[(static_cast<size_t>(k) * in.ny + j) * in.nx + i] =
+                    keepSkel[(static_cast<size_t>(k / 2) * sny + j / 2) * snx + i / 2];
     buildCellsAndNBR(L, keep);
-    L.wallMarker.assign(L.info.cellCount, 0);
+
+    if (c.body_count > 0) {
+        // deleteExcessCells (gridBuilderFunctions.h:402-588): keep fluid plus
+        // one layer of wall cells
+        std::vector<uint8_t> fluid(L.info.cellCount, 0);
+        for (int q = 0; q < L.info.cellCount; ++q)
+            fluid[q] = isSolid(total, L.I[q], L.J[q], L.K[q]) ? 0 : 1;
+        fluid = spreadCells(L, fluid);
+        std::fill(keep.begin(), keep.end(), 0);
+        for (int q = 0; q < L.info.cellCount; ++q)
+            if (fluid[q]) keep[(static_cast<size_t>(L.K[q]) * in.ny + L.J[q]) * in.nx + L.I[q]] = 1;
+        buildCellsAndNBR(L, keep);
+        buildWalls(c, L, bodies, maps, total);
+    } else {
+        L.wallMarker.assign(L.info.cellCount, 0);
+        L.wallIndex.clear();
+        L.wallData.clear();
+        L.linkLength.clear();
+        L.wallVelocity.clear();
+    }
     compressRows(L);
     buildBoundaryLists(c, L);
     buildSegments(L);

@@ -45,7 +45,7 @@ struct HostLevel {
     Info info;
     // builder view: sorted full IJK of the kept cells
     std::vector<int> I, J, K;
-    std::vector<int> jPlus, kPlus;
+    std::vector<int> jPlus, kPlus, jMinus, kMinus;
     std::vector<uint8_t> geomBits;
     std::vector<uint8_t> wallMarker;
     // compressed IJK/NBR (CompressedIJKNBRStruct, include/types.h:162-164)
@@ -57,6 +57,12 @@ struct HostLevel {
     std::vector<OpenBCList> openBCs;
     int wallCellCount = 0;
     int wallAdjacentCount = 0;
+    // wall-adjacent fluid cells (WallStruct, include/types.h:202-204)
+    std::vector<int> wallIndex;          // cell of each wall-adjacent entry
+    std::vector<uint32_t> wallData;      // bit 0 overlap, bits 1-26 links, 27-31 wallID
+    std::vector<uint32_t> linkLength;    // [7][wallAdjacentCount] 8-bit link codes
+    std::vector<float> wallVelocity;     // [3][wallAdjacentCount] wall velocity, lattice units
+    int linksTotal = 0, linksNotFound = 0;
     // Bulk segments: runs of at most kSegmentCells plain-fluid cells (wallMap
     // -1 or -2) inside one compressed row.  Inside such a run every neighbour
     // index is the run's base plus the lane offset, so the bulk kernel needs

@@ -40,7 +40,7 @@ __global__ void __launch_bounds__(kBlock) collideStream(DevLevel g) {
     decodeNbr(g, cell, nb, nullptr);
     float f[27];
     readPre<F, S>(g, nb, f);
-    collideCumulant(f, g.coll, g.coll.lambda, 0.f, 0.f, 0.f);
+    collideCumulant(f, g.coll, g.coll.lambda, g.gx, g.gy, g.gz);
     writePost<F, S>(g, nb, f);
 }
 
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(kTile, LBM3_TMA_MIN_BLOCKS) collideBulkTma(Dev
                                     int(sizeof(S));
                     f[q] = Store<S>::ld(reinterpret_cast<const S*>(st + q * runBytes<S>()) + off + t);
                 }
-                collideCumulant(f, g.coll, g.coll.lambda, 0.f, 0.f, 0.f);
+                collideCumulant(f, g.coll, g.coll.lambda, g.gx, g.gy, g.gz);
                 writePost<F, S>(g, nb, f);
             }
         }
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(kTile, LBM3_PREFETCH_MIN_BLOCKS) collidePrefet
         segNbr(g, dNext, t, nbn);
         if (t < lNext) readPre<F, S>(g, nbn, fn);
         if (t < lCur) {
-            collideCumulant(f, g.coll, g.coll.lambda, 0.f, 0.f, 0.f);
+            collideCumulant(f, g.coll, g.coll.lambda, g.gx, g.gy, g.gz);
             writePost<F, S>(g, nb, f);
         }
 #pragma unroll
@@ -300,18 +300,112 @@ __global__ void __launch_bounds__(kTile, LBM3_PREFETCH_MIN_BLOCKS) collidePrefet
     }
 }
 
-// Cells outside the bulk segments (wall-adjacent), one thread per listed cell.
+// Cells outside the bulk segments, one thread per listed cell: wall-adjacent
+// fluid cells get the interpolated bounceback of Zhao & Yong (2017) with a
+// moving-wall term and momentum-exchange force
+// (applyIBB, include/boundaryConditions/interpolatedBouncebackFunctions.h:43-157,
+// and the write loop of include/updateGrid.h:143-176); the rest (cells whose
+// +1 neighbour wraps) collide and stream like bulk cells.
 template <bool F, class S>
 __global__ void __launch_bounds__(kBlock) collideList(DevLevel g) {
     const int idx = blockIdx.x * kBlock + threadIdx.x;
     if (idx >= g.specialCount) return;
     const int cell = __ldg(g.special + idx);
+    const int wm = __ldg(g.wallMap + cell);
     int nb[8];
     decodeNbr(g, cell, nb, nullptr);
     float f[27];
     readPre<F, S>(g, nb, f);
-    collideCumulant(f, g.coll, g.coll.lambda, 0.f, 0.f, 0.f);
-    writePost<F, S>(g, nb, f);
+    collideCumulant(f, g.coll, g.coll.lambda, g.gx, g.gy, g.gz);
+    if (wm < 0) {
+        writePost<F, S>(g, nb, f);
+        return;
+    }
+    const unsigned wallData = __ldg(g.wallData + wm);
+    const int nw = g.wallCount;
+    const float uwx = __ldg(g.wallVel + wm), uwy = __ldg(g.wallVel + nw + wm), uwz = __ldg(g.wallVel + 2 * nw + wm);
+    float dRho, ux, uy, uz;
+    macroFromF(f, dRho, ux, uy, uz);
+    float out[27];
+#pragma unroll
+    for (int d = 0; d < 27; ++d) out[d] = f[d];
+    float fx = 0.f, fy = 0.f, fz = 0.f;
+    int link = 0;
+    unsigned code = 0u;
+    const S* base = static_cast<const S*>(g.f);
+#pragma unroll
+    for (int d = 1; d < 27; ++d) {
+        if (!((wallData >> d) & 1u)) continue;
+        const int id = inv(d);
+        const float eu = float(cx(id)) * uwx + float(cy(id)) * uwy + float(cz(id)) * uwz;
+        const float wallTerm = 6.f * weight(id) * (1.f + dRho) * eu;
+        float gamma = 0.5f;
+        if (g.useIBB) {
+            if ((link & 3) == 0) code = __ldg(g.linkLength + (link >> 2) * nw + wm);
+            const unsigned c8 = (code >> (8 * (link & 3))) & 255u;
+            gamma = fminf(fmaxf(static_cast<float>(c8) / 254.f, 0.01f), 1.f);
+            ++link;
+        }
+        // pre-collision value of direction d, still unchanged in memory
+        const float fPre = Store<S>::ld(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
+        const float invDen = 1.f / (1.f + gamma);
+        const float r = ((1.f - gamma) * invDen) * fPre + (gamma * invDen) * f[id] + (gamma * invDen) * f[d] +
+                        invDen * wallTerm;
+        fx += -f[d] * (float(cx(d)) - uwx) + r * (float(cx(id)) - uwx);
+        fy += -f[d] * (float(cy(d)) - uwy) + r * (float(cy(id)) - uwy);
+        fz += -f[d] * (float(cz(d)) - uwz) + r * (float(cz(id)) - uwz);
+        out[d] = r;
+    }
+    // writes: a linked direction goes to the next pre-collision slot of its
+    // inverse (inside the wall cell), the others stream as usual
+    S* wbase = static_cast<S*>(g.f);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        const bool linked = d != 0 && ((wallData >> d) & 1u);
+        const int slot = linked ? (F ? inv(d) : d) : postSlot<F>(d);
+        Store<S>::st(wbase + (long long)slot * g.stride + nb[postNbr(d)], out[d]);
+    }
+    if (g.trackWallForce && !(wallData & 1u)) {
+        g.wallForce[wm] += fx;
+        g.wallForce[nw + wm] += fy;
+        g.wallForce[2 * nw + wm] += fz;
+    }
+}
+
+// FP64 force and torque about the origin of the cells of one wall ID
+// (updateTracker wall branch, include/trackerFunctions.h:386-428).
+__global__ void __launch_bounds__(kBlock) wallForceSum(DevLevel g, int wallID, double* out) {
+    const int w = blockIdx.x * kBlock + threadIdx.x;
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    if (w < g.wallCount) {
+        const unsigned data = __ldg(g.wallData + w);
+        if (static_cast<int>((data >> 27) & 31u) == wallID) {
+            const int cell = __ldg(g.wallIndex + w);
+            int nb[8], ijk[3];
+            decodeNbr(g, cell, nb, ijk);
+            const double x = double(ijk[0] * g.res + g.ox), y = double(ijk[1] * g.res + g.oy),
+                         z = double(ijk[2] * g.res + g.oz);
+            const double gx = g.wallForce[w], gy = g.wallForce[g.wallCount + w], gz = g.wallForce[2 * g.wallCount + w];
+            v[0] = gx; v[1] = gy; v[2] = gz;
+            v[3] = y * gz - z * gy;
+            v[4] = z * gx - x * gz;
+            v[5] = x * gy - y * gx;
+        }
+    }
+    __shared__ double part[6][kBlock / 32];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        double a = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+        if ((threadIdx.x & 31) == 0) part[q][threadIdx.x >> 5] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double a = 0.0;
+        for (int k = 0; k < kBlock / 32; ++k) a += part[threadIdx.x][k];
+        atomicAdd(out + threadIdx.x, a);
+    }
 }
 
 // F is the flipper after streaming, i.e. the state the ghosts are read in.
@@ -374,7 +468,8 @@ __global__ void __launch_bounds__(kBlock) kineticEnergy(DevLevel g, double* out)
         const int wm = __ldg(g.wallMap + cell);
         // walls, interface duplicates and periodic ghosts are excluded
         // (cases/taylorGreenVortex/taylorGreenVortexMain.cu:139-141)
-        if (wm != -3 && wm != -2) {
+        const bool overlap = wm >= 0 && (__ldg(g.wallData + wm) & 1u);
+        if (wm != -3 && wm != -2 && !overlap) {
             int nb[8];
             decodeNbr(g, cell, nb, nullptr);
             float f[27];
@@ -553,6 +648,9 @@ void launchKineticEnergy(const DevLevel& g, bool flip, cudaStream_t s, double* o
 void launchMacro(const DevLevel& g, bool flip, cudaStream_t s, float* out) { dispatch<RunMacro>(g, flip, s, out); }
 void launchGatherF(const DevLevel& g, cudaStream_t s, float* out) { dispatch<RunGather>(g, false, s, out); }
 void launchScatterF(const DevLevel& g, cudaStream_t s, const float* in) { dispatch<RunScatter>(g, false, s, in); }
+void launchWallForce(const DevLevel& g, int wallID, cudaStream_t s, double* out) {
+    if (g.wallCount > 0) wallForceSum<<<blocksFor(g.wallCount), kBlock, 0, s>>>(g, wallID, out);
+}
 void launchCollideBatch(float* f, int n, const CollisionConsts& P, float gx, float gy, float gz,
                         cudaStream_t s) {
     collideBatch<<<blocksFor(n), kBlock, 0, s>>>(f, n, P, gx, gy, gz);

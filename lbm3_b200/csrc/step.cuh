@@ -37,6 +37,16 @@ struct DevLevel {
     const int* special;
     int specialCount;
     int* errorFlag;          // set to nonzero when a bounded device wait gives up
+    // wall-adjacent cells (WallStruct)
+    const unsigned* wallData;      // [wallCount]
+    const unsigned* linkLength;    // [7][wallCount] packed 8-bit link codes
+    const float* wallVel;          // [3][wallCount] wall velocity, lattice units
+    float* wallForce;              // [3][wallCount] momentum-exchange force accumulators
+    const int* wallIndex;          // [wallCount] cell of each entry
+    int wallCount;
+    int trackWallForce;
+    int useIBB;
+    float gx, gy, gz;              // body force (getLocalBC)
     int nx, ny, nz;
     float res, ox, oy, oz;
     CollisionConsts coll;

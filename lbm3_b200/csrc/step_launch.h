@@ -15,6 +15,7 @@ void launchKineticEnergy(const DevLevel& g, bool flip, cudaStream_t s, double* o
 void launchMacro(const DevLevel& g, bool flip, cudaStream_t s, float* out);
 void launchGatherF(const DevLevel& g, cudaStream_t s, float* out);
 void launchScatterF(const DevLevel& g, cudaStream_t s, const float* in);
+void launchWallForce(const DevLevel& g, int wallID, cudaStream_t s, double* out);
 void launchCollideBatch(float* f, int n, const CollisionConsts& P, float gx, float gy, float gz,
                         cudaStream_t s);
 

@@ -1,0 +1,108 @@
+"""Procedural triangle soups and binary STL I/O for static bodies.
+
+The generated surfaces stand in for the reference's CAD STLs: an axis
+aligned box (exact voxelization checks), an icosphere (flow around a sphere)
+and a 4-blade rotor.  All coordinates are in millimetres, triangles are
+float32 [n][9] arrays (ax ay az bx by bz cx cy cz) with outward normals.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import struct
+from pathlib import Path
+
+import numpy as np
+
+from . import _abi as A
+
+
+def box(lo, hi) -> np.ndarray:
+    """Closed axis-aligned box, 12 triangles."""
+    x0, y0, z0 = (float(v) for v in lo)
+    x1, y1, z1 = (float(v) for v in hi)
+    v = np.array([[x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0],
+                  [x0, y0, z1], [x1, y0, z1], [x1, y1, z1], [x0, y1, z1]], dtype=np.float64)
+    faces = [(0, 2, 1), (0, 3, 2), (4, 5, 6), (4, 6, 7), (0, 1, 5), (0, 5, 4),
+             (3, 7, 6), (3, 6, 2), (0, 4, 7), (0, 7, 3), (1, 2, 6), (1, 6, 5)]
+    return np.array([np.concatenate([v[a], v[b], v[c]]) for a, b, c in faces], dtype=np.float32)
+
+
+def icosphere(subdivisions: int, radius: float, center=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """Geodesic sphere: an icosahedron whose faces are split into 4
+    `subdivisions` times, vertices projected onto the sphere
+    (20 * 4**subdivisions triangles)."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+             (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    verts = [np.array(p, dtype=np.float64) / np.linalg.norm(p) for p in verts]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5),
+             (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdivisions):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        nxt = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nxt += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nxt
+    v = np.array(verts) * float(radius) + np.asarray(center, dtype=np.float64)
+    return np.array([np.concatenate([v[a], v[b], v[c]]) for a, b, c in faces], dtype=np.float32)
+
+
+def write_binary_stl(path, tris: np.ndarray) -> None:
+    tris = np.asarray(tris, dtype=np.float32).reshape(-1, 9)
+    with open(path, "wb") as fh:
+        fh.write(b"lbm3_b200 generated".ljust(80, b" "))
+        fh.write(struct.pack("<I", len(tris)))
+        for t in tris:
+            a, b, c = t[0:3], t[3:6], t[6:9]
+            n = np.cross(b - a, c - a)
+            ln = np.linalg.norm(n)
+            n = n / ln if ln > 0 else n
+            fh.write(struct.pack("<3f", *n))
+            fh.write(t.astype("<f4").tobytes())
+            fh.write(b"\0\0")
+
+
+def read_binary_stl(path) -> np.ndarray:
+    """Binary STL reader (readSTL, include/STLFunctions.h:317-462); degenerate
+    triangles are kept here and dropped by the grid builder."""
+    data = Path(path).read_bytes()
+    (n,) = struct.unpack_from("<I", data, 80)
+    rec = np.frombuffer(data, dtype=np.dtype([("n", "<f4", 3), ("v", "<f4", 9), ("a", "<u2")]), count=n,
+                        offset=84)
+    return np.ascontiguousarray(rec["v"], dtype=np.float32)
+
+
+def set_bodies(case: A.LbmCase, bodies) -> A.LbmCase:
+    """Attach static bodies to a case.  `bodies` is a list of triangle arrays
+    or (triangles, motion_dict) pairs; the body index is its wallID.  The
+    arrays are kept alive on the case object."""
+    if len(bodies) > A.LBM_MAX_BODIES:
+        raise ValueError("too many bodies")
+    keep = []
+    case.body_count = len(bodies)
+    for b, item in enumerate(bodies):
+        tris, motion = (item, {}) if not isinstance(item, tuple) else item
+        arr = np.ascontiguousarray(tris, dtype=np.float32).reshape(-1, 9)
+        keep.append(arr)
+        body = case.body[b]
+        body.triangles = arr.ctypes.data_as(C.POINTER(C.c_float))
+        body.triangle_count = len(arr)
+        body.motion = motion.get("motion", A.LBM_WALL_STATIC)
+        body.axis = motion.get("axis", 2)
+        o = motion.get("origin", (0.0, 0.0, 0.0))
+        for a in range(3):
+            body.origin[a] = o[a]
+        body.radians_per_second = motion.get("radians_per_second", 0.0)
+    case._bodies = keep
+    return case

@@ -18,7 +18,9 @@ _INT_ARRAYS = {
     "row_k": A.ARRAY_ROW_K, "row_jplus": A.ARRAY_ROW_JPLUS, "row_kplus": A.ARRAY_ROW_KPLUS,
     "row_jkplus": A.ARRAY_ROW_JKPLUS, "wall_map": A.ARRAY_WALL_MAP,
     "periodic_index": A.ARRAY_PERIODIC_INDEX, "periodic_source": A.ARRAY_PERIODIC_SOURCE,
+    "wall_index": A.ARRAY_WALL_INDEX,
 }
+_UINT_ARRAYS = {"wall_data": A.ARRAY_WALL_DATA, "link_length": A.ARRAY_LINK_LENGTH}
 
 
 def _int_len(info: A.LbmGridInfo, which: int) -> int:
@@ -26,6 +28,10 @@ def _int_len(info: A.LbmGridInfo, which: int) -> int:
         return info.cell_count
     if which in (A.ARRAY_PERIODIC_INDEX, A.ARRAY_PERIODIC_SOURCE):
         return info.periodic_count
+    if which in (A.ARRAY_WALL_INDEX, A.ARRAY_WALL_DATA):
+        return info.wall_adjacent_count
+    if which == A.ARRAY_LINK_LENGTH:
+        return 7 * info.wall_adjacent_count
     return info.row_count
 
 
@@ -38,6 +44,22 @@ class Plan:
         fu = C.c_longlong()
         A.check(lib.lbm_plan_grids(C.byref(case), C.byref(self._h), C.byref(fu)))
         self.fluid_updates_per_iteration = fu.value
+        self.case = case
+
+    def uint_array(self, name: str, level: int = 0) -> np.ndarray:
+        which = _UINT_ARRAYS[name]
+        n = _int_len(self.info(level), which)
+        out = np.empty(n, dtype=np.uint32)
+        A.check(A.lib().lbm_plan_read_array(self._h, level, which, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def wall_velocity(self, level: int = 0) -> np.ndarray:
+        """[3][wallCount] wall velocity of every wall-adjacent cell (lattice units)."""
+        n = self.info(level).wall_adjacent_count
+        out = np.empty((3, n), dtype=np.float32)
+        A.check(A.lib().lbm_plan_read_array(self._h, level, A.ARRAY_WALL_VELOCITY,
+                                            out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
 
     def close(self):
         if self._h:
@@ -161,6 +183,20 @@ class Grids:
         out = C.c_double()
         A.check(A.lib().lbm_kinetic_energy(self._h, u_ref_phys, domain_length, C.byref(out)))
         return out.value
+
+    def wall_force(self, wall_id: int, reset: bool = False) -> np.ndarray:
+        """{Fx, Fy, Fz [N], Tx, Ty, Tz [N m]} on a body, averaged since the last reset."""
+        out = (C.c_double * 6)()
+        A.check(A.lib().lbm_wall_force(self._h, wall_id, int(reset), out))
+        return np.array(out[:])
+
+    def wall_force_raw(self, level: int = 0) -> np.ndarray:
+        """Per-cell force accumulators float32 [3][wallCount] (lattice units)."""
+        n = self.info(level).wall_adjacent_count
+        out = np.empty((3, n), dtype=np.float32)
+        A.check(A.lib().lbm_read_array(self._h, level, A.ARRAY_WALL_FORCE, out.ctypes.data_as(C.c_void_p),
+                                       out.nbytes))
+        return out
 
 
 def build_grids(case: A.LbmCase) -> Grids:

@@ -43,6 +43,10 @@ class OGrid(C.Structure):
         ("wallMap", _IP), ("perCount", C.c_int), ("perIndex", _IP), ("perSource", _IP),
         ("openBCCount", C.c_int), ("f", C.POINTER(C.c_float)), ("fluidUpdates", C.c_longlong),
         ("limiter", C.c_float), ("nuMultiplier", C.c_float),
+        ("gx", C.c_float), ("gy", C.c_float), ("gz", C.c_float), ("useIBB", C.c_int),
+        ("wallCount", C.c_int), ("wallIndex", _IP), ("wallData", C.POINTER(C.c_uint)),
+        ("linkLength", C.POINTER(C.c_uint)), ("wallVel", C.POINTER(C.c_float)),
+        ("wallForce", C.POINTER(C.c_float)), ("trackWallForce", C.c_int),
     ]
 
 
@@ -76,6 +80,10 @@ def lib() -> C.CDLL:
         h.oracle_macro.argtypes = [C.POINTER(OGrid), C.POINTER(C.c_float)]
         h.oracle_threads.restype = C.c_int
         h.oracle_collide_range.argtypes = [C.POINTER(OGrid), C.c_int, C.c_int]
+        h.oracle_from_tables.argtypes = [C.c_void_p, C.POINTER(OGrid), C.c_int, C.c_int] + [C.c_void_p] * 8 + \
+            [C.c_int, C.c_void_p, C.c_void_p, C.c_int] + [C.c_void_p] * 4
+        h.oracle_from_tables.restype = C.c_int
+        h.oracle_wall_force.argtypes = [C.POINTER(OGrid), C.c_int, C.POINTER(C.c_double)]
         _lib = h
     return _lib
 
@@ -127,14 +135,42 @@ def drho_u(f: np.ndarray) -> np.ndarray:
     return out
 
 
-class OracleGrid:
-    """Single-level box domain run by the oracle."""
+def _vp(a):
+    return a.ctypes.data_as(C.c_void_p)
 
-    def __init__(self, case):
+
+class OracleGrid:
+    """Single-level domain run by the oracle: built by the oracle itself for
+    box domains, or from a host plan's tables when geometry is present."""
+
+    def __init__(self, case, plan=None):
         self.g = OGrid()
-        rc = lib().oracle_build(C.cast(C.byref(case), C.c_void_p), C.byref(self.g))
+        if plan is None:
+            rc = lib().oracle_build(C.cast(C.byref(case), C.c_void_p), C.byref(self.g))
+            if rc != 0:
+                raise RuntimeError(f"oracle_build failed with status {rc}")
+            return
+        info = plan.info()
+        arrays = {k: plan.array(k) for k in ("shifter", "row_i", "row_j", "row_k", "row_jplus", "row_kplus",
+                                              "row_jkplus", "wall_map", "periodic_index", "periodic_source",
+                                              "wall_index")}
+        wd = plan.uint_array("wall_data")
+        ll = plan.uint_array("link_length")
+        wv = np.ascontiguousarray(plan.wall_velocity(), dtype=np.float32)
+        self._keep = (arrays, wd, ll, wv)
+        rc = lib().oracle_from_tables(
+            C.cast(C.byref(case), C.c_void_p), C.byref(self.g), info.cell_count, info.row_count,
+            *[_vp(arrays[k]) for k in ("shifter", "row_i", "row_j", "row_k", "row_jplus", "row_kplus",
+                                       "row_jkplus", "wall_map")],
+            info.periodic_count, _vp(arrays["periodic_index"]), _vp(arrays["periodic_source"]),
+            info.wall_adjacent_count, _vp(arrays["wall_index"]), _vp(wd), _vp(ll), _vp(wv))
         if rc != 0:
-            raise RuntimeError(f"oracle_build failed with status {rc}")
+            raise RuntimeError(f"oracle_from_tables failed with status {rc}")
+
+    def wall_force(self, wall_id: int) -> np.ndarray:
+        out = (C.c_double * 6)()
+        lib().oracle_wall_force(C.byref(self.g), wall_id, out)
+        return np.array(out[:])
 
     def close(self):
         if self.g.f:

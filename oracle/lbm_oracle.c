@@ -427,25 +427,16 @@ static int find_cell(const ogrid* g, int i, int j, int k) {
 }
 
 static void get_nbr(const ogrid* g, int cell, int nb[8]);
+static void init_info(const lbm_case* c, ogrid* g);
+static void apply_initial_condition(const lbm_case* c, ogrid* g);
 
 int oracle_build(const lbm_case* c, ogrid* g) {
     memset(g, 0, sizeof(*g));
     if (c->grid_level_count != 1) return LBM_ERR_UNSUPPORTED;
     /* initializeGridInfo (:9-64), level 0 */
-    const float* b = c->bounds;
-    g->res = c->res_global;
-    const float sres = g->res * 2.f;
-    const int snx = (int)((b[3] - b[0]) / sres), sny = (int)((b[4] - b[1]) / sres), snz = (int)((b[5] - b[2]) / sres);
-    if (snx < 1 || sny < 1 || snz < 1) return LBM_ERR_INVALID;
-    const float sox = b[0] + ((b[3] - b[0]) - (snx * sres) + sres) / 2.0f;
-    const float soy = b[1] + ((b[4] - b[1]) - (sny * sres) + sres) / 2.0f;
-    const float soz = b[2] + ((b[5] - b[2]) - (snz * sres) + sres) / 2.0f;
-    g->nx = snx * 2; g->ny = sny * 2; g->nz = snz * 2;
-    g->ox = sox - g->res * 0.5f; g->oy = soy - g->res * 0.5f; g->oz = soz - g->res * 0.5f;
-    g->dtPhys = c->dt_phys_global;
-    g->nu = (g->dtPhys * c->nu_phys) / ((g->res / 1000.f) * (g->res / 1000.f));
-    g->limiter = c->collision_limiter;
-    g->nuMultiplier = c->nu_multiplier;
+    init_info(c, g);
+    if (g->nx < 2) return LBM_ERR_INVALID;
+    const int snx = g->nx / 2, sny = g->ny / 2, snz = g->nz / 2;
 
     /* buildFinerGridBuilder from the skeleton (:66-132): every skeleton cell
      * is kept without geometry; 8 children each, then sortIJK (:204-234) */
@@ -571,15 +562,62 @@ int oracle_build(const lbm_case* c, ogrid* g) {
         g->perCount++;
     }
     g->fluidUpdates = (long long)n;
+    apply_initial_condition(c, g);
+    return 0;
+}
 
-    /* allocateFArray + applyInitialCondition (applyInitialCondition.h:8-41) */
+void oracle_free(ogrid* g) {
+    free(g->I); free(g->J); free(g->K); free(g->jPlus); free(g->kPlus); free(g->geomBits);
+    free(g->wallMarker); free(g->shifter); free(g->rowI); free(g->rowJ); free(g->rowK);
+    free(g->rowJP); free(g->rowKP); free(g->rowJKP); free(g->wallMap); free(g->perIndex);
+    free(g->perSource); free(g->f);
+    free(g->wallIndex); free(g->wallData); free(g->linkLength); free(g->wallVel); free(g->wallForce);
+    memset(g, 0, sizeof(*g));
+}
+
+
+static void init_info(const lbm_case* c, ogrid* g) {
+    const float* b = c->bounds;
+    g->res = c->res_global;
+    const float sres = g->res * 2.f;
+    const int snx = (int)((b[3] - b[0]) / sres), sny = (int)((b[4] - b[1]) / sres), snz = (int)((b[5] - b[2]) / sres);
+    const float sox = b[0] + ((b[3] - b[0]) - (snx * sres) + sres) / 2.0f;
+    const float soy = b[1] + ((b[4] - b[1]) - (sny * sres) + sres) / 2.0f;
+    const float soz = b[2] + ((b[5] - b[2]) - (snz * sres) + sres) / 2.0f;
+    g->nx = snx * 2; g->ny = sny * 2; g->nz = snz * 2;
+    g->ox = sox - g->res * 0.5f; g->oy = soy - g->res * 0.5f; g->oz = soz - g->res * 0.5f;
+    g->dtPhys = c->dt_phys_global;
+    g->nu = (g->dtPhys * c->nu_phys) / ((g->res / 1000.f) * (g->res / 1000.f));
+    g->limiter = c->collision_limiter;
+    g->nuMultiplier = c->nu_multiplier;
+    g->gx = c->gx; g->gy = c->gy; g->gz = c->gz;
+    g->useIBB = c->use_ibb;
+    g->trackWallForce = c->track_wall_force;
+}
+
+/* getCompressedIJK (include/cellFunctions.h:51-72) */
+static void get_ijk(const ogrid* g, int cell, int* i, int* j, int* k) {
+    const int shift = g->shifter[cell];
+    if (shift >= 0) { *i = g->rowI[shift]; *j = g->rowJ[shift]; *k = g->rowK[shift]; }
+    else {
+        const int ci = g->shifter[cell + shift];
+        *i = g->rowI[ci] - shift; *j = g->rowJ[ci]; *k = g->rowK[ci];
+    }
+}
+
+/* allocateFArray + applyInitialCondition (applyInitialCondition.h:8-41) */
+static void apply_initial_condition(const lbm_case* c, ogrid* g) {
+    const int n = g->cellCount;
+    free(g->f);
     g->f = (float*)malloc(sizeof(float) * 27 * (size_t)n);
 #pragma omp parallel for schedule(static)
     for (int q = 0; q < n; ++q) {
         obc bc;
         oracle_default_bc(&bc);
+        int ci, cj, ck;
+        get_ijk(g, q, &ci, &cj, &ck);
         if (c->ic_kind == LBM_IC_TAYLOR_GREEN) {
-            const float x = g->I[q] * g->res + g->ox, y = g->J[q] * g->res + g->oy, z = g->K[q] * g->res + g->oz;
+            const float x = ci * g->res + g->ox, y = cj * g->res + g->oy, z = ck * g->res + g->oz;
             const float X = x / c->tgv_length, Y = y / c->tgv_length, Z = z / c->tgv_length;
             const float u0 = c->tgv_u0;
             bc.ux = u0 * sinf(X) * cosf(Y) * cosf(Z);
@@ -598,15 +636,62 @@ int oracle_build(const lbm_case* c, ogrid* g) {
             g->f[(size_t)slot * n + nb[pre_nbr(d)]] = feq[d];
         }
     }
+}
+
+static int* copy_ints(const int* src, int n) {
+    int* d = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    if (n > 0) memcpy(d, src, sizeof(int) * (size_t)n);
+    return d;
+}
+
+int oracle_from_tables(const lbm_case* c, ogrid* g, int cellCount, int rowCount, const int* shifter,
+                       const int* rowI, const int* rowJ, const int* rowK, const int* rowJP,
+                       const int* rowKP, const int* rowJKP, const int* wallMap, int perCount,
+                       const int* perIndex, const int* perSource, int wallCount, const int* wallIndex,
+                       const unsigned* wallData, const unsigned* linkLength, const float* wallVel) {
+    memset(g, 0, sizeof(*g));
+    init_info(c, g);
+    g->cellCount = cellCount;
+    g->rowCount = rowCount;
+    g->shifter = copy_ints(shifter, cellCount);
+    g->rowI = copy_ints(rowI, rowCount); g->rowJ = copy_ints(rowJ, rowCount); g->rowK = copy_ints(rowK, rowCount);
+    g->rowJP = copy_ints(rowJP, rowCount); g->rowKP = copy_ints(rowKP, rowCount); g->rowJKP = copy_ints(rowJKP, rowCount);
+    g->wallMap = copy_ints(wallMap, cellCount);
+    g->perCount = perCount;
+    g->perIndex = copy_ints(perIndex, perCount);
+    g->perSource = copy_ints(perSource, perCount);
+    g->wallCount = wallCount;
+    g->wallIndex = copy_ints(wallIndex, wallCount);
+    g->wallData = (unsigned*)malloc(sizeof(unsigned) * (size_t)(wallCount > 0 ? wallCount : 1));
+    g->linkLength = (unsigned*)malloc(sizeof(unsigned) * 7 * (size_t)(wallCount > 0 ? wallCount : 1));
+    g->wallVel = (float*)malloc(sizeof(float) * 3 * (size_t)(wallCount > 0 ? wallCount : 1));
+    g->wallForce = (float*)calloc(3 * (size_t)(wallCount > 0 ? wallCount : 1), sizeof(float));
+    if (wallCount > 0) {
+        memcpy(g->wallData, wallData, sizeof(unsigned) * (size_t)wallCount);
+        memcpy(g->linkLength, linkLength, sizeof(unsigned) * 7 * (size_t)wallCount);
+        memcpy(g->wallVel, wallVel, sizeof(float) * 3 * (size_t)wallCount);
+    }
+    long long walls = 0;
+    for (int q = 0; q < cellCount; ++q) walls += g->wallMap[q] == -3;
+    g->fluidUpdates = (long long)cellCount - walls;
+    apply_initial_condition(c, g);
     return 0;
 }
 
-void oracle_free(ogrid* g) {
-    free(g->I); free(g->J); free(g->K); free(g->jPlus); free(g->kPlus); free(g->geomBits);
-    free(g->wallMarker); free(g->shifter); free(g->rowI); free(g->rowJ); free(g->rowK);
-    free(g->rowJP); free(g->rowKP); free(g->rowJKP); free(g->wallMap); free(g->perIndex);
-    free(g->perSource); free(g->f);
-    memset(g, 0, sizeof(*g));
+void oracle_wall_force(const ogrid* g, int wallID, double* out) {
+    for (int q = 0; q < 6; ++q) out[q] = 0.0;
+    for (int w = 0; w < g->wallCount; ++w) {
+        if ((int)((g->wallData[w] >> 27) & 31u) != wallID) continue;
+        int ci, cj, ck;
+        get_ijk(g, g->wallIndex[w], &ci, &cj, &ck);
+        const double x = (double)(ci * g->res + g->ox), y = (double)(cj * g->res + g->oy),
+                     z = (double)(ck * g->res + g->oz);
+        const double fx = g->wallForce[w], fy = g->wallForce[g->wallCount + w], fz = g->wallForce[2 * g->wallCount + w];
+        out[0] += fx; out[1] += fy; out[2] += fz;
+        out[3] += y * fz - z * fy;
+        out[4] += z * fx - x * fz;
+        out[5] += x * fy - y * fx;
+    }
 }
 
 /* getCompressedNBR + finishNBRPlus (include/cellFunctions.h:74-94,
@@ -639,7 +724,8 @@ void oracle_step(ogrid* g, int steps) {
         /* K1: cell lambda (:51-177) */
 #pragma omp parallel for schedule(static)
         for (int cell = 0; cell < g->cellCount; ++cell) {
-            if (g->wallMap[cell] == -3) continue;
+            const int wm = g->wallMap[cell];
+            if (wm == -3) continue;
             int nb[8];
             get_nbr(g, cell, nb);
             float f[27];
@@ -649,10 +735,72 @@ void oracle_step(ogrid* g, int steps) {
             float m[4];
             oracle_get_drho_u(f, m);
             bc.dRho = m[0]; bc.ux = m[1]; bc.uy = m[2]; bc.uz = m[3];
+            unsigned wallData = 0u;
+            if (wm >= 0) {
+                wallData = g->wallData[wm];
+                bc.wallID = (int)((wallData >> 27) & 31u);
+            }
+            /* getLocalBC: limiter, forcing, IBB switch and the wall velocity */
             bc.collisionLimiter = g->limiter;
             bc.nuMultiplier = g->nuMultiplier;
+            bc.gx = g->gx; bc.gy = g->gy; bc.gz = g->gz;
+            bc.useIBB = g->useIBB;
+            if (wm >= 0) {
+                bc.ux = g->wallVel[wm];
+                bc.uy = g->wallVel[g->wallCount + wm];
+                bc.uz = g->wallVel[2 * g->wallCount + wm];
+            }
             oracle_apply_collision(f, &bc, g->nu);
-            for (int d = 0; d < 27; ++d) g->f[(size_t)(flip ? d : INV[d]) * n + nb[post_nbr(d)]] = f[d];
+            if (wm < 0) {
+                for (int d = 0; d < 27; ++d) g->f[(size_t)(flip ? d : INV[d]) * n + nb[post_nbr(d)]] = f[d];
+                continue;
+            }
+            /* applyIBB (interpolatedBouncebackFunctions.h:43-157) */
+            float dr[4];
+            oracle_get_drho_u(f, dr);
+            float res[27];
+            for (int d = 0; d < 27; ++d) res[d] = f[d];
+            float gxw = 0.f, gyw = 0.f, gzw = 0.f;
+            int linkIndex = 0;
+            unsigned code = 0u;
+            for (int d = 1; d < 27; ++d) {
+                if (!(wallData & (1u << d))) continue;
+                const int id = INV[d];
+                const float eiDotFi = (float)CX[id] * bc.ux + (float)CY[id] * bc.uy + (float)CZ[id] * bc.uz;
+                const float wallTerm = 6.f * W[id] * (1.f + dr[0]) * eiDotFi;
+                float gamma = 0.5f;
+                if (bc.useIBB) {
+                    if (linkIndex % 4 == 0) code = g->linkLength[(size_t)(linkIndex / 4) * g->wallCount + wm];
+                    const unsigned c8 = (code >> (8 * (linkIndex % 4))) & 255u;
+                    gamma = (float)c8 / 254.f;
+                    if (gamma < 0.01f) gamma = 0.01f;
+                    if (gamma > 1.f) gamma = 1.f;
+                    ++linkIndex;
+                }
+                const float fPre = g->f[(size_t)(flip ? INV[d] : d) * n + nb[pre_nbr(d)]];
+                const float invDen = 1.f / (1.f + gamma);
+                const float r = ((1.f - gamma) * invDen) * fPre + (gamma * invDen) * f[id] +
+                                (gamma * invDen) * f[d] + invDen * wallTerm;
+                gxw += -(f[d]) * (CX[d] - bc.ux) + (r) * (CX[id] - bc.ux);
+                gyw += -(f[d]) * (CY[d] - bc.uy) + (r) * (CY[id] - bc.uy);
+                gzw += -(f[d]) * (CZ[d] - bc.uz) + (r) * (CZ[id] - bc.uz);
+                res[d] = r;
+            }
+            /* writes (updateGrid.h:150-170) */
+            for (int d = 0; d < 27; ++d) {
+                const int linked = d != 0 && (wallData & (1u << d));
+                if (linked) {
+                    /* next pre-collision slot of the inverse direction */
+                    g->f[(size_t)(flip ? INV[d] : d) * n + nb[post_nbr(d)]] = res[d];
+                } else {
+                    g->f[(size_t)(flip ? d : INV[d]) * n + nb[post_nbr(d)]] = res[d];
+                }
+            }
+            if (g->trackWallForce && !(wallData & 1u)) {
+                g->wallForce[wm] += gxw;
+                g->wallForce[g->wallCount + wm] += gyw;
+                g->wallForce[2 * g->wallCount + wm] += gzw;
+            }
         }
         /* applyStreaming (esotwistStreamingFunctions.h:6-9) */
         g->flip = !flip;
@@ -703,6 +851,7 @@ double oracle_kinetic_energy(const ogrid* g, float uRefPhys, float domainLength)
     for (int cell = 0; cell < g->cellCount; ++cell) {
         const int wm = g->wallMap[cell];
         if (wm == -3 || wm == -2) continue;
+        if (wm >= 0 && (g->wallData[wm] & 1u)) continue;
         int nb[8];
         get_nbr(g, cell, nb);
         float f[27], m[4];

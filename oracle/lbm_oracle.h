@@ -66,12 +66,33 @@ typedef struct ogrid {
     long long fluidUpdates;
     /* uniform getLocalBC */
     float limiter, nuMultiplier;
+    float gx, gy, gz;
+    int useIBB;
+    /* wall-adjacent cells */
+    int wallCount;
+    int *wallIndex;
+    unsigned *wallData, *linkLength; /* linkLength [7][wallCount] */
+    float *wallVel;                  /* [3][wallCount] */
+    float *wallForce;                /* [3][wallCount] */
+    int trackWallForce;
 } ogrid;
 
 /* buildGrids for a box domain without geometry, single level, followed by
  * applyInitialCondition.  Returns 0 or a negative LBM_ERR_* code. */
 int oracle_build(const lbm_case* c, ogrid* g);
 void oracle_free(ogrid* g);
+
+/* Single-level grid from tables built elsewhere (the product's host plan),
+ * followed by applyInitialCondition.  Arrays are copied. */
+int oracle_from_tables(const lbm_case* c, ogrid* g, int cellCount, int rowCount, const int* shifter,
+                       const int* rowI, const int* rowJ, const int* rowK, const int* rowJP,
+                       const int* rowKP, const int* rowJKP, const int* wallMap, int perCount,
+                       const int* perIndex, const int* perSource, int wallCount, const int* wallIndex,
+                       const unsigned* wallData, const unsigned* linkLength, const float* wallVel);
+
+/* Σ g and Σ r x g (lattice units, FP64) over the wall-adjacent cells of
+ * one wallID: out[6]. */
+void oracle_wall_force(const ogrid* g, int wallID, double* out);
 
 /* updateSingleGrid (include/updateGrid.h:16-386) `steps` times. */
 void oracle_step(ogrid* g, int steps);

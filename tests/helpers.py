@@ -25,3 +25,15 @@ def field_errors(got: np.ndarray, ref: np.ndarray):
     e_rho = rel_l2(got[0], ref[0])
     e_u = rel_l2(got[1:4].reshape(-1), ref[1:4].reshape(-1))
     return e_rho, e_u
+
+
+def plan_ijk(plan, level: int = 0):
+    """(i, j, k) of every cell, decoded from the compressed rows
+    (getCompressedIJK, include/cellFunctions.h:51-72)."""
+    sh = plan.array("shifter", level)
+    ri, rj, rk = plan.array("row_i", level), plan.array("row_j", level), plan.array("row_k", level)
+    idx = np.arange(len(sh))
+    head = np.where(sh >= 0, idx, idx + sh)
+    row = sh[head]
+    off = idx - head
+    return ri[row] + off, rj[row], rk[row]
