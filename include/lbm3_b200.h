@@ -80,6 +80,12 @@ extern "C" {
                                      accumulated since the last tracker reset   */
 #define LBM_ARRAY_WALL_VELOCITY 16 /* float [3][wallAdjacentCount] wall velocity the
                                      body motion gives each wall-adjacent cell   */
+#define LBM_ARRAY_OPEN_INDEX   17 /* int32  [openBCCount]   openBCs[id].indexArray of all
+                                     IDs concatenated in ID order               */
+#define LBM_ARRAY_OPEN_SOURCE  18 /* int32  [openBCCount]   openBCs[id].sourceArray, same order */
+#define LBM_ARRAY_OPEN_REFERENCE 19 /* float [2][openBCCount] dRhoRefArray, uNormalRefArray */
+#define LBM_ARRAY_OPEN_CUMULATIVE 20 /* float [2][openBCCount] dRhoCumulativeArray,
+                                     uNormalCumulativeArray since the last tracker reset */
 
 /* ---- case description -------------------------------------------------- */
 
@@ -184,7 +190,9 @@ int lbm_plan_grids(const lbm_case* c, lbm_plan** out, long long* fluid_updates_p
 void lbm_free_plan(lbm_plan* p);
 int lbm_plan_level_count(lbm_plan* p);
 int lbm_plan_info(lbm_plan* p, int level, lbm_grid_info* out);
-/* Same array ids as lbm_read_array except LBM_ARRAY_F and LBM_ARRAY_MACRO. */
+/* Same array ids as lbm_read_array except the device state: LBM_ARRAY_F,
+ * LBM_ARRAY_MACRO, LBM_ARRAY_WALL_FORCE, LBM_ARRAY_OPEN_REFERENCE and
+ * LBM_ARRAY_OPEN_CUMULATIVE. */
 int lbm_plan_read_array(lbm_plan* p, int level, int which, void* host, size_t bytes);
 
 /* Build every grid level on the current CUDA device, allocate the populations
@@ -245,6 +253,18 @@ int lbm_kinetic_energy(lbm_grids* g, float u_ref_phys, float domain_length,
  * the coordinate origin.  `reset` != 0 zeroes the accumulators afterwards.
  * Replaces the wall branch of updateTracker (include/trackerFunctions.h:366-497). */
 int lbm_wall_force(lbm_grids* g, int wall_id, int reset, double* out);
+
+/* Flow through one open boundary (openBCID), from the sums the open-boundary
+ * update accumulates while the case's track_open_boundaries is set, averaged
+ * over the steps since the last tracker reset and converted to SI units:
+ * out = {area [m^2], area-averaged normal velocity [m/s], mass flow [kg/s],
+ * momentum thrust [N], area-averaged pressure [Pa], pressure power [W],
+ * normal kinetic power [W]}; the normal is the outer normal.  Sums are FP64
+ * on the device.  `reset` != 0 then resets every tracker accumulator of the
+ * grids (wall forces and open-boundary sums), as updateTracker does.
+ * Replaces the open-boundary branch of updateTracker
+ * (include/trackerFunctions.h:127-214). */
+int lbm_open_boundary_flow(lbm_grids* g, int open_bc_id, int reset, double* out);
 
 /* Cell-wise collision on a device batch of shifted populations laid out as
  * float [27][n] (structure of arrays), in place.

@@ -70,6 +70,10 @@ ARRAY_WALL_DATA = 13
 ARRAY_LINK_LENGTH = 14
 ARRAY_WALL_FORCE = 15
 ARRAY_WALL_VELOCITY = 16
+ARRAY_OPEN_INDEX = 17
+ARRAY_OPEN_SOURCE = 18
+ARRAY_OPEN_REFERENCE = 19
+ARRAY_OPEN_CUMULATIVE = 20
 LBM_ERR_DEVICE_WAIT = -7
 
 
@@ -135,6 +139,7 @@ SIGNATURES = [
     ("lbm_write_f", C.c_int, [_P, C.c_int, _P, C.c_size_t]),
     ("lbm_kinetic_energy", C.c_int, [_P, C.c_float, C.c_float, C.POINTER(C.c_double)]),
     ("lbm_wall_force", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    ("lbm_open_boundary_flow", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     ("lbm_apply_collision_batch", C.c_int,
      [_P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, _P]),
 ]

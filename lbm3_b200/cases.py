@@ -129,3 +129,83 @@ def periodic_box(nx: int, ny: int, nz: int, nu_lattice: float = 0.01, ux: float 
     c.ic_ux, c.ic_uy, c.ic_uz = ux, uy, uz
     c.storage = storage
     return c
+
+
+def open_channel(nx: int, ny: int, nz: int, u_in: float = 0.04, nu_lattice: float = 0.01,
+                 sides: str = "velocity", outlet_non_reflective: bool = True, inlet_non_reflective: bool = False,
+                 beta: float = 7.0, collision_limiter: float = 0.1, storage: int = A.LBM_STORE_F32) -> A.LbmCase:
+    """Channel along x with nx*ny*nz cells (boundary layers included), 1 mm
+    cells, uniform initial flow u_in.
+
+    Faces follow the reference's flow-around-sphere driver
+    (cases/flowAroundSphere/flowAroundSphereMain.cu:104-134): velocity inlet
+    at x = 0 (openBCID 0), pressure outlet dRho = 0 at x = nx-1 (openBCID 1,
+    non-reflective), and on the four sides either a strict velocity boundary
+    u = (u_in, 0, 0) that also owns every edge and corner (``sides =
+    "velocity"``, openBCID 2) or periodic faces (``sides = "periodic"``).
+    The time step is chosen so that u_in is 1 m/s.
+    """
+    if nx % 2 or ny % 2 or nz % 2:
+        raise ValueError("cell counts must be even")
+    c = _blank_case()
+    res = f32(1.0)
+    c.res_global = res
+    dt = f32(f32(u_in) * f32(res / f32(1000.0)))  # u_in lattice == 1 m/s
+    c.dt_phys_global = dt
+    r = float(res) / 1000.0
+    c.nu_phys = f32(float(nu_lattice) * r * r / float(dt))
+    eps = f32(1e-3)
+    for a, n in enumerate((nx, ny, nz)):
+        c.bounds[a] = -eps
+        c.bounds[a + 3] = f32(n) + eps
+    c.face[A.FACE_XMIN] = _face(A.LBM_BC_VELOCITY, open_bc_id=0, priority=1,
+                                    non_reflective=inlet_non_reflective, beta=beta, ux=u_in)
+    c.face[A.FACE_XMAX] = _face(A.LBM_BC_PRESSURE, open_bc_id=1, priority=1,
+                                    non_reflective=outlet_non_reflective, beta=beta, dRho=0.0)
+    for f in (A.FACE_YMIN, A.FACE_YMAX, A.FACE_ZMIN, A.FACE_ZMAX):
+        if sides == "velocity":
+            c.face[f] = _face(A.LBM_BC_VELOCITY, open_bc_id=2, priority=2, ux=u_in)
+        elif sides == "periodic":
+            c.face[f] = _face(A.LBM_BC_PERIODIC, priority=0)
+        else:
+            raise ValueError("sides must be 'velocity' or 'periodic'")
+    c.ic_kind = A.LBM_IC_UNIFORM
+    c.ic_ux = u_in
+    c.collision_limiter = collision_limiter
+    c.track_open_boundaries = 1
+    c.storage = storage
+    return c
+
+
+@dataclass
+class SphereSetup:
+    """Flow around a sphere: the case and what the drag coefficient needs."""
+    case: A.LbmCase
+    diameter_cells: float
+    u_lattice: float
+    u_phys: float            # m/s
+    rho_phys: float          # kg/m^3
+    diameter_m: float
+
+    def drag_coefficient(self, fx: float) -> float:
+        """Cd from the tracked x force, which acts on the fluid: drag = -Fx
+        (cases/flowAroundSphere/flowAroundSphereMain.cu:212-213)."""
+        area = math.pi * self.diameter_m ** 2 / 4.0
+        return -fx / (0.5 * self.rho_phys * self.u_phys ** 2 * area)
+
+
+def flow_around_sphere(nx: int = 256, ny: int = 128, nz: int = 128, diameter: float = 24.0,
+                       center=(64.0, 64.0, 64.0), u_in: float = 0.04, nu_lattice: float = 0.0096,
+                       subdivisions: int = 5, storage: int = A.LBM_STORE_F32,
+                       sides: str = "velocity") -> SphereSetup:
+    """Single-level flow around an icosphere (20 * 4**subdivisions triangles)
+    of `diameter` cells centred at `center` (cell units, cell i spans
+    [i, i+1)), in an open channel (see :func:`open_channel`), Re = u_in D / nu.
+    The body is treated with interpolated bounceback and its force tracked."""
+    from .geometry import icosphere, set_bodies
+    c = open_channel(nx, ny, nz, u_in=u_in, nu_lattice=nu_lattice, sides=sides, storage=storage)
+    c.track_wall_force = 1
+    c.use_ibb = 1
+    tris = icosphere(subdivisions, 0.5 * diameter, center)
+    set_bodies(c, [tris])
+    return SphereSetup(c, float(diameter), float(u_in), 1.0, float(c.rho_phys), float(diameter) / 1000.0)

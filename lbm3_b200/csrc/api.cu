@@ -3,6 +3,7 @@
 // failure into a status code plus a thread-local message.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <exception>
@@ -73,6 +74,8 @@ struct LevelState {
     int wallCellCount = 0;
     int wallAdjacentCount = 0;
     int openBCCount = 0;
+    std::vector<int> openTrackCount;   // trackFlowCount per openBCID
+    int* obSource = nullptr;           // openBCs[id].sourceArray, concatenated
     unsigned long long memBytes = 0;
     lbm::DevLevel dev{};
     std::vector<void*> owned;
@@ -151,7 +154,8 @@ void fillInfo(const lbm::HostLevel& H, int storage, lbm_grid_info* out) {
 
 namespace {
 
-// updateSingleGrid (include/updateGrid.h:16-386): K1, flip, periodic copy.
+// updateSingleGrid (include/updateGrid.h:16-386): K1, flip, open boundary,
+// periodic copy.
 void updateSingleGrid(lbm_grids* g, LevelState& L) {
     const bool flip = L.info.esotwistFlipper;
     if (g->timingKernels) {
@@ -164,6 +168,7 @@ void updateSingleGrid(lbm_grids* g, LevelState& L) {
         lbm::launchCollideStream(L.dev, flip, g->stream);
     }
     L.info.esotwistFlipper = !flip;  // applyStreaming
+    lbm::launchOpenBoundary(L.dev, L.info.esotwistFlipper, g->stream, L.info.iterationsFinished);
     lbm::launchPeriodic(L.dev, L.info.esotwistFlipper, g->stream);
     L.info.iterationsFinished++;
     L.iterationsSinceTrackerReset++;
@@ -262,6 +267,11 @@ int lbm_plan_read_array(lbm_plan* p, int level, int which, void* host, size_t by
     const lbm::HostLevel& H = p->host.levels[level];
     const std::vector<int>* v = nullptr;
     const std::vector<uint32_t>* u = nullptr;
+    std::vector<int> openIndex, openSource;
+    for (const auto& ob : H.openBCs) {
+        openIndex.insert(openIndex.end(), ob.index.begin(), ob.index.end());
+        openSource.insert(openSource.end(), ob.source.begin(), ob.source.end());
+    }
     if (which == LBM_ARRAY_WALL_VELOCITY) {
         const size_t need = H.wallVelocity.size() * sizeof(float);
         if (bytes != need) return fail(LBM_ERR_INVALID, "lbm_plan_read_array: byte count does not match array size");
@@ -280,6 +290,8 @@ int lbm_plan_read_array(lbm_plan* p, int level, int which, void* host, size_t by
         case LBM_ARRAY_PERIODIC_INDEX: v = &H.perIndex; break;
         case LBM_ARRAY_PERIODIC_SOURCE: v = &H.perSource; break;
         case LBM_ARRAY_WALL_INDEX: v = &H.wallIndex; break;
+        case LBM_ARRAY_OPEN_INDEX: v = &openIndex; break;
+        case LBM_ARRAY_OPEN_SOURCE: v = &openSource; break;
         case LBM_ARRAY_WALL_DATA: u = &H.wallData; break;
         case LBM_ARRAY_LINK_LENGTH: u = &H.linkLength; break;
         default: return fail(LBM_ERR_INVALID, "lbm_plan_read_array: array not available in a plan");
@@ -326,11 +338,10 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
             L.wallCellCount = H.wallCellCount;
             L.wallAdjacentCount = H.wallAdjacentCount;
             L.openBCCount = 0;
-            for (const auto& ob : H.openBCs) L.openBCCount += static_cast<int>(ob.index.size());
-            if (L.openBCCount > 0)
-                throw std::invalid_argument(
-                    "open (velocity/pressure) boundaries are not available in this build; "
-                    "use periodic faces");
+            for (const auto& ob : H.openBCs) {
+                L.openBCCount += static_cast<int>(ob.index.size());
+                L.openTrackCount.push_back(ob.trackFlowCount);
+            }
             const long long n = H.info.cellCount;
             lbm::DevLevel& d = L.dev;
             d.cellCount = H.info.cellCount;
@@ -370,6 +381,34 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
             d.wallVel = own(upload(H.wallVelocity, s));
             d.wallForce = own(devAlloc<float>(3 * H.wallIndex.size()));
             if (d.wallForce) ck(cudaMemsetAsync(d.wallForce, 0, 3 * H.wallIndex.size() * sizeof(float), s), "memset");
+            {
+                // open boundaries: per-cell records in ID order; the two
+                // reference and two cumulative arrays are contiguous pairs
+                const size_t m = H.openCells.size();
+                std::vector<int> cell(m), info(m), source;
+                std::vector<float4> target(m);
+                std::vector<float> beta(m);
+                for (size_t q = 0; q < m; ++q) {
+                    const lbm::OpenBCCell& oc = H.openCells[q];
+                    cell[q] = oc.cell;
+                    info[q] = oc.info;
+                    target[q] = make_float4(oc.dRho, oc.ux, oc.uy, oc.uz);
+                    beta[q] = oc.beta;
+                }
+                for (const auto& ob : H.openBCs) source.insert(source.end(), ob.source.begin(), ob.source.end());
+                d.obCount = static_cast<int>(m);
+                d.obCell = own(upload(cell, s));
+                d.obInfo = own(upload(info, s));
+                d.obTarget = own(upload(target, s));
+                d.obBeta = own(upload(beta, s));
+                L.obSource = own(upload(source, s));
+                d.obRhoRef = own(devAlloc<float>(2 * m));
+                d.obUnRef = d.obRhoRef ? d.obRhoRef + m : nullptr;
+                d.obRhoCum = own(devAlloc<float>(2 * m));
+                d.obUnCum = d.obRhoCum ? d.obRhoCum + m : nullptr;
+                if (m) ck(cudaMemsetAsync(d.obRhoCum, 0, 2 * m * sizeof(float), s), "memset");
+                d.trackOpen = c->track_open_boundaries ? 1 : 0;
+            }
             d.trackWallForce = c->track_wall_force ? 1 : 0;
             d.useIBB = c->use_ibb ? 1 : 0;
             d.gx = c->gx;
@@ -399,6 +438,8 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
             } else {
                 lbm::launchInit(d, L.info.esotwistFlipper, s, nullptr, uni);
             }
+            // reference values of the open boundary from the initial state
+            lbm::launchOpenBoundaryInit(d, L.info.esotwistFlipper, s);
             ck(cudaGetLastError(), "init launch");
         }
         ck(cudaStreamSynchronize(s), "build sync");
@@ -541,6 +582,10 @@ int lbm_read_array(lbm_grids* g, int level, int which, void* host, size_t bytes)
         case LBM_ARRAY_LINK_LENGTH: src = d.linkLength; need = size_t(d.wallCount) * 7 * 4; break;
         case LBM_ARRAY_WALL_FORCE: src = d.wallForce; need = size_t(d.wallCount) * 3 * 4; break;
         case LBM_ARRAY_WALL_VELOCITY: src = d.wallVel; need = size_t(d.wallCount) * 3 * 4; break;
+        case LBM_ARRAY_OPEN_INDEX: src = d.obCell; need = size_t(d.obCount) * 4; break;
+        case LBM_ARRAY_OPEN_SOURCE: src = L.obSource; need = size_t(d.obCount) * 4; break;
+        case LBM_ARRAY_OPEN_REFERENCE: src = d.obRhoRef; need = size_t(d.obCount) * 2 * 4; break;
+        case LBM_ARRAY_OPEN_CUMULATIVE: src = d.obRhoCum; need = size_t(d.obCount) * 2 * 4; break;
         case LBM_ARRAY_F: need = 27 * n * 4; break;
         case LBM_ARRAY_MACRO: need = 4 * n * 4; break;
         default: return fail(LBM_ERR_INVALID, "lbm_read_array: unknown array id");
@@ -591,6 +636,17 @@ int lbm_write_f(lbm_grids* g, int level, const float* host, size_t bytes) {
     });
 }
 
+// Zero every tracker accumulator of every level (trackerFunctions.h:474-497).
+static void resetTracker(lbm_grids* g) {
+    for (LevelState& L : g->levels) {
+        const lbm::DevLevel& d = L.dev;
+        if (d.wallForce) ck(cudaMemsetAsync(d.wallForce, 0, 3 * size_t(d.wallCount) * sizeof(float), g->stream), "memset");
+        if (d.obRhoCum) ck(cudaMemsetAsync(d.obRhoCum, 0, 2 * size_t(d.obCount) * sizeof(float), g->stream), "memset");
+        L.iterationsSinceTrackerReset = 0;
+    }
+    ck(cudaStreamSynchronize(g->stream), "sync");
+}
+
 int lbm_kinetic_energy(lbm_grids* g, float uRefPhys, float domainLength, double* out) {
     if (!g || !out) return fail(LBM_ERR_INVALID, "lbm_kinetic_energy: bad argument");
     return guarded("lbm_kinetic_energy", [&] {
@@ -629,15 +685,50 @@ int lbm_wall_force(lbm_grids* g, int wallID, int reset, double* out) {
             const double conv = double(g->c.rho_phys) * rm * rm * rm * rm / (double(L.info.dtPhys) * L.info.dtPhys);
             for (int q = 0; q < 3; ++q) acc[q] += r[q] / span * conv;
             for (int q = 3; q < 6; ++q) acc[q] += r[q] / span * conv * 0.001;
-            if (reset) {
-                if (L.dev.wallForce)
-                    ck(cudaMemsetAsync(L.dev.wallForce, 0, 3 * size_t(L.dev.wallCount) * sizeof(float), g->stream),
-                       "memset");
-                L.iterationsSinceTrackerReset = 0;
-            }
         }
-        if (reset) ck(cudaStreamSynchronize(g->stream), "sync");
+        if (reset) resetTracker(g);
         for (int q = 0; q < 6; ++q) out[q] = acc[q];
+    });
+}
+
+int lbm_open_boundary_flow(lbm_grids* g, int openBCID, int reset, double* out) {
+    if (!g || !out || openBCID < 0) return fail(LBM_ERR_INVALID, "lbm_open_boundary_flow: bad argument");
+    return guarded("lbm_open_boundary_flow", [&] {
+        double area = 0.0, acc[6] = {0, 0, 0, 0, 0, 0};
+        bool found = false;
+        for (LevelState& L : g->levels) {
+            if (openBCID >= static_cast<int>(L.openTrackCount.size())) continue;
+            found = true;
+            ck(cudaMemsetAsync(g->scratch, 0, 6 * sizeof(double), g->stream), "memset");
+            const double span = L.iterationsSinceTrackerReset > 0 ? L.iterationsSinceTrackerReset : 1;
+            lbm::launchOpenFlow(L.dev, openBCID, static_cast<float>(1.0 / span), g->stream, g->scratch);
+            ck(cudaGetLastError(), "flow launch");
+            double r[6];
+            ck(cudaMemcpyAsync(r, g->scratch, sizeof(r), cudaMemcpyDeviceToHost, g->stream), "copy");
+            ck(cudaStreamSynchronize(g->stream), "sync");
+            // unit conversion of updateTracker (include/trackerFunctions.h:176-186)
+            const double cellArea = (double(L.info.res) / 1000.0) * (double(L.info.res) / 1000.0);
+            const double v = (double(L.info.res) / 1000.0) / double(L.info.dtPhys);
+            const double rho = g->c.rho_phys;
+            const double cs = v / std::sqrt(3.0);
+            const double p = rho * cs * cs;  // convertToPhysicalPressure
+            acc[0] += r[0] * cellArea * v;
+            acc[1] += r[1] * cellArea * v * rho;
+            acc[2] += r[2] * cellArea * v * v * rho;
+            acc[3] += r[3] * p * cellArea;
+            acc[4] += r[4] * p * cellArea * v;
+            acc[5] += r[5] * cellArea * v * v * v * rho;
+            area += L.openTrackCount[openBCID] * cellArea;
+        }
+        if (!found) throw std::invalid_argument("no open boundary with this ID");
+        out[0] = area;
+        out[1] = area > 0 ? acc[0] / area : 0.0;
+        out[2] = acc[1];
+        out[3] = acc[2];
+        out[4] = area > 0 ? acc[3] / area : 0.0;
+        out[5] = acc[4];
+        out[6] = acc[5];
+        if (reset) resetTracker(g);
     });
 }
 

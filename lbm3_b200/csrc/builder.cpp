@@ -9,6 +9,7 @@
 // column instead of bin + insertion sort.  The resulting tables are the same
 // as the reference's (the oracle checks them element by element).
 #include "builder.h"
+#include "mbbc_tables.h"
 #include "geometry.h"
 #include "lattice.h"
 
@@ -343,6 +344,38 @@ void buildBoundaryLists(const lbm_case& c, HostLevel& L) {
             ob.source[q] = src;
         }
     }
+    // per-cell records for the open-boundary kernel (include/updateGrid.h:183-355)
+    L.openCells.clear();
+    for (const auto& ob : L.openBCs)
+        for (size_t q = 0; q < ob.index.size(); ++q) {
+            const int cidx = ob.index[q];
+            const int i = L.I[cidx], j = L.J[cidx], k = L.K[cidx];
+            const int onx = i == 0 ? -1 : (i == in.nx - 1 ? 1 : 0);
+            const int ony = j == 0 ? -1 : (j == in.ny - 1 ? 1 : 0);
+            const int onz = k == 0 ? -1 : (k == in.nz - 1 ? 1 : 0);
+            const BC bc = evalOpenBC(c, in, i, j, k);
+            // non-reflectivity is defined for face cells only (:262-265)
+            const bool nonRefl = bc.nonReflective && (std::abs(onx) + std::abs(ony) + std::abs(onz) == 1);
+            int kind = bc.dirichletRho ? 2 : (bc.dirichletU ? 1 : 0);
+            const int wm = L.wallMap[cidx];
+            bool track = wm != -2;
+            if (wm >= 0 && (L.wallData[wm] & 1u)) track = false;
+            const int code = (onx + 5) * 100 + (ony + 5) * 10 + (onz + 5);
+            int row = -1;
+            for (int t = 0; t < LBM_MBBC_NORMALS; ++t)
+                if (kLbmMbbc[t].code == code) row = t;
+            if (row < 0) throw std::logic_error("open boundary cell without an outer normal");
+            OpenBCCell oc;
+            oc.cell = cidx;
+            oc.info = kind | (nonRefl ? 4 : 0) | ((onx + 1) << 3) | ((ony + 1) << 5) | ((onz + 1) << 7) |
+                      (track ? 512 : 0) | (row << 10) | (ob.openBCID << 16);
+            oc.dRho = bc.dRho;
+            oc.ux = bc.ux;
+            oc.uy = bc.uy;
+            oc.uz = bc.uz;
+            oc.beta = bc.nonReflectiveBeta;
+            L.openCells.push_back(oc);
+        }
 
     // Periodic ghost lists (:1486-1564).
     L.perIndex.clear();

@@ -41,6 +41,16 @@ struct OpenBCList {
     int trackFlowCount = 0;
 };
 
+// What the open-boundary kernel needs per boundary cell: getOpenBC of the
+// cell resolved at setup.  info bits: 0-1 kind (1 velocity, 2 pressure),
+// 2 non-reflective, 3-8 outer normal (nx+1, ny+1, nz+1 in 2 bits each),
+// 9 track flow, 10-14 row of the normal in the boundary tables, 16-31 openBCID.
+struct OpenBCCell {
+    int cell;
+    int info;
+    float dRho, ux, uy, uz, beta;
+};
+
 struct HostLevel {
     Info info;
     // builder view: sorted full IJK of the kept cells
@@ -55,6 +65,7 @@ struct HostLevel {
     // periodic ghost copies (PeriodicBCStruct)
     std::vector<int> perIndex, perSource;
     std::vector<OpenBCList> openBCs;
+    std::vector<OpenBCCell> openCells;   // all IDs, in ID then cell order
     int wallCellCount = 0;
     int wallAdjacentCount = 0;
     // wall-adjacent fluid cells (WallStruct, include/types.h:202-204)

@@ -2,6 +2,7 @@
 //
 //   collideStream  K1: fused read -> cumulant collision -> esotwist write
 //                  (updateSingleGrid cell lambda, include/updateGrid.h:51-178)
+//   openBoundary   K2: moment-based open boundary on the streamed state (:181-355)
 //   periodicCopy   K3: ghost <- interior pre-collision copy (:358-382)
 //   initFeq        equilibrium initial condition (applyInitialCondition.h:23-41)
 //   kineticEnergy  FP64 reduction of the Taylor–Green driver's energy
@@ -15,6 +16,7 @@
 // exactly one thread per step, so the kernel needs no second buffer and no
 // synchronisation between cells.
 #include "builder.h"
+#include "mbbc.h"
 #include "step_launch.h"
 
 #include <cuda_runtime.h>
@@ -408,6 +410,39 @@ __global__ void __launch_bounds__(kBlock) wallForceSum(DevLevel g, int wallID, d
     }
 }
 
+// Flow sums of one open boundary from the cumulative arrays
+// (include/trackerFunctions.h:143-172): per cell, in FP32 as the reference
+// forms them, {uN, rho uN, rho uN |uN|, dRho, dRho uN, rho uN^3 / 2}; summed
+// in FP64 into out[6].
+__global__ void __launch_bounds__(kBlock) openFlowSum(DevLevel g, int openBCID, float invSpan, double* out) {
+    __shared__ double part[6][kBlock / 32];
+    const int idx = blockIdx.x * kBlock + threadIdx.x;
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    if (idx < g.obCount && (__ldg(g.obInfo + idx) >> 16) == openBCID) {
+        const float dRho = g.obRhoCum[idx] * invSpan;
+        const float uN = g.obUnCum[idx] * invSpan;
+        const float rho = 1.0f + dRho;
+        v[0] = uN;
+        v[1] = rho * uN;
+        v[2] = rho * uN * fabsf(uN);
+        v[3] = dRho;
+        v[4] = dRho * uN;
+        v[5] = 0.5f * rho * uN * uN * uN;
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        double a = v[q];
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+        if ((threadIdx.x & 31) == 0) part[q][threadIdx.x >> 5] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double a = 0.0;
+        for (int w = 0; w < kBlock / 32; ++w) a += part[threadIdx.x][w];
+        atomicAdd(out + threadIdx.x, a);
+    }
+}
+
 // F is the flipper after streaming, i.e. the state the ghosts are read in.
 template <bool F, class S>
 __global__ void __launch_bounds__(kBlock) periodicCopy(DevLevel g) {
@@ -421,6 +456,118 @@ __global__ void __launch_bounds__(kBlock) periodicCopy(DevLevel g) {
     readPre<F, S>(g, nb, f);
     decodeNbr(g, cell, nb, nullptr);
     writePre<F, S>(g, nb, f);
+}
+
+// Characteristic (non-reflective) normal velocity of a face cell: the
+// outgoing Riemann invariant of the streamed state against the reference
+// values (include/updateGrid.h:268-308).
+__device__ __forceinline__ float nonReflectiveUNormal(float uTarget, float dRhoZ, float dRhoRef) {
+    const float cs = 0.57735026918962576f;  // 1/sqrt(3)
+    const float rhoRef = dRhoRef + 1.f;
+    const float rhoTerm = (dRhoZ - dRhoRef) / rhoRef;
+    const float numerator = 2.f * (uTarget + cs * rhoTerm);
+    const float root = (1.f + cs - uTarget) * (1.f + cs - uTarget) + 4.f * (uTarget + cs * rhoTerm);
+    const float denominator = 1.f + cs - uTarget + sqrtf(root);
+    return numerator / denominator;
+}
+
+// K2 (include/updateGrid.h:181-355): one thread per open-boundary cell, run
+// after the flip, so F is the flipper of the next step's pre-collision read.
+// Known populations (c.n >= 0 on every axis) are read and weight-compensated,
+// the missing macroscopic quantity is restored, the unknown populations are
+// closed from equilibrium moments and written to the cell's own
+// pre-collision slots.  All open-boundary IDs go in one launch: their cells
+// are disjoint and a cell touches only its own 27 slots, so the reference's
+// loop over IDs gives the same result in any order.
+template <bool F, class S>
+__global__ void __launch_bounds__(kBlock) openBoundary(DevLevel g, int iterationsFinished) {
+    const int idx = blockIdx.x * kBlock + threadIdx.x;
+    if (idx >= g.obCount) return;
+    const int cell = __ldg(g.obCell + idx);
+    const int info = __ldg(g.obInfo + idx);
+    const int nx = ((info >> 3) & 3) - 1, ny = ((info >> 5) & 3) - 1, nz = ((info >> 7) & 3) - 1;
+    const LbmMbbcTable& T = kLbmMbbc[(info >> 10) & 31];
+    int nb[8];
+    decodeNbr(g, cell, nb, nullptr);
+    S* base = static_cast<S*>(g.f);
+    float f[27];
+    float dRhoZ = 0.f;
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        f[d] = 0.f;
+        if (nx * cx(d) < 0 || ny * cy(d) < 0 || nz * cz(d) < 0) continue;
+        f[d] = Store<S>::ld(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
+        if (nx * cx(d) + ny * cy(d) + nz * cz(d) == 0) dRhoZ += f[d];
+        else dRhoZ += 2.f * f[d];
+        f[d] += weight(d);  // the closure is ill-conditioned on shifted populations
+    }
+    const float dRhoRef = g.obRhoRef[idx];
+    const float uNormalRef = g.obUnRef[idx];
+    const float4 target = __ldg(g.obTarget + idx);
+    float dRho = target.x, ux = target.y, uy = target.z, uz = target.w;
+    const bool nonReflective = info & 4;
+    if ((info & 3) == 2) {  // pressure: density given, velocity restored
+        if (nonReflective) {
+            const float uNormal = nonReflectiveUNormal(uNormalRef, dRhoZ, dRho);
+            dRho = (dRhoZ - uNormal) / (1.f + uNormal);
+        }
+        mbbcRestoreU(T, nx, ny, nz, dRho + 1.f, f, ux, uy, uz);
+    } else if ((info & 3) == 1) {  // velocity: velocity given, density restored
+        if (nonReflective) {
+            float uTarget = 0.f;
+            if (nx != 0) uTarget = nx > 0 ? ux : -ux;
+            if (ny != 0) uTarget = ny > 0 ? uy : -uy;
+            if (nz != 0) uTarget = nz > 0 ? uz : -uz;
+            const float uNormal = nonReflectiveUNormal(uTarget, dRhoZ, dRhoRef);
+            if (nx != 0) ux = nx > 0 ? uNormal : -uNormal;
+            if (ny != 0) uy = ny > 0 ? uNormal : -uNormal;
+            if (nz != 0) uz = nz > 0 ? uNormal : -uNormal;
+        }
+        dRho = mbbcRestoreRho(T, ux, uy, uz, f) - 1.f;
+    }
+    mbbcApply(T, dRho + 1.f, ux, uy, uz, f);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        if (!(nx * cx(d) < 0 || ny * cy(d) < 0 || nz * cz(d) < 0)) continue;
+        Store<S>::st(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)], f[d] - weight(d));
+    }
+    // reference values: exponential average whose weight decays with the
+    // iteration count; below 1e-5 the weight is tripled and the update runs
+    // every 3^k iterations instead (include/updateGrid.h:325-347)
+    const float uNormal = (float)nx * ux + (float)ny * uy + (float)nz * uz;
+    const float beta = __ldg(g.obBeta + idx);
+    float alpha = beta / ((float)iterationsFinished + beta + 10.f);
+    int updateEvery = 1;
+    while (alpha < 1.e-5f) {
+        alpha *= 3.f;
+        updateEvery *= 3;
+    }
+    if (iterationsFinished % updateEvery == 0) {
+        g.obRhoRef[idx] = fmaf(alpha, dRho - dRhoRef, dRhoRef);
+        g.obUnRef[idx] = fmaf(alpha, uNormal - uNormalRef, uNormalRef);
+    }
+    if (g.trackOpen && (info & 512)) {
+        g.obRhoCum[idx] += dRho;
+        g.obUnCum[idx] += uNormal;
+    }
+}
+
+// Initial reference values of the open boundary (applyInitialCondition.h:43-81).
+template <bool F, class S>
+__global__ void __launch_bounds__(kBlock) openBoundaryInit(DevLevel g) {
+    const int idx = blockIdx.x * kBlock + threadIdx.x;
+    if (idx >= g.obCount) return;
+    const int cell = __ldg(g.obCell + idx);
+    const int info = __ldg(g.obInfo + idx);
+    const int nx = ((info >> 3) & 3) - 1, ny = ((info >> 5) & 3) - 1, nz = ((info >> 7) & 3) - 1;
+    int nb[8];
+    decodeNbr(g, cell, nb, nullptr);
+    float f[27];
+    readPre<F, S>(g, nb, f);
+    float dRho, ux, uy, uz;
+    macroFromF(f, dRho, ux, uy, uz);
+    g.obRhoRef[idx] = dRho;
+    g.obUnRef[idx] = (float)nx * ux + (float)ny * uy + (float)nz * uz;
 }
 
 // getFeq (include/cellFunctions.h:125-148) with rounding-exact intrinsics so
@@ -609,6 +756,16 @@ template <bool F, class S> struct RunPeriodic {
         if (g.perCount > 0) periodicCopy<F, S><<<blocksFor(g.perCount), kBlock, 0, s>>>(g);
     }
 };
+template <bool F, class S> struct RunOpen {
+    static void run(const DevLevel& g, cudaStream_t s, int iterationsFinished) {
+        if (g.obCount > 0) openBoundary<F, S><<<blocksFor(g.obCount), kBlock, 0, s>>>(g, iterationsFinished);
+    }
+};
+template <bool F, class S> struct RunOpenInit {
+    static void run(const DevLevel& g, cudaStream_t s) {
+        if (g.obCount > 0) openBoundaryInit<F, S><<<blocksFor(g.obCount), kBlock, 0, s>>>(g);
+    }
+};
 template <bool F, class S> struct RunInit {
     static void run(const DevLevel& g, cudaStream_t s, const float4* macro, float4 u) {
         initFeq<F, S><<<blocksFor(g.cellCount), kBlock, 0, s>>>(g, macro, u);
@@ -639,6 +796,10 @@ template <bool F, class S> struct RunScatter {
 
 void launchCollideStream(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunCollide>(g, flip, s); }
 void launchPeriodic(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunPeriodic>(g, flip, s); }
+void launchOpenBoundary(const DevLevel& g, bool flip, cudaStream_t s, int iterationsFinished) {
+    dispatch<RunOpen>(g, flip, s, iterationsFinished);
+}
+void launchOpenBoundaryInit(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunOpenInit>(g, flip, s); }
 void launchInit(const DevLevel& g, bool flip, cudaStream_t s, const float4* macro, float4 uniform) {
     dispatch<RunInit>(g, flip, s, macro, uniform);
 }
@@ -650,6 +811,9 @@ void launchGatherF(const DevLevel& g, cudaStream_t s, float* out) { dispatch<Run
 void launchScatterF(const DevLevel& g, cudaStream_t s, const float* in) { dispatch<RunScatter>(g, false, s, in); }
 void launchWallForce(const DevLevel& g, int wallID, cudaStream_t s, double* out) {
     if (g.wallCount > 0) wallForceSum<<<blocksFor(g.wallCount), kBlock, 0, s>>>(g, wallID, out);
+}
+void launchOpenFlow(const DevLevel& g, int openBCID, float invSpan, cudaStream_t s, double* out) {
+    if (g.obCount > 0) openFlowSum<<<blocksFor(g.obCount), kBlock, 0, s>>>(g, openBCID, invSpan, out);
 }
 void launchCollideBatch(float* f, int n, const CollisionConsts& P, float gx, float gy, float gz,
                         cudaStream_t s) {

@@ -47,6 +47,17 @@ struct DevLevel {
     int trackWallForce;
     int useIBB;
     float gx, gy, gz;              // body force (getLocalBC)
+    // open-boundary cells (OpenBCArrayStruct, all IDs concatenated)
+    const int* obCell;
+    const int* obInfo;             // packed, see OpenBCCell
+    const float4* obTarget;        // dRho, ux, uy, uz of getOpenBC
+    const float* obBeta;
+    float* obRhoRef;               // dRhoRefArray
+    float* obUnRef;                // uNormalRefArray
+    float* obRhoCum;               // dRhoCumulativeArray
+    float* obUnCum;                // uNormalCumulativeArray
+    int obCount;
+    int trackOpen;
     int nx, ny, nz;
     float res, ox, oy, oz;
     CollisionConsts coll;

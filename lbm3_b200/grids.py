@@ -18,7 +18,7 @@ _INT_ARRAYS = {
     "row_k": A.ARRAY_ROW_K, "row_jplus": A.ARRAY_ROW_JPLUS, "row_kplus": A.ARRAY_ROW_KPLUS,
     "row_jkplus": A.ARRAY_ROW_JKPLUS, "wall_map": A.ARRAY_WALL_MAP,
     "periodic_index": A.ARRAY_PERIODIC_INDEX, "periodic_source": A.ARRAY_PERIODIC_SOURCE,
-    "wall_index": A.ARRAY_WALL_INDEX,
+    "wall_index": A.ARRAY_WALL_INDEX, "open_index": A.ARRAY_OPEN_INDEX, "open_source": A.ARRAY_OPEN_SOURCE,
 }
 _UINT_ARRAYS = {"wall_data": A.ARRAY_WALL_DATA, "link_length": A.ARRAY_LINK_LENGTH}
 
@@ -32,6 +32,8 @@ def _int_len(info: A.LbmGridInfo, which: int) -> int:
         return info.wall_adjacent_count
     if which == A.ARRAY_LINK_LENGTH:
         return 7 * info.wall_adjacent_count
+    if which in (A.ARRAY_OPEN_INDEX, A.ARRAY_OPEN_SOURCE):
+        return info.open_bc_count
     return info.row_count
 
 
@@ -189,6 +191,29 @@ class Grids:
         out = (C.c_double * 6)()
         A.check(A.lib().lbm_wall_force(self._h, wall_id, int(reset), out))
         return np.array(out[:])
+
+    def open_boundary_flow(self, open_bc_id: int, reset: bool = False) -> dict:
+        """Flow through one open boundary averaged since the last tracker reset
+        (SI units; the normal is the outer normal)."""
+        out = (C.c_double * 7)()
+        A.check(A.lib().lbm_open_boundary_flow(self._h, open_bc_id, int(reset), out))
+        keys = ("area", "normal_velocity", "mass_flow", "momentum_thrust", "pressure", "pressure_power",
+                "normal_kinetic_power")
+        return dict(zip(keys, out[:]))
+
+    def _float_pair(self, which: int, level: int) -> np.ndarray:
+        m = self.info(level).open_bc_count
+        out = np.empty((2, m), dtype=np.float32)
+        A.check(A.lib().lbm_read_array(self._h, level, which, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def open_reference(self, level: int = 0) -> np.ndarray:
+        """Reference values of the open boundary: float32 [2][openBCCount] (dRho, uNormal)."""
+        return self._float_pair(A.ARRAY_OPEN_REFERENCE, level)
+
+    def open_cumulative(self, level: int = 0) -> np.ndarray:
+        """Tracked sums since the last reset: float32 [2][openBCCount] (dRho, uNormal)."""
+        return self._float_pair(A.ARRAY_OPEN_CUMULATIVE, level)
 
     def wall_force_raw(self, level: int = 0) -> np.ndarray:
         """Per-cell force accumulators float32 [3][wallCount] (lattice units)."""

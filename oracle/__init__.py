@@ -30,6 +30,15 @@ class OBC(C.Structure):
 _IP = C.POINTER(C.c_int)
 
 
+class FaceBC(C.Structure):
+    """lbm_face_bc of the public header (same layout)."""
+    _fields_ = [
+        ("kind", C.c_int), ("open_bc_id", C.c_int), ("priority", C.c_int),
+        ("non_reflective", C.c_int), ("non_reflective_beta", C.c_float),
+        ("dRho", C.c_float), ("ux", C.c_float), ("uy", C.c_float), ("uz", C.c_float),
+    ]
+
+
 class OGrid(C.Structure):
     _fields_ = [
         ("gridID", C.c_int), ("res", C.c_float), ("ox", C.c_float), ("oy", C.c_float), ("oz", C.c_float),
@@ -47,6 +56,8 @@ class OGrid(C.Structure):
         ("wallCount", C.c_int), ("wallIndex", _IP), ("wallData", C.POINTER(C.c_uint)),
         ("linkLength", C.POINTER(C.c_uint)), ("wallVel", C.POINTER(C.c_float)),
         ("wallForce", C.POINTER(C.c_float)), ("trackWallForce", C.c_int),
+        ("face", FaceBC * 6), ("openCount", C.c_int), ("openIndex", _IP),
+        ("openRef", C.POINTER(C.c_float)), ("openCum", C.POINTER(C.c_float)), ("trackOpen", C.c_int),
     ]
 
 
@@ -84,6 +95,9 @@ def lib() -> C.CDLL:
             [C.c_int, C.c_void_p, C.c_void_p, C.c_int] + [C.c_void_p] * 4
         h.oracle_from_tables.restype = C.c_int
         h.oracle_wall_force.argtypes = [C.POINTER(OGrid), C.c_int, C.POINTER(C.c_double)]
+        h.oracle_mbbc_apply.argtypes = [C.c_int] + [C.c_float] * 4 + [C.POINTER(C.c_float)]
+        h.oracle_mbbc_restore_rho.argtypes = [C.c_int] + [C.c_float] * 3 + [C.POINTER(C.c_float)] * 2
+        h.oracle_mbbc_restore_u.argtypes = [C.c_int, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
         _lib = h
     return _lib
 
@@ -132,6 +146,30 @@ def drho_u(f: np.ndarray) -> np.ndarray:
     v = np.ascontiguousarray(f, dtype=np.float32)
     out = np.empty(4, dtype=np.float32)
     lib().oracle_get_drho_u(_fp(v), _fp(out))
+    return out
+
+
+def mbbc_apply(code: int, rho: float, u, f: np.ndarray) -> np.ndarray:
+    """applyMBBC on full populations; returns the completed 27 values."""
+    v = np.ascontiguousarray(f, dtype=np.float32).copy()
+    if lib().oracle_mbbc_apply(int(code), rho, u[0], u[1], u[2], _fp(v)) != 0:
+        raise ValueError(f"no outer normal with code {code}")
+    return v
+
+
+def mbbc_restore_rho(code: int, u, f: np.ndarray) -> float:
+    v = np.ascontiguousarray(f, dtype=np.float32)
+    out = np.zeros(1, dtype=np.float32)
+    if lib().oracle_mbbc_restore_rho(int(code), u[0], u[1], u[2], _fp(v), _fp(out)) != 0:
+        raise ValueError(f"no outer normal with code {code}")
+    return out[0]
+
+
+def mbbc_restore_u(code: int, rho: float, f: np.ndarray) -> np.ndarray:
+    v = np.ascontiguousarray(f, dtype=np.float32)
+    out = np.zeros(3, dtype=np.float32)
+    if lib().oracle_mbbc_restore_u(int(code), rho, _fp(v), _fp(out)) != 0:
+        raise ValueError(f"no outer normal with code {code}")
     return out
 
 
@@ -209,6 +247,19 @@ class OracleGrid:
         n = self.g.cellCount
         dst = np.ctypeslib.as_array(self.g.f, shape=(27 * n,))
         dst[:] = np.ascontiguousarray(f, dtype=np.float32).reshape(-1)
+
+    def open_index(self) -> np.ndarray:
+        m = self.g.openCount
+        return np.ctypeslib.as_array(self.g.openIndex, shape=(m,)).copy() if m else np.empty(0, np.int32)
+
+    def open_reference(self) -> np.ndarray:
+        """[2][openCount]: dRhoRef, uNormalRef."""
+        m = self.g.openCount
+        return np.ctypeslib.as_array(self.g.openRef, shape=(2 * m,)).reshape(2, m).copy()
+
+    def open_cumulative(self) -> np.ndarray:
+        m = self.g.openCount
+        return np.ctypeslib.as_array(self.g.openCum, shape=(2 * m,)).reshape(2, m).copy()
 
     def int_array(self, name: str) -> np.ndarray:
         lengths = {"I": self.g.cellCount, "J": self.g.cellCount, "K": self.g.cellCount,

@@ -6,6 +6,9 @@
  * Citations are path:line inside the reference project.
  */
 #include "lbm_oracle.h"
+/* generated coefficient tables of the moment-based open boundary (plain C
+ * data; pinned against the reference's generated code by the golden vectors) */
+#include "../lbm3_b200/csrc/mbbc_tables.h"
 
 #include <math.h>
 #include <stdlib.h>
@@ -359,18 +362,144 @@ void oracle_apply_collision_batch(float* f, int n, float nu, float limiter, floa
     }
 }
 
+/* ---- moment-based open boundary ------------------------------------------ */
+
+static const LbmMbbcTable* mbbc_table(int code) {
+    for (int t = 0; t < LBM_MBBC_NORMALS; ++t)
+        if (kLbmMbbc[t].code == code) return &kLbmMbbc[t];
+    return NULL;
+}
+
+/* acc + c v, written as the generated code writes each term */
+static float mbbc_term(float acc, float c, float v) {
+    if (c == 1.f) return acc + v;
+    if (c == -1.f) return acc - v;
+    return acc + c * v;
+}
+
+/* equilibrium moment m of the 23 in table order (helperMain.py meq) */
+static float mbbc_meq(int m, float rho, float ux, float uy, float uz) {
+    const float t = 1.f / 3.f, n = 1.f / 9.f;
+    switch (m) {
+        case 0: return rho;
+        case 1: return rho * ux;
+        case 2: return rho * uy;
+        case 3: return rho * uz;
+        case 4: return t * rho + rho * ux * ux;
+        case 5: return t * rho + rho * uy * uy;
+        case 6: return t * rho + rho * uz * uz;
+        case 7: return rho * uy * uz;
+        case 8: return rho * ux * uz;
+        case 9: return rho * ux * uy;
+        case 10: return 0.f;
+        case 11: return t * rho * uy + rho * ux * ux * uy;
+        case 12: return t * rho * uz + rho * ux * ux * uz;
+        case 13: return t * rho * ux + rho * ux * uy * uy;
+        case 14: return t * rho * uz + rho * uy * uy * uz;
+        case 15: return t * rho * ux + rho * ux * uz * uz;
+        case 16: return t * rho * uy + rho * uy * uz * uz;
+        case 17: return n * rho + t * rho * uy * uy + t * rho * uz * uz + rho * uy * uy * uz * uz;
+        case 18: return n * rho + t * rho * ux * ux + t * rho * uz * uz + rho * ux * ux * uz * uz;
+        case 19: return n * rho + t * rho * ux * ux + t * rho * uy * uy + rho * ux * ux * uy * uy;
+        case 20: return t * rho * uy * uz;
+        case 21: return t * rho * ux * uz;
+        default: return t * rho * ux * uy;
+    }
+}
+
+/* applyMBBC: unknowns = (S Mfu)^-1 (m_eq(S) - S Mfk f_k) */
+int oracle_mbbc_apply(int code, float rho, float ux, float uy, float uz, float f[27]) {
+    const LbmMbbcTable* T = mbbc_table(code);
+    if (!T) return -1;
+    float s[LBM_MBBC_MAX_UNKNOWN];
+    for (int i = 0; i < T->nu; ++i) {
+        float smf = 0.f;
+        for (int k = 0; k < T->nk; ++k)
+            if (T->smfk[i][k] != 0) smf = mbbc_term(smf, (float)T->smfk[i][k], f[T->known[k]]);
+        s[i] = mbbc_meq(T->moment[i], rho, ux, uy, uz) - smf;
+    }
+    float out[LBM_MBBC_MAX_UNKNOWN];
+    for (int r = 0; r < T->nu; ++r) {
+        float v = 0.f;
+        for (int j = 0; j < T->nu; ++j)
+            if (T->inv[r][j] != 0.f) v = mbbc_term(v, T->inv[r][j], s[j]);
+        out[r] = v;
+    }
+    for (int r = 0; r < T->nu; ++r) f[T->unknown[r]] = out[r];
+    return 0;
+}
+
+/* restoreRho: rho = (C Mfk f_k) / (C Q + C Qu u) */
+int oracle_mbbc_restore_rho(int code, float ux, float uy, float uz, const float f[27], float* rho) {
+    const LbmMbbcTable* T = mbbc_table(code);
+    if (!T) return -1;
+    const float scqu = T->rhoQu[0] * ux + T->rhoQu[1] * uy + T->rhoQu[2] * uz;
+    const float sden = T->rhoQ + scqu;
+    float scmf = 0.f;
+    for (int k = 0; k < T->nk; ++k)
+        if (T->rhoMfk[k] != 0.f) scmf = mbbc_term(scmf, T->rhoMfk[k], f[T->known[k]]);
+    *rho = scmf / sden;
+    return 0;
+}
+
+/* restoreUxUyUz: faces by the closed form (normal velocity from the
+ * known-population density, tangential from a vanishing k_nnt), edges and
+ * corners from three unknown-free moment relations */
+int oracle_mbbc_restore_u(int code, float rho, const float f[27], float u[3]) {
+    const LbmMbbcTable* T = mbbc_table(code);
+    if (!T) return -1;
+    const int n[3] = {code / 100 - 5, (code / 10) % 10 - 5, code % 10 - 5};
+    if (T->face) {
+        float fZero = 0.f, fPlus = 0.f;
+        for (int d = 0; d < 27; ++d) {
+            const int cn = CX[d] * n[0] + CY[d] * n[1] + CZ[d] * n[2];
+            if (cn == 0) fZero = fZero + f[d];
+            else if (cn == 1) fPlus = fPlus + f[d];
+        }
+        const float uN = (fZero + 2.f * fPlus) / rho - 1.f;
+        const float den = fZero + 2.f * (uN + 1.f) * rho * uN;
+        for (int a = 0; a < 3; ++a) {
+            if (n[a] != 0) { u[a] = n[a] > 0 ? uN : -uN; continue; }
+            float jZero = 0.f, jPlus = 0.f;
+            for (int d = 0; d < 27; ++d) {
+                const int cn = CX[d] * n[0] + CY[d] * n[1] + CZ[d] * n[2];
+                const int ca = a == 0 ? CX[d] : (a == 1 ? CY[d] : CZ[d]);
+                if (ca == 0) continue;
+                if (cn == 0) jZero = ca > 0 ? jZero + f[d] : jZero - f[d];
+                else if (cn == 1) jPlus = ca > 0 ? jPlus + f[d] : jPlus - f[d];
+            }
+            u[a] = ((2.f * uN + 1.f) * jZero + 4.f * uN * jPlus) / den;
+        }
+        return 0;
+    }
+    float s[3];
+    for (int i = 0; i < 3; ++i) {
+        float acc = 0.f;
+        for (int k = 0; k < T->nk; ++k)
+            if (T->uMfk[i][k] != 0.f) acc = mbbc_term(acc, T->uMfk[i][k], f[T->known[k]]);
+        s[i] = acc / rho - T->uQ[i];
+    }
+    for (int a = 0; a < 3; ++a) {
+        float v = 0.f;
+        for (int j = 0; j < 3; ++j)
+            if (T->uInv[a][j] != 0.f) v = mbbc_term(v, T->uInv[a][j], s[j]);
+        u[a] = v;
+    }
+    return 0;
+}
+
 /* ---- grid construction (include/gridBuilderFunctions.h) ------------------ */
 
-static obc open_bc(const lbm_case* c, const ogrid* g, int i, int j, int k) {
+static obc open_bc_faces(const lbm_face_bc* face, const ogrid* g, int i, int j, int k) {
     /* getOpenBC as the face table defines it (include/lbm3_b200.h) */
     obc bc;
     oracle_default_bc(&bc);
     const int touch[6] = {i == 0, i == g->nx - 1, j == 0, j == g->ny - 1, k == 0, k == g->nz - 1};
     int best = -1;
     for (int f = 0; f < 6; ++f)
-        if (touch[f] && (best < 0 || c->face[f].priority > c->face[best].priority)) best = f;
+        if (touch[f] && (best < 0 || face[f].priority > face[best].priority)) best = f;
     if (best < 0) return bc;
-    const lbm_face_bc* fb = &c->face[best];
+    const lbm_face_bc* fb = &face[best];
     bc.openBCID = fb->open_bc_id;
     bc.nonReflective = fb->non_reflective;
     bc.nonReflectiveBeta = fb->non_reflective_beta;
@@ -378,6 +507,10 @@ static obc open_bc(const lbm_case* c, const ogrid* g, int i, int j, int k) {
     else if (fb->kind == LBM_BC_VELOCITY) { bc.dirichletU = 1; bc.ux = fb->ux; bc.uy = fb->uy; bc.uz = fb->uz; }
     else if (fb->kind == LBM_BC_PRESSURE) { bc.dirichletRho = 1; bc.dRho = fb->dRho; }
     return bc;
+}
+
+static obc open_bc(const lbm_case* c, const ogrid* g, int i, int j, int k) {
+    return open_bc_faces(c->face, g, i, j, k);
 }
 
 static int cmp_kji(const void* a, const void* b) {
@@ -429,6 +562,8 @@ static int find_cell(const ogrid* g, int i, int j, int k) {
 static void get_nbr(const ogrid* g, int cell, int nb[8]);
 static void init_info(const lbm_case* c, ogrid* g);
 static void apply_initial_condition(const lbm_case* c, ogrid* g);
+static void get_ijk(const ogrid* g, int cell, int* i, int* j, int* k);
+static void build_open_list(ogrid* g);
 
 int oracle_build(const lbm_case* c, ogrid* g) {
     memset(g, 0, sizeof(*g));
@@ -534,14 +669,7 @@ int oracle_build(const lbm_case* c, ogrid* g) {
         if (k < layers || k >= g->nz - layers) ov |= open_bc(c, g, i, j, k < layers ? 0 : g->nz - 1).periodic;
         if (ov && g->wallMap[q] == -1) g->wallMap[q] = -2;
     }
-    /* open boundaries are not restated in this oracle build */
-    g->openBCCount = 0;
-    for (int q = 0; q < n; ++q) {
-        const int i = g->I[q], j = g->J[q], k = g->K[q];
-        if (i == 0 || i == g->nx - 1 || j == 0 || j == g->ny - 1 || k == 0 || k == g->nz - 1)
-            if (!open_bc(c, g, i, j, k).periodic) g->openBCCount++;
-    }
-    if (g->openBCCount > 0) { oracle_free(g); return LBM_ERR_UNSUPPORTED; }
+    build_open_list(g);
 
     /* periodic lists (:1486-1564) */
     g->perIndex = (int*)malloc(sizeof(int) * n);
@@ -572,6 +700,7 @@ void oracle_free(ogrid* g) {
     free(g->rowJP); free(g->rowKP); free(g->rowJKP); free(g->wallMap); free(g->perIndex);
     free(g->perSource); free(g->f);
     free(g->wallIndex); free(g->wallData); free(g->linkLength); free(g->wallVel); free(g->wallForce);
+    free(g->openIndex); free(g->openRef); free(g->openCum);
     memset(g, 0, sizeof(*g));
 }
 
@@ -593,6 +722,44 @@ static void init_info(const lbm_case* c, ogrid* g) {
     g->gx = c->gx; g->gy = c->gy; g->gz = c->gz;
     g->useIBB = c->use_ibb;
     g->trackWallForce = c->track_wall_force;
+    g->trackOpen = c->track_open_boundaries;
+    memcpy(g->face, c->face, sizeof(g->face));
+}
+
+/* Open-boundary lists (gridBuilderFunctions.h:1276-1330): boundary cells that
+ * are neither walls nor periodic, grouped by openBCID in ID order, each group
+ * in cell order. */
+static void build_open_list(ogrid* g) {
+    const int n = g->cellCount;
+    int* id = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    int maxId = -1;
+    for (int q = 0; q < n; ++q) {
+        id[q] = -1;
+        if (g->wallMap[q] == -3) continue;
+        int i, j, k;
+        get_ijk(g, q, &i, &j, &k);
+        if (!(i == 0 || i == g->nx - 1 || j == 0 || j == g->ny - 1 || k == 0 || k == g->nz - 1)) continue;
+        const obc bc = open_bc_faces(g->face, g, i, j, k);
+        if (bc.periodic) continue;
+        id[q] = bc.openBCID;
+        if (id[q] > maxId) maxId = id[q];
+    }
+    g->openCount = 0;
+    g->openIndex = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    for (int b = 0; b <= maxId; ++b)
+        for (int q = 0; q < n; ++q)
+            if (id[q] == b) g->openIndex[g->openCount++] = q;
+    g->openBCCount = g->openCount;
+    g->openRef = (float*)calloc(2 * (size_t)(g->openCount > 0 ? g->openCount : 1), sizeof(float));
+    g->openCum = (float*)calloc(2 * (size_t)(g->openCount > 0 ? g->openCount : 1), sizeof(float));
+    free(id);
+}
+
+static void outer_normal(const ogrid* g, int i, int j, int k, int n[3]) {
+    /* getOuterNormal (include/cellFunctions.h:110-122) */
+    n[0] = i == 0 ? -1 : (i == g->nx - 1 ? 1 : 0);
+    n[1] = j == 0 ? -1 : (j == g->ny - 1 ? 1 : 0);
+    n[2] = k == 0 ? -1 : (k == g->nz - 1 ? 1 : 0);
 }
 
 /* getCompressedIJK (include/cellFunctions.h:51-72) */
@@ -636,6 +803,19 @@ static void apply_initial_condition(const lbm_case* c, ogrid* g) {
             g->f[(size_t)slot * n + nb[pre_nbr(d)]] = feq[d];
         }
     }
+    /* previous values of the open boundary (applyInitialCondition.h:43-81) */
+    for (int q = 0; q < g->openCount; ++q) {
+        const int cell = g->openIndex[q];
+        int ci, cj, ck, on[3], nb[8];
+        get_ijk(g, cell, &ci, &cj, &ck);
+        outer_normal(g, ci, cj, ck, on);
+        get_nbr(g, cell, nb);
+        float f[27], m[4];
+        for (int d = 0; d < 27; ++d) f[d] = g->f[(size_t)(g->flip ? INV[d] : d) * n + nb[pre_nbr(d)]];
+        oracle_get_drho_u(f, m);
+        g->openRef[q] = m[0];
+        g->openRef[g->openCount + q] = (float)on[0] * m[1] + (float)on[1] * m[2] + (float)on[2] * m[3];
+    }
 }
 
 static int* copy_ints(const int* src, int n) {
@@ -674,6 +854,7 @@ int oracle_from_tables(const lbm_case* c, ogrid* g, int cellCount, int rowCount,
     long long walls = 0;
     for (int q = 0; q < cellCount; ++q) walls += g->wallMap[q] == -3;
     g->fluidUpdates = (long long)cellCount - walls;
+    build_open_list(g);
     apply_initial_condition(c, g);
     return 0;
 }
@@ -714,6 +895,99 @@ static void get_nbr(const ogrid* g, int cell, int nb[8]) {
     nb[5] = kP + 1 >= n ? 0 : kP + 1;
     nb[6] = jkP;
     nb[7] = jkP + 1 >= n ? 0 : jkP + 1;
+}
+
+/* one open-boundary cell after streaming (include/updateGrid.h:191-353) */
+static void open_boundary(ogrid* g) {
+    const size_t n = (size_t)g->cellCount;
+    const int m = g->openCount;
+#pragma omp parallel for schedule(static)
+    for (int q = 0; q < m; ++q) {
+        const int cell = g->openIndex[q];
+        const int wm = g->wallMap[cell];
+        int trackFlow = wm != -2;
+        if (wm >= 0 && (g->wallData[wm] & 1u)) trackFlow = 0;
+        int ci, cj, ck, on[3], nb[8];
+        get_ijk(g, cell, &ci, &cj, &ck);
+        outer_normal(g, ci, cj, ck, on);
+        get_nbr(g, cell, nb);
+        float f[27];
+        float dRhoZ = 0.f;
+        for (int d = 0; d < 27; ++d) {
+            f[d] = 0.f;
+            if (on[0] * CX[d] < 0 || on[1] * CY[d] < 0 || on[2] * CZ[d] < 0) continue;
+            f[d] = g->f[(size_t)(g->flip ? INV[d] : d) * n + nb[pre_nbr(d)]];
+            const int product = on[0] * CX[d] + on[1] * CY[d] + on[2] * CZ[d];
+            if (product == 0) dRhoZ += f[d];
+            else dRhoZ += 2.f * f[d];
+            f[d] += W[d];
+        }
+        const float dRhoRef = g->openRef[q];
+        const float uNormalRef = g->openRef[m + q];
+        obc bc = open_bc_faces(g->face, g, ci, cj, ck);
+        if (abs(on[0]) + abs(on[1]) + abs(on[2]) != 1) bc.nonReflective = 0;
+        const float cs = 0.57735026918962576f;
+        const int code = (on[0] + 5) * 100 + (on[1] + 5) * 10 + (on[2] + 5);
+        if (bc.dirichletRho) {
+            if (bc.nonReflective) {
+                const float dRhoTarget = bc.dRho;
+                const float rhoTarget = dRhoTarget + 1.f;
+                const float rhoTerm = ((dRhoZ - dRhoTarget) / rhoTarget);
+                const float numerator = 2.f * (uNormalRef + cs * rhoTerm);
+                const float rootContent = (1.f + cs - uNormalRef) * (1.f + cs - uNormalRef) +
+                                          4.f * (uNormalRef + cs * rhoTerm);
+                const float denominator = 1.f + cs - uNormalRef + sqrtf(rootContent);
+                const float uNormal = numerator / denominator;
+                bc.dRho = (dRhoZ - uNormal) / (1.f + uNormal);
+            }
+            float u[3];
+            oracle_mbbc_restore_u(code, bc.dRho + 1.f, f, u);
+            bc.ux = u[0]; bc.uy = u[1]; bc.uz = u[2];
+        } else if (bc.dirichletU) {
+            if (bc.nonReflective) {
+                float uT = 0.f;
+                if (on[0] > 0) uT = bc.ux;
+                if (on[0] < 0) uT = -bc.ux;
+                if (on[1] > 0) uT = bc.uy;
+                if (on[1] < 0) uT = -bc.uy;
+                if (on[2] > 0) uT = bc.uz;
+                if (on[2] < 0) uT = -bc.uz;
+                const float rhoRef = dRhoRef + 1.f;
+                const float rhoTerm = ((dRhoZ - dRhoRef) / rhoRef);
+                const float numerator = 2.f * (uT + cs * rhoTerm);
+                const float rootContent = (1.f + cs - uT) * (1.f + cs - uT) + 4.f * (uT + cs * rhoTerm);
+                const float denominator = 1.f + cs - uT + sqrtf(rootContent);
+                const float uNormal = numerator / denominator;
+                if (on[0] > 0) bc.ux = uNormal;
+                if (on[0] < 0) bc.ux = -uNormal;
+                if (on[1] > 0) bc.uy = uNormal;
+                if (on[1] < 0) bc.uy = -uNormal;
+                if (on[2] > 0) bc.uz = uNormal;
+                if (on[2] < 0) bc.uz = -uNormal;
+            }
+            float rho;
+            oracle_mbbc_restore_rho(code, bc.ux, bc.uy, bc.uz, f, &rho);
+            bc.dRho = rho - 1.f;
+        }
+        oracle_mbbc_apply(code, bc.dRho + 1.f, bc.ux, bc.uy, bc.uz, f);
+        for (int d = 0; d < 27; ++d) {
+            if (!(on[0] * CX[d] < 0 || on[1] * CY[d] < 0 || on[2] * CZ[d] < 0)) continue;
+            f[d] -= W[d];
+            g->f[(size_t)(g->flip ? INV[d] : d) * n + nb[pre_nbr(d)]] = f[d];
+        }
+        const float uNormal = (float)on[0] * bc.ux + (float)on[1] * bc.uy + (float)on[2] * bc.uz;
+        const float beta = bc.nonReflectiveBeta;
+        float alpha = beta / (g->iterationsFinished + beta + 10.f);
+        int updateEvery = 1;
+        while (alpha < 1.e-5f) { alpha *= 3.f; updateEvery *= 3; }
+        if (g->iterationsFinished % updateEvery == 0) {
+            g->openRef[q] = fmaf(alpha, bc.dRho - dRhoRef, dRhoRef);
+            g->openRef[m + q] = fmaf(alpha, uNormal - uNormalRef, uNormalRef);
+        }
+        if (!g->trackOpen || !trackFlow) continue;
+        g->openCum[q] += bc.dRho;
+        g->openCum[m + q] += uNormal;
+    }
 }
 
 /* ---- updateSingleGrid (include/updateGrid.h:16-386) --------------------- */
@@ -804,6 +1078,8 @@ void oracle_step(ogrid* g, int steps) {
         }
         /* applyStreaming (esotwistStreamingFunctions.h:6-9) */
         g->flip = !flip;
+        /* K2: open boundaries (:181-355) */
+        open_boundary(g);
         /* K3: periodic copy (:358-382) */
 #pragma omp parallel for schedule(static)
         for (int p = 0; p < g->perCount; ++p) {

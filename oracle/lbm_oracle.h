@@ -75,6 +75,13 @@ typedef struct ogrid {
     float *wallVel;                  /* [3][wallCount] */
     float *wallForce;                /* [3][wallCount] */
     int trackWallForce;
+    /* open boundaries (OpenBCArrayStruct, all IDs concatenated in ID order) */
+    lbm_face_bc face[6];             /* the case's face table (getOpenBC) */
+    int openCount;
+    int* openIndex;
+    float* openRef;                  /* [2][openCount] dRhoRef, uNormalRef */
+    float* openCum;                  /* [2][openCount] dRho, uNormal sums */
+    int trackOpen;
 } ogrid;
 
 /* buildGrids for a box domain without geometry, single level, followed by
@@ -106,6 +113,15 @@ double oracle_kinetic_energy(const ogrid* g, float uRefPhys, float domainLength)
 
 /* dRho,ux,uy,uz of every cell: out[4][cellCount]. */
 void oracle_macro(const ogrid* g, float* out);
+
+/* Moment-based open boundary of one cell with outer normal code
+ * (nx+5)*100+(ny+5)*10+(nz+5), on full (weight-compensated) populations:
+ * applyMBBC, restoreRho and restoreUxUyUz
+ * (include/boundaryConditions/{applyMBBC,restoreRho,restoreUxUyUz}.h).
+ * Return 0, or -1 for a code without an outer normal. */
+int oracle_mbbc_apply(int code, float rho, float ux, float uy, float uz, float f[27]);
+int oracle_mbbc_restore_rho(int code, float ux, float uy, float uz, const float f[27], float* rho);
+int oracle_mbbc_restore_u(int code, float rho, const float f[27], float u[3]);
 
 /* number of OpenMP threads the oracle uses */
 int oracle_threads(void);

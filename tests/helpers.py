@@ -27,6 +27,15 @@ def field_errors(got: np.ndarray, ref: np.ndarray):
     return e_rho, e_u
 
 
+def density_velocity_errors(got: np.ndarray, ref: np.ndarray):
+    """(rel L2 of rho = 1 + dRho, rel L2 of the velocity vector field, max
+    |delta dRho|) for [4][n] macro arrays.  For states near rest density the
+    dRho field itself is tiny and its relative error only measures rounding."""
+    e_rho = rel_l2(1.0 + got[0].astype(np.float64), 1.0 + ref[0].astype(np.float64))
+    e_u = rel_l2(got[1:4].reshape(-1), ref[1:4].reshape(-1))
+    return e_rho, e_u, float(np.max(np.abs(got[0] - ref[0]))) if got.shape[1] else 0.0
+
+
 def plan_ijk(plan, level: int = 0):
     """(i, j, k) of every cell, decoded from the compressed rows
     (getCompressedIJK, include/cellFunctions.h:51-72)."""
