@@ -247,6 +247,23 @@ int lbm_write_f(lbm_grids* g, int level, const float* host, size_t bytes);
 int lbm_kinetic_energy(lbm_grids* g, float u_ref_phys, float domain_length,
                        double* out);
 
+/* The same kinetic energy for callers that cannot allocate device memory:
+ * a serving loop that admits domains by HBM footprint has committed all of
+ * it, and an allocation on the side can fail or (cudaFree) synchronize the
+ * device mid-pipeline.  Its scratch (FP64 partial sums of 256-cell blocks and
+ * the total) is a fixed static device array of 128 KB that every GPU loading
+ * the library holds until exit, so the call allocates nothing.  Every level
+ * must have at most LBM_KINETIC_ENERGY_NOALLOC_MAX_CELLS cells; larger ones
+ * are rejected with LBM_ERR_INVALID.  Call it with the grids' device current;
+ * its first call on a device looks up the array's device address, so make
+ * that call before any stream capture begins.  All calls on a device share
+ * the array: calls that overlap on the GPU race.  The sum is deterministic
+ * (fixed order, no atomics).
+ * No counterpart in the reference. */
+#define LBM_KINETIC_ENERGY_NOALLOC_MAX_CELLS 4194304
+int lbm_kinetic_energy_noalloc(lbm_grids* g, float u_ref_phys, float domain_length,
+                               double* out);
+
 /* Momentum-exchange force and torque on one body (wallID), accumulated in
  * FP64 on the device over the wall-adjacent cells and averaged over the
  * steps since the last reset: out = {Fx, Fy, Fz [N], Tx, Ty, Tz [N m]} about

@@ -138,6 +138,7 @@ SIGNATURES = [
     ("lbm_read_array", C.c_int, [_P, C.c_int, C.c_int, _P, C.c_size_t]),
     ("lbm_write_f", C.c_int, [_P, C.c_int, _P, C.c_size_t]),
     ("lbm_kinetic_energy", C.c_int, [_P, C.c_float, C.c_float, C.POINTER(C.c_double)]),
+    ("lbm_kinetic_energy_noalloc", C.c_int, [_P, C.c_float, C.c_float, C.POINTER(C.c_double)]),
     ("lbm_wall_force", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     ("lbm_open_boundary_flow", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     ("lbm_apply_collision_batch", C.c_int,

@@ -17,9 +17,9 @@ LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "liblbm3_b200.so"
 OBJ_DIR = PKG / "_build"
 
-SOURCES = ["step.cu", "api.cu", "builder.cpp", "geometry.cpp"]
+SOURCES = ["step.cu", "api.cu", "builder.cpp", "geometry.cpp", "energy_noalloc.cu"]
 HEADERS = ["lattice.h", "cumulant.cuh", "step.cuh", "step_launch.h", "builder.h", "geometry.h", "mbbc.h",
-           "mbbc_tables.h"]
+           "mbbc_tables.h", "energy_noalloc.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
     "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",

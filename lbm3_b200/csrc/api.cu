@@ -14,6 +14,7 @@
 
 #include "../../include/lbm3_b200.h"
 #include "builder.h"
+#include "energy_noalloc.h"
 #include "step_launch.h"
 
 namespace {
@@ -658,6 +659,30 @@ int lbm_kinetic_energy(lbm_grids* g, float uRefPhys, float domainLength, double*
             double sum = 0.0;
             ck(cudaMemcpyAsync(&sum, g->scratch, sizeof(double), cudaMemcpyDeviceToHost, g->stream), "copy");
             ck(cudaStreamSynchronize(g->stream), "sync");
+            const double dx = double(L.info.res) / 1000.0;
+            const double vs = dx / (double(L.info.dtPhys) * uRefPhys);
+            energy += sum * dx * dx * dx * vs * vs;
+        }
+        const double len = double(domainLength) / 1000.0;
+        *out = energy / (len * len * len);
+    });
+}
+
+int lbm_kinetic_energy_noalloc(lbm_grids* g, float uRefPhys, float domainLength, double* out) {
+    static_assert(lbm::kNoAllocEnergyMaxCells == LBM_KINETIC_ENERGY_NOALLOC_MAX_CELLS,
+                  "header limit and scratch size disagree");
+    if (!g || !out) return fail(LBM_ERR_INVALID, "lbm_kinetic_energy_noalloc: bad argument");
+    for (const LevelState& L : g->levels)
+        if (L.dev.cellCount > lbm::kNoAllocEnergyMaxCells)
+            return fail(LBM_ERR_INVALID, "lbm_kinetic_energy_noalloc: level " + std::to_string(L.info.gridID) +
+                                             " has " + std::to_string(L.dev.cellCount) +
+                                             " cells; the static scratch covers at most " +
+                                             std::to_string(lbm::kNoAllocEnergyMaxCells));
+    return guarded("lbm_kinetic_energy_noalloc", [&] {
+        double energy = 0.0;
+        for (LevelState& L : g->levels) {
+            double sum = 0.0;
+            ck(lbm::kineticEnergyNoAlloc(L.dev, L.info.esotwistFlipper, g->stream, &sum), "energy");
             const double dx = double(L.info.res) / 1000.0;
             const double vs = dx / (double(L.info.dtPhys) * uRefPhys);
             energy += sum * dx * dx * dx * vs * vs;
