@@ -13,6 +13,7 @@ implementation (the C oracle, all host threads) on the same workload.
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -41,6 +42,20 @@ def make_case(name: str, storage: str):
     import lbm3_b200 as L
     from lbm3_b200 import _abi as A
     st = {"f32": A.LBM_STORE_F32, "f16": A.LBM_STORE_F16, "bf16": A.LBM_STORE_BF16}[storage]
+    if name.startswith("sphere"):
+        # flow around a sphere: single level, icosphere of 20,480 triangles with
+        # D = 24 cells at (64, 64, 64) on the 256x128x128 grid (scaled with the
+        # grid for other sizes), velocity inlet u = 0.04, non-reflective
+        # pressure outlet, strict-velocity sides, nu = 0.0096 (Re 100)
+        dims = name[len("sphere"):] or "256x128x128"
+        nx, ny, nz = (int(v) for v in dims.split("x"))
+        k = nx / 256.0
+        s = L.flow_around_sphere(nx, ny, nz, diameter=24.0 * k, center=(64.0 * k, ny / 2.0, nz / 2.0),
+                                 storage=st)
+        desc = (f"flow around a sphere {nx}x{ny}x{nz} single level: icosphere 20480 triangles, "
+                f"D={24.0 * k:g} cells at ({64.0 * k:g},{ny / 2.0:g},{nz / 2.0:g}), IBB, velocity inlet u=0.04, "
+                f"non-reflective pressure outlet, strict-velocity sides, nu=0.0096 (Re 100)")
+        return s.case, desc, s
     if name == "box256x128x128":
         # the 256x128x128 single-level grid of the flow-around-sphere
         # configuration, fully periodic and without the obstacle
@@ -59,7 +74,9 @@ def make_case(name: str, storage: str):
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
-    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi samples every 100 ms while the timed region runs; only the
+    samples taken inside the [start, stop] window are summarised."""
+    FIELDS = ("timestamp,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -67,16 +84,28 @@ class ClockSampler:
         self.uuid = uuid
         self.proc = None
         self.file = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=self.file, stderr=subprocess.DEVNULL)
+            # wait for the first sample so the window is covered from its start
+            deadline = time.time() + 5.0
+            while time.time() < deadline and os.path.getsize(self.file.name) == 0:
+                time.sleep(0.05)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
+
+    def start(self):
+        self.t0 = datetime.datetime.now()
+
+    def stop(self):
+        self.t1 = datetime.datetime.now()
+        time.sleep(0.25)  # let the sampler flush one more line
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -90,31 +119,49 @@ class ClockSampler:
         if self.proc is None or self.file is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.file.flush()
-        rows = [l.split(",") for l in Path(self.file.name).read_text().splitlines() if l.strip()]
+        rows = [[c.strip() for c in l.split(",")] for l in Path(self.file.name).read_text().splitlines()
+                if l.strip()]
         os.unlink(self.file.name)
         if self.uuid:
-            rows = [r for r in rows if r[0].strip() == self.uuid] or rows
-        sm, smax, reasons = [], None, set()
+            rows = [r for r in rows if len(r) > 1 and r[1] == self.uuid] or rows
+        sm, smax, reasons, power = [], None, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        lo = self.t0 - datetime.timedelta(milliseconds=100) if self.t0 else None
+        hi = self.t1 + datetime.timedelta(milliseconds=100) if self.t1 else None
         for r in rows:
             try:
-                sm.append(float(r[1]))
-                smax = float(r[2])
+                ts = datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f")
+                if lo and hi and not (lo <= ts <= hi):
+                    continue
+                sm.append(float(r[2]))
+                smax = float(r[3])
+                power.append(float(r[4]))
             except (ValueError, IndexError):
                 continue
-            for nme, v in zip(names, r[5:9]):
-                if v.strip().lower() == "active":
+            for nme, v in zip(names, r[6:10]):
+                if v.lower() == "active":
                     reasons.add(nme)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "power_w_median": statistics.median(power) if power else None,
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
 # ---------------------------------------------------------------- CPU legs
+def oracle_grid(case):
+    """The oracle on the workload: built by itself for box domains, from the
+    product's host plan (tables checked bit-exact by the tests) with bodies."""
+    import oracle as O
+    if case.body_count > 0:
+        import lbm3_b200 as L
+        return O.OracleGrid(case, L.Plan(case))
+    return O.OracleGrid(case)
+
+
 def time_oracle(case, target_s: float, min_steps: int = 1):
     """Time the C oracle (all host threads) on the same workload: returns
     (MLUPS, steps, seconds, threads)."""
+    g = oracle_grid(case)
     import oracle as O
-    g = O.OracleGrid(case)
     cells = g.g.fluidUpdates
     g.step(1)  # warm the pages
     steps, t0 = 0, time.perf_counter()
@@ -138,7 +185,7 @@ def run_reference(args):
         return 0
     case, desc, _ = make_case(args.workload, "f32")
     import oracle as O
-    g = O.OracleGrid(case)
+    g = oracle_grid(case)
     n = g.cell_count
     # estimate the rate on a small slice, then size the per-step slice
     probe = min(n, 200_000)
@@ -215,9 +262,12 @@ def run_ours(args):
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(uuid) as clk:
+        clk.start()
         ms = g.time_steps(args.steps)          # CUDA events on the grid stream
+        clk.stop()
     torch.cuda.synchronize()
     kernel_ms, launches = g.last_kernel_time()
+    all_launches = g.last_launch_count()
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if dist:
         dist.barrier()
@@ -249,9 +299,12 @@ def run_ours(args):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     g.set_populations(f_np)
+    sphere = tgv is not None and hasattr(tgv, "drag_coefficient")
     for _ in range(e2e_steps):
         g.update_all_grids(1)
-        if tgv is not None:
+        if sphere:
+            g.wall_force(0)                    # drag and torque, 6 doubles
+        elif tgv is not None:
             g.kinetic_energy(tgv.u_initial_phys, tgv.domain_length)
         else:
             g.kinetic_energy(1.0, 1000.0)
@@ -286,15 +339,17 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
-                         "kernel": "collideStream", "kernel_ms_per_launch": round(per_launch_ms, 5),
+                         "kernel": "collide-stream (bulk collidePrefetch + special-cell collideList)",
+                         "kernel_ms_per_launch": round(per_launch_ms, 5),
                          "algorithmic_bytes_per_launch": alg_bytes},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS",
-                    "h2d_bytes_per_step": int(f0.nbytes // e2e_steps), "d2h_bytes_per_step": 8,
+                    "h2d_bytes_per_step": int(f0.nbytes // e2e_steps), "d2h_bytes_per_step": 48 if sphere else 8,
                     "steps": e2e_steps,
                     "note": "initial populations uploaded from pinned host memory inside the timed "
-                            "region; every step reads its kinetic energy back (tracker period 1)"},
-            "gpu_launches": launches + (launches if info.periodic_count > 0 else 0),
+                            "region; every step reads its tracked observable back (tracker period 1: "
+                            + ("wall force and torque" if sphere else "kinetic energy") + ")"},
+            "gpu_launches": all_launches,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
@@ -310,7 +365,8 @@ def main():
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="box256x128x128")
+    ap.add_argument("--workload", default="sphere256x128x128",
+                    help="sphere256x128x128 (default; sphereNXxNYxNZ scales it), box256x128x128, tgv64, tgv128")
     ap.add_argument("--storage", choices=["f32", "f16", "bf16"], default="f32")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=90.0)

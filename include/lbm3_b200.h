@@ -227,6 +227,10 @@ int lbm_time_steps(lbm_grids* g, int steps, float* ms);
  * lbm_time_steps call, each bracketed by CUDA events on the grid stream:
  * summed kernel milliseconds and the number of launches. */
 int lbm_last_kernel_time(lbm_grids* g, float* kernel_ms, int* launches);
+/* Number of kernels the last lbm_time_steps call launched, all kernels of the
+ * step schedule (collide-stream, special cells, open boundary, periodic copy).
+ * No counterpart in the reference (instrumentation). */
+int lbm_last_launch_count(lbm_grids* g, long long* kernels);
 
 int lbm_level_count(lbm_grids* g);
 int lbm_get_grid_info(lbm_grids* g, int level, lbm_grid_info* out);

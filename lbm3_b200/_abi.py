@@ -133,6 +133,7 @@ SIGNATURES = [
     ("lbm_synchronize", C.c_int, [_P]),
     ("lbm_time_steps", C.c_int, [_P, C.c_int, C.POINTER(C.c_float)]),
     ("lbm_last_kernel_time", C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
+    ("lbm_last_launch_count", C.c_int, [_P, C.POINTER(C.c_longlong)]),
     ("lbm_level_count", C.c_int, [_P]),
     ("lbm_get_grid_info", C.c_int, [_P, C.c_int, C.POINTER(LbmGridInfo)]),
     ("lbm_read_array", C.c_int, [_P, C.c_int, C.c_int, _P, C.c_size_t]),

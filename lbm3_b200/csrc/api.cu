@@ -3,6 +3,7 @@
 // failure into a status code plus a thread-local message.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -15,6 +16,7 @@
 #include "../../include/lbm3_b200.h"
 #include "builder.h"
 #include "energy_noalloc.h"
+#include "mbbc.h"
 #include "step_launch.h"
 
 namespace {
@@ -91,6 +93,7 @@ struct lbm_grids {
     int* errorFlag = nullptr;  // device word the kernels set when a bounded wait gives up
     float lastKernelMs = 0.f;
     int lastLaunches = 0;
+    long long lastStepKernels = 0;  // every kernel launch of the last lbm_time_steps
     // event pairs bracketing collide-stream launches while lbm_time_steps runs
     std::vector<cudaEvent_t> kernelEvents;
     bool timingKernels = false;
@@ -409,6 +412,25 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
                 d.obUnCum = d.obRhoCum ? d.obRhoCum + m : nullptr;
                 if (m) ck(cudaMemsetAsync(d.obRhoCum, 0, 2 * m * sizeof(float), s), "memset");
                 d.trackOpen = c->track_open_boundaries ? 1 : 0;
+                // group the cells by outer normal into CTA-sized chunks; the
+                // boundary kernel stages one normal's tables per CTA
+                std::vector<int> order;
+                std::vector<int4> chunks;
+                order.reserve(m);
+                for (int row = 0; row < LBM_MBBC_NORMALS; ++row) {
+                    const int first = static_cast<int>(order.size());
+                    for (size_t q = 0; q < m; ++q)
+                        if (((info[q] >> 10) & 31) == row) order.push_back(static_cast<int>(q));
+                    const int count = static_cast<int>(order.size()) - first;
+                    for (int c0 = 0; c0 < count; c0 += lbm::kOpenChunk)
+                        chunks.push_back(make_int4(first + c0, std::min(lbm::kOpenChunk, count - c0), row, 0));
+                }
+                std::vector<lbm::MbbcDir> tables(LBM_MBBC_NORMALS);
+                for (int t = 0; t < LBM_MBBC_NORMALS; ++t) tables[t] = lbm::mbbcDirFromTable(kLbmMbbc[t]);
+                d.obOrder = own(upload(order, s));
+                d.obChunk = own(upload(chunks, s));
+                d.obChunkCount = static_cast<int>(chunks.size());
+                d.obTables = m ? own(upload(tables, s)) : nullptr;
             }
             d.trackWallForce = c->track_wall_force ? 1 : 0;
             d.useIBB = c->use_ibb ? 1 : 0;
@@ -515,6 +537,9 @@ int lbm_time_steps(lbm_grids* g, int steps, float* ms) {
         }
         g->lastKernelMs = kernel;
         g->lastLaunches = g->kernelEventsUsed / 2;
+        g->lastStepKernels = 0;
+        for (const LevelState& L : g->levels)
+            g->lastStepKernels += (static_cast<long long>(steps) << L.info.gridID) * lbm::stepLaunchCount(L.dev);
     });
 }
 
@@ -522,6 +547,12 @@ int lbm_last_kernel_time(lbm_grids* g, float* kernel_ms, int* launches) {
     if (!g || !kernel_ms || !launches) return fail(LBM_ERR_INVALID, "lbm_last_kernel_time: bad argument");
     *kernel_ms = g->lastKernelMs;
     *launches = g->lastLaunches;
+    return LBM_OK;
+}
+
+int lbm_last_launch_count(lbm_grids* g, long long* kernels) {
+    if (!g || !kernels) return fail(LBM_ERR_INVALID, "lbm_last_launch_count: bad argument");
+    *kernels = g->lastStepKernels;
     return LBM_OK;
 }
 

@@ -121,8 +121,8 @@ def emit(path: Path):
     L.append("/* GENERATED by gen_mbbc.py -- do not edit. */")
     L.append("/* Moment-based open-boundary tables for the 26 outer normals (see gen_mbbc.py).")
     L.append(" * Plain C aggregate data, readable from C, C++ and CUDA device code. */")
-    L.append("#ifndef LBM_MBBC_TABLES_H")
-    L.append("#define LBM_MBBC_TABLES_H")
+    L.append("#ifndef LBM_MBBC_TABLES_TYPE_H")
+    L.append("#define LBM_MBBC_TABLES_TYPE_H")
     L.append("")
     L.append("#define LBM_MBBC_NORMALS 26")
     L.append("#define LBM_MBBC_MAX_UNKNOWN 19")
@@ -144,16 +144,14 @@ def emit(path: Path):
     L.append("    float uQ[3];")
     L.append("} LbmMbbcTable;")
     L.append("")
-    L.append("/* 26 tables of 2.5 KB exceed the 64 KB constant bank: device code reads")
-    L.append(" * them from global memory (cached read-only). */")
-    L.append("#if defined(__CUDACC__)")
-    L.append("#define LBM_MBBC_STORAGE static __device__ const")
-    L.append("#else")
-    L.append("#define LBM_MBBC_STORAGE static const")
     L.append("#endif")
     L.append("")
+    L.append("/* host data; define LBM_MBBC_TYPES_ONLY to include the type alone */")
+    L.append("#if !defined(LBM_MBBC_TYPES_ONLY) && !defined(LBM_MBBC_TABLES_DATA_H)")
+    L.append("#define LBM_MBBC_TABLES_DATA_H")
+    L.append("")
     L.append("/* coefficients are correctly rounded num.f / den.f of the exact rationals */")
-    L.append("LBM_MBBC_STORAGE LbmMbbcTable kLbmMbbc[LBM_MBBC_NORMALS] = {")
+    L.append("static const LbmMbbcTable kLbmMbbc[LBM_MBBC_NORMALS] = {")
     for r in rows:
         n = r["normal"]
         code = (n[0] + 5) * 100 + (n[1] + 5) * 10 + (n[2] + 5)

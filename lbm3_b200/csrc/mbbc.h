@@ -1,11 +1,14 @@
-// Moment-based open boundary: restore the missing macroscopic quantity and
-// close the unknown populations of a boundary cell from the generated tables
-// (mbbc_tables.h).  Sums run over the known populations in direction order
-// and products are formed as the reference's generated code forms them
+// Moment-based open boundary in the form the device evaluates: the
+// coefficient tables of one outer normal (mbbc_tables.h) re-indexed by
+// population direction, so a kernel sweeps all 27 directions with static
+// indices (populations stay in registers) and plain FMA chains (zero
+// coefficients of unknown or unused populations add nothing).
+//
+// Sums run in ascending direction order, which is the order of the known
+// populations in the generated tables and in the reference's generated code
 // (include/boundaryConditions/{restoreRho,restoreUxUyUz,applyMBBC}.h), so the
-// results agree with it to rounding.  All populations here are full
-// (weight-compensated) f, as at the reference's call site
-// (include/updateGrid.h:223-240).
+// results agree with it to rounding.  Populations are full (weight-
+// compensated) f, as at the reference's call site (include/updateGrid.h:223-240).
 #pragma once
 
 #include "lattice.h"
@@ -13,91 +16,120 @@
 
 namespace lbm {
 
-// Table code of an outer normal; the row holding a code is found on the host
-// (the tables live in device memory for device code).
-LBM_HD int mbbcCode(int nx, int ny, int nz) { return (nx + 5) * 100 + (ny + 5) * 10 + (nz + 5); }
+struct MbbcDir {
+    float smf[LBM_MBBC_MAX_UNKNOWN][27];  // S Mfk: weight of population d in equation i
+    float inv[27][LBM_MBBC_MAX_UNKNOWN];  // row of (S Mfu)^-1 producing unknown population d
+    float rhoMfk[27];                     // restoreRho numerator weights
+    float uMfk[3][27];                    // restoreUxUyUz (edges, corners)
+    float uInv[3][3];
+    float uQ[3];
+    float rhoQ, rhoQu[3];
+    signed char moment[LBM_MBBC_MAX_UNKNOWN];  // equilibrium moment of equation i
+    int nu;                                    // unknown count
+    int face;                                  // 1: velocity from the face closed form
+    unsigned unknownMask;                      // bit d: population d is unknown
+    int nx, ny, nz;                            // outer normal
+};
 
-// Equilibrium value of moment m (the 23 moments in table order), with the
-// reference generator's expressions (helperMain.py meq list).
+// Direction-indexed form of one generated table (host, at grid build).
+inline MbbcDir mbbcDirFromTable(const LbmMbbcTable& T) {
+    MbbcDir D{};
+    D.nu = T.nu;
+    D.face = T.face;
+    D.nx = T.code / 100 - 5;
+    D.ny = (T.code / 10) % 10 - 5;
+    D.nz = T.code % 10 - 5;
+    for (int i = 0; i < T.nu; ++i) {
+        D.moment[i] = T.moment[i];
+        for (int k = 0; k < T.nk; ++k) D.smf[i][T.known[k]] = float(T.smfk[i][k]);
+    }
+    for (int r = 0; r < T.nu; ++r) {
+        D.unknownMask |= 1u << T.unknown[r];
+        for (int j = 0; j < T.nu; ++j) D.inv[T.unknown[r]][j] = T.inv[r][j];
+    }
+    for (int k = 0; k < T.nk; ++k) {
+        D.rhoMfk[T.known[k]] = T.rhoMfk[k];
+        for (int a = 0; a < 3; ++a) D.uMfk[a][T.known[k]] = T.uMfk[a][k];
+    }
+    for (int a = 0; a < 3; ++a) {
+        D.uQ[a] = T.uQ[a];
+        D.rhoQu[a] = T.rhoQu[a];
+        for (int b = 0; b < 3; ++b) D.uInv[a][b] = T.uInv[a][b];
+    }
+    D.rhoQ = T.rhoQ;
+    return D;
+}
+
+// Equilibrium value of moment m (the 23 moments in table order).
 LBM_HD float mbbcMomentEq(int m, float rho, float ux, float uy, float uz) {
+    const float t = 1.f / 3.f, n = 1.f / 9.f;
     switch (m) {
         case 0: return rho;
         case 1: return rho * ux;
         case 2: return rho * uy;
         case 3: return rho * uz;
-        case 4: return (1.f / 3.f) * rho + rho * ux * ux;
-        case 5: return (1.f / 3.f) * rho + rho * uy * uy;
-        case 6: return (1.f / 3.f) * rho + rho * uz * uz;
+        case 4: return t * rho + rho * ux * ux;
+        case 5: return t * rho + rho * uy * uy;
+        case 6: return t * rho + rho * uz * uz;
         case 7: return rho * uy * uz;
         case 8: return rho * ux * uz;
         case 9: return rho * ux * uy;
         case 10: return 0.f;
-        case 11: return (1.f / 3.f) * rho * uy + rho * ux * ux * uy;
-        case 12: return (1.f / 3.f) * rho * uz + rho * ux * ux * uz;
-        case 13: return (1.f / 3.f) * rho * ux + rho * ux * uy * uy;
-        case 14: return (1.f / 3.f) * rho * uz + rho * uy * uy * uz;
-        case 15: return (1.f / 3.f) * rho * ux + rho * ux * uz * uz;
-        case 16: return (1.f / 3.f) * rho * uy + rho * uy * uz * uz;
-        case 17: return (1.f / 9.f) * rho + (1.f / 3.f) * rho * uy * uy + (1.f / 3.f) * rho * uz * uz +
-                        rho * uy * uy * uz * uz;
-        case 18: return (1.f / 9.f) * rho + (1.f / 3.f) * rho * ux * ux + (1.f / 3.f) * rho * uz * uz +
-                        rho * ux * ux * uz * uz;
-        case 19: return (1.f / 9.f) * rho + (1.f / 3.f) * rho * ux * ux + (1.f / 3.f) * rho * uy * uy +
-                        rho * ux * ux * uy * uy;
-        case 20: return (1.f / 3.f) * rho * uy * uz;
-        case 21: return (1.f / 3.f) * rho * ux * uz;
-        default: return (1.f / 3.f) * rho * ux * uy;
+        case 11: return t * rho * uy + rho * ux * ux * uy;
+        case 12: return t * rho * uz + rho * ux * ux * uz;
+        case 13: return t * rho * ux + rho * ux * uy * uy;
+        case 14: return t * rho * uz + rho * uy * uy * uz;
+        case 15: return t * rho * ux + rho * ux * uz * uz;
+        case 16: return t * rho * uy + rho * uy * uz * uz;
+        case 17: return n * rho + t * rho * uy * uy + t * rho * uz * uz + rho * uy * uy * uz * uz;
+        case 18: return n * rho + t * rho * ux * ux + t * rho * uz * uz + rho * ux * ux * uz * uz;
+        case 19: return n * rho + t * rho * ux * ux + t * rho * uy * uy + rho * ux * ux * uy * uy;
+        case 20: return t * rho * uy * uz;
+        case 21: return t * rho * ux * uz;
+        default: return t * rho * ux * uy;
     }
 }
 
-// acc + c * v written the way the generated code writes the term.
-LBM_HD float mbbcTerm(float acc, float c, float v) {
-    if (c == 1.f) return acc + v;
-    if (c == -1.f) return acc - v;
-    return acc + c * v;
-}
-
-// applyMBBC: fill the unknown populations of f.
-LBM_HD void mbbcApply(const LbmMbbcTable& T, float rho, float ux, float uy, float uz, float (&f)[27]) {
+// applyMBBC: overwrite the unknown populations of f.
+LBM_HD void mbbcApply(const MbbcDir& T, float rho, float ux, float uy, float uz, float (&f)[27]) {
     float s[LBM_MBBC_MAX_UNKNOWN];
-    for (int i = 0; i < T.nu; ++i) {
+#pragma unroll
+    for (int i = 0; i < LBM_MBBC_MAX_UNKNOWN; ++i) {
+        s[i] = 0.f;
+        if (i >= T.nu) continue;
         float smf = 0.f;
-        for (int k = 0; k < T.nk; ++k) {
-            const int c = T.smfk[i][k];
-            if (c != 0) smf = mbbcTerm(smf, float(c), f[T.known[k]]);
-        }
+#pragma unroll
+        for (int d = 0; d < 27; ++d) smf = fmaf(T.smf[i][d], f[d], smf);
         s[i] = mbbcMomentEq(T.moment[i], rho, ux, uy, uz) - smf;
     }
-    for (int r = 0; r < T.nu; ++r) {
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        if (!(T.unknownMask >> d & 1u)) continue;
         float v = 0.f;
-        for (int j = 0; j < T.nu; ++j) {
-            const float c = T.inv[r][j];
-            if (c != 0.f) v = mbbcTerm(v, c, s[j]);
-        }
-        f[T.unknown[r]] = v;
+#pragma unroll
+        for (int j = 0; j < LBM_MBBC_MAX_UNKNOWN; ++j) v = fmaf(T.inv[d][j], s[j], v);
+        f[d] = v;
     }
 }
 
 // restoreRho: density from the known populations and the velocity.
-LBM_HD float mbbcRestoreRho(const LbmMbbcTable& T, float ux, float uy, float uz, const float (&f)[27]) {
+LBM_HD float mbbcRestoreRho(const MbbcDir& T, float ux, float uy, float uz, const float (&f)[27]) {
     const float scqu = T.rhoQu[0] * ux + T.rhoQu[1] * uy + T.rhoQu[2] * uz;
     const float s = T.rhoQ + scqu;
     float scmf = 0.f;
-    for (int k = 0; k < T.nk; ++k) {
-        const float c = T.rhoMfk[k];
-        if (c != 0.f) scmf = mbbcTerm(scmf, c, f[T.known[k]]);
-    }
+#pragma unroll
+    for (int d = 0; d < 27; ++d) scmf = fmaf(T.rhoMfk[d], f[d], scmf);
     return scmf / s;
 }
 
-// restoreUxUyUz: velocity from the known populations and the density.
-// Faces use the closed form (normal velocity from rhoZ, tangential velocity
-// from k_nnt = 0); edges and corners solve the table's 3x3 relation.
-LBM_HD void mbbcRestoreU(const LbmMbbcTable& T, int nx, int ny, int nz, float rho, const float (&f)[27],
-                         float& ux, float& uy, float& uz) {
+// restoreUxUyUz: faces by the closed form (normal velocity from the
+// known-population density, tangential velocity from a vanishing k_nnt),
+// edges and corners from three moment relations free of the unknowns.
+LBM_HD void mbbcRestoreU(const MbbcDir& T, float rho, const float (&f)[27], float& ux, float& uy, float& uz) {
+    const int nx = T.nx, ny = T.ny, nz = T.nz;
     if (T.face) {
-        const int n[3] = {nx, ny, nz};
         float fZero = 0.f, fPlus = 0.f;
+#pragma unroll
         for (int d = 0; d < 27; ++d) {
             const int cn = cx(d) * nx + cy(d) * ny + cz(d) * nz;
             if (cn == 0) fZero = fZero + f[d];
@@ -106,12 +138,15 @@ LBM_HD void mbbcRestoreU(const LbmMbbcTable& T, int nx, int ny, int nz, float rh
         const float uNormal = (fZero + 2.f * fPlus) / rho - 1.f;
         const float den = fZero + 2.f * (uNormal + 1.f) * rho * uNormal;
         float u[3];
+#pragma unroll
         for (int a = 0; a < 3; ++a) {
-            if (n[a] != 0) {
-                u[a] = n[a] > 0 ? uNormal : -uNormal;
+            const int na = a == 0 ? nx : a == 1 ? ny : nz;
+            if (na != 0) {
+                u[a] = na > 0 ? uNormal : -uNormal;
                 continue;
             }
             float jZero = 0.f, jPlus = 0.f;
+#pragma unroll
             for (int d = 0; d < 27; ++d) {
                 const int cn = cx(d) * nx + cy(d) * ny + cz(d) * nz;
                 const int ca = a == 0 ? cx(d) : a == 1 ? cy(d) : cz(d);
@@ -127,21 +162,19 @@ LBM_HD void mbbcRestoreU(const LbmMbbcTable& T, int nx, int ny, int nz, float rh
         return;
     }
     float s[3];
+#pragma unroll
     for (int i = 0; i < 3; ++i) {
         float acc = 0.f;
-        for (int k = 0; k < T.nk; ++k) {
-            const float c = T.uMfk[i][k];
-            if (c != 0.f) acc = mbbcTerm(acc, c, f[T.known[k]]);
-        }
+#pragma unroll
+        for (int d = 0; d < 27; ++d) acc = fmaf(T.uMfk[i][d], f[d], acc);
         s[i] = acc / rho - T.uQ[i];
     }
     float u[3];
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
         float v = 0.f;
-        for (int j = 0; j < 3; ++j) {
-            const float c = T.uInv[a][j];
-            if (c != 0.f) v = mbbcTerm(v, c, s[j]);
-        }
+#pragma unroll
+        for (int j = 0; j < 3; ++j) v = fmaf(T.uInv[a][j], s[j], v);
         u[a] = v;
     }
     ux = u[0];

@@ -15,6 +15,7 @@
 // most one cell).  The esotwist scheme makes every slot read and written by
 // exactly one thread per step, so the kernel needs no second buffer and no
 // synchronisation between cells.
+#define LBM_MBBC_TYPES_ONLY
 #include "builder.h"
 #include "mbbc.h"
 #include "step_launch.h"
@@ -471,22 +472,33 @@ __device__ __forceinline__ float nonReflectiveUNormal(float uTarget, float dRhoZ
     return numerator / denominator;
 }
 
-// K2 (include/updateGrid.h:181-355): one thread per open-boundary cell, run
-// after the flip, so F is the flipper of the next step's pre-collision read.
-// Known populations (c.n >= 0 on every axis) are read and weight-compensated,
-// the missing macroscopic quantity is restored, the unknown populations are
-// closed from equilibrium moments and written to the cell's own
-// pre-collision slots.  All open-boundary IDs go in one launch: their cells
-// are disjoint and a cell touches only its own 27 slots, so the reference's
-// loop over IDs gives the same result in any order.
+// K2 (include/updateGrid.h:181-355), run after the flip, so F is the flipper
+// of the next step's pre-collision read.  Open cells are grouped by outer
+// normal into chunks of kOpenChunk; one CTA takes one chunk and stages that
+// normal's direction-indexed closure tables in shared memory, so every thread
+// of the CTA follows the same branches and its 27 populations stay in
+// registers.  Known populations (c.n >= 0 on every axis) are read and
+// weight-compensated, the missing macroscopic quantity is restored, the
+// unknown populations are closed from equilibrium moments and written to the
+// cell's own pre-collision slots.  All open-boundary IDs go in one launch:
+// their cells are disjoint and a cell touches only its own 27 slots, so the
+// reference's loop over IDs gives the same result in any order.
 template <bool F, class S>
-__global__ void __launch_bounds__(kBlock) openBoundary(DevLevel g, int iterationsFinished) {
-    const int idx = blockIdx.x * kBlock + threadIdx.x;
-    if (idx >= g.obCount) return;
+__global__ void __launch_bounds__(kOpenChunk) openBoundary(DevLevel g, int iterationsFinished) {
+    __shared__ MbbcDir T;
+    const int4 chunk = g.obChunk[blockIdx.x];  // {first, count, normal row, -}
+    {
+        const int* src = reinterpret_cast<const int*>(g.obTables + chunk.z);
+        int* dst = reinterpret_cast<int*>(&T);
+        for (int q = threadIdx.x; q < int(sizeof(MbbcDir) / 4); q += kOpenChunk) dst[q] = __ldg(src + q);
+    }
+    __syncthreads();
+    if (int(threadIdx.x) >= chunk.y) return;
+    const int idx = __ldg(g.obOrder + chunk.x + threadIdx.x);
     const int cell = __ldg(g.obCell + idx);
     const int info = __ldg(g.obInfo + idx);
-    const int nx = ((info >> 3) & 3) - 1, ny = ((info >> 5) & 3) - 1, nz = ((info >> 7) & 3) - 1;
-    const LbmMbbcTable& T = kLbmMbbc[(info >> 10) & 31];
+    const int nx = T.nx, ny = T.ny, nz = T.nz;
+    const unsigned unknown = T.unknownMask;
     int nb[8];
     decodeNbr(g, cell, nb, nullptr);
     S* base = static_cast<S*>(g.f);
@@ -495,7 +507,7 @@ __global__ void __launch_bounds__(kBlock) openBoundary(DevLevel g, int iteration
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         f[d] = 0.f;
-        if (nx * cx(d) < 0 || ny * cy(d) < 0 || nz * cz(d) < 0) continue;
+        if (unknown >> d & 1u) continue;
         f[d] = Store<S>::ld(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
         if (nx * cx(d) + ny * cy(d) + nz * cz(d) == 0) dRhoZ += f[d];
         else dRhoZ += 2.f * f[d];
@@ -511,7 +523,7 @@ __global__ void __launch_bounds__(kBlock) openBoundary(DevLevel g, int iteration
             const float uNormal = nonReflectiveUNormal(uNormalRef, dRhoZ, dRho);
             dRho = (dRhoZ - uNormal) / (1.f + uNormal);
         }
-        mbbcRestoreU(T, nx, ny, nz, dRho + 1.f, f, ux, uy, uz);
+        mbbcRestoreU(T, dRho + 1.f, f, ux, uy, uz);
     } else if ((info & 3) == 1) {  // velocity: velocity given, density restored
         if (nonReflective) {
             float uTarget = 0.f;
@@ -528,7 +540,7 @@ __global__ void __launch_bounds__(kBlock) openBoundary(DevLevel g, int iteration
     mbbcApply(T, dRho + 1.f, ux, uy, uz, f);
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
-        if (!(nx * cx(d) < 0 || ny * cy(d) < 0 || nz * cz(d) < 0)) continue;
+        if (!(unknown >> d & 1u)) continue;
         Store<S>::st(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)], f[d] - weight(d));
     }
     // reference values: exponential average whose weight decays with the
@@ -758,7 +770,7 @@ template <bool F, class S> struct RunPeriodic {
 };
 template <bool F, class S> struct RunOpen {
     static void run(const DevLevel& g, cudaStream_t s, int iterationsFinished) {
-        if (g.obCount > 0) openBoundary<F, S><<<blocksFor(g.obCount), kBlock, 0, s>>>(g, iterationsFinished);
+        if (g.obChunkCount > 0) openBoundary<F, S><<<g.obChunkCount, kOpenChunk, 0, s>>>(g, iterationsFinished);
     }
 };
 template <bool F, class S> struct RunOpenInit {
@@ -795,6 +807,12 @@ template <bool F, class S> struct RunScatter {
 }  // namespace
 
 void launchCollideStream(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunCollide>(g, flip, s); }
+int stepLaunchCount(const DevLevel& g) {
+    int n = 0;
+    if (collideVariant() == CollideVariant::Simple) n += g.cellCount > 0;
+    else n += (g.segCount > 0) + (g.specialCount > 0);
+    return n + (g.obCount > 0) + (g.perCount > 0);
+}
 void launchPeriodic(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunPeriodic>(g, flip, s); }
 void launchOpenBoundary(const DevLevel& g, bool flip, cudaStream_t s, int iterationsFinished) {
     dispatch<RunOpen>(g, flip, s, iterationsFinished);

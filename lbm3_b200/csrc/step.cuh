@@ -12,6 +12,11 @@
 
 namespace lbm {
 
+// open-boundary cells per CTA of the boundary kernel
+constexpr int kOpenChunk = 128;
+
+struct MbbcDir;
+
 // Everything a kernel needs for one level, passed by value.
 struct DevLevel {
     void* f;                 // populations [27][stride], element type per storage
@@ -58,6 +63,12 @@ struct DevLevel {
     float* obUnCum;                // uNormalCumulativeArray
     int obCount;
     int trackOpen;
+    // open cells grouped by outer normal: obOrder lists ID-order indices, each
+    // chunk {first, count, normal row, 0} is one CTA of the boundary kernel
+    const int* obOrder;
+    const int4* obChunk;
+    int obChunkCount;
+    const MbbcDir* obTables;          // [26] direction-indexed closure tables
     int nx, ny, nz;
     float res, ox, oy, oz;
     CollisionConsts coll;

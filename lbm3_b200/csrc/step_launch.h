@@ -9,6 +9,8 @@
 namespace lbm {
 
 void launchCollideStream(const DevLevel& g, bool flip, cudaStream_t s);
+// kernels one updateSingleGrid launches for this level
+int stepLaunchCount(const DevLevel& g);
 void launchPeriodic(const DevLevel& g, bool flip, cudaStream_t s);
 void launchOpenBoundary(const DevLevel& g, bool flip, cudaStream_t s, int iterationsFinished);
 void launchOpenBoundaryInit(const DevLevel& g, bool flip, cudaStream_t s);

@@ -140,6 +140,12 @@ class Grids:
         A.check(A.lib().lbm_time_steps(self._h, int(steps), C.byref(ms)))
         return ms.value
 
+    def last_launch_count(self) -> int:
+        """Every kernel launch of the last time_steps call."""
+        n = C.c_longlong()
+        A.check(A.lib().lbm_last_launch_count(self._h, C.byref(n)))
+        return n.value
+
     def last_kernel_time(self):
         """(summed ms, launch count) of the collide-stream launches of the last time_steps."""
         ms, n = C.c_float(), C.c_int()
