@@ -78,7 +78,8 @@ struct LevelState {
     int wallAdjacentCount = 0;
     int openBCCount = 0;
     std::vector<int> openTrackCount;   // trackFlowCount per openBCID
-    int* obSource = nullptr;           // openBCs[id].sourceArray, concatenated
+    int* obSource = nullptr;           // openBCs[id].sourceArray, concatenated (ID order)
+    std::vector<int> obPerm;           // kernel position -> ID-order index of open cells
     unsigned long long memBytes = 0;
     lbm::DevLevel dev{};
     std::vector<void*> owned;
@@ -357,6 +358,8 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
             // 256 bytes of tail so bulk copies rounded up to 16 bytes stay inside
             d.f = own(devAlloc<unsigned char>(27ULL * d.stride * storageBytes(c->storage) + 256));
             d.errorFlag = g->errorFlag;
+            d.work = own(devAlloc<int>(2));
+            ck(cudaMemsetAsync(d.work, 0, 2 * sizeof(int), s), "memset");
             d.shifter = own(upload(H.shifter, s));
             d.rowI = own(upload(H.rowI, s));
             d.rowJ = own(upload(H.rowJ, s));
@@ -386,22 +389,43 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
             d.wallForce = own(devAlloc<float>(3 * H.wallIndex.size()));
             if (d.wallForce) ck(cudaMemsetAsync(d.wallForce, 0, 3 * H.wallIndex.size() * sizeof(float), s), "memset");
             {
-                // open boundaries: per-cell records in ID order; the two
-                // reference and two cumulative arrays are contiguous pairs
+                // open boundaries.  The device keeps the per-cell records in
+                // kernel order: cells grouped by outer normal (table row) into
+                // CTA-sized chunks, each group in ID order.  obPerm maps a
+                // kernel position back to the ID order the ABI reports.
                 const size_t m = H.openCells.size();
+                std::vector<lbm::MbbcDir> tables(LBM_MBBC_NORMALS);
+                for (int t = 0; t < LBM_MBBC_NORMALS; ++t) tables[t] = lbm::mbbcDirFromTable(kLbmMbbc[t]);
+                std::vector<int> order;
+                std::vector<int4> chunks;
+                order.reserve(m);
+                for (int row = 0; row < LBM_MBBC_NORMALS; ++row) {
+                    const int first = static_cast<int>(order.size());
+                    for (size_t q = 0; q < m; ++q)
+                        if (((H.openCells[q].info >> 10) & 31) == row) order.push_back(static_cast<int>(q));
+                    const int count = static_cast<int>(order.size()) - first;
+                    for (int c0 = 0; c0 < count; c0 += lbm::kOpenChunk)
+                        chunks.push_back(make_int4(first + c0, std::min(lbm::kOpenChunk, count - c0), row,
+                                                   static_cast<int>(tables[row].unknownMask)));
+                }
                 std::vector<int> cell(m), info(m), source;
+                std::vector<int4> nbr(m);
                 std::vector<float4> target(m);
                 std::vector<float> beta(m);
-                for (size_t q = 0; q < m; ++q) {
-                    const lbm::OpenBCCell& oc = H.openCells[q];
-                    cell[q] = oc.cell;
-                    info[q] = oc.info;
-                    target[q] = make_float4(oc.dRho, oc.ux, oc.uy, oc.uz);
-                    beta[q] = oc.beta;
+                for (size_t p = 0; p < m; ++p) {
+                    const lbm::OpenBCCell& oc = H.openCells[order[p]];
+                    cell[p] = oc.cell;
+                    const int jp = H.jPlus[oc.cell], kp = H.kPlus[oc.cell];
+                    nbr[p] = make_int4(oc.cell, jp, kp, H.jPlus[kp]);
+                    info[p] = oc.info;
+                    target[p] = make_float4(oc.dRho, oc.ux, oc.uy, oc.uz);
+                    beta[p] = oc.beta;
                 }
                 for (const auto& ob : H.openBCs) source.insert(source.end(), ob.source.begin(), ob.source.end());
+                L.obPerm = order;
                 d.obCount = static_cast<int>(m);
                 d.obCell = own(upload(cell, s));
+                d.obNbr = own(upload(nbr, s));
                 d.obInfo = own(upload(info, s));
                 d.obTarget = own(upload(target, s));
                 d.obBeta = own(upload(beta, s));
@@ -412,22 +436,6 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
                 d.obUnCum = d.obRhoCum ? d.obRhoCum + m : nullptr;
                 if (m) ck(cudaMemsetAsync(d.obRhoCum, 0, 2 * m * sizeof(float), s), "memset");
                 d.trackOpen = c->track_open_boundaries ? 1 : 0;
-                // group the cells by outer normal into CTA-sized chunks; the
-                // boundary kernel stages one normal's tables per CTA
-                std::vector<int> order;
-                std::vector<int4> chunks;
-                order.reserve(m);
-                for (int row = 0; row < LBM_MBBC_NORMALS; ++row) {
-                    const int first = static_cast<int>(order.size());
-                    for (size_t q = 0; q < m; ++q)
-                        if (((info[q] >> 10) & 31) == row) order.push_back(static_cast<int>(q));
-                    const int count = static_cast<int>(order.size()) - first;
-                    for (int c0 = 0; c0 < count; c0 += lbm::kOpenChunk)
-                        chunks.push_back(make_int4(first + c0, std::min(lbm::kOpenChunk, count - c0), row, 0));
-                }
-                std::vector<lbm::MbbcDir> tables(LBM_MBBC_NORMALS);
-                for (int t = 0; t < LBM_MBBC_NORMALS; ++t) tables[t] = lbm::mbbcDirFromTable(kLbmMbbc[t]);
-                d.obOrder = own(upload(order, s));
                 d.obChunk = own(upload(chunks, s));
                 d.obChunkCount = static_cast<int>(chunks.size());
                 d.obTables = m ? own(upload(tables, s)) : nullptr;
@@ -640,6 +648,16 @@ int lbm_read_array(lbm_grids* g, int level, int which, void* host, size_t bytes)
                 throw;
             }
             cudaFree(tmp);
+        } else if (which == LBM_ARRAY_OPEN_INDEX || which == LBM_ARRAY_OPEN_REFERENCE ||
+                   which == LBM_ARRAY_OPEN_CUMULATIVE) {
+            // device arrays are in kernel order; report them in ID order
+            std::vector<uint32_t> tmp(need / 4);
+            ck(cudaMemcpyAsync(tmp.data(), src, need, cudaMemcpyDeviceToHost, g->stream), "copy");
+            ck(cudaStreamSynchronize(g->stream), "sync");
+            const size_t m = L.obPerm.size();
+            uint32_t* out = static_cast<uint32_t*>(host);
+            for (size_t part = 0; part < tmp.size() / (m ? m : 1); ++part)
+                for (size_t p = 0; p < m; ++p) out[part * m + L.obPerm[p]] = tmp[part * m + p];
         } else {
             ck(cudaMemcpyAsync(host, src, need, cudaMemcpyDeviceToHost, g->stream), "copy");
             ck(cudaStreamSynchronize(g->stream), "sync");

@@ -267,42 +267,6 @@ __global__ void __launch_bounds__(kTile, LBM3_TMA_MIN_BLOCKS) collideBulkTma(Dev
     }
 }
 
-template <bool F, class S>
-__global__ void __launch_bounds__(kTile, LBM3_PREFETCH_MIN_BLOCKS) collidePrefetch(DevLevel g) {
-    const int T = g.segCount;
-    const int G = gridDim.x;
-    const int t = threadIdx.x;
-    int tile = blockIdx.x;
-    int4 dCur, dNext;
-    int lCur, lNext;
-    loadDesc(g, tile, dCur, lCur);
-    loadDesc(g, tile + G, dNext, lNext);
-    int nb[8];
-    segNbr(g, dCur, t, nb);
-    float fn[27];
-    if (t < lCur) readPre<F, S>(g, nb, fn);
-    for (; tile < T; tile += G) {
-        int4 dAfter;
-        int lAfter;
-        loadDesc(g, tile + 2 * G, dAfter, lAfter);
-        float f[27];
-#pragma unroll
-        for (int q = 0; q < 27; ++q) f[q] = fn[q];
-        int nbn[8];
-        segNbr(g, dNext, t, nbn);
-        if (t < lNext) readPre<F, S>(g, nbn, fn);
-        if (t < lCur) {
-            collideCumulant(f, g.coll, g.coll.lambda, g.gx, g.gy, g.gz);
-            writePost<F, S>(g, nb, f);
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) nb[q] = nbn[q];
-        lCur = lNext;
-        dNext = dAfter;
-        lNext = lAfter;
-    }
-}
-
 // Cells outside the bulk segments, one thread per listed cell: wall-adjacent
 // fluid cells get the interpolated bounceback of Zhao & Yong (2017) with a
 // moving-wall term and momentum-exchange force
@@ -310,10 +274,7 @@ __global__ void __launch_bounds__(kTile, LBM3_PREFETCH_MIN_BLOCKS) collidePrefet
 // and the write loop of include/updateGrid.h:143-176); the rest (cells whose
 // +1 neighbour wraps) collide and stream like bulk cells.
 template <bool F, class S>
-__global__ void __launch_bounds__(kBlock) collideList(DevLevel g) {
-    const int idx = blockIdx.x * kBlock + threadIdx.x;
-    if (idx >= g.specialCount) return;
-    const int cell = __ldg(g.special + idx);
+__device__ __forceinline__ void collideSpecialCell(const DevLevel& g, int cell) {
     const int wm = __ldg(g.wallMap + cell);
     int nb[8];
     decodeNbr(g, cell, nb, nullptr);
@@ -372,6 +333,76 @@ __global__ void __launch_bounds__(kBlock) collideList(DevLevel g) {
         g.wallForce[wm] += fx;
         g.wallForce[nw + wm] += fy;
         g.wallForce[2 * nw + wm] += fz;
+    }
+}
+
+template <bool F, class S>
+__global__ void __launch_bounds__(kBlock) collideList(DevLevel g) {
+    const int idx = blockIdx.x * kBlock + threadIdx.x;
+    if (idx >= g.specialCount) return;
+    collideSpecialCell<F, S>(g, __ldg(g.special + idx));
+}
+
+// Work items of one launch: special chunks [0, S) first (kTile listed cells
+// each), then the bulk segments [S, S + segCount).  CTAs take items from an
+// atomic counter, so the long-latency wall-adjacent cells land on whichever
+// CTAs are free first and the bulk tail stays balanced; the last CTA to
+// finish resets the counter for the next launch.  Thread 0 fetches; the
+// value reaches the CTA through a two-slot shared buffer and one barrier.
+template <bool F, class S>
+__global__ void __launch_bounds__(kTile, LBM3_PREFETCH_MIN_BLOCKS) collidePrefetch(DevLevel g) {
+    __shared__ int slot[2];
+    const int nSpecial = (g.specialCount + kTile - 1) / kTile;
+    const int t = threadIdx.x;
+    int parity = 0;
+    auto fetch = [&]() {
+        if (t == 0) slot[parity] = atomicAdd(g.work, 1);
+        __syncthreads();
+        const int v = slot[parity];
+        parity ^= 1;
+        return v;
+    };
+    int item = fetch();
+    while (item < nSpecial) {
+        const int q = item * kTile + t;
+        if (q < g.specialCount) collideSpecialCell<F, S>(g, __ldg(g.special + q));
+        item = fetch();
+    }
+    int4 dCur, dNext;
+    int lCur, lNext;
+    loadDesc(g, item - nSpecial, dCur, lCur);
+    loadDesc(g, fetch() - nSpecial, dNext, lNext);
+    int nb[8];
+    segNbr(g, dCur, t, nb);
+    float fn[27];
+    if (t < lCur) readPre<F, S>(g, nb, fn);
+    while (lCur > 0) {  // CTA-uniform: lengths come from the shared descriptors
+        int4 dAfter;
+        int lAfter;
+        loadDesc(g, fetch() - nSpecial, dAfter, lAfter);
+        float f[27];
+#pragma unroll
+        for (int q = 0; q < 27; ++q) f[q] = fn[q];
+        int nbn[8];
+        segNbr(g, dNext, t, nbn);
+        if (t < lNext) readPre<F, S>(g, nbn, fn);
+        if (t < lCur) {
+            collideCumulant(f, g.coll, g.coll.lambda, g.gx, g.gy, g.gz);
+            writePost<F, S>(g, nb, f);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) nb[q] = nbn[q];
+        lCur = lNext;
+        dNext = dAfter;
+        lNext = lAfter;
+    }
+    if (t == 0) {
+        __threadfence();
+        if (atomicAdd(g.work + 1, 1) == int(gridDim.x) - 1) {
+            g.work[0] = 0;
+            g.work[1] = 0;
+            __threadfence();
+        }
     }
 }
 
@@ -486,29 +517,44 @@ __device__ __forceinline__ float nonReflectiveUNormal(float uTarget, float dRhoZ
 template <bool F, class S>
 __global__ void __launch_bounds__(kOpenChunk) openBoundary(DevLevel g, int iterationsFinished) {
     __shared__ MbbcDir T;
-    const int4 chunk = g.obChunk[blockIdx.x];  // {first, count, normal row, -}
+    const int4 chunk = __ldg(g.obChunk + blockIdx.x);  // {first, count, normal row, unknown mask}
     {
         const int* src = reinterpret_cast<const int*>(g.obTables + chunk.z);
         int* dst = reinterpret_cast<int*>(&T);
         for (int q = threadIdx.x; q < int(sizeof(MbbcDir) / 4); q += kOpenChunk) dst[q] = __ldg(src + q);
     }
-    __syncthreads();
-    if (int(threadIdx.x) >= chunk.y) return;
-    const int idx = __ldg(g.obOrder + chunk.x + threadIdx.x);
-    const int cell = __ldg(g.obCell + idx);
+    // everything that does not need the tables is loaded before the barrier,
+    // so the population gathers overlap the table staging
+    const bool active = int(threadIdx.x) < chunk.y;
+    const int idx = chunk.x + (active ? int(threadIdx.x) : 0);
     const int info = __ldg(g.obInfo + idx);
-    const int nx = T.nx, ny = T.ny, nz = T.nz;
-    const unsigned unknown = T.unknownMask;
+    const int4 rows = __ldg(g.obNbr + idx);
+    const int nx = ((info >> 3) & 3) - 1, ny = ((info >> 5) & 3) - 1, nz = ((info >> 7) & 3) - 1;
+    const unsigned unknown = static_cast<unsigned>(chunk.w);
+    const int n = g.cellCount;
     int nb[8];
-    decodeNbr(g, cell, nb, nullptr);
+    nb[0] = rows.x;
+    nb[1] = rows.x + 1 < n ? rows.x + 1 : 0;
+    nb[2] = rows.y;
+    nb[3] = rows.y + 1 < n ? rows.y + 1 : 0;
+    nb[4] = rows.z;
+    nb[5] = rows.z + 1 < n ? rows.z + 1 : 0;
+    nb[6] = rows.w;
+    nb[7] = rows.w + 1 < n ? rows.w + 1 : 0;
     S* base = static_cast<S*>(g.f);
     float f[27];
-    float dRhoZ = 0.f;
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         f[d] = 0.f;
+        if (active && !(unknown >> d & 1u))
+            f[d] = Store<S>::ld(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
+    }
+    __syncthreads();
+    if (!active) return;
+    float dRhoZ = 0.f;
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
         if (unknown >> d & 1u) continue;
-        f[d] = Store<S>::ld(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
         if (nx * cx(d) + ny * cy(d) + nz * cz(d) == 0) dRhoZ += f[d];
         else dRhoZ += 2.f * f[d];
         f[d] += weight(d);  // the closure is ill-conditioned on shifted populations
@@ -753,11 +799,17 @@ template <bool F, class S> struct RunCollide {
                     persistentGrid(collideBulkTma<!F, S>, tmaSmemBytes<S>());
                 }
                 collideBulkTma<F, S><<<std::min(grid, g.segCount), kTile, tmaSmemBytes<S>(), s>>>(g);
-            } else {
+            }
+        }
+        if (v == CollideVariant::Prefetch) {
+            // bulk segments and listed cells in one persistent launch
+            const int items = g.segCount + (g.specialCount + kTile - 1) / kTile;
+            if (items > 0) {
                 static int grid = 0;
                 if (grid == 0) grid = persistentGrid(collidePrefetch<F, S>, 0);
-                collidePrefetch<F, S><<<std::min(grid, g.segCount), kTile, 0, s>>>(g);
+                collidePrefetch<F, S><<<std::min(grid, items), kTile, 0, s>>>(g);
             }
+            return;
         }
         if (g.specialCount > 0) collideList<F, S><<<blocksFor(g.specialCount), kBlock, 0, s>>>(g);
     }
@@ -809,7 +861,9 @@ template <bool F, class S> struct RunScatter {
 void launchCollideStream(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunCollide>(g, flip, s); }
 int stepLaunchCount(const DevLevel& g) {
     int n = 0;
-    if (collideVariant() == CollideVariant::Simple) n += g.cellCount > 0;
+    const CollideVariant v = collideVariant();
+    if (v == CollideVariant::Simple) n += g.cellCount > 0;
+    else if (v == CollideVariant::Prefetch) n += (g.segCount + g.specialCount) > 0;
     else n += (g.segCount > 0) + (g.specialCount > 0);
     return n + (g.obCount > 0) + (g.perCount > 0);
 }

@@ -42,6 +42,8 @@ struct DevLevel {
     const int* special;
     int specialCount;
     int* errorFlag;          // set to nonzero when a bounded device wait gives up
+    int* work;               // [2] work-item counter and finished-CTA count of the
+                             // persistent collide-stream (zero between launches)
     // wall-adjacent cells (WallStruct)
     const unsigned* wallData;      // [wallCount]
     const unsigned* linkLength;    // [7][wallCount] packed 8-bit link codes
@@ -52,8 +54,9 @@ struct DevLevel {
     int trackWallForce;
     int useIBB;
     float gx, gy, gz;              // body force (getLocalBC)
-    // open-boundary cells (OpenBCArrayStruct, all IDs concatenated)
+    // open-boundary cells (OpenBCArrayStruct, all IDs), in kernel order
     const int* obCell;
+    const int4* obNbr;             // {cell, jPlus, kPlus, jkPlus} row neighbours
     const int* obInfo;             // packed, see OpenBCCell
     const float4* obTarget;        // dRho, ux, uy, uz of getOpenBC
     const float* obBeta;
@@ -63,9 +66,8 @@ struct DevLevel {
     float* obUnCum;                // uNormalCumulativeArray
     int obCount;
     int trackOpen;
-    // open cells grouped by outer normal: obOrder lists ID-order indices, each
-    // chunk {first, count, normal row, 0} is one CTA of the boundary kernel
-    const int* obOrder;
+    // cells are grouped by outer normal; each chunk {first, count, normal row,
+    // unknown-direction mask} is one CTA of the boundary kernel
     const int4* obChunk;
     int obChunkCount;
     const MbbcDir* obTables;          // [26] direction-indexed closure tables
