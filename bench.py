@@ -287,7 +287,7 @@ def run_ours(args):
     if tfile.exists():
         tr = json.loads(tfile.read_text()).get(f"{args.workload}:{args.storage}")
         if tr:
-            traffic = tr
+            traffic = int(tr)  # bytes per launch, like algorithmic_bytes_per_launch
 
     # end to end through the public API: upload the initial state from pinned
     # host memory, then run steps that each read the step's observable back
@@ -339,9 +339,9 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
-                         "kernel": "collide-stream (bulk collidePrefetch + special-cell collideList)",
+                         "kernel": "collidePrefetch (bulk segments + wall-adjacent cells, one persistent launch)",
                          "kernel_ms_per_launch": round(per_launch_ms, 5),
-                         "algorithmic_bytes_per_launch": alg_bytes},
+                         "algorithmic_bytes_per_launch": alg_bytes, "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)"},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS",
                     "h2d_bytes_per_step": int(f0.nbytes // e2e_steps), "d2h_bytes_per_step": 48 if sphere else 8,
