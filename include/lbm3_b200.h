@@ -84,8 +84,42 @@ extern "C" {
                                      IDs concatenated in ID order               */
 #define LBM_ARRAY_OPEN_SOURCE  18 /* int32  [openBCCount]   openBCs[id].sourceArray, same order */
 #define LBM_ARRAY_OPEN_REFERENCE 19 /* float [2][openBCCount] dRhoRefArray, uNormalRefArray */
+/* rotor tables: id = LBM_ARRAY_ROTOR_BASE + 4 * rotor + one of:
+ *   0 int32  [block_count]              rotorMapArray (-1 or compact block index)
+ *   1 int32  [nonzero_block_count]      indexArray
+ *   2 uint32 [64 * nonzero_block_count] interpolationArray (8 x 4-bit counts)
+ *   3 float  [3][27 * nonzero_block_count] gx, gy, gz force bins in the rotor
+ *            frame, accumulated since the last tracker reset (grids only) */
+#define LBM_ARRAY_ROTOR_BASE   32
 #define LBM_ARRAY_OPEN_CUMULATIVE 20 /* float [2][openBCCount] dRhoCumulativeArray,
                                      uNormalCumulativeArray since the last tracker reset */
+
+/* A rotor forced towards rigid rotation (RotorStruct, include/types.h:206-219):
+ * triangles of its surface at angle 0 (mm), the axis it turns about (parallel
+ * to x, y or z through `origin`) and its speed.  Cells inside the rotor, in
+ * the rotor's own frame, are forced towards the rotor velocity with a
+ * smooth volume fraction (processRotor, include/rotorFunctions.h:211-304). */
+#define LBM_MAX_ROTORS 4
+typedef struct lbm_rotor {
+    const float* triangles;     /* [triangle_count][9]                        */
+    int   triangle_count;
+    int   axis;                 /* 0: rotateAlongX, 1: Y, 2: Z                */
+    float origin[3];            /* InfoRotor.ox, oy, oz (mm)                  */
+    float radians_per_second;   /* InfoRotor.radiansPerSecond                 */
+} lbm_rotor;
+
+/* Rotor tables of one level (RotorInfoStruct plus table sizes). */
+typedef struct lbm_rotor_info {
+    float res;                  /* half the level spacing (mm)                */
+    float bounds[6];            /* xMin, yMin, zMin, xMax, yMax, zMax (mm)    */
+    int   cell_count[3];        /* interpolation cells, multiples of 4        */
+    int   block_count;          /* 4x4x4 blocks in the bounds                 */
+    int   nonzero_block_count;  /* blocks with rotor volume                   */
+    int   axis;
+    float origin[3];
+    float radians_per_second;
+    double radians_elapsed;
+} lbm_rotor_info;
 
 /* ---- case description -------------------------------------------------- */
 
@@ -154,6 +188,11 @@ typedef struct lbm_case {
 
     /* storage */
     int   storage;              /* LBM_STORE_*                                 */
+
+    /* rotorSTLs: volume-fraction forcing rotors (include/rotorFunctions.h) */
+    int       rotor_count;
+    lbm_rotor rotor[LBM_MAX_ROTORS];
+    int       track_rotor_force;  /* TRACK_ROTOR_FORCE                         */
 } lbm_case;
 
 /* Per-level summary (InfoStruct, include/types.h:120-129, plus table sizes). */
@@ -286,6 +325,21 @@ int lbm_wall_force(lbm_grids* g, int wall_id, int reset, double* out);
  * Replaces the open-boundary branch of updateTracker
  * (include/trackerFunctions.h:127-214). */
 int lbm_open_boundary_flow(lbm_grids* g, int open_bc_id, int reset, double* out);
+
+/* Rotor tables of one level of a plan or of built grids. */
+int lbm_plan_rotor_info(lbm_plan* p, int level, int rotor, lbm_rotor_info* out);
+int lbm_get_rotor_info(lbm_grids* g, int level, int rotor, lbm_rotor_info* out);
+
+/* Change a rotor's speed between steps, as drivers set
+ * rotors[i].Info.radiansPerSecond (cases/BruteforcePumpOnly/BruteforcePump.cu:226-229). */
+int lbm_set_rotor_speed(lbm_grids* g, int rotor, float radians_per_second);
+
+/* Force and torque the rotor exerts on the fluid, in the rotor frame,
+ * averaged over the steps since the last tracker reset and summed in FP64 on
+ * the device: out = {Fx, Fy, Fz [N], Tx, Ty, Tz [N m]} about the rotor
+ * origin.  `reset` != 0 then resets every tracker accumulator.
+ * Replaces the rotor branch of updateTracker (include/trackerFunctions.h:225-300). */
+int lbm_rotor_force(lbm_grids* g, int rotor, int reset, double* out);
 
 /* Cell-wise collision on a device batch of shifted populations laid out as
  * float [27][n] (structure of arrays), in place.

@@ -84,6 +84,25 @@ class LbmBody(C.Structure):
     ]
 
 
+LBM_MAX_ROTORS = 4
+ARRAY_ROTOR_BASE = 32
+
+
+class LbmRotor(C.Structure):
+    _fields_ = [
+        ("triangles", C.POINTER(C.c_float)), ("triangle_count", C.c_int), ("axis", C.c_int),
+        ("origin", C.c_float * 3), ("radians_per_second", C.c_float),
+    ]
+
+
+class LbmRotorInfo(C.Structure):
+    _fields_ = [
+        ("res", C.c_float), ("bounds", C.c_float * 6), ("cell_count", C.c_int * 3), ("block_count", C.c_int),
+        ("nonzero_block_count", C.c_int), ("axis", C.c_int), ("origin", C.c_float * 3),
+        ("radians_per_second", C.c_float), ("radians_elapsed", C.c_double),
+    ]
+
+
 class LbmCase(C.Structure):
     _fields_ = [
         ("grid_level_count", C.c_int), ("wall_refinement_count", C.c_int),
@@ -98,6 +117,7 @@ class LbmCase(C.Structure):
         ("gx", C.c_float), ("gy", C.c_float), ("gz", C.c_float), ("use_ibb", C.c_int),
         ("body_count", C.c_int), ("body", LbmBody * LBM_MAX_BODIES),
         ("storage", C.c_int),
+        ("rotor_count", C.c_int), ("rotor", LbmRotor * LBM_MAX_ROTORS), ("track_rotor_force", C.c_int),
     ]
 
 
@@ -142,6 +162,10 @@ SIGNATURES = [
     ("lbm_kinetic_energy_noalloc", C.c_int, [_P, C.c_float, C.c_float, C.POINTER(C.c_double)]),
     ("lbm_wall_force", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     ("lbm_open_boundary_flow", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    ("lbm_plan_rotor_info", C.c_int, [_P, C.c_int, C.c_int, C.c_void_p]),
+    ("lbm_get_rotor_info", C.c_int, [_P, C.c_int, C.c_int, C.c_void_p]),
+    ("lbm_set_rotor_speed", C.c_int, [_P, C.c_int, C.c_float]),
+    ("lbm_rotor_force", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     ("lbm_apply_collision_batch", C.c_int,
      [_P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, _P]),
 ]

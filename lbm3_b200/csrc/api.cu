@@ -80,6 +80,8 @@ struct LevelState {
     std::vector<int> openTrackCount;   // trackFlowCount per openBCID
     int* obSource = nullptr;           // openBCs[id].sourceArray, concatenated (ID order)
     std::vector<int> obPerm;           // kernel position -> ID-order index of open cells
+    std::vector<lbm::HostRotor> rotors;  // host copies: info, tables (device copies in dev.rotor)
+    std::vector<int*> rotorIndex;        // device indexArray per rotor
     unsigned long long memBytes = 0;
     lbm::DevLevel dev{};
     std::vector<void*> owned;
@@ -161,7 +163,24 @@ namespace {
 
 // updateSingleGrid (include/updateGrid.h:16-386): K1, flip, open boundary,
 // periodic copy.
+// Advance every rotor's angle by one step (include/updateGrid.h:36-49) and
+// hand its cosine and sine to the kernels.
+void advanceRotors(LevelState& L) {
+    constexpr double twoPi = 6.283185307179586476925286766559;
+    for (size_t r = 0; r < L.rotors.size(); ++r) {
+        lbm::HostRotor& R = L.rotors[r];
+        R.radiansElapsed = std::fmod(R.radiansElapsed + static_cast<double>(L.info.dtPhys) * R.radiansPerSecond, twoPi);
+        if (R.radiansElapsed < 0.0) R.radiansElapsed += twoPi;
+        if (R.radiansElapsed >= twoPi) R.radiansElapsed = 0.0;
+        const float angle = static_cast<float>(R.radiansElapsed);
+        L.dev.rotor[r].c = std::cos(angle);
+        L.dev.rotor[r].s = std::sin(angle);
+        L.dev.rotor[r].scale = R.radiansPerSecond * L.info.dtPhys / L.info.res;
+    }
+}
+
 void updateSingleGrid(lbm_grids* g, LevelState& L) {
+    if (!L.rotors.empty()) advanceRotors(L);
     const bool flip = L.info.esotwistFlipper;
     if (g->timingKernels) {
         const size_t k = static_cast<size_t>(g->kernelEventsUsed);
@@ -277,6 +296,18 @@ int lbm_plan_read_array(lbm_plan* p, int level, int which, void* host, size_t by
         openIndex.insert(openIndex.end(), ob.index.begin(), ob.index.end());
         openSource.insert(openSource.end(), ob.source.begin(), ob.source.end());
     }
+    if (which >= LBM_ARRAY_ROTOR_BASE) {
+        const int r = (which - LBM_ARRAY_ROTOR_BASE) / 4, part = (which - LBM_ARRAY_ROTOR_BASE) % 4;
+        if (r >= (int)H.rotors.size() || part == 3)
+            return fail(LBM_ERR_INVALID, "lbm_plan_read_array: no such rotor table in a plan");
+        const lbm::HostRotor& R = H.rotors[r];
+        const void* src = part == 0 ? (const void*)R.rotorMap.data() : part == 1 ? (const void*)R.index.data()
+                                                                                 : (const void*)R.interpolation.data();
+        const size_t need = 4 * (part == 0 ? R.rotorMap.size() : part == 1 ? R.index.size() : R.interpolation.size());
+        if (bytes != need) return fail(LBM_ERR_INVALID, "lbm_plan_read_array: byte count does not match array size");
+        if (bytes) std::memcpy(host, src, bytes);
+        return LBM_OK;
+    }
     if (which == LBM_ARRAY_WALL_VELOCITY) {
         const size_t need = H.wallVelocity.size() * sizeof(float);
         if (bytes != need) return fail(LBM_ERR_INVALID, "lbm_plan_read_array: byte count does not match array size");
@@ -380,6 +411,31 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
                 d.segCount = static_cast<int>(seg.size());
                 d.special = own(upload(H.specialCells, s));
                 d.specialCount = static_cast<int>(H.specialCells.size());
+                d.rotorCells = own(upload(H.rotorCells, s));
+                d.rotorCellCount = static_cast<int>(H.rotorCells.size());
+            }
+            {
+                // rotors: tables, force bins, and the per-step frame in dev.rotor
+                L.rotors = H.rotors;
+                d.rotorCount = static_cast<int>(H.rotors.size());
+                d.trackRotorForce = c->track_rotor_force ? 1 : 0;
+                for (size_t r = 0; r < H.rotors.size(); ++r) {
+                    const lbm::HostRotor& R = H.rotors[r];
+                    lbm::DevRotor& D = d.rotor[r];
+                    D.rotorMap = own(upload(R.rotorMap, s));
+                    D.interp = own(upload(R.interpolation, s));
+                    D.nonzero = static_cast<int>(R.index.size());
+                    D.force = own(devAlloc<float>(3 * 27 * R.index.size()));
+                    if (D.force) ck(cudaMemsetAsync(D.force, 0, 3 * 27 * R.index.size() * sizeof(float), s), "memset");
+                    L.rotorIndex.push_back(own(upload(R.index, s)));
+                    D.cntX = R.cntX; D.cntY = R.cntY; D.cntZ = R.cntZ; D.axis = R.axis;
+                    D.res = R.res;
+                    D.xMin = R.xMin; D.yMin = R.yMin; D.zMin = R.zMin;
+                    D.xMax = R.xMax; D.yMax = R.yMax; D.zMax = R.zMax;
+                    D.ox = R.ox; D.oy = R.oy; D.oz = R.oz;
+                    D.c = 1.f; D.s = 0.f;
+                    D.scale = R.radiansPerSecond * H.info.dtPhys / H.info.res;
+                }
             }
             d.wallCount = static_cast<int>(H.wallIndex.size());
             d.wallIndex = own(upload(H.wallIndex, s));
@@ -627,8 +683,18 @@ int lbm_read_array(lbm_grids* g, int level, int which, void* host, size_t bytes)
         case LBM_ARRAY_OPEN_REFERENCE: src = d.obRhoRef; need = size_t(d.obCount) * 2 * 4; break;
         case LBM_ARRAY_OPEN_CUMULATIVE: src = d.obRhoCum; need = size_t(d.obCount) * 2 * 4; break;
         case LBM_ARRAY_F: need = 27 * n * 4; break;
+        default:
+            if (which >= LBM_ARRAY_ROTOR_BASE && (which - LBM_ARRAY_ROTOR_BASE) / 4 < d.rotorCount) {
+                const int r = (which - LBM_ARRAY_ROTOR_BASE) / 4, part = (which - LBM_ARRAY_ROTOR_BASE) % 4;
+                const lbm::HostRotor& R = L.rotors[r];
+                if (part == 0) { src = d.rotor[r].rotorMap; need = R.rotorMap.size() * 4; }
+                else if (part == 1) { src = L.rotorIndex[r]; need = R.index.size() * 4; }
+                else if (part == 2) { src = d.rotor[r].interp; need = R.interpolation.size() * 4; }
+                else { src = d.rotor[r].force; need = 3 * 27 * R.index.size() * 4; }
+                break;
+            }
+            return fail(LBM_ERR_INVALID, "lbm_read_array: unknown array id");
         case LBM_ARRAY_MACRO: need = 4 * n * 4; break;
-        default: return fail(LBM_ERR_INVALID, "lbm_read_array: unknown array id");
     }
     if (bytes != need)
         return fail(LBM_ERR_INVALID, "lbm_read_array: byte count does not match array size (expected " +
@@ -692,6 +758,10 @@ static void resetTracker(lbm_grids* g) {
         const lbm::DevLevel& d = L.dev;
         if (d.wallForce) ck(cudaMemsetAsync(d.wallForce, 0, 3 * size_t(d.wallCount) * sizeof(float), g->stream), "memset");
         if (d.obRhoCum) ck(cudaMemsetAsync(d.obRhoCum, 0, 2 * size_t(d.obCount) * sizeof(float), g->stream), "memset");
+        for (int r = 0; r < d.rotorCount; ++r)
+            if (d.rotor[r].force)
+                ck(cudaMemsetAsync(d.rotor[r].force, 0, 3 * 27 * size_t(d.rotor[r].nonzero) * sizeof(float), g->stream),
+                   "memset");
         L.iterationsSinceTrackerReset = 0;
     }
     ck(cudaStreamSynchronize(g->stream), "sync");
@@ -760,6 +830,76 @@ int lbm_wall_force(lbm_grids* g, int wallID, int reset, double* out) {
             for (int q = 0; q < 3; ++q) acc[q] += r[q] / span * conv;
             for (int q = 3; q < 6; ++q) acc[q] += r[q] / span * conv * 0.001;
         }
+        if (reset) resetTracker(g);
+        for (int q = 0; q < 6; ++q) out[q] = acc[q];
+    });
+}
+
+static void fillRotorInfo(const lbm::HostRotor& R, lbm_rotor_info* out) {
+    std::memset(out, 0, sizeof(*out));
+    out->res = R.res;
+    out->bounds[0] = R.xMin; out->bounds[1] = R.yMin; out->bounds[2] = R.zMin;
+    out->bounds[3] = R.xMax; out->bounds[4] = R.yMax; out->bounds[5] = R.zMax;
+    out->cell_count[0] = R.cntX; out->cell_count[1] = R.cntY; out->cell_count[2] = R.cntZ;
+    out->block_count = static_cast<int>(R.rotorMap.size());
+    out->nonzero_block_count = static_cast<int>(R.index.size());
+    out->axis = R.axis;
+    out->origin[0] = R.ox; out->origin[1] = R.oy; out->origin[2] = R.oz;
+    out->radians_per_second = R.radiansPerSecond;
+    out->radians_elapsed = R.radiansElapsed;
+}
+
+int lbm_plan_rotor_info(lbm_plan* p, int level, int rotor, lbm_rotor_info* out) {
+    if (!p || !out || level < 0 || level >= (int)p->host.levels.size() || rotor < 0 ||
+        rotor >= (int)p->host.levels[level].rotors.size())
+        return fail(LBM_ERR_INVALID, "lbm_plan_rotor_info: bad argument");
+    fillRotorInfo(p->host.levels[level].rotors[rotor], out);
+    return LBM_OK;
+}
+
+int lbm_get_rotor_info(lbm_grids* g, int level, int rotor, lbm_rotor_info* out) {
+    if (!g || !out || level < 0 || level >= (int)g->levels.size() || rotor < 0 ||
+        rotor >= (int)g->levels[level].rotors.size())
+        return fail(LBM_ERR_INVALID, "lbm_get_rotor_info: bad argument");
+    fillRotorInfo(g->levels[level].rotors[rotor], out);
+    return LBM_OK;
+}
+
+int lbm_set_rotor_speed(lbm_grids* g, int rotor, float radiansPerSecond) {
+    if (!g || rotor < 0) return fail(LBM_ERR_INVALID, "lbm_set_rotor_speed: bad argument");
+    bool found = false;
+    for (LevelState& L : g->levels) {
+        if (rotor >= (int)L.rotors.size()) continue;
+        L.rotors[rotor].radiansPerSecond = radiansPerSecond;
+        L.dev.rotor[rotor].scale = radiansPerSecond * L.info.dtPhys / L.info.res;
+        found = true;
+    }
+    if (!found) return fail(LBM_ERR_INVALID, "lbm_set_rotor_speed: no rotor with this index");
+    return LBM_OK;
+}
+
+int lbm_rotor_force(lbm_grids* g, int rotor, int reset, double* out) {
+    if (!g || !out || rotor < 0) return fail(LBM_ERR_INVALID, "lbm_rotor_force: bad argument");
+    return guarded("lbm_rotor_force", [&] {
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        bool found = false;
+        for (LevelState& L : g->levels) {
+            if (rotor >= L.dev.rotorCount) continue;
+            found = true;
+            ck(cudaMemsetAsync(g->scratch, 0, 6 * sizeof(double), g->stream), "memset");
+            lbm::launchRotorForce(L.dev.rotor[rotor], L.rotorIndex[rotor], g->stream, g->scratch);
+            ck(cudaGetLastError(), "rotor force launch");
+            double r[6];
+            ck(cudaMemcpyAsync(r, g->scratch, sizeof(r), cudaMemcpyDeviceToHost, g->stream), "copy");
+            ck(cudaStreamSynchronize(g->stream), "sync");
+            const double span = L.iterationsSinceTrackerReset > 0 ? L.iterationsSinceTrackerReset : 1;
+            // convertToPhysicalForce (include/cellFunctions.h:296-301); torque from N mm to N m
+            const double rm = double(L.info.res) / 1000.0;
+            const double conv = double(g->c.rho_phys) * rm * rm * rm * rm / (double(L.info.dtPhys) * L.info.dtPhys);
+            for (int q = 0; q < 3; ++q) acc[q] += r[q] / span * conv;
+            for (int q = 3; q < 6; ++q) acc[q] += r[q] / span * conv * 0.001;
+        }
+        if (!found) throw std::invalid_argument("no rotor with this index");
         if (reset) resetTracker(g);
         for (int q = 0; q < 6; ++q) out[q] = acc[q];
     });

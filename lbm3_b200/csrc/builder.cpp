@@ -115,6 +115,14 @@ void validateCase(const lbm_case& c) {
         if (bd.motion == LBM_WALL_ROTATING && (bd.axis < 0 || bd.axis > 2))
             throw std::runtime_error("rotation axis must be 0, 1 or 2");
     }
+    if (c.rotor_count < 0 || c.rotor_count > LBM_MAX_ROTORS)
+        throw std::runtime_error("rotor_count must be in [0, LBM_MAX_ROTORS]");
+    for (int r = 0; r < c.rotor_count; ++r) {
+        const lbm_rotor& rt = c.rotor[r];
+        if (rt.triangle_count <= 0 || !rt.triangles)
+            throw std::runtime_error("voxelizeSTL failed: the passed STL has 0 triangles.");
+        if (rt.axis < 0 || rt.axis > 2) throw std::runtime_error("rotor axis must be 0, 1 or 2");
+    }
 }
 
 // initializeGridInfo, level 0 (include/gridBuilderFunctions.h:9-64): the
@@ -666,9 +674,121 @@ void buildWalls(const lbm_case& c, HostLevel& L, const std::vector<Triangles>& b
 
 }  // namespace
 
+void buildRotors(const lbm_case& c, HostLevel& L) {
+    L.rotors.clear();
+    L.rotorCell.assign(L.info.cellCount, 0);
+    for (int r = 0; r < c.rotor_count; ++r) {
+        const lbm_rotor& rt = c.rotor[r];
+        Triangles t;
+        loadTriangles(rt.triangles, rt.triangle_count, t);
+        if (t.count == 0) throw std::runtime_error("voxelizeSTL failed: the passed STL has 0 triangles.");
+        // 1) voxelize at half the level spacing over the rotor's own bounds
+        const float vres = L.info.res * 0.5f;
+        const int vnx = static_cast<int>((t.xMax - t.xMin) / vres) + 2;
+        const int vny = static_cast<int>((t.yMax - t.yMin) / vres) + 2;
+        const int vnz = static_cast<int>((t.zMax - t.zMin) / vres) + 2;
+        RayMap map;
+        voxelize(t, t.xMin, t.yMin, t.zMin, vres, vnx, vny, map);
+        HostRotor R;
+        R.res = vres;
+        R.xMin = t.xMin - 1.5f * vres;
+        R.yMin = t.yMin - 1.5f * vres;
+        R.zMin = t.zMin - 1.5f * vres;
+        // two cells of overlap, rounded up to whole blocks of 4
+        R.cntX = ((vnx + 2 + 3) / 4) * 4;
+        R.cntY = ((vny + 2 + 3) / 4) * 4;
+        R.cntZ = ((vnz + 2 + 3) / 4) * 4;
+        R.xMax = R.xMin + R.res * static_cast<float>(R.cntX);
+        R.yMax = R.yMin + R.res * static_cast<float>(R.cntY);
+        R.zMax = R.zMin + R.res * static_cast<float>(R.cntZ);
+        R.axis = rt.axis;
+        R.ox = rt.origin[0];
+        R.oy = rt.origin[1];
+        R.oz = rt.origin[2];
+        R.radiansPerSecond = rt.radians_per_second;
+        const int bx = R.cntX / 4, by = R.cntY / 4, bz = R.cntZ / 4;
+        const int blocks = bx * by * bz;
+        // 6x6x6 voxel marks around a block: voxel v of block b sits at
+        // local (v - (4 b - 2)); its corner counters are local c..c+1
+        auto marks = [&](int ib, int jb, int kb, uint8_t (&m)[216]) {
+            bool any = false;
+            for (int q = 0; q < 216; ++q) m[q] = 0;
+            for (int j = std::max(0, jb * 4 - 2); j < std::min(vny, jb * 4 + 4); ++j)
+                for (int i = std::max(0, ib * 4 - 2); i < std::min(vnx, ib * 4 + 4); ++i)
+                    for (int k = kb * 4 - 2; k < kb * 4 + 4; ++k)
+                        if (isSolid(map, i, j, k)) {
+                            m[(k - (kb * 4 - 2)) * 36 + (j - (jb * 4 - 2)) * 6 + (i - (ib * 4 - 2))] = 1;
+                            any = true;
+                        }
+            return any;
+        };
+        // 2-3) rotorMap and the compact block index
+        R.rotorMap.assign(blocks, -1);
+        for (int b = 0; b < blocks; ++b) {
+            const int kb = b / (bx * by), rem = b % (bx * by), jb = rem / bx, ib = rem % bx;
+            uint8_t m[216];
+            if (marks(ib, jb, kb, m)) {
+                R.rotorMap[b] = static_cast<int>(R.index.size());
+                R.index.push_back(b);
+            }
+        }
+        // 4) counter points (5x5x5 per block) and packed corner counts
+        R.interpolation.assign(R.index.size() * 64, 0u);
+        for (size_t n = 0; n < R.index.size(); ++n) {
+            const int b = R.index[n];
+            const int kb = b / (bx * by), rem = b % (bx * by), jb = rem / bx, ib = rem % bx;
+            uint8_t m[216];
+            marks(ib, jb, kb, m);
+            uint8_t counter[125];
+            for (int kc = 0; kc < 5; ++kc)
+                for (int jc = 0; jc < 5; ++jc)
+                    for (int ic = 0; ic < 5; ++ic) {
+                        int cnt = 0;
+                        for (int km = kc; km <= kc + 1; ++km)
+                            for (int jm = jc; jm <= jc + 1; ++jm)
+                                for (int im = ic; im <= ic + 1; ++im) cnt += m[km * 36 + jm * 6 + im];
+                        counter[kc * 25 + jc * 5 + ic] = static_cast<uint8_t>(cnt);
+                    }
+            for (int ki = 0; ki < 4; ++ki)
+                for (int ji = 0; ji < 4; ++ji)
+                    for (int ii = 0; ii < 4; ++ii) {
+                        uint32_t packedCounts = 0u;
+                        int corner = 0;
+                        for (int kc = ki; kc <= ki + 1; ++kc)
+                            for (int jc = ji; jc <= ji + 1; ++jc)
+                                for (int ic = ii; ic <= ii + 1; ++ic, ++corner)
+                                    packedCounts |= static_cast<uint32_t>(counter[kc * 25 + jc * 5 + ic]) << (4 * corner);
+                        R.interpolation[n * 64 + ki * 16 + ji * 4 + ii] = packedCounts;
+                    }
+        }
+        // cells the rotor can reach while it turns: inside the cylinder about
+        // the axis that the bounds sweep (radius of the farthest corner)
+        const float lo[3] = {R.xMin, R.yMin, R.zMin}, hi[3] = {R.xMax, R.yMax, R.zMax};
+        const float org[3] = {R.ox, R.oy, R.oz};
+        const int a = R.axis, p1 = (a + 1) % 3, p2 = (a + 2) % 3;
+        double r2max = 0.0;
+        for (int u = 0; u < 2; ++u)
+            for (int v = 0; v < 2; ++v) {
+                const double d1 = (u ? hi[p1] : lo[p1]) - org[p1], d2 = (v ? hi[p2] : lo[p2]) - org[p2];
+                r2max = std::max(r2max, d1 * d1 + d2 * d2);
+            }
+        const double margin = 0.01 * L.info.res;
+        const double rmax = std::sqrt(r2max) + margin;
+        for (int q = 0; q < L.info.cellCount; ++q) {
+            const double pos[3] = {L.I[q] * L.info.res + L.info.ox, L.J[q] * L.info.res + L.info.oy,
+                                   L.K[q] * L.info.res + L.info.oz};
+            if (pos[a] < lo[a] - margin || pos[a] > hi[a] + margin) continue;
+            const double d1 = pos[p1] - org[p1], d2 = pos[p2] - org[p2];
+            if (d1 * d1 + d2 * d2 <= rmax * rmax) L.rotorCell[q] = 1;
+        }
+        L.rotors.push_back(std::move(R));
+    }
+}
+
 void buildSegments(HostLevel& L) {
     L.segCell.clear(); L.segJP.clear(); L.segKP.clear(); L.segJKP.clear(); L.segLen.clear();
     L.specialCells.clear();
+    L.rotorCells.clear();
     const int n = L.info.cellCount;
     int c = 0;
     while (c < n) {
@@ -687,10 +807,12 @@ void buildSegments(HostLevel& L) {
             return q + 1 >= n || jP(off) + 1 >= n || kP(off) + 1 >= n || jkP(off) + 1 >= n;
         };
         auto bulk = [&](int q) {
-            return (L.wallMap[q] == -1 || L.wallMap[q] == -2) && !wraps(q);
+            return (L.wallMap[q] == -1 || L.wallMap[q] == -2) && !wraps(q) &&
+                   (L.rotorCell.empty() || !L.rotorCell[q]);
         };
         for (int q = c; q < end;) {
             if (L.wallMap[q] == -3) { ++q; continue; }
+            if (!L.rotorCell.empty() && L.rotorCell[q]) { L.rotorCells.push_back(q); ++q; continue; }
             if (!bulk(q)) { L.specialCells.push_back(q); ++q; continue; }
             int r = q;
             while (r < end && r - q < kSegmentCells && bulk(r)) ++r;
@@ -710,6 +832,7 @@ void buildDomain(const lbm_case& c, HostDomain& out) {
     validateCase(c);
     out.c = c;
     out.c.body_count = 0;  // triangle pointers are not kept past this call
+    for (int r = 0; r < LBM_MAX_ROTORS; ++r) out.c.rotor[r].triangles = nullptr;
     out.levels.assign(1, HostLevel{});
     HostLevel& L = out.levels[0];
     Info skel;
@@ -773,6 +896,7 @@ void buildDomain(const lbm_case& c, HostDomain& out) {
     }
     compressRows(L);
     buildBoundaryLists(c, L);
+    buildRotors(c, L);
     buildSegments(L);
 
     out.fluidUpdatesPerIteration = 0;

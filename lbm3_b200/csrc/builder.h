@@ -51,6 +51,24 @@ struct OpenBCCell {
     float dRho, ux, uy, uz, beta;
 };
 
+// One rotor of a level (RotorStruct, include/types.h:206-219): the rotor is
+// voxelized at half the level spacing; its bounds (with margins) are cut into
+// 4x4x4 blocks of interpolation cells, and for every block that holds rotor
+// volume each interpolation cell stores its 8 corner counts (0..8 marked
+// voxels around the corner) as 4-bit fields.
+struct HostRotor {
+    float res = 0.f;
+    float xMin = 0, yMin = 0, zMin = 0, xMax = 0, yMax = 0, zMax = 0;
+    int cntX = 0, cntY = 0, cntZ = 0;
+    int axis = 2;
+    float ox = 0, oy = 0, oz = 0;
+    float radiansPerSecond = 0.f;
+    double radiansElapsed = 0.0;
+    std::vector<int> rotorMap;            // [blocks] compact index or -1
+    std::vector<int> index;               // [nonzero] block of each compact index
+    std::vector<uint32_t> interpolation;  // [64 * nonzero]
+};
+
 struct HostLevel {
     Info info;
     // builder view: sorted full IJK of the kept cells
@@ -82,6 +100,11 @@ struct HostLevel {
     // cells outside the bulk segments that still collide (wall-adjacent, or
     // whose +1 neighbour wraps around the end of the cell list)
     std::vector<int> specialCells;
+    // rotors, and the cells their swept volume can reach (collided with the
+    // special cells, since they need their position)
+    std::vector<HostRotor> rotors;
+    std::vector<uint8_t> rotorCell;
+    std::vector<int> rotorCells;          // collided by the rotor kernel
 };
 
 constexpr int kSegmentCells = 128;
@@ -99,7 +122,11 @@ void evalLocalBC(const lbm_case& c, BC& bc);
 // getInitialCondition.
 BC evalInitialCondition(const lbm_case& c, const Info& info, int i, int j, int k);
 
-// Split the compressed rows into bulk segments (needs wallMap).
+// buildRotors (include/rotorFunctions.h:315-585) for one level, plus the
+// rotorCell marks of the cells inside any rotor's swept cylinder.
+void buildRotors(const lbm_case& c, HostLevel& L);
+
+// Split the compressed rows into bulk segments (needs wallMap and rotorCell).
 void buildSegments(HostLevel& L);
 
 // Build all tables; throws std::runtime_error on an invalid case (the

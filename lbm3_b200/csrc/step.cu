@@ -33,17 +33,125 @@ namespace {
 
 constexpr int kBlock = 256;
 
+// ---- rotors ---------------------------------------------------------------
+// Volume-fraction forcing towards rigid rotation (processRotor,
+// include/rotorFunctions.h:211-304, and its call in the cell update,
+// include/updateGrid.h:97-128).  For the cell at (x, y, z): rotate the point
+// into each rotor's frame, look up the rotor volume fraction by trilinear
+// interpolation of the packed corner counts, and add the forcing
+// rho (u_rotor - u) times the smoothstep of the fraction, the fractions of
+// all rotors capped at 1 in total.  The collision limiter is scaled by
+// 1 - total fraction.  uxPre.. is the velocity after the local body force.
+__device__ __forceinline__ void rotorForcing(const DevLevel& g, float x, float y, float z, float rho, float uxPre,
+                                             float uyPre, float uzPre, bool trackForce, float& gx, float& gy,
+                                             float& gz, float& lambda) {
+    float cum = 0.f;
+    for (int r = 0; r < g.rotorCount; ++r) {
+        const DevRotor& R = g.rotor[r];
+        const float dx = x - R.ox, dy = y - R.oy, dz = z - R.oz;
+        float xr = x, yr = y, zr = z;
+        if (R.axis == 0) {
+            yr = R.oy + R.c * dy + R.s * dz;
+            zr = R.oz - R.s * dy + R.c * dz;
+        } else if (R.axis == 1) {
+            xr = R.ox + R.c * dx - R.s * dz;
+            zr = R.oz + R.s * dx + R.c * dz;
+        } else {
+            xr = R.ox + R.c * dx + R.s * dy;
+            yr = R.oy - R.s * dx + R.c * dy;
+        }
+        if (xr < R.xMin || xr >= R.xMax || yr < R.yMin || yr >= R.yMax || zr < R.zMin || zr >= R.zMax) continue;
+        const float xRel = xr - R.xMin, yRel = yr - R.yMin, zRel = zr - R.zMin;
+        const int ii = static_cast<int>(xRel / R.res);
+        const int jj = static_cast<int>(yRel / R.res);
+        const int kk = static_cast<int>(zRel / R.res);
+        if (ii >= R.cntX || jj >= R.cntY || kk >= R.cntZ) continue;
+        const int bx = R.cntX / 4, by = R.cntY / 4;
+        const int block = (kk / 4) * bx * by + (jj / 4) * bx + ii / 4;
+        const int map = __ldg(R.rotorMap + block);
+        if (map < 0) continue;
+        const unsigned packedCounts = __ldg(R.interp + map * 64 + (kk % 4) * 16 + (jj % 4) * 4 + (ii % 4));
+        const float xw = xRel / R.res - ii, yw = yRel / R.res - jj, zw = zRel / R.res - kk;
+        float v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = static_cast<float>((packedCounts >> (4u * q)) & 0xFu);
+        const float v00 = v[0] + xw * (v[1] - v[0]);
+        const float v10 = v[2] + xw * (v[3] - v[2]);
+        const float v01 = v[4] + xw * (v[5] - v[4]);
+        const float v11 = v[6] + xw * (v[7] - v[6]);
+        const float v0 = v00 + yw * (v10 - v00);
+        const float v1 = v01 + yw * (v11 - v01);
+        const float frac = (v0 + zw * (v1 - v0)) * 0.125f;
+        if (frac == 0.f) continue;
+        // target: rigid rotation about the axis, in lattice units
+        float ut[3] = {0.f, 0.f, 0.f};
+        if (R.axis == 0) { ut[1] = -R.scale * dz; ut[2] = R.scale * dy; }
+        else if (R.axis == 1) { ut[0] = R.scale * dz; ut[2] = -R.scale * dx; }
+        else { ut[0] = -R.scale * dy; ut[1] = R.scale * dx; }
+        float gxR = rho * (ut[0] - uxPre), gyR = rho * (ut[1] - uyPre), gzR = rho * (ut[2] - uzPre);
+        float ff = frac * frac * (3.f - 2.f * frac);
+        if (cum + ff > 1.f) {
+            ff = 1.f - cum;
+            cum = 1.f;
+        } else {
+            cum += ff;
+        }
+        gxR *= ff;
+        gyR *= ff;
+        gzR *= ff;
+        gx += gxR;
+        gy += gyR;
+        gz += gzR;
+        if (g.trackRotorForce && trackForce) {
+            // the force in the rotor frame, binned 3x3x3 per block
+            float fx = gxR, fy = gyR, fz = gzR;
+            if (R.axis == 0) { fy = R.c * gyR + R.s * gzR; fz = -R.s * gyR + R.c * gzR; }
+            else if (R.axis == 1) { fx = R.c * gxR - R.s * gzR; fz = R.s * gxR + R.c * gzR; }
+            else { fx = R.c * gxR + R.s * gyR; fy = -R.s * gxR + R.c * gyR; }
+            const int iF = max(0, min(2, static_cast<int>(0.75f * ((ii % 4) + xw))));
+            const int jF = max(0, min(2, static_cast<int>(0.75f * ((jj % 4) + yw))));
+            const int kF = max(0, min(2, static_cast<int>(0.75f * ((kk % 4) + zw))));
+            const int bin = map * 27 + kF * 9 + jF * 3 + iF;
+            const int nb = 27 * R.nonzero;
+            atomicAdd(R.force + bin, fx);
+            atomicAdd(R.force + nb + bin, fy);
+            atomicAdd(R.force + 2 * nb + bin, fz);
+        }
+        if (cum >= 1.f) break;
+    }
+    if (cum > 0.f) lambda *= 1.f - fminf(fmaxf(cum, 0.f), 1.f);
+}
+
+// Rotor forcing of one cell before its collision (needs the cell's indices).
+template <bool F, class S>
+__device__ __forceinline__ void cellRotorForcing(const DevLevel& g, const int (&ijk)[3], int wm, const float (&f)[27],
+                                                 float& gx, float& gy, float& gz, float& lambda) {
+    float dRho, ux, uy, uz;
+    macroFromF(f, dRho, ux, uy, uz);
+    const float rho = dRho + 1.f;
+    const float rhoInv = 1.f / rho;
+    const float uxPre = (ux * rho + gx) * rhoInv;
+    const float uyPre = (uy * rho + gy) * rhoInv;
+    const float uzPre = (uz * rho + gz) * rhoInv;
+    bool track = wm != -2;
+    if (wm >= 0 && (__ldg(g.wallData + wm) & 1u)) track = false;
+    const float x = ijk[0] * g.res + g.ox, y = ijk[1] * g.res + g.oy, z = ijk[2] * g.res + g.oz;
+    rotorForcing(g, x, y, z, rho, uxPre, uyPre, uzPre, track, gx, gy, gz, lambda);
+}
+
 template <bool F, class S>
 __global__ void __launch_bounds__(kBlock) collideStream(DevLevel g) {
     const int cell = blockIdx.x * kBlock + threadIdx.x;
     if (cell >= g.cellCount) return;
     const int wm = __ldg(g.wallMap + cell);
     if (wm == -3) return;  // the cell itself is a wall
-    int nb[8];
-    decodeNbr(g, cell, nb, nullptr);
+    int nb[8], ijk[3];
+    decodeNbr(g, cell, nb, g.rotorCount > 0 ? ijk : nullptr);
     float f[27];
     readPre<F, S>(g, nb, f);
-    collideCumulant(f, g.coll, g.coll.lambda, g.gx, g.gy, g.gz);
+    float gx = g.gx, gy = g.gy, gz = g.gz, lambda = g.coll.lambda;
+    if (g.rotorCount > 0) cellRotorForcing<F, S>(g, ijk, wm, f, gx, gy, gz, lambda);
+    collideCumulant(f, g.coll, lambda, gx, gy, gz);
     writePost<F, S>(g, nb, f);
 }
 
@@ -273,14 +381,16 @@ __global__ void __launch_bounds__(kTile, LBM3_TMA_MIN_BLOCKS) collideBulkTma(Dev
 // (applyIBB, include/boundaryConditions/interpolatedBouncebackFunctions.h:43-157,
 // and the write loop of include/updateGrid.h:143-176); the rest (cells whose
 // +1 neighbour wraps) collide and stream like bulk cells.
-template <bool F, class S>
+template <bool F, class S, bool kRotors = false>
 __device__ __forceinline__ void collideSpecialCell(const DevLevel& g, int cell) {
     const int wm = __ldg(g.wallMap + cell);
-    int nb[8];
-    decodeNbr(g, cell, nb, nullptr);
+    int nb[8], ijk[3];
+    decodeNbr(g, cell, nb, kRotors ? ijk : nullptr);
     float f[27];
     readPre<F, S>(g, nb, f);
-    collideCumulant(f, g.coll, g.coll.lambda, g.gx, g.gy, g.gz);
+    float gx = g.gx, gy = g.gy, gz = g.gz, lambda = g.coll.lambda;
+    if (kRotors) cellRotorForcing<F, S>(g, ijk, wm, f, gx, gy, gz, lambda);
+    collideCumulant(f, g.coll, lambda, gx, gy, gz);
     if (wm < 0) {
         writePost<F, S>(g, nb, f);
         return;
@@ -341,6 +451,15 @@ __global__ void __launch_bounds__(kBlock) collideList(DevLevel g) {
     const int idx = blockIdx.x * kBlock + threadIdx.x;
     if (idx >= g.specialCount) return;
     collideSpecialCell<F, S>(g, __ldg(g.special + idx));
+}
+
+// Cells a rotor can reach while it turns, one thread each: special-cell
+// update with the rotor forcing before the collision.
+template <bool F, class S>
+__global__ void __launch_bounds__(kBlock) collideRotorList(DevLevel g) {
+    const int idx = blockIdx.x * kBlock + threadIdx.x;
+    if (idx >= g.rotorCellCount) return;
+    collideSpecialCell<F, S, true>(g, __ldg(g.rotorCells + idx));
 }
 
 // Work items of one launch: special chunks [0, S) first (kTile listed cells
@@ -424,6 +543,48 @@ __global__ void __launch_bounds__(kBlock) wallForceSum(DevLevel g, int wallID, d
             v[3] = y * gz - z * gy;
             v[4] = z * gx - x * gz;
             v[5] = x * gy - y * gx;
+        }
+    }
+    __shared__ double part[6][kBlock / 32];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        double a = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+        if ((threadIdx.x & 31) == 0) part[q][threadIdx.x >> 5] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double a = 0.0;
+        for (int k = 0; k < kBlock / 32; ++k) a += part[threadIdx.x][k];
+        atomicAdd(out + threadIdx.x, a);
+    }
+}
+
+// FP64 force and torque of one rotor from its force bins, about the rotor
+// origin in the rotor frame (updateTracker rotor branch,
+// include/trackerFunctions.h:240-290); one thread per nonzero block.
+__global__ void __launch_bounds__(kBlock) rotorForceSum(DevRotor R, const int* index, double* out) {
+    const int n = blockIdx.x * kBlock + threadIdx.x;
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    if (n < R.nonzero) {
+        const int b = __ldg(index + n);
+        const int bx = R.cntX / 4, by = R.cntY / 4;
+        const int kb = b / (bx * by), rem = b % (bx * by), jb = rem / bx, ib = rem % bx;
+        const float resBlock = R.res * 4.f;
+        const float resForce = resBlock / 3.f;
+        const float x0 = ib * resBlock + R.xMin - R.ox + 0.5f * resForce;
+        const float y0 = jb * resBlock + R.yMin - R.oy + 0.5f * resForce;
+        const float z0 = kb * resBlock + R.zMin - R.oz + 0.5f * resForce;
+        const int nb = 27 * R.nonzero;
+        for (int q = 0; q < 27; ++q) {
+            const int kF = q / 9, jF = (q / 3) % 3, iF = q % 3;
+            const double x = x0 + iF * resForce, y = y0 + jF * resForce, z = z0 + kF * resForce;
+            const double fx = R.force[n * 27 + q], fy = R.force[nb + n * 27 + q], fz = R.force[2 * nb + n * 27 + q];
+            v[0] += fx; v[1] += fy; v[2] += fz;
+            v[3] += y * fz - z * fy;
+            v[4] += z * fx - x * fz;
+            v[5] += x * fy - y * fx;
         }
     }
     __shared__ double part[6][kBlock / 32];
@@ -809,9 +970,10 @@ template <bool F, class S> struct RunCollide {
                 if (grid == 0) grid = persistentGrid(collidePrefetch<F, S>, 0);
                 collidePrefetch<F, S><<<std::min(grid, items), kTile, 0, s>>>(g);
             }
-            return;
+        } else if (g.specialCount > 0) {
+            collideList<F, S><<<blocksFor(g.specialCount), kBlock, 0, s>>>(g);
         }
-        if (g.specialCount > 0) collideList<F, S><<<blocksFor(g.specialCount), kBlock, 0, s>>>(g);
+        if (g.rotorCellCount > 0) collideRotorList<F, S><<<blocksFor(g.rotorCellCount), kBlock, 0, s>>>(g);
     }
 };
 
@@ -863,8 +1025,8 @@ int stepLaunchCount(const DevLevel& g) {
     int n = 0;
     const CollideVariant v = collideVariant();
     if (v == CollideVariant::Simple) n += g.cellCount > 0;
-    else if (v == CollideVariant::Prefetch) n += (g.segCount + g.specialCount) > 0;
-    else n += (g.segCount > 0) + (g.specialCount > 0);
+    else if (v == CollideVariant::Prefetch) n += ((g.segCount + g.specialCount) > 0) + (g.rotorCellCount > 0);
+    else n += (g.segCount > 0) + (g.specialCount > 0) + (g.rotorCellCount > 0);
     return n + (g.obCount > 0) + (g.perCount > 0);
 }
 void launchPeriodic(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunPeriodic>(g, flip, s); }
@@ -883,6 +1045,9 @@ void launchGatherF(const DevLevel& g, cudaStream_t s, float* out) { dispatch<Run
 void launchScatterF(const DevLevel& g, cudaStream_t s, const float* in) { dispatch<RunScatter>(g, false, s, in); }
 void launchWallForce(const DevLevel& g, int wallID, cudaStream_t s, double* out) {
     if (g.wallCount > 0) wallForceSum<<<blocksFor(g.wallCount), kBlock, 0, s>>>(g, wallID, out);
+}
+void launchRotorForce(const DevRotor& R, const int* index, cudaStream_t s, double* out) {
+    if (R.nonzero > 0) rotorForceSum<<<blocksFor(R.nonzero), kBlock, 0, s>>>(R, index, out);
 }
 void launchOpenFlow(const DevLevel& g, int openBCID, float invSpan, cudaStream_t s, double* out) {
     if (g.obCount > 0) openFlowSum<<<blocksFor(g.obCount), kBlock, 0, s>>>(g, openBCID, invSpan, out);

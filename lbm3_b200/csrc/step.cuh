@@ -17,6 +17,21 @@ constexpr int kOpenChunk = 128;
 
 struct MbbcDir;
 
+// One forcing rotor as the collide kernels see it (RotorViewStruct,
+// include/types.h:217-219), with this step's angle as cosine and sine.
+struct DevRotor {
+    const int* rotorMap;           // [blocks] compact block index or -1
+    const unsigned* interp;        // [64 * nonzero] packed corner counts
+    float* force;                  // [3][27 * nonzero] force bins, rotor frame
+    int nonzero;
+    int cntX, cntY, cntZ, axis;
+    float res, xMin, yMin, zMin, xMax, yMax, zMax;
+    float ox, oy, oz;
+    float c, s;                    // cos, sin of radiansElapsed (float angle)
+    float scale;                   // radiansPerSecond * dtPhys / res of the level
+};
+constexpr int kMaxRotors = 4;
+
 // Everything a kernel needs for one level, passed by value.
 struct DevLevel {
     void* f;                 // populations [27][stride], element type per storage
@@ -74,6 +89,11 @@ struct DevLevel {
     int nx, ny, nz;
     float res, ox, oy, oz;
     CollisionConsts coll;
+    DevRotor rotor[kMaxRotors];
+    int rotorCount;
+    const int* rotorCells;         // cells inside a rotor's swept cylinder
+    int rotorCellCount;
+    int trackRotorForce;
 };
 
 // Neighbour cells of `cell` in the order self, +i, +j, +ij, +k, +ik, +jk, +ijk

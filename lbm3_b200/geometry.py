@@ -58,6 +58,83 @@ def icosphere(subdivisions: int, radius: float, center=(0.0, 0.0, 0.0)) -> np.nd
     return np.array([np.concatenate([v[a], v[b], v[c]]) for a, b, c in faces], dtype=np.float32)
 
 
+def rotor(blades: int = 4, hub_radius: float = 8.0, tip_radius: float = 40.0, pitch_deg: float = 30.0,
+          chord: float = 12.0, thickness: float = 2.0, hub_length: float = 16.0, center=(0.0, 0.0, 0.0),
+          segments: int = 64, radial_cells: int = 8, seed: int = 0) -> np.ndarray:
+    """Axial rotor about z through `center`: a closed hub cylinder and
+    `blades` closed flat blades (chord x thickness plates from just outside
+    the hub to the tip, pitched by `pitch_deg` about their radial axis),
+    spaced evenly in angle from a seeded phase.  The solids touch nowhere,
+    so ray parity gives their union.  Faces are subdivided radially into
+    `radial_cells` strips."""
+    rng = np.random.default_rng(seed)
+    phase = float(rng.uniform(0.0, 2.0 * np.pi / blades))
+    c = np.asarray(center, dtype=np.float64)
+    tris = []
+    # hub: closed cylinder
+    h0, h1 = -0.5 * hub_length, 0.5 * hub_length
+    ang = np.linspace(0.0, 2.0 * np.pi, segments, endpoint=False)
+    ring = np.stack([hub_radius * np.cos(ang), hub_radius * np.sin(ang)], axis=1)
+    for q in range(segments):
+        a, b = ring[q], ring[(q + 1) % segments]
+        p00, p01 = np.array([a[0], a[1], h0]), np.array([b[0], b[1], h0])
+        p10, p11 = np.array([a[0], a[1], h1]), np.array([b[0], b[1], h1])
+        tris += [(p00, p01, p11), (p00, p11, p10)]
+        tris += [(np.array([0, 0, h0]), p01, p00), (np.array([0, 0, h1]), p10, p11)]
+    # blades: boxes in local (radial r, chord s, thickness t) coordinates
+    r0 = hub_radius * 1.03
+    pitch = np.deg2rad(pitch_deg)
+    for bidx in range(blades):
+        th = phase + 2.0 * np.pi * bidx / blades
+        er = np.array([np.cos(th), np.sin(th), 0.0])
+        et = np.array([-np.sin(th), np.cos(th), 0.0])
+        ez = np.array([0.0, 0.0, 1.0])
+        es = np.cos(pitch) * et + np.sin(pitch) * ez      # chord direction
+        en = -np.sin(pitch) * et + np.cos(pitch) * ez     # thickness direction
+
+        def P(r, sc, tn):
+            return r * er + sc * es + tn * en
+
+        rs = np.linspace(r0, tip_radius, radial_cells + 1)
+        hs, ht = 0.5 * chord, 0.5 * thickness
+        for q in range(radial_cells):
+            ra, rb = rs[q], rs[q + 1]
+            for (s0, t0), (s1, t1) in (((-hs, -ht), (hs, -ht)), ((hs, -ht), (hs, ht)),
+                                       ((hs, ht), (-hs, ht)), ((-hs, ht), (-hs, -ht))):
+                a0, a1, b0, b1 = P(ra, s0, t0), P(ra, s1, t1), P(rb, s0, t0), P(rb, s1, t1)
+                tris += [(a0, b0, b1), (a0, b1, a1)]
+        for r_end, sign in ((r0, -1.0), (tip_radius, 1.0)):
+            p = [P(r_end, -hs, -ht), P(r_end, hs, -ht), P(r_end, hs, ht), P(r_end, -hs, ht)]
+            if sign > 0:
+                tris += [(p[0], p[1], p[2]), (p[0], p[2], p[3])]
+            else:
+                tris += [(p[0], p[2], p[1]), (p[0], p[3], p[2])]
+    out = np.array([np.concatenate([a + c, b + c, d + c]) for a, b, d in tris], dtype=np.float32)
+    return out
+
+
+def set_rotors(case: A.LbmCase, rotors) -> A.LbmCase:
+    """Attach forcing rotors: a list of (triangles, dict(axis=0|1|2,
+    origin=(x, y, z), radians_per_second=w)).  Arrays are kept alive on the case."""
+    if len(rotors) > A.LBM_MAX_ROTORS:
+        raise ValueError("too many rotors")
+    keep = []
+    case.rotor_count = len(rotors)
+    for r, (tris, spec) in enumerate(rotors):
+        arr = np.ascontiguousarray(tris, dtype=np.float32).reshape(-1, 9)
+        keep.append(arr)
+        rt = case.rotor[r]
+        rt.triangles = arr.ctypes.data_as(C.POINTER(C.c_float))
+        rt.triangle_count = len(arr)
+        rt.axis = spec.get("axis", 2)
+        o = spec.get("origin", (0.0, 0.0, 0.0))
+        for a in range(3):
+            rt.origin[a] = o[a]
+        rt.radians_per_second = spec.get("radians_per_second", 0.0)
+    case._rotors = keep
+    return case
+
+
 def write_binary_stl(path, tris: np.ndarray) -> None:
     tris = np.asarray(tris, dtype=np.float32).reshape(-1, 9)
     with open(path, "wb") as fh:

@@ -55,6 +55,31 @@ class Plan:
         A.check(A.lib().lbm_plan_read_array(self._h, level, which, out.ctypes.data_as(C.c_void_p), out.nbytes))
         return out
 
+    def rotor_count(self, level: int = 0) -> int:
+        n = 0
+        while n < A.LBM_MAX_ROTORS:
+            info = A.LbmRotorInfo()
+            if A.lib().lbm_plan_rotor_info(self._h, level, n, C.byref(info)) != 0:
+                break
+            n += 1
+        return n
+
+    def rotor_info(self, r: int, level: int = 0) -> A.LbmRotorInfo:
+        info = A.LbmRotorInfo()
+        A.check(A.lib().lbm_plan_rotor_info(self._h, level, r, C.byref(info)))
+        return info
+
+    def rotor_array(self, r: int, part: str, level: int = 0) -> np.ndarray:
+        """Rotor tables: part 'map' (int32 [blocks]), 'index' (int32 [nonzero]),
+        'interpolation' (uint32 [64 * nonzero])."""
+        info = self.rotor_info(r, level)
+        which, n, dt = {"map": (0, info.block_count, np.int32), "index": (1, info.nonzero_block_count, np.int32),
+                        "interpolation": (2, 64 * info.nonzero_block_count, np.uint32)}[part]
+        out = np.empty(n, dtype=dt)
+        A.check(A.lib().lbm_plan_read_array(self._h, level, A.ARRAY_ROTOR_BASE + 4 * r + which,
+                                            out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
     def wall_velocity(self, level: int = 0) -> np.ndarray:
         """[3][wallCount] wall velocity of every wall-adjacent cell (lattice units)."""
         n = self.info(level).wall_adjacent_count
@@ -197,6 +222,29 @@ class Grids:
         out = (C.c_double * 6)()
         A.check(A.lib().lbm_wall_force(self._h, wall_id, int(reset), out))
         return np.array(out[:])
+
+    def rotor_info(self, r: int, level: int = 0) -> A.LbmRotorInfo:
+        info = A.LbmRotorInfo()
+        A.check(A.lib().lbm_get_rotor_info(self._h, level, r, C.byref(info)))
+        return info
+
+    def set_rotor_speed(self, r: int, radians_per_second: float):
+        A.check(A.lib().lbm_set_rotor_speed(self._h, r, radians_per_second))
+
+    def rotor_force(self, r: int, reset: bool = False) -> np.ndarray:
+        """{Fx, Fy, Fz [N], Tx, Ty, Tz [N m]} the rotor exerts on the fluid, rotor
+        frame, averaged since the last tracker reset."""
+        out = (C.c_double * 6)()
+        A.check(A.lib().lbm_rotor_force(self._h, r, int(reset), out))
+        return np.array(out[:])
+
+    def rotor_bins(self, r: int, level: int = 0) -> np.ndarray:
+        """Force bins of rotor r, float32 [3][27 * nonzero] (lattice units, rotor frame)."""
+        n = self.rotor_info(r, level).nonzero_block_count
+        out = np.empty((3, 27 * n), dtype=np.float32)
+        A.check(A.lib().lbm_read_array(self._h, level, A.ARRAY_ROTOR_BASE + 4 * r + 3,
+                                       out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
 
     def open_boundary_flow(self, open_bc_id: int, reset: bool = False) -> dict:
         """Flow through one open boundary averaged since the last tracker reset

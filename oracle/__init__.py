@@ -58,6 +58,7 @@ class OGrid(C.Structure):
         ("wallForce", C.POINTER(C.c_float)), ("trackWallForce", C.c_int),
         ("face", FaceBC * 6), ("openCount", C.c_int), ("openIndex", _IP),
         ("openRef", C.POINTER(C.c_float)), ("openCum", C.POINTER(C.c_float)), ("trackOpen", C.c_int),
+        ("rotorCount", C.c_int), ("rotors", C.c_void_p), ("trackRotorForce", C.c_int),
     ]
 
 
@@ -95,6 +96,10 @@ def lib() -> C.CDLL:
             [C.c_int, C.c_void_p, C.c_void_p, C.c_int] + [C.c_void_p] * 4
         h.oracle_from_tables.restype = C.c_int
         h.oracle_wall_force.argtypes = [C.POINTER(OGrid), C.c_int, C.POINTER(C.c_double)]
+        h.oracle_set_rotor.argtypes = [C.POINTER(OGrid), C.c_int, C.c_float, C.c_void_p, C.c_void_p, C.c_int,
+                                       C.c_void_p, C.c_float, C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+        h.oracle_set_rotor.restype = C.c_int
+        h.oracle_rotor_bins.argtypes = [C.POINTER(OGrid), C.c_int, C.POINTER(C.c_float)]
         h.oracle_mbbc_apply.argtypes = [C.c_int] + [C.c_float] * 4 + [C.POINTER(C.c_float)]
         h.oracle_mbbc_restore_rho.argtypes = [C.c_int] + [C.c_float] * 3 + [C.POINTER(C.c_float)] * 2
         h.oracle_mbbc_restore_u.argtypes = [C.c_int, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
@@ -204,6 +209,20 @@ class OracleGrid:
             info.wall_adjacent_count, _vp(arrays["wall_index"]), _vp(wd), _vp(ll), _vp(wv))
         if rc != 0:
             raise RuntimeError(f"oracle_from_tables failed with status {rc}")
+        self._rotor_nonzero = []
+        for r in range(plan.rotor_count()):
+            ri = plan.rotor_info(r)
+            self._rotor_nonzero.append(ri.nonzero_block_count)
+            rmap = plan.rotor_array(r, "map")
+            interp = plan.rotor_array(r, "interpolation")
+            bounds = np.array(ri.bounds[:], dtype=np.float32)
+            counts = np.array(ri.cell_count[:], dtype=np.int32)
+            origin = np.array(ri.origin[:], dtype=np.float32)
+            self._keep += (rmap, interp, bounds, counts, origin)
+            if lib().oracle_set_rotor(C.byref(self.g), r, ri.res, _vp(bounds), _vp(counts), ri.axis, _vp(origin),
+                                      ri.radians_per_second, _vp(rmap), len(rmap), _vp(interp),
+                                      ri.nonzero_block_count) != 0:
+                raise RuntimeError("oracle_set_rotor failed")
 
     def wall_force(self, wall_id: int) -> np.ndarray:
         out = (C.c_double * 6)()
@@ -247,6 +266,14 @@ class OracleGrid:
         n = self.g.cellCount
         dst = np.ctypeslib.as_array(self.g.f, shape=(27 * n,))
         dst[:] = np.ascontiguousarray(f, dtype=np.float32).reshape(-1)
+
+    def rotor_bins(self, r: int) -> np.ndarray:
+        """Force bins of rotor r, float32 [3][27 * nonzero]."""
+        import ctypes as _C
+        R = self._rotor_nonzero[r]
+        out = np.empty(3 * 27 * R, dtype=np.float32)
+        lib().oracle_rotor_bins(C.byref(self.g), r, _fp(out))
+        return out.reshape(3, -1)
 
     def open_index(self) -> np.ndarray:
         m = self.g.openCount

@@ -564,6 +564,7 @@ static void init_info(const lbm_case* c, ogrid* g);
 static void apply_initial_condition(const lbm_case* c, ogrid* g);
 static void get_ijk(const ogrid* g, int cell, int* i, int* j, int* k);
 static void build_open_list(ogrid* g);
+static void free_rotors(ogrid* g);
 
 int oracle_build(const lbm_case* c, ogrid* g) {
     memset(g, 0, sizeof(*g));
@@ -701,6 +702,7 @@ void oracle_free(ogrid* g) {
     free(g->perSource); free(g->f);
     free(g->wallIndex); free(g->wallData); free(g->linkLength); free(g->wallVel); free(g->wallForce);
     free(g->openIndex); free(g->openRef); free(g->openCum);
+    free_rotors(g);
     memset(g, 0, sizeof(*g));
 }
 
@@ -723,6 +725,7 @@ static void init_info(const lbm_case* c, ogrid* g) {
     g->useIBB = c->use_ibb;
     g->trackWallForce = c->track_wall_force;
     g->trackOpen = c->track_open_boundaries;
+    g->trackRotorForce = c->track_rotor_force;
     memcpy(g->face, c->face, sizeof(g->face));
 }
 
@@ -990,11 +993,139 @@ static void open_boundary(ogrid* g) {
     }
 }
 
+/* ---- rotors (include/rotorFunctions.h) ---------------------------------- */
+
+typedef struct orotor {
+    float res, xMin, yMin, zMin, xMax, yMax, zMax;
+    int cntX, cntY, cntZ, axis;
+    float ox, oy, oz, radiansPerSecond;
+    double radiansElapsed;
+    int blocks, nonzero;
+    int* rotorMap;
+    unsigned* interp;
+    float* force;
+} orotor;
+
+int oracle_set_rotor(ogrid* g, int r, float res, const float* bounds, const int* cellCount, int axis,
+                     const float* origin, float radiansPerSecond, const int* rotorMap, int blocks,
+                     const unsigned* interpolation, int nonzero) {
+    if (r < 0 || r >= 4) return -1;
+    if (!g->rotors) g->rotors = calloc(4, sizeof(orotor));
+    orotor* R = (orotor*)g->rotors + r;
+    R->res = res;
+    R->xMin = bounds[0]; R->yMin = bounds[1]; R->zMin = bounds[2];
+    R->xMax = bounds[3]; R->yMax = bounds[4]; R->zMax = bounds[5];
+    R->cntX = cellCount[0]; R->cntY = cellCount[1]; R->cntZ = cellCount[2];
+    R->axis = axis;
+    R->ox = origin[0]; R->oy = origin[1]; R->oz = origin[2];
+    R->radiansPerSecond = radiansPerSecond;
+    R->radiansElapsed = 0.0;
+    R->blocks = blocks;
+    R->nonzero = nonzero;
+    R->rotorMap = (int*)malloc(sizeof(int) * (size_t)(blocks > 0 ? blocks : 1));
+    memcpy(R->rotorMap, rotorMap, sizeof(int) * (size_t)blocks);
+    R->interp = (unsigned*)malloc(sizeof(unsigned) * 64 * (size_t)(nonzero > 0 ? nonzero : 1));
+    memcpy(R->interp, interpolation, sizeof(unsigned) * 64 * (size_t)nonzero);
+    R->force = (float*)calloc(3 * 27 * (size_t)(nonzero > 0 ? nonzero : 1), sizeof(float));
+    if (r + 1 > g->rotorCount) g->rotorCount = r + 1;
+    return 0;
+}
+
+void oracle_rotor_bins(const ogrid* g, int r, float* out) {
+    const orotor* R = (const orotor*)g->rotors + r;
+    memcpy(out, R->force, sizeof(float) * 3 * 27 * (size_t)R->nonzero);
+}
+
+static void free_rotors(ogrid* g) {
+    if (!g->rotors) return;
+    orotor* R = (orotor*)g->rotors;
+    for (int r = 0; r < g->rotorCount; ++r) { free(R[r].rotorMap); free(R[r].interp); free(R[r].force); }
+    free(g->rotors);
+    g->rotors = NULL;
+    g->rotorCount = 0;
+}
+
+/* processRotor (include/rotorFunctions.h:211-304) for every rotor, with the
+ * cumulative fraction cap and break of include/updateGrid.h:113-128 */
+static void rotor_forcing(ogrid* g, float x, float y, float z, float rho, float uxPre, float uyPre, float uzPre,
+                          int trackForce, obc* bc) {
+    float cum = 0.f;
+    for (int r = 0; r < g->rotorCount; ++r) {
+        orotor* R = (orotor*)g->rotors + r;
+        const float angle = (float)R->radiansElapsed;
+        const float c = cosf(angle), s = sinf(angle);
+        float xr = x, yr = y, zr = z;
+        const float dx = x - R->ox, dy = y - R->oy, dz = z - R->oz;
+        if (R->axis == 0) { yr = R->oy + c * dy + s * dz; zr = R->oz - s * dy + c * dz; }
+        else if (R->axis == 1) { xr = R->ox + c * dx - s * dz; zr = R->oz + s * dx + c * dz; }
+        else { xr = R->ox + c * dx + s * dy; yr = R->oy - s * dx + c * dy; }
+        if (xr < R->xMin || xr >= R->xMax || yr < R->yMin || yr >= R->yMax || zr < R->zMin || zr >= R->zMax) continue;
+        const float xRel = xr - R->xMin, yRel = yr - R->yMin, zRel = zr - R->zMin;
+        const int ii = (int)(xRel / R->res), jj = (int)(yRel / R->res), kk = (int)(zRel / R->res);
+        if (ii >= R->cntX || jj >= R->cntY || kk >= R->cntZ) continue;
+        const int bx = R->cntX / 4, by = R->cntY / 4;
+        const int block = (kk / 4) * bx * by + (jj / 4) * bx + ii / 4;
+        const int map = R->rotorMap[block];
+        if (map < 0) continue;
+        const unsigned packed = R->interp[map * 64 + (kk % 4) * 16 + (jj % 4) * 4 + (ii % 4)];
+        const float xw = (xRel / R->res) - ii, yw = (yRel / R->res) - jj, zw = (zRel / R->res) - kk;
+        float v[8];
+        for (int q = 0; q < 8; ++q) v[q] = (float)((packed >> (4u * q)) & 0xFu);
+        const float v00 = v[0] + xw * (v[1] - v[0]);
+        const float v10 = v[2] + xw * (v[3] - v[2]);
+        const float v01 = v[4] + xw * (v[5] - v[4]);
+        const float v11 = v[6] + xw * (v[7] - v[6]);
+        const float v0 = v00 + yw * (v10 - v00);
+        const float v1 = v01 + yw * (v11 - v01);
+        const float frac = (v0 + zw * (v1 - v0)) * 0.125f;
+        if (frac == 0.f) continue;
+        /* getRotorForcing: rho (u_target - u) with rigid rotation about the axis */
+        const float scale = R->radiansPerSecond * g->dtPhys / g->res;
+        float ut[3] = {0.f, 0.f, 0.f};
+        if (R->axis == 0) { ut[1] = -scale * dz; ut[2] = scale * dy; }
+        else if (R->axis == 1) { ut[0] = scale * dz; ut[2] = -scale * dx; }
+        else { ut[0] = -scale * dy; ut[1] = scale * dx; }
+        float gx = rho * (ut[0] - uxPre), gy = rho * (ut[1] - uyPre), gz = rho * (ut[2] - uzPre);
+        float ff = frac * frac * (3.f - 2.f * frac);
+        if (cum + ff > 1.f) { ff = 1.f - cum; cum = 1.f; }
+        else cum += ff;
+        gx *= ff; gy *= ff; gz *= ff;
+        bc->gx += gx; bc->gy += gy; bc->gz += gz;
+        if (g->trackRotorForce && trackForce) {
+            float fx = gx, fy = gy, fz = gz;
+            if (R->axis == 0) { fy = c * gy + s * gz; fz = -s * gy + c * gz; }
+            else if (R->axis == 1) { fx = c * gx - s * gz; fz = s * gx + c * gz; }
+            else { fx = c * gx + s * gy; fy = -s * gx + c * gy; }
+            int iF = (int)(0.75f * ((ii % 4) + xw)), jF = (int)(0.75f * ((jj % 4) + yw)), kF = (int)(0.75f * ((kk % 4) + zw));
+            iF = iF < 0 ? 0 : (iF > 2 ? 2 : iF);
+            jF = jF < 0 ? 0 : (jF > 2 ? 2 : jF);
+            kF = kF < 0 ? 0 : (kF > 2 ? 2 : kF);
+            const int bin = map * 27 + kF * 9 + jF * 3 + iF, nb = 27 * R->nonzero;
+#pragma omp atomic
+            R->force[bin] += fx;
+#pragma omp atomic
+            R->force[nb + bin] += fy;
+#pragma omp atomic
+            R->force[2 * nb + bin] += fz;
+        }
+        if (cum >= 1.f) break;
+    }
+    if (cum > 0.f) bc->collisionLimiter *= 1.f - (cum < 0.f ? 0.f : (cum > 1.f ? 1.f : cum));
+}
+
 /* ---- updateSingleGrid (include/updateGrid.h:16-386) --------------------- */
 void oracle_step(ogrid* g, int steps) {
     const long long n = g->cellCount;
     for (int s = 0; s < steps; ++s) {
         const int flip = g->flip;
+        /* advance the rotors (include/updateGrid.h:36-49) */
+        for (int r = 0; r < g->rotorCount; ++r) {
+            orotor* R = (orotor*)g->rotors + r;
+            const double twoPi = 6.283185307179586476925286766559;
+            R->radiansElapsed = fmod(R->radiansElapsed + (double)g->dtPhys * R->radiansPerSecond, twoPi);
+            if (R->radiansElapsed < 0.0) R->radiansElapsed += twoPi;
+            if (R->radiansElapsed >= twoPi) R->radiansElapsed = 0.0;
+        }
         /* K1: cell lambda (:51-177) */
 #pragma omp parallel for schedule(static)
         for (int cell = 0; cell < g->cellCount; ++cell) {
@@ -1023,6 +1154,19 @@ void oracle_step(ogrid* g, int steps) {
                 bc.ux = g->wallVel[wm];
                 bc.uy = g->wallVel[g->wallCount + wm];
                 bc.uz = g->wallVel[2 * g->wallCount + wm];
+            }
+            if (g->rotorCount > 0) {
+                /* include/updateGrid.h:97-128 */
+                int ci, cj, ck;
+                get_ijk(g, cell, &ci, &cj, &ck);
+                const float x = ci * g->res + g->ox, y = cj * g->res + g->oy, z = ck * g->res + g->oz;
+                const float rho = m[0] + 1.f;
+                const float rhoInv = 1.f / rho;
+                const float uxPre = (m[1] * rho + bc.gx) * rhoInv;
+                const float uyPre = (m[2] * rho + bc.gy) * rhoInv;
+                const float uzPre = (m[3] * rho + bc.gz) * rhoInv;
+                const int track = wm != -2 && !(wm >= 0 && (wallData & 1u));
+                rotor_forcing(g, x, y, z, rho, uxPre, uyPre, uzPre, track, &bc);
             }
             oracle_apply_collision(f, &bc, g->nu);
             if (wm < 0) {

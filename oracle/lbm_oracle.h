@@ -82,6 +82,10 @@ typedef struct ogrid {
     float* openRef;                  /* [2][openCount] dRhoRef, uNormalRef */
     float* openCum;                  /* [2][openCount] dRho, uNormal sums */
     int trackOpen;
+    /* forcing rotors (RotorStruct), set with oracle_set_rotor */
+    int rotorCount;
+    void* rotors;                    /* orotor[4], private to lbm_oracle.c */
+    int trackRotorForce;
 } ogrid;
 
 /* buildGrids for a box domain without geometry, single level, followed by
@@ -122,6 +126,15 @@ void oracle_macro(const ogrid* g, float* out);
 int oracle_mbbc_apply(int code, float rho, float ux, float uy, float uz, float f[27]);
 int oracle_mbbc_restore_rho(int code, float ux, float uy, float uz, const float f[27], float* rho);
 int oracle_mbbc_restore_u(int code, float rho, const float f[27], float u[3]);
+
+/* Attach rotor `r` of a grid: its info (RotorInfoStruct) and tables as a
+ * plan built them (rotorMap [blocks], interpolation [64 * nonzero]).  Arrays
+ * are copied; force bins [3][27 * nonzero] start at zero.  Returns 0 or -1. */
+int oracle_set_rotor(ogrid* g, int r, float res, const float* bounds, const int* cellCount, int axis,
+                     const float* origin, float radiansPerSecond, const int* rotorMap, int blocks,
+                     const unsigned* interpolation, int nonzero);
+/* force bins of rotor r: out[3][27 * nonzero] */
+void oracle_rotor_bins(const ogrid* g, int r, float* out);
 
 /* number of OpenMP threads the oracle uses */
 int oracle_threads(void);

@@ -30,8 +30,9 @@ def test_every_declared_symbol_is_exported():
 def test_struct_layouts_match_the_header(tmp_path):
     src = tmp_path / "sizes.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "lbm3_b200.h"\n'
-                   'int main(void){printf("%zu %zu %zu %zu %zu\\n", sizeof(lbm_case), sizeof(lbm_face_bc),'
-                   ' sizeof(lbm_grid_info), offsetof(lbm_case, storage), offsetof(lbm_grid_info, grid_memory_bytes));'
+                   'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(lbm_case), sizeof(lbm_face_bc),'
+                   ' sizeof(lbm_grid_info), offsetof(lbm_case, storage), offsetof(lbm_grid_info, grid_memory_bytes),'
+                   ' offsetof(lbm_case, track_rotor_force), sizeof(lbm_rotor), sizeof(lbm_rotor_info));'
                    'return 0;}\n')
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
@@ -41,6 +42,9 @@ def test_struct_layouts_match_the_header(tmp_path):
     assert int(out[2]) == C.sizeof(A.LbmGridInfo)
     assert int(out[3]) == A.LbmCase.storage.offset
     assert int(out[4]) == A.LbmGridInfo.grid_memory_bytes.offset
+    assert int(out[5]) == A.LbmCase.track_rotor_force.offset
+    assert int(out[6]) == C.sizeof(A.LbmRotor)
+    assert int(out[7]) == C.sizeof(A.LbmRotorInfo)
 
 
 def test_null_arguments_are_rejected_without_a_device():
