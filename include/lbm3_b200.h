@@ -341,6 +341,33 @@ int lbm_set_rotor_speed(lbm_grids* g, int rotor, float radians_per_second);
  * Replaces the rotor branch of updateTracker (include/trackerFunctions.h:225-300). */
 int lbm_rotor_force(lbm_grids* g, int rotor, int reset, double* out);
 
+/* Section planes of lbm_flow_report; the normal is the +axis direction. */
+#define LBM_PLANE_XY 0   /* cut at z */
+#define LBM_PLANE_ZY 1   /* cut at x */
+#define LBM_PLANE_ZX 2   /* cut at y */
+
+/* Flow through a section plane (FlowReportStruct): the cell layer nearest to
+ * the coordinate `cut` (mm), cropped to `bounds` {xMin, yMin, zMin, xMax,
+ * yMax, zMax} (mm; NULL or all zero: no crop).  Pixels that are walls or
+ * mostly rotor volume are left out.  out = {area-averaged normal velocity
+ * [m/s], mass flow [kg/s], momentum thrust [N], area-averaged pressure [Pa],
+ * pressure power [W], normal kinetic power [W], fluid area [mm^2]}; sums in
+ * FP64 on the device.  A cut outside the grid is LBM_ERR_INVALID.
+ * Replaces getFlowReportXY/ZY/ZX (include/flowReportFunctions.h:11-373) for a
+ * single-level grid. */
+int lbm_flow_report(lbm_grids* g, int plane, float cut, const float* bounds, double* out);
+
+/* Checkpoint and resume (preemption of long runs and of served domains).
+ * The state is everything a run carries from step to step: the populations at
+ * their storage precision, the esotwist flipper, the iteration counters, the
+ * open-boundary reference and cumulative values, the wall and rotor force
+ * accumulators, and the rotor angles and speeds.  It is restored into grids
+ * built from the same case; a mismatch of sizes is LBM_ERR_INVALID.
+ * No counterpart in the reference. */
+int lbm_state_bytes(lbm_grids* g, size_t* bytes);
+int lbm_save_state(lbm_grids* g, void* host, size_t bytes);
+int lbm_load_state(lbm_grids* g, const void* host, size_t bytes);
+
 /* Cell-wise collision on a device batch of shifted populations laid out as
  * float [27][n] (structure of arrays), in place.
  * Replaces applyCollision (include/applyCollision.h:17-491) applied per cell

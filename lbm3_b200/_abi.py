@@ -86,6 +86,7 @@ class LbmBody(C.Structure):
 
 LBM_MAX_ROTORS = 4
 ARRAY_ROTOR_BASE = 32
+PLANE_XY, PLANE_ZY, PLANE_ZX = 0, 1, 2
 
 
 class LbmRotor(C.Structure):
@@ -166,6 +167,10 @@ SIGNATURES = [
     ("lbm_get_rotor_info", C.c_int, [_P, C.c_int, C.c_int, C.c_void_p]),
     ("lbm_set_rotor_speed", C.c_int, [_P, C.c_int, C.c_float]),
     ("lbm_rotor_force", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    ("lbm_flow_report", C.c_int, [_P, C.c_int, C.c_float, C.c_void_p, C.POINTER(C.c_double)]),
+    ("lbm_state_bytes", C.c_int, [_P, C.POINTER(C.c_size_t)]),
+    ("lbm_save_state", C.c_int, [_P, C.c_void_p, C.c_size_t]),
+    ("lbm_load_state", C.c_int, [_P, C.c_void_p, C.c_size_t]),
     ("lbm_apply_collision_batch", C.c_int,
      [_P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, _P]),
 ]

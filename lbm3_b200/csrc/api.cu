@@ -905,6 +905,185 @@ int lbm_rotor_force(lbm_grids* g, int rotor, int reset, double* out) {
     });
 }
 
+int lbm_flow_report(lbm_grids* g, int plane, float cut, const float* bounds, double* out) {
+    if (!g || !out || plane < 0 || plane > 2) return fail(LBM_ERR_INVALID, "lbm_flow_report: bad argument");
+    if (g->levels.size() != 1) return fail(LBM_ERR_UNSUPPORTED, "lbm_flow_report: single-level grids only");
+    LevelState& L = g->levels[0];
+    const lbm::Info& in = L.info;
+    const int n[3] = {in.nx, in.ny, in.nz};
+    const float o[3] = {in.ox, in.oy, in.oz};
+    const int axis = plane == LBM_PLANE_XY ? 2 : plane == LBM_PLANE_ZY ? 0 : 1;
+    // getIJKCellIndexFromXYZ (include/cellFunctions.h:96-101)
+    const int layer = static_cast<int>((cut - o[axis]) / in.res + 0.5f);
+    if (layer < 0 || layer >= n[axis]) return fail(LBM_ERR_INVALID, "lbm_flow_report: cut outside the grid");
+    // crop (include/flowReportFunctions.h:36-55)
+    int lo[3] = {0, 0, 0}, hi[3] = {n[0], n[1], n[2]};
+    if (bounds && (bounds[0] != 0.f || bounds[1] != 0.f || bounds[2] != 0.f || bounds[3] != 0.f ||
+                   bounds[4] != 0.f || bounds[5] != 0.f))
+        for (int a = 0; a < 3; ++a) {
+            const float tMin = o[a] - 0.5f * in.res;
+            const float tMax = o[a] + in.res * (n[a] - 0.5f);
+            lo[a] = std::max(0, static_cast<int>(std::ceil((bounds[a] - tMin) / in.res)));
+            hi[a] = std::min(n[a], n[a] - static_cast<int>(std::ceil((tMax - bounds[a + 3]) / in.res)));
+        }
+    const int hAxis = plane == LBM_PLANE_XY ? 0 : 2, vAxis = plane == LBM_PLANE_ZX ? 0 : 1;
+    if (hi[hAxis] <= lo[hAxis] || hi[vAxis] <= lo[vAxis])
+        return fail(LBM_ERR_INVALID, "lbm_flow_report: empty crop");
+    return guarded("lbm_flow_report", [&] {
+        ck(cudaMemsetAsync(g->scratch, 0, 6 * sizeof(double), g->stream), "memset");
+        lbm::launchFlowReport(L.dev, in.esotwistFlipper, g->stream, plane, layer, lo[hAxis], hi[hAxis], lo[vAxis],
+                              hi[vAxis], g->scratch);
+        ck(cudaGetLastError(), "flow report launch");
+        double t[6];
+        ck(cudaMemcpyAsync(t, g->scratch, sizeof(t), cudaMemcpyDeviceToHost, g->stream), "copy");
+        ck(cudaStreamSynchronize(g->stream), "sync");
+        for (int q = 0; q < 7; ++q) out[q] = 0.0;
+        if (t[5] == 0.0) return;
+        // unit conversion (include/flowReportFunctions.h:322-351)
+        const double px = double(in.res) / 1000.0, area = px * px, vs = px / double(in.dtPhys);
+        const double ps = double(g->c.rho_phys) * vs * vs / 3.0;  // convertToPhysicalPressure of 1
+        const double mfs = double(g->c.rho_phys) * area * vs;
+        out[0] = t[0] / t[5] * vs;
+        out[1] = (t[0] + t[1]) * mfs;
+        out[2] = t[2] * mfs * vs;
+        out[3] = t[3] / t[5] * ps;
+        out[4] = t[1] * area * ps * vs;
+        out[5] = t[4] * mfs * vs * vs;
+        out[6] = t[5] * double(in.res) * in.res;
+    });
+}
+
+namespace {
+
+// One device region of the saved state of a level.
+struct StateRegion {
+    void* ptr;
+    size_t bytes;
+};
+
+std::vector<StateRegion> stateRegions(LevelState& L) {
+    lbm::DevLevel& d = L.dev;
+    std::vector<StateRegion> r;
+    r.push_back({d.f, 27ULL * size_t(d.stride) * storageBytes(d.storage)});
+    if (d.obCount) {
+        r.push_back({d.obRhoRef, 2ULL * d.obCount * sizeof(float)});
+        r.push_back({d.obRhoCum, 2ULL * d.obCount * sizeof(float)});
+    }
+    if (d.wallCount) r.push_back({d.wallForce, 3ULL * d.wallCount * sizeof(float)});
+    for (int q = 0; q < d.rotorCount; ++q)
+        if (d.rotor[q].nonzero) r.push_back({d.rotor[q].force, 3ULL * 27 * d.rotor[q].nonzero * sizeof(float)});
+    return r;
+}
+
+// host scalars of a level: counts (to check the target), flipper, counters,
+// rotor angle and speed
+struct StateHeader {
+    long long cellCount, stride;
+    int storage, obCount, wallCount, rotorCount;
+    int flipper, iterationsFinished, iterationsSinceTrackerReset, pad;
+    double radiansElapsed[LBM_MAX_ROTORS];
+    float radiansPerSecond[LBM_MAX_ROTORS];
+};
+
+constexpr unsigned long long kStateMagic = 0x3154504b43334d42ULL;  // "BM3CKPT1"
+
+size_t stateSize(lbm_grids* g) {
+    size_t n = 16;
+    for (LevelState& L : g->levels) {
+        n += sizeof(StateHeader);
+        for (const StateRegion& r : stateRegions(L)) n += r.bytes;
+    }
+    return n;
+}
+
+}  // namespace
+
+int lbm_state_bytes(lbm_grids* g, size_t* bytes) {
+    if (!g || !bytes) return fail(LBM_ERR_INVALID, "lbm_state_bytes: bad argument");
+    *bytes = stateSize(g);
+    return LBM_OK;
+}
+
+int lbm_save_state(lbm_grids* g, void* host, size_t bytes) {
+    if (!g || !host) return fail(LBM_ERR_INVALID, "lbm_save_state: bad argument");
+    if (bytes != stateSize(g))
+        return fail(LBM_ERR_INVALID, "lbm_save_state: byte count does not match lbm_state_bytes");
+    return guarded("lbm_save_state", [&] {
+        unsigned char* out = static_cast<unsigned char*>(host);
+        const unsigned long long head[2] = {kStateMagic, g->levels.size()};
+        std::memcpy(out, head, 16);
+        out += 16;
+        for (LevelState& L : g->levels) {
+            StateHeader h{};
+            h.cellCount = L.dev.cellCount;
+            h.stride = L.dev.stride;
+            h.storage = L.dev.storage;
+            h.obCount = L.dev.obCount;
+            h.wallCount = L.dev.wallCount;
+            h.rotorCount = L.dev.rotorCount;
+            h.flipper = L.info.esotwistFlipper ? 1 : 0;
+            h.iterationsFinished = L.info.iterationsFinished;
+            h.iterationsSinceTrackerReset = L.iterationsSinceTrackerReset;
+            for (size_t q = 0; q < L.rotors.size(); ++q) {
+                h.radiansElapsed[q] = L.rotors[q].radiansElapsed;
+                h.radiansPerSecond[q] = L.rotors[q].radiansPerSecond;
+            }
+            std::memcpy(out, &h, sizeof(h));
+            out += sizeof(h);
+            for (const StateRegion& r : stateRegions(L)) {
+                ck(cudaMemcpyAsync(out, r.ptr, r.bytes, cudaMemcpyDeviceToHost, g->stream), "copy");
+                out += r.bytes;
+            }
+        }
+        ck(cudaStreamSynchronize(g->stream), "sync");
+    });
+}
+
+int lbm_load_state(lbm_grids* g, const void* host, size_t bytes) {
+    if (!g || !host) return fail(LBM_ERR_INVALID, "lbm_load_state: bad argument");
+    if (bytes != stateSize(g))
+        return fail(LBM_ERR_INVALID, "lbm_load_state: the state does not belong to grids of this size");
+    const unsigned char* in = static_cast<const unsigned char*>(host);
+    unsigned long long head[2];
+    std::memcpy(head, in, 16);
+    if (head[0] != kStateMagic || head[1] != g->levels.size())
+        return fail(LBM_ERR_INVALID, "lbm_load_state: not a saved state of these grids");
+    // check every level header before changing anything
+    {
+        const unsigned char* p = in + 16;
+        for (LevelState& L : g->levels) {
+            StateHeader h;
+            std::memcpy(&h, p, sizeof(h));
+            if (h.cellCount != L.dev.cellCount || h.stride != L.dev.stride || h.storage != L.dev.storage ||
+                h.obCount != L.dev.obCount || h.wallCount != L.dev.wallCount || h.rotorCount != L.dev.rotorCount)
+                return fail(LBM_ERR_INVALID, "lbm_load_state: the state belongs to a different case");
+            p += sizeof(h);
+            for (const StateRegion& r : stateRegions(L)) p += r.bytes;
+        }
+    }
+    return guarded("lbm_load_state", [&] {
+        const unsigned char* p = in + 16;
+        for (LevelState& L : g->levels) {
+            StateHeader h;
+            std::memcpy(&h, p, sizeof(h));
+            p += sizeof(h);
+            L.info.esotwistFlipper = h.flipper != 0;
+            L.info.iterationsFinished = h.iterationsFinished;
+            L.iterationsSinceTrackerReset = h.iterationsSinceTrackerReset;
+            for (size_t q = 0; q < L.rotors.size(); ++q) {
+                L.rotors[q].radiansElapsed = h.radiansElapsed[q];
+                L.rotors[q].radiansPerSecond = h.radiansPerSecond[q];
+                L.dev.rotor[q].scale = h.radiansPerSecond[q] * L.info.dtPhys / L.info.res;
+            }
+            for (const StateRegion& r : stateRegions(L)) {
+                ck(cudaMemcpyAsync(r.ptr, p, r.bytes, cudaMemcpyHostToDevice, g->stream), "copy");
+                p += r.bytes;
+            }
+        }
+        ck(cudaStreamSynchronize(g->stream), "sync");
+    });
+}
+
 int lbm_open_boundary_flow(lbm_grids* g, int openBCID, int reset, double* out) {
     if (!g || !out || openBCID < 0) return fail(LBM_ERR_INVALID, "lbm_open_boundary_flow: bad argument");
     return guarded("lbm_open_boundary_flow", [&] {

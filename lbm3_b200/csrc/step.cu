@@ -155,6 +155,96 @@ __global__ void __launch_bounds__(kBlock) collideStream(DevLevel g) {
     writePost<F, S>(g, nb, f);
 }
 
+// Rotor volume fraction at (x, y, z) of one rotor (getRotorFraction,
+// include/rotorFunctions.h:155-209).
+__device__ __forceinline__ float rotorFractionAt(const DevRotor& R, float x, float y, float z) {
+    const float dx = x - R.ox, dy = y - R.oy, dz = z - R.oz;
+    float xr = x, yr = y, zr = z;
+    if (R.axis == 0) {
+        yr = R.oy + R.c * dy + R.s * dz;
+        zr = R.oz - R.s * dy + R.c * dz;
+    } else if (R.axis == 1) {
+        xr = R.ox + R.c * dx - R.s * dz;
+        zr = R.oz + R.s * dx + R.c * dz;
+    } else {
+        xr = R.ox + R.c * dx + R.s * dy;
+        yr = R.oy - R.s * dx + R.c * dy;
+    }
+    if (xr < R.xMin || xr >= R.xMax || yr < R.yMin || yr >= R.yMax || zr < R.zMin || zr >= R.zMax) return 0.f;
+    const float xRel = xr - R.xMin, yRel = yr - R.yMin, zRel = zr - R.zMin;
+    const int ii = static_cast<int>(xRel / R.res), jj = static_cast<int>(yRel / R.res), kk = static_cast<int>(zRel / R.res);
+    if (ii >= R.cntX || jj >= R.cntY || kk >= R.cntZ) return 0.f;
+    const int bx = R.cntX / 4, by = R.cntY / 4;
+    const int map = __ldg(R.rotorMap + (kk / 4) * bx * by + (jj / 4) * bx + ii / 4);
+    if (map < 0) return 0.f;
+    const unsigned packedCounts = __ldg(R.interp + map * 64 + (kk % 4) * 16 + (jj % 4) * 4 + (ii % 4));
+    const float xw = xRel / R.res - ii, yw = yRel / R.res - jj, zw = zRel / R.res - kk;
+    float v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = static_cast<float>((packedCounts >> (4u * q)) & 0xFu);
+    const float v00 = v[0] + xw * (v[1] - v[0]);
+    const float v10 = v[2] + xw * (v[3] - v[2]);
+    const float v01 = v[4] + xw * (v[5] - v[4]);
+    const float v11 = v[6] + xw * (v[7] - v[6]);
+    const float v0 = v00 + yw * (v10 - v00);
+    const float v1 = v01 + yw * (v11 - v01);
+    return (v0 + zw * (v1 - v0)) * 0.125f;
+}
+
+// Section-plane flow sums (getFlowReportGeneral, include/flowReportFunctions.h:11-352)
+// on one level: cells of layer `layer` along the plane normal inside the
+// in-plane index ranges [h0, h1) x [v0, v1); walls and pixels that are at
+// least half rotor are skipped.  Per pixel, in FP32 as the reference forms
+// them: {u, dRho u, (1 + dRho) u |u|, dRho, (1 + dRho) u^3 / 2, 1}, summed in
+// FP64 into out[6].
+template <bool F, class S>
+__global__ void __launch_bounds__(kBlock) flowReportSum(DevLevel g, int plane, int layer, int h0, int h1, int v0,
+                                                        int v1, double* out) {
+    const int cell = blockIdx.x * kBlock + threadIdx.x;
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    if (cell < g.cellCount) {
+        int nb[8], ijk[3];
+        decodeNbr(g, cell, nb, ijk);
+        const int normal = plane == LBM_PLANE_XY ? ijk[2] : plane == LBM_PLANE_ZY ? ijk[0] : ijk[1];
+        const int horiz = plane == LBM_PLANE_XY ? ijk[0] : ijk[2];
+        const int vert = plane == LBM_PLANE_ZX ? ijk[0] : ijk[1];
+        if (normal == layer && horiz >= h0 && horiz < h1 && vert >= v0 && vert < v1 && __ldg(g.wallMap + cell) != -3) {
+            float f[27];
+            readPre<F, S>(g, nb, f);
+            float dRho, ux, uy, uz;
+            macroFromF(f, dRho, ux, uy, uz);
+            float marker = 0.f;
+            const float x = ijk[0] * g.res + g.ox, y = ijk[1] * g.res + g.oy, z = ijk[2] * g.res + g.oz;
+            for (int r = 0; r < g.rotorCount; ++r) marker += rotorFractionAt(g.rotor[r], x, y, z);
+            marker = fminf(fmaxf(marker, 0.f), 1.f);
+            if (marker < 0.5f) {
+                const float u = plane == LBM_PLANE_XY ? uz : plane == LBM_PLANE_ZY ? ux : uy;
+                const float rhoU = fmaf(dRho, u, u);
+                v[0] = u;
+                v[1] = dRho * u;
+                v[2] = rhoU * fabsf(u);
+                v[3] = dRho;
+                v[4] = 0.5f * rhoU * u * u;
+                v[5] = 1.0;
+            }
+        }
+    }
+    __shared__ double part[6][kBlock / 32];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        double a = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+        if ((threadIdx.x & 31) == 0) part[q][threadIdx.x >> 5] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double a = 0.0;
+        for (int k = 0; k < kBlock / 32; ++k) a += part[threadIdx.x][k];
+        atomicAdd(out + threadIdx.x, a);
+    }
+}
+
 // ---- bulk collide-stream ---------------------------------------------------
 // Persistent CTAs walk the bulk segments: runs of up to kSegmentCells plain
 // fluid cells inside one compressed row, one segment per CTA iteration, one
@@ -992,6 +1082,12 @@ template <bool F, class S> struct RunOpenInit {
         if (g.obCount > 0) openBoundaryInit<F, S><<<blocksFor(g.obCount), kBlock, 0, s>>>(g);
     }
 };
+template <bool F, class S> struct RunFlowReport {
+    static void run(const DevLevel& g, cudaStream_t s, int plane, int layer, int h0, int h1, int v0, int v1,
+                    double* out) {
+        flowReportSum<F, S><<<blocksFor(g.cellCount), kBlock, 0, s>>>(g, plane, layer, h0, h1, v0, v1, out);
+    }
+};
 template <bool F, class S> struct RunInit {
     static void run(const DevLevel& g, cudaStream_t s, const float4* macro, float4 u) {
         initFeq<F, S><<<blocksFor(g.cellCount), kBlock, 0, s>>>(g, macro, u);
@@ -1045,6 +1141,10 @@ void launchGatherF(const DevLevel& g, cudaStream_t s, float* out) { dispatch<Run
 void launchScatterF(const DevLevel& g, cudaStream_t s, const float* in) { dispatch<RunScatter>(g, false, s, in); }
 void launchWallForce(const DevLevel& g, int wallID, cudaStream_t s, double* out) {
     if (g.wallCount > 0) wallForceSum<<<blocksFor(g.wallCount), kBlock, 0, s>>>(g, wallID, out);
+}
+void launchFlowReport(const DevLevel& g, bool flip, cudaStream_t s, int plane, int layer, int h0, int h1, int v0,
+                      int v1, double* out) {
+    dispatch<RunFlowReport>(g, flip, s, plane, layer, h0, h1, v0, v1, out);
 }
 void launchRotorForce(const DevRotor& R, const int* index, cudaStream_t s, double* out) {
     if (R.nonzero > 0) rotorForceSum<<<blocksFor(R.nonzero), kBlock, 0, s>>>(R, index, out);

@@ -20,6 +20,8 @@ void launchMacro(const DevLevel& g, bool flip, cudaStream_t s, float* out);
 void launchGatherF(const DevLevel& g, cudaStream_t s, float* out);
 void launchScatterF(const DevLevel& g, cudaStream_t s, const float* in);
 void launchWallForce(const DevLevel& g, int wallID, cudaStream_t s, double* out);
+void launchFlowReport(const DevLevel& g, bool flip, cudaStream_t s, int plane, int layer, int h0, int h1, int v0,
+                      int v1, double* out);
 void launchRotorForce(const DevRotor& R, const int* index, cudaStream_t s, double* out);
 void launchOpenFlow(const DevLevel& g, int openBCID, float invSpan, cudaStream_t s, double* out);
 void launchCollideBatch(float* f, int n, const CollisionConsts& P, float gx, float gy, float gz,

@@ -223,6 +223,31 @@ class Grids:
         A.check(A.lib().lbm_wall_force(self._h, wall_id, int(reset), out))
         return np.array(out[:])
 
+    def flow_report(self, plane: int, cut: float, bounds=None) -> dict:
+        """getFlowReportXY/ZY/ZX: flow through the layer nearest to `cut` (mm)."""
+        out = (C.c_double * 7)()
+        b = None
+        if bounds is not None:
+            barr = (C.c_float * 6)(*bounds)
+            b = C.cast(barr, C.c_void_p)
+        A.check(A.lib().lbm_flow_report(self._h, int(plane), float(cut), b, out))
+        keys = ("normal_velocity", "mass_flow", "momentum_thrust", "pressure", "pressure_power",
+                "normal_kinetic_power", "area_mm2")
+        return dict(zip(keys, out[:]))
+
+    def save_state(self) -> bytes:
+        """Checkpoint of everything the run carries between steps."""
+        n = C.c_size_t()
+        A.check(A.lib().lbm_state_bytes(self._h, C.byref(n)))
+        buf = (C.c_ubyte * n.value)()
+        A.check(A.lib().lbm_save_state(self._h, buf, n.value))
+        return bytes(buf)
+
+    def load_state(self, state: bytes):
+        """Resume from a checkpoint of grids built from the same case."""
+        buf = (C.c_ubyte * len(state)).from_buffer_copy(state)
+        A.check(A.lib().lbm_load_state(self._h, buf, len(state)))
+
     def rotor_info(self, r: int, level: int = 0) -> A.LbmRotorInfo:
         info = A.LbmRotorInfo()
         A.check(A.lib().lbm_get_rotor_info(self._h, level, r, C.byref(info)))

@@ -100,6 +100,7 @@ def lib() -> C.CDLL:
                                        C.c_void_p, C.c_float, C.c_void_p, C.c_int, C.c_void_p, C.c_int]
         h.oracle_set_rotor.restype = C.c_int
         h.oracle_rotor_bins.argtypes = [C.POINTER(OGrid), C.c_int, C.POINTER(C.c_float)]
+        h.oracle_flow_sums.argtypes = [C.POINTER(OGrid)] + [C.c_int] * 6 + [C.POINTER(C.c_double)]
         h.oracle_mbbc_apply.argtypes = [C.c_int] + [C.c_float] * 4 + [C.POINTER(C.c_float)]
         h.oracle_mbbc_restore_rho.argtypes = [C.c_int] + [C.c_float] * 3 + [C.POINTER(C.c_float)] * 2
         h.oracle_mbbc_restore_u.argtypes = [C.c_int, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
@@ -274,6 +275,11 @@ class OracleGrid:
         out = np.empty(3 * 27 * R, dtype=np.float32)
         lib().oracle_rotor_bins(C.byref(self.g), r, _fp(out))
         return out.reshape(3, -1)
+
+    def flow_sums(self, plane: int, layer: int, h0: int, h1: int, v0: int, v1: int) -> np.ndarray:
+        out = (C.c_double * 6)()
+        lib().oracle_flow_sums(C.byref(self.g), plane, layer, h0, h1, v0, v1, out)
+        return np.array(out[:])
 
     def open_index(self) -> np.ndarray:
         m = self.g.openCount

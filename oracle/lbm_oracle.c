@@ -1113,6 +1113,64 @@ static void rotor_forcing(ogrid* g, float x, float y, float z, float rho, float 
     if (cum > 0.f) bc->collisionLimiter *= 1.f - (cum < 0.f ? 0.f : (cum > 1.f ? 1.f : cum));
 }
 
+/* getRotorFraction (include/rotorFunctions.h:155-209) */
+static float rotor_fraction(const orotor* R, float x, float y, float z) {
+    const float angle = (float)R->radiansElapsed;
+    const float c = cosf(angle), s = sinf(angle);
+    float xr = x, yr = y, zr = z;
+    const float dx = x - R->ox, dy = y - R->oy, dz = z - R->oz;
+    if (R->axis == 0) { yr = R->oy + c * dy + s * dz; zr = R->oz - s * dy + c * dz; }
+    else if (R->axis == 1) { xr = R->ox + c * dx - s * dz; zr = R->oz + s * dx + c * dz; }
+    else { xr = R->ox + c * dx + s * dy; yr = R->oy - s * dx + c * dy; }
+    if (xr < R->xMin || xr >= R->xMax || yr < R->yMin || yr >= R->yMax || zr < R->zMin || zr >= R->zMax) return 0.f;
+    const float xRel = xr - R->xMin, yRel = yr - R->yMin, zRel = zr - R->zMin;
+    const int ii = (int)(xRel / R->res), jj = (int)(yRel / R->res), kk = (int)(zRel / R->res);
+    if (ii >= R->cntX || jj >= R->cntY || kk >= R->cntZ) return 0.f;
+    const int bx = R->cntX / 4, by = R->cntY / 4;
+    const int map = R->rotorMap[(kk / 4) * bx * by + (jj / 4) * bx + ii / 4];
+    if (map < 0) return 0.f;
+    const unsigned packed = R->interp[map * 64 + (kk % 4) * 16 + (jj % 4) * 4 + (ii % 4)];
+    const float xw = (xRel / R->res) - ii, yw = (yRel / R->res) - jj, zw = (zRel / R->res) - kk;
+    float v[8];
+    for (int q = 0; q < 8; ++q) v[q] = (float)((packed >> (4u * q)) & 0xFu);
+    const float v00 = v[0] + xw * (v[1] - v[0]), v10 = v[2] + xw * (v[3] - v[2]);
+    const float v01 = v[4] + xw * (v[5] - v[4]), v11 = v[6] + xw * (v[7] - v[6]);
+    const float v0 = v00 + yw * (v10 - v00), v1 = v01 + yw * (v11 - v01);
+    return (v0 + zw * (v1 - v0)) * 0.125f;
+}
+
+void oracle_flow_sums(const ogrid* g, int plane, int layer, int h0, int h1, int v0, int v1, double* out) {
+    for (int q = 0; q < 6; ++q) out[q] = 0.0;
+    const size_t n = (size_t)g->cellCount;
+    for (int cell = 0; cell < g->cellCount; ++cell) {
+        int ci, cj, ck;
+        get_ijk(g, cell, &ci, &cj, &ck);
+        const int normal = plane == 0 ? ck : (plane == 1 ? ci : cj);
+        const int horiz = plane == 0 ? ci : ck;
+        const int vert = plane == 2 ? ci : cj;
+        if (normal != layer || horiz < h0 || horiz >= h1 || vert < v0 || vert >= v1) continue;
+        if (g->wallMap[cell] == -3) continue;
+        int nb[8];
+        get_nbr(g, cell, nb);
+        float f[27], m[4];
+        for (int d = 0; d < 27; ++d) f[d] = g->f[(size_t)(g->flip ? INV[d] : d) * n + nb[pre_nbr(d)]];
+        oracle_get_drho_u(f, m);
+        float marker = 0.f;
+        const float x = ci * g->res + g->ox, y = cj * g->res + g->oy, z = ck * g->res + g->oz;
+        for (int r = 0; r < g->rotorCount; ++r) marker += rotor_fraction((const orotor*)g->rotors + r, x, y, z);
+        marker = marker < 0.f ? 0.f : (marker > 1.f ? 1.f : marker);
+        if (!(marker < 0.5f)) continue;
+        const float u = plane == 0 ? m[3] : (plane == 1 ? m[1] : m[2]);
+        const float rhoU = fmaf(m[0], u, u);
+        out[0] += u;
+        out[1] += m[0] * u;
+        out[2] += rhoU * fabsf(u);
+        out[3] += m[0];
+        out[4] += 0.5f * rhoU * u * u;
+        out[5] += 1.0;
+    }
+}
+
 /* ---- updateSingleGrid (include/updateGrid.h:16-386) --------------------- */
 void oracle_step(ogrid* g, int steps) {
     const long long n = g->cellCount;

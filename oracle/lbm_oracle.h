@@ -136,6 +136,12 @@ int oracle_set_rotor(ogrid* g, int r, float res, const float* bounds, const int*
 /* force bins of rotor r: out[3][27 * nonzero] */
 void oracle_rotor_bins(const ogrid* g, int r, float* out);
 
+/* Section-plane sums of getFlowReportGeneral (include/flowReportFunctions.h:11-352)
+ * on a single level: cells of layer `layer` along the plane normal (plane 0:
+ * z, 1: x, 2: y) inside in-plane index ranges [h0,h1) x [v0,v1); out[6] =
+ * {sum u, sum dRho u, sum (1+dRho) u |u|, sum dRho, sum (1+dRho) u^3/2, count}. */
+void oracle_flow_sums(const ogrid* g, int plane, int layer, int h0, int h1, int v0, int v1, double* out);
+
 /* number of OpenMP threads the oracle uses */
 int oracle_threads(void);
 
