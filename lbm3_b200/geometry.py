@@ -135,6 +135,44 @@ def set_rotors(case: A.LbmCase, rotors) -> A.LbmCase:
     return case
 
 
+def cylinder(radius: float, z0: float, z1: float, center=(0.0, 0.0), segments: int = 128) -> np.ndarray:
+    """Closed cylinder along z with flat end caps (outward normals)."""
+    cx, cy = float(center[0]), float(center[1])
+    a = np.linspace(0.0, 2.0 * np.pi, segments, endpoint=False)
+    p = np.stack([cx + radius * np.cos(a), cy + radius * np.sin(a)], axis=1)
+    tris = []
+    for q in range(segments):
+        (x0, y0), (x1, y1) = p[q], p[(q + 1) % segments]
+        tris += [((x0, y0, z0), (x1, y1, z0), (x1, y1, z1)), ((x0, y0, z0), (x1, y1, z1), (x0, y0, z1)),
+                 ((cx, cy, z0), (x1, y1, z0), (x0, y0, z0)), ((cx, cy, z1), (x0, y0, z1), (x1, y1, z1))]
+    return np.array([np.concatenate(t) for t in np.array(tris, dtype=np.float64)], dtype=np.float32)
+
+
+def bored_block(half: float, radius: float, z0: float, z1: float, center=(0.0, 0.0), segments: int = 128) -> np.ndarray:
+    """Closed solid: the square prism |x|, |y| <= half (about `center`) along z
+    with a cylindrical bore of `radius`, i.e. the fixed outer wall of a
+    Taylor-Couette cell.  `segments` must be a multiple of 8 so that the
+    square's corners are vertices of the outer polygon."""
+    if segments % 8:
+        raise ValueError("segments must be a multiple of 8")
+    cx, cy = float(center[0]), float(center[1])
+    a = np.linspace(0.0, 2.0 * np.pi, segments, endpoint=False)
+    c, s = np.cos(a), np.sin(a)
+    inner = np.stack([cx + radius * c, cy + radius * s], axis=1)
+    scale = half / np.maximum(np.abs(c), np.abs(s))   # ray from the axis to the square
+    outer = np.stack([cx + scale * c, cy + scale * s], axis=1)
+    tris = []
+    for q in range(segments):
+        r = (q + 1) % segments
+        i0, i1, o0, o1 = inner[q], inner[r], outer[q], outer[r]
+        # bore (normal towards the axis), outer sides, end caps (annular strips)
+        tris += [((*i0, z0), (*i1, z1), (*i1, z0)), ((*i0, z0), (*i0, z1), (*i1, z1))]
+        tris += [((*o0, z0), (*o1, z0), (*o1, z1)), ((*o0, z0), (*o1, z1), (*o0, z1))]
+        tris += [((*i0, z0), (*i1, z0), (*o1, z0)), ((*i0, z0), (*o1, z0), (*o0, z0))]
+        tris += [((*i0, z1), (*o1, z1), (*i1, z1)), ((*i0, z1), (*o0, z1), (*o1, z1))]
+    return np.array([np.concatenate(t) for t in np.array(tris, dtype=np.float64)], dtype=np.float32)
+
+
 def write_binary_stl(path, tris: np.ndarray) -> None:
     tris = np.asarray(tris, dtype=np.float32).reshape(-1, 9)
     with open(path, "wb") as fh:

@@ -128,3 +128,39 @@ def test_oracle_poiseuille_matches_the_analytic_profile():
     err = np.max(np.abs(ux - ua)) / ua.max()
     assert err < 0.01, err
     o.close()
+
+
+def couette_case(nu=0.1, u_wall=0.01, r1=10.0, r2=16.0, nz=4, storage=A.LBM_STORE_F32):
+    """Periodic Taylor-Couette annulus (cases/torqueTest/torqueTestMain.cu:1-60):
+    a voxelized inner cylinder turning about z inside a fixed bore, both
+    extending past the periodic z range; 1 mm cells, dt = 1 ms."""
+    c = L.periodic_box(36, 36, nz, nu_lattice=nu, storage=storage)
+    c.collision_limiter = 0.0
+    omega = u_wall / r1 / 1e-3  # rad/s so that the wall moves u_wall cells per step
+    G.set_bodies(c, [(G.cylinder(r1, -10, 10), dict(motion=A.LBM_WALL_ROTATING, axis=2, origin=(0, 0, 0),
+                                                     radians_per_second=omega)),
+                     G.bored_block(19.5, r2, -10, 10)])
+    c.track_wall_force = 1
+    return c
+
+
+def couette_torque_lattice(nu=0.1, u_wall=0.01, r1=10.0, r2=16.0, nz=4):
+    """Analytic torque on an annulus of length nz (torqueTestMain.cu:45-54), lattice units."""
+    om = u_wall / r1
+    return 4 * np.pi * nu * om * r1 ** 2 * r2 ** 2 / (r2 ** 2 - r1 ** 2) * nz
+
+
+def test_oracle_taylor_couette_torque():
+    """Steady torque of the inner and outer walls against the analytic value
+    (moving-wall interpolated bounceback and the momentum-exchange tracker)."""
+    c = couette_case()
+    o = O.OracleGrid(c, L.Plan(c))
+    o.step(3000)
+    a0, a1 = o.wall_force(0)[5], o.wall_force(1)[5]
+    o.step(500)
+    t_in = (o.wall_force(0)[5] - a0) / 500
+    t_out = (o.wall_force(1)[5] - a1) / 500
+    t = couette_torque_lattice()
+    assert t_in == pytest.approx(t, rel=0.01)
+    assert t_out == pytest.approx(-t, rel=0.01)
+    o.close()
