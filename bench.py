@@ -227,6 +227,23 @@ def run_reference(args):
     return 0
 
 
+# ---------------------------------------------------------------- ranks
+def max_over_ranks(value: float, dist, device: str) -> float:
+    """The largest `value` over all ranks (the slowest rank sets the job
+    time); `dist` is torch.distributed or None for a single process."""
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(updates_per_step: int, steps: int, world: int, seconds: float) -> float:
+    """MLUPS of the whole job: every rank advances its own replica of the
+    workload, all ranks are done after `seconds`."""
+    return updates_per_step * steps * world / seconds / 1e6
+
+
 # ---------------------------------------------------------------- GPU leg
 def run_ours(args):
     import torch
@@ -268,12 +285,10 @@ def run_ours(args):
     torch.cuda.synchronize()
     kernel_ms, launches = g.last_kernel_time()
     all_launches = g.last_launch_count()
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if dist:
         dist.barrier()
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = updates * args.steps * world / (ms_max * 1e-3) / 1e6
+    ms_max = max_over_ranks(ms, dist, "cuda")
+    value = whole_job_rate(updates, args.steps, world, ms_max * 1e-3)
 
     # roofline of the dominant kernel (collide-stream): algorithmic bytes =
     # 2 x 27 populations per fluid cell update at the storage width
@@ -310,10 +325,7 @@ def run_ours(args):
             g.kinetic_energy(1.0, 1000.0)
     g.synchronize()
     e2e_s = time.perf_counter() - t0
-    t2 = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-    e2e_value = updates * e2e_steps * world / float(t2.item()) / 1e6
+    e2e_value = whole_job_rate(updates, e2e_steps, world, max_over_ranks(e2e_s, dist, "cuda"))
     del np
 
     cpu = None
