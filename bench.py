@@ -371,6 +371,97 @@ def run_ours(args):
     return 0
 
 
+def run_batch(args, copies: int, base: str):
+    """Many-domain batch: `copies` independent domains of workload `base`, each
+    on its own stream, advanced together by update_batch.  Device-timed: a
+    start event on the launching stream, every domain stream waits on it, and
+    the end event waits for every domain stream."""
+    import torch
+    import lbm3_b200 as L
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        raise SystemExit("batch workloads run on one GPU")
+    torch.cuda.set_device(0)
+    made = [make_case(base, args.storage) for _ in range(copies)]
+    desc = made[0][1]
+    grids = [L.build_grids(c) for c, _, _ in made]
+    streams = [torch.cuda.Stream() for _ in grids]
+    for g, s in zip(grids, streams):
+        g.set_stream(s.cuda_stream)
+    per_step_launches = 0
+    for g in grids:
+        g.time_steps(1)
+        per_step_launches += g.last_launch_count()
+    L.update_batch(grids, args.warmup)
+    torch.cuda.synchronize()
+    updates = sum(g.fluid_updates_per_iteration for g in grids)
+    main_stream = torch.cuda.current_stream()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(0).uuid)
+        uuid = "GPU-" + uuid if not uuid.startswith("GPU-") else uuid
+    except Exception:
+        pass
+    with ClockSampler(uuid) as clk:
+        clk.start()
+        start.record(main_stream)
+        for s in streams:
+            s.wait_event(start)
+        L.update_batch(grids, args.steps)
+        for s in streams:
+            ev = torch.cuda.Event()
+            ev.record(s)
+            main_stream.wait_event(ev)
+        end.record(main_stream)
+        end.synchronize()
+        clk.stop()
+    ms = start.elapsed_time(end)
+    value = whole_job_rate(updates, args.steps, 1, ms * 1e-3)
+    bpp = BYTES_PER_POP[args.storage]
+    alg_bytes = updates * 2 * 27 * bpp
+    achieved = alg_bytes / (ms / args.steps * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    # end to end: upload every domain's state from pinned memory, then steps that
+    # each read every domain's kinetic energy back
+    import numpy as np
+    e2e_steps = max(10, min(args.steps // 10, 200))
+    states = [torch.from_numpy(g.populations()).pin_memory().numpy() for g in grids]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for g, f0 in zip(grids, states):
+        g.set_populations(f0)
+    for _ in range(e2e_steps):
+        L.update_batch(grids, 1)
+        for g, (_, _, tg) in zip(grids, made):
+            g.kinetic_energy(tg.u_initial_phys, tg.domain_length) if tg is not None else g.kinetic_energy(1.0, 1000.0)
+    e2e_s = time.perf_counter() - t0
+    clocks = clk.summary()
+    h2d = sum(f.nbytes for f in states)
+    for g in grids:
+        g.close()
+    del np
+    line = {
+        "metric": "MLUPS", "value": round(value, 2), "unit": "MLUPS", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
+        "config": {"workload": f"batch of {copies} independent domains, each: {desc}", "domains": copies,
+                   "fluid_updates_per_step": updates, "storage": args.storage, "compute": "f32",
+                   "l2": "all domains' populations %.0f MB" % (alg_bytes / 2 / 1e6), "parallelism": "one stream per domain"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
+                     "kernel": "whole batch step (all kernels of all domains, overlapped)",
+                     "algorithmic_bytes_per_step": alg_bytes},
+        "cpu_baseline": None,
+        "e2e": {"value": round(whole_job_rate(updates, e2e_steps, 1, e2e_s), 2), "unit": "MLUPS",
+                "h2d_bytes_per_step": int(h2d // e2e_steps), "d2h_bytes_per_step": 8 * copies, "steps": e2e_steps},
+        "gpu_launches": per_step_launches * args.steps,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -378,7 +469,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="sphere256x128x128",
-                    help="sphere256x128x128 (default; sphereNXxNYxNZ scales it), box256x128x128, tgv64, tgv128")
+                    help="sphere256x128x128 (default; sphereNXxNYxNZ scales it), box256x128x128, tgv64, tgv128, "
+                         "batchK_<workload> (K domains on K streams)")
     ap.add_argument("--storage", choices=["f32", "f16", "bf16"], default="f32")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=90.0)
@@ -388,6 +480,9 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload.startswith("batch"):
+        copies, base = args.workload[len("batch"):].split("_", 1)
+        return run_batch(args, int(copies), base)
     return run_ours(args)
 
 

@@ -255,6 +255,16 @@ int lbm_set_stream(lbm_grids* g, void* stream);
  * (include/updateGrid.h:388-396, one call per coarse step). */
 int lbm_update_all_grids(lbm_grids* g, int coarse_steps);
 
+/* Many-domain batch: advance `count` independent domains by `coarse_steps`,
+ * issuing every domain's step schedule on its own stream, step by step
+ * interleaved, so that the kernels of different domains overlap on the GPU
+ * (small domains alone leave it mostly idle between launches).  Give each
+ * grids object its own stream with lbm_set_stream; domains sharing a stream
+ * run one after the other.  Asynchronous like lbm_update_all_grids; each
+ * domain's result is the one it gets when stepped alone.
+ * No counterpart in the reference (one domain per driver process). */
+int lbm_update_batch(lbm_grids* const* grids, int count, int coarse_steps);
+
 /* Block until the grid stream is idle; returns a pending CUDA error, if any. */
 int lbm_synchronize(lbm_grids* g);
 

@@ -151,6 +151,7 @@ SIGNATURES = [
     ("lbm_free_grids", None, [_P]),
     ("lbm_set_stream", C.c_int, [_P, _P]),
     ("lbm_update_all_grids", C.c_int, [_P, C.c_int]),
+    ("lbm_update_batch", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int]),
     ("lbm_synchronize", C.c_int, [_P]),
     ("lbm_time_steps", C.c_int, [_P, C.c_int, C.POINTER(C.c_float)]),
     ("lbm_last_kernel_time", C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int)]),

@@ -560,6 +560,17 @@ int lbm_update_all_grids(lbm_grids* g, int steps) {
     });
 }
 
+int lbm_update_batch(lbm_grids* const* grids, int count, int steps) {
+    if (!grids || count < 0 || steps < 0) return fail(LBM_ERR_INVALID, "lbm_update_batch: bad argument");
+    for (int q = 0; q < count; ++q)
+        if (!grids[q]) return fail(LBM_ERR_INVALID, "lbm_update_batch: null grids in the batch");
+    return guarded("lbm_update_batch", [&] {
+        for (int s = 0; s < steps; ++s)
+            for (int q = 0; q < count; ++q) updateAllGrids(grids[q], 0);
+        ck(cudaGetLastError(), "step launch");
+    });
+}
+
 int lbm_synchronize(lbm_grids* g) {
     if (!g) return fail(LBM_ERR_INVALID, "lbm_synchronize: null grids");
     return guarded("lbm_synchronize", [&] {

@@ -303,6 +303,13 @@ class Grids:
         return out
 
 
+def update_batch(grids, coarse_steps: int = 1):
+    """Advance independent domains together, each on its own stream (set with
+    Grids.set_stream), so that their kernels overlap on the GPU."""
+    arr = (C.c_void_p * len(grids))(*[g.handle for g in grids])
+    A.check(A.lib().lbm_update_batch(arr, len(grids), int(coarse_steps)))
+
+
 def build_grids(case: A.LbmCase) -> Grids:
     """buildGrids (include/gridBuilderFunctions.h:1577-1670) on the current device."""
     return Grids(case)

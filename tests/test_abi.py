@@ -53,6 +53,32 @@ def test_null_arguments_are_rejected_without_a_device():
     assert b"null" in lib.lbm_last_error()
     assert lib.lbm_update_all_grids(None, 1) == A.LBM_ERR_INVALID
     assert lib.lbm_read_array(None, 0, 0, None, 0) == A.LBM_ERR_INVALID
+    assert lib.lbm_update_batch(None, 1, 1) == A.LBM_ERR_INVALID
+    out = (C.c_double * 7)()
+    assert lib.lbm_flow_report(None, 0, 0.0, None, out) == A.LBM_ERR_INVALID
+    assert lib.lbm_rotor_force(None, 0, 0, out) == A.LBM_ERR_INVALID
+    assert lib.lbm_set_rotor_speed(None, 0, 1.0) == A.LBM_ERR_INVALID
+    assert lib.lbm_open_boundary_flow(None, 0, 0, out) == A.LBM_ERR_INVALID
+    n = C.c_size_t()
+    assert lib.lbm_state_bytes(None, C.byref(n)) == A.LBM_ERR_INVALID
+    assert lib.lbm_save_state(None, None, 0) == A.LBM_ERR_INVALID
+    assert lib.lbm_load_state(None, None, 0) == A.LBM_ERR_INVALID
+    assert lib.lbm_kinetic_energy_noalloc(None, 1.0, 1.0, out) == A.LBM_ERR_INVALID
+
+
+def test_plan_rotor_queries_on_the_host():
+    import lbm3_b200 as L
+    from lbm3_b200 import geometry as G
+    c = L.periodic_box(24, 24, 16, nu_lattice=0.02)
+    G.set_rotors(c, [(G.rotor(hub_radius=2, tip_radius=7, chord=3, thickness=1.0, hub_length=4),
+                      dict(axis=2, origin=(0.0, 0.0, 0.0), radians_per_second=2.0))])
+    p = L.Plan(c)
+    assert p.rotor_count() == 1
+    info = A.LbmRotorInfo()
+    assert A.lib().lbm_plan_rotor_info(p._h, 0, 1, C.byref(info)) == A.LBM_ERR_INVALID
+    # the force bins live on the device only
+    buf = (C.c_uint * 4)()
+    assert A.lib().lbm_plan_read_array(p._h, 0, A.ARRAY_ROTOR_BASE + 3, buf, 16) == A.LBM_ERR_INVALID
 
 
 def test_build_without_device_fails_loudly():
