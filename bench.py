@@ -462,6 +462,65 @@ def run_batch(args, copies: int, base: str):
     return 0
 
 
+def run_serving(args):
+    """Serving stream: seeded requests (2e x e x e channels, e from {16, 24, 32},
+    obstacle and Reynolds number drawn per request, FP16 storage, 200-1000
+    steps) with Poisson arrivals at 80% of the capacity measured on a warm
+    batch, served by the continuous-batching loop; value = aggregate MLUPS,
+    plus p50/p99 time-to-result."""
+    import numpy as np
+    import torch
+    import lbm3_b200 as L
+    from lbm3_b200 import serving as S
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(12345)
+    n_req = max(8, args.steps // 25)
+    edges = rng.choice([16, 24, 32], size=n_req)
+    steps = rng.integers(200, 1001, size=n_req)
+    reqs = [S.channel_request(q, int(e), rng, int(n)) for q, (e, n) in enumerate(zip(edges, steps))]
+    # capacity: aggregate MLUPS of a warm batch of the first eight requests
+    cal = [L.build_grids(r.case) for r in reqs[:8]]
+    streams = [torch.cuda.Stream() for _ in cal]
+    for g, st in zip(cal, streams):
+        g.set_stream(st.cuda_stream)
+    L.update_batch(cal, 20)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    L.update_batch(cal, 100)
+    torch.cuda.synchronize()
+    cap = sum(g.fluid_updates_per_iteration for g in cal) * 100 / (time.perf_counter() - t0) / 1e6
+    for g in cal:
+        g.close()
+    plans = [L.Plan(r.case) for r in reqs]
+    work = [p.fluid_updates_per_iteration * int(r.steps) / 1e6 for p, r in zip(plans, reqs)]
+    footprint = max(p.info().grid_memory_bytes for p in plans)
+    for p in plans:
+        p.close()
+    rate = 0.8 * cap / float(np.mean(work))          # requests per second
+    t = 0.0
+    for r in reqs:
+        t += float(rng.exponential(1.0 / rate))
+        r.arrival = t
+    server = S.Server(hbm_budget=64 * footprint, max_slots=16, chunk_steps=50)
+    t0 = time.perf_counter()
+    results = server.run(reqs)
+    wall = time.perf_counter() - t0
+    summ = S.summarize(results, wall)
+    line = {
+        "metric": "MLUPS", "value": round(summ["mlups"], 2), "unit": "MLUPS", "n_gpus": 1,
+        "steps": int(sum(int(r.steps) for r in reqs)), "warmup": 20, "ms_per_step": None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16", "data": "synthetic",
+        "config": {"workload": f"serving stream of {len(reqs)} requests: 2e x e x e channels, e in {{16,24,32}}, "
+                               "ellipsoid/icosphere obstacle, Re 20-200, 200-1000 steps, FP16 storage, Poisson "
+                               "arrivals at 80% of measured capacity", "capacity_mlups": round(cap, 1),
+                   "arrival_rate_per_s": round(rate, 3), "parallelism": "continuous batching, one stream per domain"},
+        "serving": {"requests": summ["requests"], "p50_s": round(summ["p50_s"], 4), "p99_s": round(summ["p99_s"], 4),
+                    "wall_s": round(wall, 3)},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -470,7 +529,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="sphere256x128x128",
                     help="sphere256x128x128 (default; sphereNXxNYxNZ scales it), box256x128x128, tgv64, tgv128, "
-                         "batchK_<workload> (K domains on K streams)")
+                         "batchK_<workload> (K domains on K streams), serving (continuous-batching request stream)")
     ap.add_argument("--storage", choices=["f32", "f16", "bf16"], default="f32")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=90.0)
@@ -480,6 +539,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "serving":
+        return run_serving(args)
     if args.workload.startswith("batch"):
         copies, base = args.workload[len("batch"):].split("_", 1)
         return run_batch(args, int(copies), base)

@@ -1,0 +1,42 @@
+"""The serving loop: requests that arrive while others run are admitted by
+footprint and batched, and each result is the same as the request run alone."""
+import numpy as np
+import pytest
+
+import lbm3_b200 as L
+from lbm3_b200 import serving as S
+
+pytestmark = pytest.mark.gpu
+
+
+def requests():
+    rng = np.random.default_rng(7)
+    edges, steps, arrivals = [16, 16, 24, 16, 24], [60, 120, 90, 150, 60], [0.0, 0.0, 0.02, 0.05, 0.3]
+    return [S.channel_request(q, e, rng, n, arrival=a) for q, (e, n, a) in enumerate(zip(edges, steps, arrivals))]
+
+
+def test_results_in_the_mix_equal_results_alone():
+    reqs = requests()
+    # budget for about two domains at a time, at most three slots
+    budget = int(2.5 * max(L.Plan(r.case).info().grid_memory_bytes for r in reqs))
+    server = S.Server(hbm_budget=budget, max_slots=3, chunk_steps=40, keep_fields=True)
+    results = {r.rid: r for r in server.run(reqs)}
+    assert sorted(results) == [r.rid for r in reqs]
+    for req in requests():
+        with L.build_grids(req.case) as g:
+            g.update_all_grids(req.steps)
+            np.testing.assert_array_equal(g.macro(), results[req.rid].macro)
+            np.testing.assert_array_equal(g.wall_force(0), results[req.rid].force)
+    # requests wait for memory, not only for slots
+    admitted = sorted((r.admitted, r.finished) for r in results.values())
+    overlap = max(sum(1 for a, f in admitted if a <= t < f) for t, _ in admitted)
+    assert 2 <= overlap <= 3
+    summary = S.summarize(list(results.values()), max(r.finished for r in results.values()))
+    assert summary["requests"] == 5 and summary["p99_s"] >= summary["p50_s"] > 0
+
+
+def test_request_larger_than_the_budget_is_rejected():
+    req = requests()[2]
+    server = S.Server(hbm_budget=1000, max_slots=2)
+    with pytest.raises(ValueError):
+        server.run([req])
