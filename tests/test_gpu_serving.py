@@ -26,7 +26,9 @@ def test_results_in_the_mix_equal_results_alone():
         with L.build_grids(req.case) as g:
             g.update_all_grids(req.steps)
             np.testing.assert_array_equal(g.macro(), results[req.rid].macro)
-            np.testing.assert_array_equal(g.wall_force(0), results[req.rid].force)
+            # per-cell forces are identical; their FP64 total is summed with
+            # atomics, so only its last bits may depend on ordering
+            np.testing.assert_allclose(g.wall_force(0), results[req.rid].force, rtol=1e-12, atol=1e-300)
     # requests wait for memory, not only for slots
     admitted = sorted((r.admitted, r.finished) for r in results.values())
     overlap = max(sum(1 for a, f in admitted if a <= t < f) for t, _ in admitted)
