@@ -491,9 +491,14 @@ def run_serving(args):
     cap = sum(g.fluid_updates_per_iteration for g in cal) * 100 / (time.perf_counter() - t0) / 1e6
     for g in cal:
         g.close()
+    # submission: each request is planned once when it is submitted (before
+    # the stream starts); its footprint and work travel with it
     plans = [L.Plan(r.case) for r in reqs]
-    work = [p.fluid_updates_per_iteration * int(r.steps) / 1e6 for p, r in zip(plans, reqs)]
-    footprint = max(p.info().grid_memory_bytes for p in plans)
+    for p, r in zip(plans, reqs):
+        r.footprint = int(p.info().grid_memory_bytes)
+        r.updates = int(p.fluid_updates_per_iteration)
+    work = [r.updates * int(r.steps) / 1e6 for r in reqs]
+    footprint = max(r.footprint for r in reqs)
     for p in plans:
         p.close()
     rate = 0.8 * cap / float(np.mean(work))          # requests per second

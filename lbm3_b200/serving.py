@@ -29,6 +29,8 @@ class Request:
     steps: int
     arrival: float = 0.0        # seconds after the server starts
     wall_id: int = 0            # body whose force is the result (-1: kinetic energy)
+    footprint: int = 0          # device bytes, if known at submission (else planned at admission)
+    updates: int = 0            # fluid cell updates per step, with footprint
 
 
 @dataclass
@@ -79,10 +81,13 @@ class Server:
             # admission: arrived, a free slot, and the footprint fits
             while pending and pending[0].arrival <= now and len(active) < self.max_slots:
                 req = pending[0]
-                plan = Plan(req.case)
-                footprint = int(plan.info().grid_memory_bytes)
-                updates = int(plan.fluid_updates_per_iteration) * req.steps
-                plan.close()
+                if req.footprint > 0:
+                    footprint, updates = req.footprint, req.updates * req.steps
+                else:
+                    plan = Plan(req.case)
+                    footprint = int(plan.info().grid_memory_bytes)
+                    updates = int(plan.fluid_updates_per_iteration) * req.steps
+                    plan.close()
                 if footprint > self.hbm_budget:
                     raise ValueError(f"request {req.rid} needs {footprint} bytes, more than the whole budget")
                 if used + footprint > self.hbm_budget:
