@@ -74,7 +74,8 @@ def build() -> Path:
 def lib() -> C.CDLL:
     global _lib
     if _lib is None:
-        if not LIB.exists() or LIB.stat().st_mtime < (HERE / "lbm_oracle.c").stat().st_mtime:
+        sources = ("lbm_oracle.c", "oracle_geometry.c", "lbm_oracle.h", "oracle_internal.h")
+        if not LIB.exists() or any(LIB.stat().st_mtime < (HERE / f).stat().st_mtime for f in sources):
             build()
         h = C.CDLL(str(LIB))
         h.oracle_default_bc.argtypes = [C.POINTER(OBC)]
@@ -100,6 +101,10 @@ def lib() -> C.CDLL:
                                        C.c_void_p, C.c_float, C.c_void_p, C.c_int, C.c_void_p, C.c_int]
         h.oracle_set_rotor.restype = C.c_int
         h.oracle_rotor_bins.argtypes = [C.POINTER(OGrid), C.c_int, C.POINTER(C.c_float)]
+        h.oracle_rotor_tables.argtypes = [C.POINTER(OGrid), C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                          C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                          C.POINTER(C.POINTER(C.c_int)), C.POINTER(C.POINTER(C.c_uint))]
+        h.oracle_rotor_tables.restype = C.c_int
         h.oracle_flow_sums.argtypes = [C.POINTER(OGrid)] + [C.c_int] * 6 + [C.POINTER(C.c_double)]
         h.oracle_mbbc_apply.argtypes = [C.c_int] + [C.c_float] * 4 + [C.POINTER(C.c_float)]
         h.oracle_mbbc_restore_rho.argtypes = [C.c_int] + [C.c_float] * 3 + [C.POINTER(C.c_float)] * 2
@@ -184,8 +189,11 @@ def _vp(a):
 
 
 class OracleGrid:
-    """Single-level domain run by the oracle: built by the oracle itself for
-    box domains, or from a host plan's tables when geometry is present."""
+    """Single-level domain run by the oracle.  By default the oracle builds
+    every table itself from the case (voxelizer, markers, wall links, rotors:
+    its own restatement of the reference's setup chain); passing a host
+    ``plan`` instead loads the product's tables (used only to isolate a time
+    step difference from a setup difference)."""
 
     def __init__(self, case, plan=None):
         self.g = OGrid()
@@ -193,6 +201,7 @@ class OracleGrid:
             rc = lib().oracle_build(C.cast(C.byref(case), C.c_void_p), C.byref(self.g))
             if rc != 0:
                 raise RuntimeError(f"oracle_build failed with status {rc}")
+            self._rotor_nonzero = [self.rotor_tables(r)["nonzero"] for r in range(self.g.rotorCount)]
             return
         info = plan.info()
         arrays = {k: plan.array(k) for k in ("shifter", "row_i", "row_j", "row_k", "row_jplus", "row_kplus",
@@ -293,6 +302,37 @@ class OracleGrid:
     def open_cumulative(self) -> np.ndarray:
         m = self.g.openCount
         return np.ctypeslib.as_array(self.g.openCum, shape=(2 * m,)).reshape(2, m).copy()
+
+    def wall_arrays(self) -> dict:
+        """Wall-adjacent tables: index [nW], wall_data [nW] (uint32),
+        link_length [7][nW] (uint32), wall_velocity [3][nW] (float32)."""
+        nw = self.g.wallCount
+        if nw == 0:
+            return {"index": np.empty(0, np.int32), "wall_data": np.empty(0, np.uint32),
+                    "link_length": np.empty((7, 0), np.uint32), "wall_velocity": np.empty((3, 0), np.float32)}
+        return {"index": np.ctypeslib.as_array(self.g.wallIndex, shape=(nw,)).copy(),
+                "wall_data": np.ctypeslib.as_array(self.g.wallData, shape=(nw,)).copy(),
+                "link_length": np.ctypeslib.as_array(self.g.linkLength, shape=(7 * nw,)).reshape(7, nw).copy(),
+                "wall_velocity": np.ctypeslib.as_array(self.g.wallVel, shape=(3 * nw,)).reshape(3, nw).copy()}
+
+    def rotor_tables(self, r: int) -> dict:
+        """Rotor r as the oracle built it: res, bounds, cell counts, rotorMap,
+        interpolation (uint32 [64 * nonzero])."""
+        res = C.c_float()
+        bounds = (C.c_float * 6)()
+        counts = (C.c_int * 3)()
+        blocks, nonzero = C.c_int(), C.c_int()
+        rmap = C.POINTER(C.c_int)()
+        interp = C.POINTER(C.c_uint)()
+        if lib().oracle_rotor_tables(C.byref(self.g), r, C.byref(res), bounds, counts, C.byref(blocks),
+                                     C.byref(nonzero), C.byref(rmap), C.byref(interp)) != 0:
+            raise IndexError(f"no rotor {r}")
+        nz = nonzero.value
+        return {"res": res.value, "bounds": np.array(bounds[:], np.float32), "cell_count": np.array(counts[:]),
+                "block_count": blocks.value, "nonzero": nz,
+                "map": np.ctypeslib.as_array(rmap, shape=(blocks.value,)).copy(),
+                "interpolation": np.ctypeslib.as_array(interp, shape=(64 * nz,)).copy() if nz
+                else np.empty(0, np.uint32)}
 
     def int_array(self, name: str) -> np.ndarray:
         lengths = {"I": self.g.cellCount, "J": self.g.cellCount, "K": self.g.cellCount,

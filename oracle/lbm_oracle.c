@@ -6,6 +6,7 @@
  * Citations are path:line inside the reference project.
  */
 #include "lbm_oracle.h"
+#include "oracle_internal.h"
 /* generated coefficient tables of the moment-based open boundary (plain C
  * data; pinned against the reference's generated code by the golden vectors) */
 #include "../lbm3_b200/csrc/mbbc_tables.h"
@@ -566,47 +567,20 @@ static void get_ijk(const ogrid* g, int cell, int* i, int* j, int* k);
 static void build_open_list(ogrid* g);
 static void free_rotors(ogrid* g);
 
-int oracle_build(const lbm_case* c, ogrid* g) {
-    memset(g, 0, sizeof(*g));
-    if (c->grid_level_count != 1) return LBM_ERR_UNSUPPORTED;
-    /* initializeGridInfo (:9-64), level 0 */
-    init_info(c, g);
-    if (g->nx < 2) return LBM_ERR_INVALID;
-    const int snx = g->nx / 2, sny = g->ny / 2, snz = g->nz / 2;
-
-    /* buildFinerGridBuilder from the skeleton (:66-132): every skeleton cell
-     * is kept without geometry; 8 children each, then sortIJK (:204-234) */
-    const int n = 8 * snx * sny * snz;
-    int* ijk = (int*)malloc(sizeof(int) * 3 * (size_t)n);
-    int cf = 0;
-    for (int sc = 0; sc < snx * sny * snz; ++sc) {
-        const int ks = sc / (snx * sny), rem = sc % (snx * sny), js = rem / snx, is = rem % snx;
-        for (int ka = 0; ka < 2; ++ka)
-            for (int ja = 0; ja < 2; ++ja)
-                for (int ia = 0; ia < 2; ++ia) {
-                    ijk[3 * cf] = 2 * is + ia;
-                    ijk[3 * cf + 1] = 2 * js + ja;
-                    ijk[3 * cf + 2] = 2 * ks + ka;
-                    ++cf;
-                }
-    }
-    qsort(ijk, (size_t)n, 3 * sizeof(int), cmp_kji);
-    g->cellCount = n;
-    g->I = (int*)malloc(sizeof(int) * n); g->J = (int*)malloc(sizeof(int) * n); g->K = (int*)malloc(sizeof(int) * n);
-    for (int q = 0; q < n; ++q) { g->I[q] = ijk[3 * q]; g->J[q] = ijk[3 * q + 1]; g->K[q] = ijk[3 * q + 2]; }
-    free(ijk);
-
-    /* buildNBRPlus (include/NBRFunctions.h:82-152) */
-    g->jPlus = (int*)malloc(sizeof(int) * n);
-    g->kPlus = (int*)malloc(sizeof(int) * n);
-    int* key = (int*)malloc(sizeof(int) * n);
+/* buildNBRPlus (include/NBRFunctions.h:82-152) and markGeometricNBRPlus
+ * (:154-194) over the current sorted cell list. */
+static void nbr_plus(ogrid* g) {
+    const int n = g->cellCount;
+    free(g->jPlus); free(g->kPlus); free(g->geomBits);
+    g->jPlus = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    g->kPlus = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    int* key = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
     for (int q = 0; q < n; ++q) key[q] = g->K[q] * g->nx + g->I[q];
     connect_rows(n, key, g->nx * g->nz, g->jPlus);
     for (int q = 0; q < n; ++q) key[q] = g->J[q] * g->nx + g->I[q];
     connect_rows(n, key, g->nx * g->ny, g->kPlus);
     free(key);
-    /* markGeometricNBRPlus (:154-194) */
-    g->geomBits = (unsigned char*)calloc((size_t)n, 1);
+    g->geomBits = (unsigned char*)calloc((size_t)(n > 0 ? n : 1), 1);
     for (int q = 0; q < n; ++q) {
         const int iP = q + 1 < n ? q + 1 : 0, jP = g->jPlus[q], ijP = jP + 1 < n ? jP + 1 : 0;
         const int kP = g->kPlus[q], ikP = kP + 1 < n ? kP + 1 : 0, jkP = g->jPlus[kP];
@@ -622,7 +596,352 @@ int oracle_build(const lbm_case* c, ogrid* g) {
         if (g->I[ijkP] == i + 1 && g->J[ijkP] == j + 1 && g->K[ijkP] == k + 1) bits |= 64;
         g->geomBits[q] = bits;
     }
-    g->wallMarker = (unsigned char*)calloc((size_t)n, 1);
+}
+
+/* The 7 plus neighbours of spreadMarkers (include/markerFunctions.h:355-362). */
+static void plus7(const ogrid* g, int q, int nb[7]) {
+    const int n = g->cellCount;
+    nb[0] = q + 1 < n ? q + 1 : 0;
+    nb[1] = g->jPlus[q];
+    nb[2] = nb[1] + 1 < n ? nb[1] + 1 : 0;
+    nb[3] = g->kPlus[q];
+    nb[4] = nb[3] + 1 < n ? nb[3] + 1 : 0;
+    nb[5] = g->jPlus[nb[3]];
+    nb[6] = nb[5] + 1 < n ? nb[5] + 1 : 0;
+}
+
+/* spreadMarkers on the cell list (include/markerFunctions.h:344-399): a cell
+ * that is marked, or has a marked geometric plus neighbour, marks itself and
+ * all its geometric plus neighbours in the target. */
+static void spread_cells(const ogrid* g, const unsigned char* src, unsigned char* dst) {
+    const int n = g->cellCount;
+    memcpy(dst, src, (size_t)n);
+    for (int q = 0; q < n; ++q) {
+        int nb[7];
+        plus7(g, q, nb);
+        const unsigned bits = g->geomBits[q];
+        int marker = src[q] != 0;
+        for (int s = 0; s < 7 && !marker; ++s)
+            if (((bits >> s) & 1u) && src[nb[s]]) marker = 1;
+        if (!marker) continue;
+        dst[q] = 1;
+        for (int s = 0; s < 7; ++s)
+            if ((bits >> s) & 1u) dst[nb[s]] = 1;
+    }
+}
+
+/* spreadMarkers on the dense skeleton (include/markerFunctions.h:290-342). */
+static void spread_dense(const unsigned char* src, unsigned char* dst, int nx, int ny, int nz) {
+    const size_t total = (size_t)nx * ny * nz;
+    memcpy(dst, src, total);
+    for (size_t cell = 0; cell < total; ++cell) {
+        if (src[cell]) continue;
+        const int k = (int)(cell / ((size_t)nx * ny)), rem = (int)(cell % ((size_t)nx * ny));
+        const int j = rem / nx, i = rem % nx;
+        int hit = 0;
+        for (int dk = -1; dk <= 1 && !hit; ++dk)
+            for (int dj = -1; dj <= 1 && !hit; ++dj)
+                for (int di = -1; di <= 1 && !hit; ++di) {
+                    if (!di && !dj && !dk) continue;
+                    const int a = i + di, b = j + dj, e = k + dk;
+                    if (a < 0 || a >= nx || b < 0 || b >= ny || e < 0 || e >= nz) continue;
+                    if (src[((size_t)e * ny + b) * nx + a]) hit = 1;
+                }
+        if (hit) dst[cell] = 1;
+    }
+}
+
+/* Keep only the marked cells (deleteExcessCells steps 7-13,
+ * include/gridBuilderFunctions.h:476-579): the list stays k-j-i sorted, the
+ * plus neighbours are rebuilt. */
+static void compact_cells(ogrid* g, const unsigned char* keep) {
+    int w = 0;
+    for (int q = 0; q < g->cellCount; ++q) {
+        if (!keep[q]) continue;
+        g->I[w] = g->I[q]; g->J[w] = g->J[q]; g->K[w] = g->K[q];
+        ++w;
+    }
+    g->cellCount = w;
+    nbr_plus(g);
+}
+
+/* Wall velocity a rotating body gives a wall-adjacent cell, evaluated at the
+ * fluid cell centre: the per-wallID branch of getLocalBC in drivers with
+ * moving walls (cases/torqueTest/torqueTestMain.cu:100-122). */
+static void body_wall_velocity(const lbm_body* body, float x, float y, float z, float dtPhys, float res, float u[3]) {
+    u[0] = u[1] = u[2] = 0.f;
+    if (body->motion != LBM_WALL_ROTATING) return;
+    const float dx = x - body->origin[0], dy = y - body->origin[1], dz = z - body->origin[2];
+    const float s = body->radians_per_second * dtPhys / res;
+    if (body->axis == 2) { u[0] = -s * dy; u[1] = s * dx; }
+    else if (body->axis == 0) { u[1] = -s * dz; u[2] = s * dy; }
+    else { u[2] = -s * dx; u[0] = s * dz; }
+}
+
+/* Full 26-neighbour list through the plus/minus chains
+ * (interpolatedBouncebackFunctions.h:227-260). */
+static void full_nbrs(const ogrid* g, const int* jMinus, const int* kMinus, int c, int nb[27]) {
+    const int n = g->cellCount;
+    const int* jP = g->jPlus;
+    const int* kP = g->kPlus;
+    const int iP = c + 1 >= n ? 0 : c + 1, iM = c - 1 < 0 ? n - 1 : c - 1;
+    nb[OOO] = c; nb[POO] = iP; nb[MOO] = iM; nb[OOM] = kMinus[c]; nb[OOP] = kP[c];
+    nb[OMO] = jMinus[c]; nb[OPO] = jP[c];
+    nb[POM] = kMinus[iP]; nb[MOP] = kP[iM]; nb[POP] = kP[iP]; nb[MOM] = kMinus[iM];
+    nb[MMO] = jMinus[iM]; nb[PPO] = jP[iP]; nb[OPM] = kMinus[jP[c]]; nb[OMP] = kP[jMinus[c]];
+    nb[MPO] = jP[iM]; nb[PMO] = jMinus[iP]; nb[OPP] = jP[kP[c]]; nb[OMM] = kMinus[jMinus[c]];
+    nb[MPM] = kMinus[jP[iM]]; nb[PMP] = kP[jMinus[iP]]; nb[MMP] = kP[jMinus[iM]]; nb[PPM] = kMinus[jP[iP]];
+    nb[PMM] = kMinus[jMinus[iP]]; nb[MPP] = jP[kP[iM]]; nb[MMM] = kMinus[jMinus[iM]]; nb[PPP] = jP[kP[iP]];
+}
+
+/* buildLinkExistenceMarkerArray for one wall-adjacent cell, single level (no
+ * interface links): interpolatedBouncebackFunctions.h:181-398.  Bit d set =
+ * link towards a wall cell in direction d. */
+static unsigned link_bits(const ogrid* g, const int* jMinus, const int* kMinus, int cell) {
+    int nb[27];
+    full_nbrs(g, jMinus, kMinus, cell, nb);
+    const int i = g->I[cell], j = g->J[cell], k = g->K[cell];
+    int geo[27];
+    int all = 1, ip = 1, jp = 1, kp = 1, im = 1, jm = 1, km = 1;
+    for (int d = 1; d < 27; ++d) {
+        geo[d] = 1;
+        const int ie = i + CX[d], je = j + CY[d], ke = k + CZ[d];
+        const int q = nb[d];
+        if (g->I[q] == ie && g->J[q] == je && g->K[q] == ke) continue;
+        geo[d] = 0;
+        if (ie < 0 || ie >= g->nx || je < 0 || je >= g->ny || ke < 0 || ke >= g->nz) continue;
+        all = 0;
+        if (CX[d] > 0) ip = 0;
+        if (CY[d] > 0) jp = 0;
+        if (CZ[d] > 0) kp = 0;
+        if (CX[d] < 0) im = 0;
+        if (CY[d] < 0) jm = 0;
+        if (CZ[d] < 0) km = 0;
+    }
+    unsigned bits = 0;
+    if (i != 0 && i != g->nx - 1 && j != 0 && j != g->ny - 1 && k != 0 && k != g->nz - 1) {
+        if (!all) return 0;
+        for (int d = 1; d < 27; ++d)
+            if (g->wallMarker[nb[d]]) bits |= 1u << d;
+        return bits;
+    }
+    for (int d = 1; d < 27; ++d) {
+        if (!geo[d] || !g->wallMarker[nb[d]]) continue;
+        if ((CX[d] > 0 && !ip) || (CY[d] > 0 && !jp) || (CZ[d] > 0 && !kp)) continue;
+        if ((CX[d] < 0 && !im) || (CY[d] < 0 && !jm) || (CZ[d] < 0 && !km)) continue;
+        bits |= 1u << d;
+    }
+    return bits;
+}
+
+/* buildWallMarkers (include/gridBuilderFunctions.h:590-739), single level,
+ * then buildLinkLengthArray (interpolatedBouncebackFunctions.h:471-660) and
+ * packWallData (:662-695).  Fills wallMarker, the wall-adjacent list in cell
+ * order, wallData, linkLength and the wall velocities. */
+static void build_walls(const lbm_case* c, ogrid* g, const ostl* bodies, const oraymap* maps, const oraymap* total) {
+    const int n = g->cellCount;
+    for (int q = 0; q < n; ++q) g->wallMarker[q] = (unsigned char)oray_solid(total, g->I[q], g->J[q], g->K[q]);
+    int* wallID = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    unsigned char* src = (unsigned char*)malloc((size_t)(n > 0 ? n : 1));
+    unsigned char* bw = (unsigned char*)malloc((size_t)(n > 0 ? n : 1));
+    for (int q = 0; q < n; ++q) wallID[q] = -1;
+    for (int b = 0; b < c->body_count; ++b) {
+        for (int q = 0; q < n; ++q) src[q] = (unsigned char)oray_solid(&maps[b], g->I[q], g->J[q], g->K[q]);
+        spread_cells(g, src, bw);
+        for (int q = 0; q < n; ++q)
+            if (bw[q] && !g->wallMarker[q]) wallID[q] = b;  /* the last body wins */
+    }
+    free(src);
+    free(bw);
+    int nw = 0;
+    for (int q = 0; q < n; ++q) nw += wallID[q] >= 0;
+    g->wallCount = nw;
+    g->wallIndex = (int*)malloc(sizeof(int) * (size_t)(nw > 0 ? nw : 1));
+    int* ids = (int*)malloc(sizeof(int) * (size_t)(nw > 0 ? nw : 1));
+    for (int q = 0, w = 0; q < n; ++q)
+        if (wallID[q] >= 0) { g->wallIndex[w] = q; ids[w] = wallID[q]; ++w; }
+    free(wallID);
+
+    /* NBR minus as the inverse permutations (gridBuilderFunctions.h:565-575) */
+    int* jMinus = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    int* kMinus = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    for (int q = 0; q < n; ++q) { jMinus[g->jPlus[q]] = q; kMinus[g->kPlus[q]] = q; }
+    unsigned* links = (unsigned*)malloc(sizeof(unsigned) * (size_t)(nw > 0 ? nw : 1));
+    for (int w = 0; w < nw; ++w) links[w] = link_bits(g, jMinus, kMinus, g->wallIndex[w]);
+    free(jMinus);
+    free(kMinus);
+
+    /* link lengths: the shortest accepted crossing over every body's triangles
+     * in the bin of the cell centre */
+    float* len = (float*)malloc(sizeof(float) * 27 * (size_t)(nw > 0 ? nw : 1));
+    for (size_t q = 0; q < 27 * (size_t)nw; ++q) len[q] = 2.f;
+    const float edgeTol = 0.1f * g->res, qTol = 0.2f;
+    for (int b = 0; b < c->body_count; ++b) {
+        const ostl* t = &bodies[b];
+        const int bxy = t->binCountX * t->binCountY;
+        for (int w = 0; w < nw; ++w) {
+            if (!links[w]) continue;
+            const int cell = g->wallIndex[w];
+            const float x = g->I[cell] * g->res + g->ox, y = g->J[cell] * g->res + g->oy,
+                        z = g->K[cell] * g->res + g->oz;
+            const int ib = (int)((x - t->oxBin) / t->binSize), jb = (int)((y - t->oyBin) / t->binSize),
+                      kb = (int)((z - t->ozBin) / t->binSize);
+            if (ib < 0 || ib >= t->binCountX || jb < 0 || jb >= t->binCountY || kb < 0 || kb >= t->binCountZ)
+                continue;
+            const int bin = bxy * kb + t->binCountX * jb + ib;
+            for (int r = t->firstInBin[bin]; r < t->firstInBin[bin + 1]; ++r) {
+                const int tri = t->bin[r];
+                const float ax = t->ax[tri] - x, ay = t->ay[tri] - y, az = t->az[tri] - z;
+                const float bx = t->bx[tri] - x, by = t->by[tri] - y, bz = t->bz[tri] - z;
+                const float cx = t->cx[tri] - x, cy = t->cy[tri] - y, cz = t->cz[tri] - z;
+                for (int d = 1; d < 27; ++d) {
+                    if (!((links[w] >> d) & 1u)) continue;
+                    float tHit;
+                    if (!oray_triangle(ax, ay, az, bx, by, bz, cx, cy, cz, (float)CX[d], (float)CY[d], (float)CZ[d],
+                                       edgeTol, &tHit))
+                        continue;
+                    float qv = tHit / g->res;
+                    float* slot = &len[(size_t)w * 27 + d];
+                    if (qv > 0 && qv <= 1.f) {
+                        qv = qv < 0.00001f ? 0.00001f : (qv > 1.f ? 1.f : qv);
+                        if (*slot < 0.f || qv < *slot) *slot = qv;
+                    } else if (qv > -qTol && qv <= 1.f + qTol) {
+                        qv = qv < 0.00001f ? 0.00001f : (qv > 1.f ? 1.f : qv);
+                        if (*slot < 0.f) {
+                            if (qv < -*slot) *slot = -qv;
+                        } else if (*slot > 1.f) {
+                            *slot = -qv;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    g->wallData = (unsigned*)calloc((size_t)(nw > 0 ? nw : 1), sizeof(unsigned));
+    g->linkLength = (unsigned*)calloc(7 * (size_t)(nw > 0 ? nw : 1), sizeof(unsigned));
+    g->wallVel = (float*)calloc(3 * (size_t)(nw > 0 ? nw : 1), sizeof(float));
+    g->wallForce = (float*)calloc(3 * (size_t)(nw > 0 ? nw : 1), sizeof(float));
+    for (int w = 0; w < nw; ++w) {
+        unsigned data = (unsigned)ids[w] << 27;
+        int li = 0;
+        for (int d = 1; d < 27; ++d) {
+            if (!((links[w] >> d) & 1u)) continue;
+            float qv = len[(size_t)w * 27 + d];
+            if (qv > 1.f) qv = 0.5f;           /* no crossing found: safe fallback */
+            else if (qv < 0.f) qv = -qv;       /* near miss kept */
+            qv = qv < 0.f ? 0.f : (qv > 1.f ? 1.f : qv);
+            data |= 1u << d;
+            const unsigned code = (unsigned)(qv * 254.f + 0.5f);
+            g->linkLength[(size_t)(li / 4) * nw + w] |= code << (8 * (li % 4));
+            ++li;
+        }
+        g->wallData[w] = data;
+        const int cell = g->wallIndex[w];
+        float u[3];
+        body_wall_velocity(&c->body[ids[w]], g->I[cell] * g->res + g->ox, g->J[cell] * g->res + g->oy,
+                           g->K[cell] * g->res + g->oz, g->dtPhys, g->res, u);
+        for (int a = 0; a < 3; ++a) g->wallVel[(size_t)a * nw + w] = u[a];
+    }
+    free(ids);
+    free(links);
+    free(len);
+}
+
+static int build_rotor(ogrid* g, int r, const lbm_rotor* rt);
+
+int oracle_build(const lbm_case* c, ogrid* g) {
+    memset(g, 0, sizeof(*g));
+    if (c->grid_level_count != 1) return LBM_ERR_UNSUPPORTED;
+    if (c->body_count < 0 || c->body_count > LBM_MAX_BODIES || c->rotor_count < 0 || c->rotor_count > 4)
+        return LBM_ERR_INVALID;
+    /* initializeGridInfo (:9-64), level 0 */
+    init_info(c, g);
+    if (g->nx < 2) return LBM_ERR_INVALID;
+    const int snx = g->nx / 2, sny = g->ny / 2, snz = g->nz / 2;
+
+    /* readSTL + sortSTLToBins for every static body, one ray map each on the
+     * level and their union (initializeVoxelizers, voxelizerFunctions.h:692-728) */
+    const int nb = c->body_count;
+    ostl* bodies = (ostl*)calloc((size_t)(nb > 0 ? nb : 1), sizeof(ostl));
+    oraymap* maps = (oraymap*)calloc((size_t)(nb > 0 ? nb : 1), sizeof(oraymap));
+    oraymap total;
+    for (int b = 0; b < nb; ++b) {
+        if (!c->body[b].triangles || ostl_load(&bodies[b], c->body[b].triangles, c->body[b].triangle_count) == 0) {
+            for (int q = 0; q <= b; ++q) ostl_free(&bodies[q]);
+            for (int q = 0; q < b; ++q) oray_free(&maps[q]);
+            free(bodies); free(maps);
+            return LBM_ERR_BUILD;
+        }
+        ostl_bins(&bodies[b], c->res_global);
+        oray_voxelize(&maps[b], &bodies[b], g->ox, g->oy, g->oz, g->res, g->nx, g->ny);
+    }
+    if (nb > 0) {
+        oray_copy(&total, &maps[0]);
+        for (int b = 1; b < nb; ++b) oray_union(&total, &maps[b]);
+    } else {
+        oray_empty(&total, g->nx, g->ny);
+    }
+
+    /* markKeepCells on the skeleton (markerFunctions.h:401-407): a skeleton
+     * cell is kept when one of its 8 level cells is fluid, plus one layer */
+    const size_t sc = (size_t)snx * sny * snz;
+    unsigned char* keepS = (unsigned char*)malloc(sc);
+    unsigned char* keepT = (unsigned char*)malloc(sc);
+    for (size_t s = 0; s < sc; ++s) {
+        const int ks = (int)(s / ((size_t)snx * sny)), rem = (int)(s % ((size_t)snx * sny));
+        keepS[s] = (unsigned char)oray_block_has_fluid(&total, rem % snx, rem / snx, ks, 2);
+    }
+    spread_dense(keepS, keepT, snx, sny, snz);
+
+    /* buildFinerGridBuilder from the skeleton (:66-132): 8 children per kept
+     * skeleton cell, then sortIJK (:204-234) */
+    int kept = 0;
+    for (size_t s = 0; s < sc; ++s) kept += keepT[s];
+    const int n0 = 8 * kept;
+    int* ijk = (int*)malloc(sizeof(int) * 3 * (size_t)(n0 > 0 ? n0 : 1));
+    int cf = 0;
+    for (size_t s = 0; s < sc; ++s) {
+        if (!keepT[s]) continue;
+        const int ks = (int)(s / ((size_t)snx * sny)), rem = (int)(s % ((size_t)snx * sny)), js = rem / snx,
+                  is = rem % snx;
+        for (int ka = 0; ka < 2; ++ka)
+            for (int ja = 0; ja < 2; ++ja)
+                for (int ia = 0; ia < 2; ++ia) {
+                    ijk[3 * cf] = 2 * is + ia;
+                    ijk[3 * cf + 1] = 2 * js + ja;
+                    ijk[3 * cf + 2] = 2 * ks + ka;
+                    ++cf;
+                }
+    }
+    free(keepS);
+    free(keepT);
+    qsort(ijk, (size_t)n0, 3 * sizeof(int), cmp_kji);
+    g->cellCount = n0;
+    g->I = (int*)malloc(sizeof(int) * (size_t)(n0 > 0 ? n0 : 1));
+    g->J = (int*)malloc(sizeof(int) * (size_t)(n0 > 0 ? n0 : 1));
+    g->K = (int*)malloc(sizeof(int) * (size_t)(n0 > 0 ? n0 : 1));
+    for (int q = 0; q < n0; ++q) { g->I[q] = ijk[3 * q]; g->J[q] = ijk[3 * q + 1]; g->K[q] = ijk[3 * q + 2]; }
+    free(ijk);
+    nbr_plus(g);
+
+    /* deleteExcessCells (:402-588), single level: keep the fluid cells plus one
+     * layer of wall cells */
+    {
+        unsigned char* fluid = (unsigned char*)malloc((size_t)(n0 > 0 ? n0 : 1));
+        unsigned char* keep = (unsigned char*)malloc((size_t)(n0 > 0 ? n0 : 1));
+        for (int q = 0; q < n0; ++q) fluid[q] = (unsigned char)!oray_solid(&total, g->I[q], g->J[q], g->K[q]);
+        spread_cells(g, fluid, keep);
+        compact_cells(g, keep);
+        free(fluid);
+        free(keep);
+    }
+    const int n = g->cellCount;
+    g->wallMarker = (unsigned char*)calloc((size_t)(n > 0 ? n : 1), 1);
+    build_walls(c, g, bodies, maps, &total);
+    for (int b = 0; b < nb; ++b) { ostl_free(&bodies[b]); oray_free(&maps[b]); }
+    free(bodies);
+    free(maps);
+    oray_free(&total);
 
     /* gridBuilderToGrid (:1032-1126): first-in-row marks, inclusive max scan,
      * exclusive sum scan, compressed arrays */
@@ -660,6 +979,7 @@ int oracle_build(const lbm_case* c, ogrid* g) {
     /* wallMap (:1128-1149) and the periodic overlap (:1232-1274) */
     g->wallMap = (int*)malloc(sizeof(int) * n);
     for (int q = 0; q < n; ++q) g->wallMap[q] = g->wallMarker[q] ? -3 : -1;
+    for (int w = 0; w < g->wallCount; ++w) g->wallMap[g->wallIndex[w]] = w;
     const int layers = 1 << g->gridID;
     for (int q = 0; q < n; ++q) {
         if (g->wallMarker[q]) continue;
@@ -668,7 +988,9 @@ int oracle_build(const lbm_case* c, ogrid* g) {
         if (i < layers || i >= g->nx - layers) ov |= open_bc(c, g, i < layers ? 0 : g->nx - 1, j, k).periodic;
         if (j < layers || j >= g->ny - layers) ov |= open_bc(c, g, i, j < layers ? 0 : g->ny - 1, k).periodic;
         if (k < layers || k >= g->nz - layers) ov |= open_bc(c, g, i, j, k < layers ? 0 : g->nz - 1).periodic;
-        if (ov && g->wallMap[q] == -1) g->wallMap[q] = -2;
+        if (!ov) continue;
+        if (g->wallMap[q] >= 0) g->wallData[g->wallMap[q]] |= 1u;
+        else if (g->wallMap[q] == -1) g->wallMap[q] = -2;
     }
     build_open_list(g);
 
@@ -678,6 +1000,7 @@ int oracle_build(const lbm_case* c, ogrid* g) {
     g->perCount = 0;
     const int per = (int)lround(pow(2.0, g->gridID));
     for (int q = 0; q < n; ++q) {
+        if (g->wallMarker[q]) continue;
         int i = g->I[q], j = g->J[q], k = g->K[q];
         if (!(i == 0 || i == g->nx - 1 || j == 0 || j == g->ny - 1 || k == 0 || k == g->nz - 1)) continue;
         if (!open_bc(c, g, i, j, k).periodic) continue;
@@ -685,12 +1008,17 @@ int oracle_build(const lbm_case* c, ogrid* g) {
         if (j == 0) j = g->ny - 2 * per; else if (j == g->ny - 1) j = 2 * per - 1;
         if (k == 0) k = g->nz - 2 * per; else if (k == g->nz - 1) k = 2 * per - 1;
         const int src = find_cell(g, i, j, k);
-        if (src < 0) { oracle_free(g); return LBM_ERR_BUILD; }
+        if (src < 0 || g->wallMarker[src]) { oracle_free(g); return LBM_ERR_BUILD; }
         g->perIndex[g->perCount] = q;
         g->perSource[g->perCount] = src;
         g->perCount++;
     }
-    g->fluidUpdates = (long long)n;
+    long long walls = 0;
+    for (int q = 0; q < n; ++q) walls += g->wallMarker[q] != 0;
+    g->fluidUpdates = (long long)n - walls;
+    /* buildRotors (include/rotorFunctions.h:315-585) */
+    for (int r = 0; r < c->rotor_count; ++r)
+        if (build_rotor(g, r, &c->rotor[r]) != 0) { oracle_free(g); return LBM_ERR_BUILD; }
     apply_initial_condition(c, g);
     return 0;
 }
@@ -1028,6 +1356,104 @@ int oracle_set_rotor(ogrid* g, int r, float res, const float* bounds, const int*
     memcpy(R->interp, interpolation, sizeof(unsigned) * 64 * (size_t)nonzero);
     R->force = (float*)calloc(3 * 27 * (size_t)(nonzero > 0 ? nonzero : 1), sizeof(float));
     if (r + 1 > g->rotorCount) g->rotorCount = r + 1;
+    return 0;
+}
+
+/* buildRotors for one rotor (include/rotorFunctions.h:315-470): voxelize the
+ * rotor at half the level spacing over its own bounds, flag every 4x4x4 block
+ * of interpolation cells whose 6x6x6 voxel neighbourhood holds rotor volume,
+ * and pack per interpolation cell the eight 4-bit corner counts (how many of
+ * the 2x2x2 voxels around each corner are inside). */
+static int build_rotor(ogrid* g, int r, const lbm_rotor* rt) {
+    if (!rt->triangles || rt->axis < 0 || rt->axis > 2) return -1;
+    ostl t;
+    if (ostl_load(&t, rt->triangles, rt->triangle_count) == 0) { ostl_free(&t); return -1; }
+    const float vres = g->res * 0.5f;
+    const int vnx = (int)((t.xMax - t.xMin) / vres) + 2;
+    const int vny = (int)((t.yMax - t.yMin) / vres) + 2;
+    const int vnz = (int)((t.zMax - t.zMin) / vres) + 2;
+    oraymap m;
+    oray_voxelize(&m, &t, t.xMin, t.yMin, t.zMin, vres, vnx, vny);
+    (void)vnz;
+    float bounds[6];
+    bounds[0] = t.xMin - 1.5f * vres;
+    bounds[1] = t.yMin - 1.5f * vres;
+    bounds[2] = t.zMin - 1.5f * vres;
+    int cnt[3];
+    cnt[0] = ((vnx + 2 + 3) / 4) * 4;
+    cnt[1] = ((vny + 2 + 3) / 4) * 4;
+    cnt[2] = ((vnz + 2 + 3) / 4) * 4;
+    bounds[3] = bounds[0] + vres * (float)cnt[0];
+    bounds[4] = bounds[1] + vres * (float)cnt[1];
+    bounds[5] = bounds[2] + vres * (float)cnt[2];
+    ostl_free(&t);
+    const int bx = cnt[0] / 4, by = cnt[1] / 4, bz = cnt[2] / 4, bxy = bx * by, blocks = bx * by * bz;
+    int* rotorMap = (int*)malloc(sizeof(int) * (size_t)blocks);
+    unsigned char(*marks)[216] = malloc(sizeof(*marks) * (size_t)blocks);
+    int nonzero = 0;
+    for (int b = 0; b < blocks; ++b) {
+        const int kb = b / bxy, rem = b % bxy, jb = rem / bx, ib = rem % bx;
+        memset(marks[b], 0, 216);
+        int any = 0;
+        for (int jc = (jb * 4 - 2 > 0 ? jb * 4 - 2 : 0); jc < (vny < jb * 4 + 4 ? vny : jb * 4 + 4); ++jc)
+            for (int ic = (ib * 4 - 2 > 0 ? ib * 4 - 2 : 0); ic < (vnx < ib * 4 + 4 ? vnx : ib * 4 + 4); ++ic)
+                for (int kc = kb * 4 - 2; kc < kb * 4 + 4; ++kc)
+                    if (oray_solid(&m, ic, jc, kc)) {
+                        marks[b][(kc - (kb * 4 - 2)) * 36 + (jc - (jb * 4 - 2)) * 6 + (ic - (ib * 4 - 2))] = 1;
+                        any = 1;
+                    }
+        rotorMap[b] = any ? nonzero++ : -1;
+    }
+    oray_free(&m);
+    unsigned* interp = (unsigned*)calloc(64 * (size_t)(nonzero > 0 ? nonzero : 1), sizeof(unsigned));
+    int* index = (int*)malloc(sizeof(int) * (size_t)(nonzero > 0 ? nonzero : 1));
+    for (int b = 0; b < blocks; ++b) {
+        const int z = rotorMap[b];
+        if (z < 0) continue;
+        index[z] = b;
+        unsigned char counter[125];
+        for (int kc = 0; kc < 5; ++kc)
+            for (int jc = 0; jc < 5; ++jc)
+                for (int ic = 0; ic < 5; ++ic) {
+                    int v = 0;
+                    for (int km = kc; km <= kc + 1; ++km)
+                        for (int jm = jc; jm <= jc + 1; ++jm)
+                            for (int im = ic; im <= ic + 1; ++im) v += marks[b][km * 36 + jm * 6 + im];
+                    counter[kc * 25 + jc * 5 + ic] = (unsigned char)v;
+                }
+        for (int ki = 0; ki < 4; ++ki)
+            for (int ji = 0; ji < 4; ++ji)
+                for (int ii = 0; ii < 4; ++ii) {
+                    unsigned packed = 0u;
+                    unsigned corner = 0;
+                    for (int kc = ki; kc <= ki + 1; ++kc)
+                        for (int jc = ji; jc <= ji + 1; ++jc)
+                            for (int ic = ii; ic <= ii + 1; ++ic, ++corner)
+                                packed |= (unsigned)counter[kc * 25 + jc * 5 + ic] << (4u * corner);
+                    interp[(size_t)z * 64 + ki * 16 + ji * 4 + ii] = packed;
+                }
+    }
+    free(marks);
+    const int rc = oracle_set_rotor(g, r, vres, bounds, cnt, rt->axis, rt->origin, rt->radians_per_second, rotorMap,
+                                    blocks, interp, nonzero);
+    free(rotorMap);
+    free(interp);
+    free(index);
+    return rc;
+}
+
+int oracle_rotor_tables(const ogrid* g, int r, float* res, float* bounds, int* cellCount, int* blocks, int* nonzero,
+                        const int** rotorMap, const unsigned** interpolation) {
+    if (r < 0 || r >= g->rotorCount || !g->rotors) return -1;
+    const orotor* R = (const orotor*)g->rotors + r;
+    *res = R->res;
+    bounds[0] = R->xMin; bounds[1] = R->yMin; bounds[2] = R->zMin;
+    bounds[3] = R->xMax; bounds[4] = R->yMax; bounds[5] = R->zMax;
+    cellCount[0] = R->cntX; cellCount[1] = R->cntY; cellCount[2] = R->cntZ;
+    *blocks = R->blocks;
+    *nonzero = R->nonzero;
+    *rotorMap = R->rotorMap;
+    *interpolation = R->interp;
     return 0;
 }
 

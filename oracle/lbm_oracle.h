@@ -88,8 +88,13 @@ typedef struct ogrid {
     int trackRotorForce;
 } ogrid;
 
-/* buildGrids for a box domain without geometry, single level, followed by
- * applyInitialCondition.  Returns 0 or a negative LBM_ERR_* code. */
+/* buildGrids (include/gridBuilderFunctions.h:1577-1670) for one level,
+ * followed by applyInitialCondition: the oracle's own restatement of the
+ * setup chain (readSTL bounds, sortSTLToBins, voxelizeSTL + sumRayMaps,
+ * markKeepCells on the skeleton, deleteExcessCells, buildWallMarkers,
+ * buildLinkExistenceMarkerArray, buildLinkLengthArray, packWallData, the
+ * compressed rows, wallMap, open-boundary and periodic lists, buildRotors).
+ * Returns 0 or a negative LBM_ERR_* code. */
 int oracle_build(const lbm_case* c, ogrid* g);
 void oracle_free(ogrid* g);
 
@@ -135,6 +140,10 @@ int oracle_set_rotor(ogrid* g, int r, float res, const float* bounds, const int*
                      const unsigned* interpolation, int nonzero);
 /* force bins of rotor r: out[3][27 * nonzero] */
 void oracle_rotor_bins(const ogrid* g, int r, float* out);
+/* tables of rotor r (built by oracle_build from the case's rotor triangles,
+ * or attached with oracle_set_rotor); pointers stay owned by the grid */
+int oracle_rotor_tables(const ogrid* g, int r, float* res, float* bounds, int* cellCount, int* blocks, int* nonzero,
+                        const int** rotorMap, const unsigned** interpolation);
 
 /* Section-plane sums of getFlowReportGeneral (include/flowReportFunctions.h:11-352)
  * on a single level: cells of layer `layer` along the plane normal (plane 0:

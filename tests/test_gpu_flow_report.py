@@ -35,7 +35,7 @@ def case():
 def test_flow_report_matches_oracle(plane, cut):
     c = case()
     p = L.Plan(c)
-    o = O.OracleGrid(c, p)
+    o = O.OracleGrid(c)
     with L.build_grids(c) as g:
         g.update_all_grids(40)
         o.step(40)

@@ -17,7 +17,7 @@ def _perturbed(c, seed=7):
     plus seeded noise, so every branch of the boundary closure sees non-trivial
     input."""
     p = L.Plan(c)
-    o = O.OracleGrid(c, p)
+    o = O.OracleGrid(c)
     g = L.build_grids(c)
     f = o.populations()
     rng = np.random.default_rng(seed)
@@ -55,7 +55,7 @@ def test_sphere_in_open_channel_matches_oracle():
     G.set_bodies(c, [G.icosphere(3, 4.0, (16.0, 12.0, 12.0))])
     c.track_wall_force = 1
     p = L.Plan(c)
-    o = O.OracleGrid(c, p)
+    o = O.OracleGrid(c)
     steps = 60
     with L.build_grids(c) as g:
         g.update_all_grids(steps)

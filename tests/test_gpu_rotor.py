@@ -28,7 +28,7 @@ def rotor_case(storage=A.LBM_STORE_F32, omega=2.0, bodies=False):
 def test_rotor_matches_oracle(steps, bodies):
     c = rotor_case(bodies=bodies)
     p = L.Plan(c)
-    o = O.OracleGrid(c, p)
+    o = O.OracleGrid(c)
     with L.build_grids(c) as g:
         g.update_all_grids(steps)
         o.step(steps)

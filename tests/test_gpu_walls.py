@@ -23,7 +23,7 @@ def sphere_case(storage=A.LBM_STORE_F32):
 def test_sphere_ibb_matches_oracle(steps):
     c = sphere_case()
     p = L.Plan(c)
-    o = O.OracleGrid(c, p)
+    o = O.OracleGrid(c)
     with L.build_grids(c) as g:
         info = g.info()
         assert info.wall_adjacent_count == p.info().wall_adjacent_count > 0

@@ -98,7 +98,7 @@ def test_open_lists_with_body_match_oracle():
     c = L.open_channel(40, 20, 20)
     G.set_bodies(c, [G.icosphere(2, 4.0, (14.0, 10.0, 10.0))])
     p = L.Plan(c)
-    o = O.OracleGrid(c, p)
+    o = O.OracleGrid(c)
     np.testing.assert_array_equal(o.open_index(), p.array("open_index"))
     o.close()
 

@@ -68,7 +68,7 @@ def test_oracle_rotor_spins_the_fluid_its_way():
     for omega in (2.0, -2.0):
         c = rotor_case(tris, omega=omega)
         p = L.Plan(c)
-        o = O.OracleGrid(c, p)
+        o = O.OracleGrid(c)
         o.step(20)
         m = o.macro()
         info = p.info()
@@ -87,7 +87,7 @@ def test_oracle_rotor_spins_the_fluid_its_way():
 def test_rotor_at_rest_leaves_fluid_at_rest():
     tris = G.rotor(hub_radius=3, tip_radius=12, chord=5, thickness=1.5, hub_length=6)
     c = rotor_case(tris, omega=0.0)
-    o = O.OracleGrid(c, L.Plan(c))
+    o = O.OracleGrid(c)
     o.step(10)
     assert np.abs(o.macro()).max() < 1e-6
     o.close()

@@ -115,7 +115,7 @@ def test_oracle_poiseuille_matches_the_analytic_profile():
     nu, g, h = 0.1, 1e-6, 10.2
     c = channel_case(nu=nu, gx=g)
     p = L.Plan(c)
-    o = O.OracleGrid(c, p)
+    o = O.OracleGrid(c)
     o.step(3000)
     m = o.macro()
     info = p.info()
@@ -154,7 +154,7 @@ def test_oracle_taylor_couette_torque():
     """Steady torque of the inner and outer walls against the analytic value
     (moving-wall interpolated bounceback and the momentum-exchange tracker)."""
     c = couette_case()
-    o = O.OracleGrid(c, L.Plan(c))
+    o = O.OracleGrid(c)
     o.step(3000)
     a0, a1 = o.wall_force(0)[5], o.wall_force(1)[5]
     o.step(500)
