@@ -26,7 +26,7 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-BYTES_PER_POP = {"f32": 4, "f16": 2, "bf16": 2}
+BYTES_PER_POP = {"f32": 4, "f16": 2, "bf16": 2, "f64": 8}
 
 
 def peaks():
@@ -41,7 +41,7 @@ def peaks():
 def make_case(name: str, storage: str):
     import lbm3_b200 as L
     from lbm3_b200 import _abi as A
-    st = {"f32": A.LBM_STORE_F32, "f16": A.LBM_STORE_F16, "bf16": A.LBM_STORE_BF16}[storage]
+    st = {"f32": A.LBM_STORE_F32, "f16": A.LBM_STORE_F16, "bf16": A.LBM_STORE_BF16, "f64": A.LBM_STORE_F64}[storage]
     if name.startswith("sphere"):
         # flow around a sphere: single level, icosphere of 20,480 triangles with
         # D = 24 cells at (64, 64, 64) on the 256x128x128 grid (scaled with the
@@ -148,18 +148,16 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- CPU legs
 def oracle_grid(case):
-    """The oracle on the workload: built by itself for box domains, from the
-    product's host plan (tables checked bit-exact by the tests) with bodies."""
+    """The oracle on the workload, every table built by the oracle itself
+    (its own restatement of the reference's setup chain)."""
     import oracle as O
-    if case.body_count > 0:
-        import lbm3_b200 as L
-        return O.OracleGrid(case, L.Plan(case))
     return O.OracleGrid(case)
 
 
-def time_oracle(case, target_s: float, min_steps: int = 1):
-    """Time the C oracle (all host threads) on the same workload: returns
-    (MLUPS, steps, seconds, threads)."""
+def time_oracle(case, target_s: float, min_steps: int = 1, max_steps: int | None = None):
+    """Time whole oracle time steps (collide-stream, open boundary, periodic
+    copy: updateSingleGrid) on the host cores: returns (MLUPS, steps,
+    seconds, threads)."""
     g = oracle_grid(case)
     import oracle as O
     cells = g.g.fluidUpdates
@@ -169,58 +167,59 @@ def time_oracle(case, target_s: float, min_steps: int = 1):
         g.step(1)
         steps += 1
         el = time.perf_counter() - t0
-        if steps >= min_steps and el >= target_s:
+        if steps >= min_steps and (el >= target_s or (max_steps is not None and steps >= max_steps)):
             break
     g.close()
     return cells * steps / el / 1e6, steps, el, O.threads()
 
 
+def workload_config(desc: str, cells: int, updates: int, storage: str, world: int) -> dict:
+    """The `config` object both arms print for a workload."""
+    bpp = BYTES_PER_POP[storage]
+    pop_bytes = updates * 27 * bpp
+    return {"workload": desc, "cells": cells, "fluid_updates_per_step": updates, "storage": storage,
+            "compute": "f32",
+            "l2": "inputs larger than L2 (populations %.0f MB > 126 MB)" % (pop_bytes / 1e6)
+            if pop_bytes > 126e6 else "inputs smaller than L2",
+            "parallelism": f"replicas x{world}"}
+
+
 def run_reference(args):
-    """CPU implementation of the reference algorithm (the C oracle, all host
-    threads) on the same workload.  Each timed step is a bounded slice of a
-    full step (a contiguous run of cells of the collide-stream), sized so the
-    whole --steps K run takes about --ref-seconds."""
+    """CPU implementation of the reference algorithm (the C oracle on all host
+    threads, tables built by the oracle itself) on the same workload.  Every
+    timed step is one whole time step; the number of timed steps is capped so
+    the run stays within --ref-seconds."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    case, desc, _ = make_case(args.workload, "f32")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    case, desc, _ = make_case(args.workload, args.storage)
     import oracle as O
     g = oracle_grid(case)
-    n = g.cell_count
-    # estimate the rate on a small slice, then size the per-step slice
-    probe = min(n, 200_000)
+    n, updates = g.cell_count, int(g.g.fluidUpdates)
+    # warm-up steps, then an estimate of the step time
     t0 = time.perf_counter()
-    g.collide_range(0, probe)
-    rate = probe / max(time.perf_counter() - t0, 1e-6)
-    per_step = int(min(n, max(1000, rate * args.ref_seconds / max(args.steps + args.warmup, 1))))
-    pos = 0
-
-    def one():
-        nonlocal pos
-        c0 = pos
-        c1 = min(n, c0 + per_step)
-        g.collide_range(c0, c1)
-        pos = 0 if c1 >= n else c1
-        return c1 - c0
-
-    for _ in range(args.warmup):
-        one()
-    done, t0 = 0, time.perf_counter()
-    for _ in range(args.steps):
-        done += one()
+    g.step(1)
+    est = max(time.perf_counter() - t0, 1e-6)
+    for _ in range(max(0, min(args.warmup, 3) - 1)):
+        g.step(1)
+    timed = int(max(1, min(args.steps, args.ref_seconds / est)))
+    t0 = time.perf_counter()
+    g.step(timed)
     el = time.perf_counter() - t0
     g.close()
-    mlups = done / el / 1e6
+    mlups = updates * timed / el / 1e6
     line = {
         "impl": "reference", "metric": "MLUPS", "value": round(mlups, 3), "unit": "MLUPS",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(1e3 * el / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "n_gpus": args.gpus, "steps": timed, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * el / timed, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": desc, "cells": n, "storage": "f32"},
+        "config": workload_config(desc, n, updates, args.storage, world),
         "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": O.threads(), "kind": "port",
-                         "sample": f"each step = collide-stream of {per_step} consecutive cells of the "
-                                   f"{n}-cell grid (C restatement of the reference time step, OpenMP, "
-                                   f"{O.threads()} threads)"},
+                         "sample": f"{timed} whole time steps (collide-stream + open boundary + periodic copy) "
+                                   f"of the {n}-cell grid of {args.steps} requested, capped at "
+                                   f"{args.ref_seconds:g} s: C restatement of the reference time step on "
+                                   f"oracle-built tables, OpenMP, {O.threads()} threads, FP32 populations"},
         "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -343,11 +342,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 5),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": args.storage if args.storage != "f32" else "f32", "data": "synthetic",
-            "config": {"workload": desc, "cells": info.cell_count, "fluid_updates_per_step": updates,
-                       "storage": args.storage, "compute": "f32",
-                       "l2": "inputs larger than L2 (populations %.0f MB > 126 MB)" % (alg_bytes / 2 / 1e6)
-                       if alg_bytes / 2 > 126e6 else "inputs smaller than L2",
-                       "parallelism": f"replicas x{world}"},
+            "config": workload_config(desc, info.cell_count, updates, args.storage, world),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
@@ -463,62 +458,68 @@ def run_batch(args, copies: int, base: str):
 
 
 def run_serving(args):
-    """Serving stream: seeded requests (2e x e x e channels, e from {16, 24, 32},
-    obstacle and Reynolds number drawn per request, FP16 storage, 200-1000
-    steps) with Poisson arrivals at 80% of the capacity measured on a warm
-    batch, served by the continuous-batching loop; value = aggregate MLUPS,
-    plus p50/p99 time-to-result."""
+    """Serving stream of the serving configuration: seeded requests (2e x e x e
+    channels, e from {32, 48, 64, 96, 128}, ellipsoid or icosphere obstacle,
+    Re 20-200, 2,000-10,000 steps, FP16 storage) with Poisson arrivals at 80%
+    of the capacity the serving loop itself delivers (admission, builds and
+    stepping, measured on a saturated calibration stream), served by the
+    continuous-batching loop; value = aggregate MLUPS, plus p50/p99
+    time-to-result.  The request count is bounded by --requests."""
     import numpy as np
     import torch
-    import lbm3_b200 as L
     from lbm3_b200 import serving as S
     torch.cuda.set_device(0)
-    rng = np.random.default_rng(12345)
-    n_req = max(8, args.steps // 25)
-    edges = rng.choice([16, 24, 32], size=n_req)
-    steps = rng.integers(200, 1001, size=n_req)
-    reqs = [S.channel_request(q, int(e), rng, int(n)) for q, (e, n) in enumerate(zip(edges, steps))]
-    # capacity: aggregate MLUPS of a warm batch of the first eight requests
-    cal = [L.build_grids(r.case) for r in reqs[:8]]
-    streams = [torch.cuda.Stream() for _ in cal]
-    for g, st in zip(cal, streams):
-        g.set_stream(st.cuda_stream)
-    L.update_batch(cal, 20)
-    torch.cuda.synchronize()
+    edges_all = [32, 48, 64, 96, 128]
+
+    def stream(seed: int, count: int):
+        rng = np.random.default_rng(seed)
+        edges = rng.choice(edges_all, size=count)
+        steps = rng.integers(2000, 10001, size=count)
+        reqs = [S.channel_request(q, int(e), rng, int(n)) for q, (e, n) in enumerate(zip(edges, steps))]
+        # submission: each request is planned once; footprint and work travel with it
+        for r in reqs:
+            p = L.Plan(r.case)
+            r.footprint = int(p.info().grid_memory_bytes)
+            r.updates = int(p.fluid_updates_per_iteration)
+            p.close()
+        return reqs
+
+    import lbm3_b200 as L
+    budget = int(args.hbm_budget_gb * (1 << 30))
+    # capacity of the serving loop: a saturated stream (everything arrives at 0)
+    cal = stream(54321, args.calibration_requests)
     t0 = time.perf_counter()
-    L.update_batch(cal, 100)
-    torch.cuda.synchronize()
-    cap = sum(g.fluid_updates_per_iteration for g in cal) * 100 / (time.perf_counter() - t0) / 1e6
-    for g in cal:
-        g.close()
-    # submission: each request is planned once when it is submitted (before
-    # the stream starts); its footprint and work travel with it
-    plans = [L.Plan(r.case) for r in reqs]
-    for p, r in zip(plans, reqs):
-        r.footprint = int(p.info().grid_memory_bytes)
-        r.updates = int(p.fluid_updates_per_iteration)
+    cal_res = S.Server(hbm_budget=budget, max_slots=16, chunk_steps=100).run(cal)
+    cal_wall = time.perf_counter() - t0
+    cap = S.summarize(cal_res, cal_wall)["mlups"]
+    reqs = stream(12345, args.requests)
     work = [r.updates * int(r.steps) / 1e6 for r in reqs]
-    footprint = max(r.footprint for r in reqs)
-    for p in plans:
-        p.close()
-    rate = 0.8 * cap / float(np.mean(work))          # requests per second
+    load = 0.8
+    rate = load * cap / float(np.mean(work))          # requests per second
+    rng = np.random.default_rng(777)
     t = 0.0
     for r in reqs:
         t += float(rng.exponential(1.0 / rate))
         r.arrival = t
-    server = S.Server(hbm_budget=64 * footprint, max_slots=16, chunk_steps=50)
+    server = S.Server(hbm_budget=budget, max_slots=16, chunk_steps=100)
     t0 = time.perf_counter()
     results = server.run(reqs)
     wall = time.perf_counter() - t0
     summ = S.summarize(results, wall)
+    offered = sum(work) / reqs[-1].arrival if reqs[-1].arrival > 0 else None
     line = {
         "metric": "MLUPS", "value": round(summ["mlups"], 2), "unit": "MLUPS", "n_gpus": 1,
-        "steps": int(sum(int(r.steps) for r in reqs)), "warmup": 20, "ms_per_step": None,
+        "steps": int(sum(int(r.steps) for r in reqs)), "warmup": 0, "ms_per_step": None,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16", "data": "synthetic",
-        "config": {"workload": f"serving stream of {len(reqs)} requests: 2e x e x e channels, e in {{16,24,32}}, "
-                               "ellipsoid/icosphere obstacle, Re 20-200, 200-1000 steps, FP16 storage, Poisson "
-                               "arrivals at 80% of measured capacity", "capacity_mlups": round(cap, 1),
-                   "arrival_rate_per_s": round(rate, 3), "parallelism": "continuous batching, one stream per domain"},
+        "config": {"workload": f"serving stream of {len(reqs)} requests: 2e x e x e channels, e in {edges_all}, "
+                               "ellipsoid/icosphere obstacle, Re 20-200, 2000-10000 steps, FP16 storage, Poisson "
+                               "arrivals at 80% of the serving loop's measured capacity",
+                   "requests": len(reqs), "hbm_budget_gb": args.hbm_budget_gb,
+                   "capacity_mlups": round(cap, 1), "capacity_sample": f"{len(cal)} requests arriving at once, "
+                   f"{cal_wall:.1f} s", "offered_load_fraction": load,
+                   "arrival_rate_per_s": round(rate, 4),
+                   "offered_mlups": round(offered, 1) if offered else None,
+                   "parallelism": "continuous batching, one stream per domain, grids built on 2 host threads"},
         "serving": {"requests": summ["requests"], "p50_s": round(summ["p50_s"], 4), "p99_s": round(summ["p99_s"], 4),
                     "wall_s": round(wall, 3)},
     }
@@ -535,10 +536,13 @@ def main():
     ap.add_argument("--workload", default="sphere256x128x128",
                     help="sphere256x128x128 (default; sphereNXxNYxNZ scales it), box256x128x128, tgv64, tgv128, "
                          "batchK_<workload> (K domains on K streams), serving (continuous-batching request stream)")
-    ap.add_argument("--storage", choices=["f32", "f16", "bf16"], default="f32")
+    ap.add_argument("--storage", choices=["f32", "f16", "bf16", "f64"], default="f32")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=90.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--requests", type=int, default=48, help="serving: requests in the measured stream")
+    ap.add_argument("--calibration-requests", type=int, default=12, help="serving: saturated capacity sample")
+    ap.add_argument("--hbm-budget-gb", type=float, default=120.0, help="serving: device memory for resident domains")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -54,10 +54,13 @@ extern "C" {
 #define LBM_IC_UNIFORM      0  /* dRho, ux, uy, uz constant                      */
 #define LBM_IC_TAYLOR_GREEN 1  /* cases/taylorGreenVortex/taylorGreenVortexMain.cu:66-87 */
 
-/* population storage precision (compute is always FP32) */
+/* population storage precision (arithmetic is FP32 for the first three) */
 #define LBM_STORE_F32  0
 #define LBM_STORE_F16  1      /* shifted populations f_i - w_i as IEEE half     */
 #define LBM_STORE_BF16 2      /* shifted populations f_i - w_i as bfloat16      */
+#define LBM_STORE_F64  3      /* FP64 populations and FP64 arithmetic: the
+                                 double-precision build of the same kernels,
+                                 the reference of the storage-precision study */
 
 /* arrays that lbm_read_array can copy out (per level) */
 #define LBM_ARRAY_F            0  /* float  [27][cellCount] (always returned as FP32) */
@@ -309,13 +312,26 @@ int lbm_kinetic_energy(lbm_grids* g, float u_ref_phys, float domain_length,
  * must have at most LBM_KINETIC_ENERGY_NOALLOC_MAX_CELLS cells; larger ones
  * are rejected with LBM_ERR_INVALID.  Call it with the grids' device current;
  * its first call on a device looks up the array's device address, so make
- * that call before any stream capture begins.  All calls on a device share
+ * that call before any stream capture begins.  The address is kept for the
+ * life of the process: after a cudaDeviceReset of a device, do not call this
+ * entry point on that device again.  All calls on a device share
  * the array: calls that overlap on the GPU race.  The sum is deterministic
  * (fixed order, no atomics).
  * No counterpart in the reference. */
 #define LBM_KINETIC_ENERGY_NOALLOC_MAX_CELLS 4194304
 int lbm_kinetic_energy_noalloc(lbm_grids* g, float u_ref_phys, float domain_length,
                                double* out);
+
+/* Global FP64 accumulators over the fluid cells of every level (walls,
+ * periodic ghosts and interface duplicates excluded), summed on the device:
+ * out = {mass [kg], mass minus the rest mass [kg], momentum x, y, z [kg m/s]
+ * (the domain's mass flow rate times its length), fluid cells, sum of rho and
+ * sum of dRho in lattice units}.  The momentum is the sum of c_i f_i, without
+ * the half body-force shift.  Mass drift of a closed domain is the change of
+ * out[7] between calls.
+ * The north star's global mass and flow-rate accumulators; the reference
+ * tracks only open-boundary and wall quantities (include/trackerFunctions.h:120-497). */
+int lbm_global_sums(lbm_grids* g, double* out);
 
 /* Momentum-exchange force and torque on one body (wallID), accumulated in
  * FP64 on the device over the wall-adjacent cells and averaged over the
@@ -366,6 +382,14 @@ int lbm_rotor_force(lbm_grids* g, int rotor, int reset, double* out);
  * Replaces getFlowReportXY/ZY/ZX (include/flowReportFunctions.h:11-373) for a
  * single-level grid. */
 int lbm_flow_report(lbm_grids* g, int plane, float cut, const float* bounds, double* out);
+
+/* Write every cell of every level to a legacy ASCII VTK file (POLYDATA, one
+ * vertex per cell centre in mm) with point data wall (0/1), velocity_m_s,
+ * pressure_Pa, grid_id, grid_resolution_mm and interface_overlap (0/1);
+ * walls carry zero velocity and pressure.  Fields come from the device state
+ * at the call (FP64 accumulators are not involved).
+ * Replaces exportVTK (include/exportVTK.h:17-158). */
+int lbm_export_vtk(lbm_grids* g, const char* filename);
 
 /* Checkpoint and resume (preemption of long runs and of served domains).
  * The state is everything a run carries from step to step: the populations at

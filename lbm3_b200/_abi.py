@@ -37,7 +37,8 @@ LBM_IC_TAYLOR_GREEN = 1
 LBM_STORE_F32 = 0
 LBM_STORE_F16 = 1
 LBM_STORE_BF16 = 2
-STORAGE_NAMES = {LBM_STORE_F32: "f32", LBM_STORE_F16: "f16", LBM_STORE_BF16: "bf16"}
+LBM_STORE_F64 = 3
+STORAGE_NAMES = {LBM_STORE_F32: "f32", LBM_STORE_F16: "f16", LBM_STORE_BF16: "bf16", LBM_STORE_F64: "f64"}
 
 # arrays
 ARRAY_F = 0
@@ -162,6 +163,7 @@ SIGNATURES = [
     ("lbm_write_f", C.c_int, [_P, C.c_int, _P, C.c_size_t]),
     ("lbm_kinetic_energy", C.c_int, [_P, C.c_float, C.c_float, C.POINTER(C.c_double)]),
     ("lbm_kinetic_energy_noalloc", C.c_int, [_P, C.c_float, C.c_float, C.POINTER(C.c_double)]),
+    ("lbm_global_sums", C.c_int, [_P, C.POINTER(C.c_double)]),
     ("lbm_wall_force", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     ("lbm_open_boundary_flow", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     ("lbm_plan_rotor_info", C.c_int, [_P, C.c_int, C.c_int, C.c_void_p]),
@@ -169,6 +171,7 @@ SIGNATURES = [
     ("lbm_set_rotor_speed", C.c_int, [_P, C.c_int, C.c_float]),
     ("lbm_rotor_force", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     ("lbm_flow_report", C.c_int, [_P, C.c_int, C.c_float, C.c_void_p, C.POINTER(C.c_double)]),
+    ("lbm_export_vtk", C.c_int, [_P, C.c_char_p]),
     ("lbm_state_bytes", C.c_int, [_P, C.POINTER(C.c_size_t)]),
     ("lbm_save_state", C.c_int, [_P, C.c_void_p, C.c_size_t]),
     ("lbm_load_state", C.c_int, [_P, C.c_void_p, C.c_size_t]),

@@ -17,7 +17,19 @@ LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "liblbm3_b200.so"
 OBJ_DIR = PKG / "_build"
 
-SOURCES = ["step.cu", "api.cu", "builder.cpp", "geometry.cpp", "energy_noalloc.cu"]
+# (source, object, extra defines): step.cu is compiled once per population
+# storage type so the three kernel sets build in parallel
+SOURCES = [
+    ("step.cu", "step_f32.o", ["-DLBM3_STEP_STORAGE=0"]),
+    ("step.cu", "step_f16.o", ["-DLBM3_STEP_STORAGE=1"]),
+    ("step.cu", "step_bf16.o", ["-DLBM3_STEP_STORAGE=2"]),
+    ("step.cu", "step_f64.o", ["-DLBM3_STEP_STORAGE=3"]),
+    ("step_dispatch.cu", "step_dispatch.o", []),
+    ("api.cu", "api.o", []),
+    ("builder.cpp", "builder.o", []),
+    ("geometry.cpp", "geometry.o", []),
+    ("energy_noalloc.cu", "energy_noalloc.o", []),
+]
 HEADERS = ["lattice.h", "cumulant.cuh", "step.cuh", "step_launch.h", "builder.h", "geometry.h", "mbbc.h",
            "mbbc_tables.h", "energy_noalloc.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -46,16 +58,23 @@ def build(verbose: bool = False, force: bool = False, extra_flags=None) -> Path:
     OBJ_DIR.mkdir(exist_ok=True)
     headers = [CSRC / h for h in HEADERS] + [PKG.parent / "include" / "lbm3_b200.h"]
     flags = NVCC_FLAGS + list(extra_flags or [])
-    objs = []
-    for src in SOURCES:
+    objs, jobs = [], []
+    for src, obj, defines in SOURCES:
         s = CSRC / src
-        o = OBJ_DIR / (src + ".o")
+        o = OBJ_DIR / obj
         objs.append(o)
         if force or _stale(o, [s, *headers, Path(__file__)]):
-            cmd = [_nvcc(), *flags, "-c", str(s), "-o", str(o)]
+            jobs.append([_nvcc(), *flags, *defines, "-c", str(s), "-o", str(o)])
+    if jobs:
+        from concurrent.futures import ThreadPoolExecutor
+
+        def run(cmd):
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
+
+        with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+            list(pool.map(run, jobs))
     if force or _stale(LIB, objs):
         cmd = [_nvcc(), *ARCH, "-shared", *map(str, objs), "-o", str(LIB), "-lcudart"]
         if verbose:

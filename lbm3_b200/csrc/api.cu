@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <exception>
@@ -53,7 +54,14 @@ template <class T> T* upload(const std::vector<T>& v, cudaStream_t s) {
     return p;
 }
 
-size_t storageBytes(int storage) { return storage == LBM_STORE_F32 ? 4 : 2; }
+size_t storageBytes(int storage) {
+    return storage == LBM_STORE_F64 ? 8 : storage == LBM_STORE_F32 ? 4 : 2;
+}
+
+// bytes of one direction-indexed closure table in the kernels' arithmetic type
+size_t mbbcTableBytes(int storage) {
+    return storage == LBM_STORE_F64 ? sizeof(lbm::MbbcDirT<double>) : sizeof(lbm::MbbcDirT<float>);
+}
 
 // Distance between consecutive population planes, in elements.  Planes start
 // on 128-byte boundaries and are an odd number of 128-byte granules apart, so
@@ -119,15 +127,44 @@ struct lbm_plan {
 
 namespace {
 
-// Device bytes of one level: populations at the storage width plus the index
-// tables, as the reference accounts them (gridBuilderFunctions.h:1630-1649).
+// Open-boundary chunks of the boundary kernel: cells grouped by outer normal
+// (table row), kOpenChunk per CTA.
+size_t openChunkCount(const lbm::HostLevel& H) {
+    std::vector<size_t> perRow(LBM_MBBC_NORMALS, 0);
+    for (const auto& oc : H.openCells) ++perRow[(oc.info >> 10) & 31];
+    size_t chunks = 0;
+    for (size_t c : perRow) chunks += (c + lbm::kOpenChunk - 1) / lbm::kOpenChunk;
+    return chunks;
+}
+
+// Device bytes of one level: every array lbm_build_grids allocates for it,
+// with the same size expressions (the reference prints a similar per-level
+// account, gridBuilderFunctions.h:1630-1649).  The domain-wide words (FP64
+// reduction scratch, error flag) are counted with level 0.
 unsigned long long levelBytes(const lbm::HostLevel& H, int storage) {
-    const unsigned long long n = static_cast<unsigned long long>(H.info.cellCount);
-    unsigned long long b = 27ULL * planeStride(static_cast<long long>(n), storage) * storageBytes(storage);
-    b += 2ULL * n * 4;                       // shifter, wallMap
-    b += 6ULL * H.rowI.size() * 4;           // compressed rows
-    b += 2ULL * H.perIndex.size() * 4;       // periodic index/source
-    for (const auto& ob : H.openBCs) b += 4ULL * ob.index.size() * 4;
+    using ull = unsigned long long;
+    auto bytes = [](size_t count, size_t each) { return static_cast<ull>(count) * each; };
+    const size_t n = static_cast<size_t>(H.info.cellCount);
+    ull b = 27ULL * planeStride(static_cast<long long>(n), storage) * storageBytes(storage) + 256;  // populations
+    b += bytes(2, sizeof(int));                                     // work counter
+    b += bytes(n, sizeof(int)) * 2;                                 // shifter, wallMap
+    b += bytes(H.rowI.size(), sizeof(int)) * 6;                     // compressed rows
+    b += bytes(H.perIndex.size(), sizeof(int)) * 2;                 // periodic index, source
+    b += bytes(H.segCell.size(), sizeof(int4)) + bytes(H.segLen.size(), sizeof(int));  // bulk segments
+    b += bytes(H.specialCells.size(), sizeof(int)) + bytes(H.rotorCells.size(), sizeof(int));
+    for (const auto& R : H.rotors)
+        b += bytes(R.rotorMap.size(), sizeof(int)) + bytes(R.interpolation.size(), sizeof(unsigned)) +
+             bytes(R.index.size(), sizeof(int)) + bytes(3 * 27 * R.index.size(), sizeof(float));
+    b += bytes(H.wallIndex.size(), sizeof(int)) + bytes(H.wallData.size(), sizeof(unsigned)) +
+         bytes(H.linkLength.size(), sizeof(unsigned)) + bytes(H.wallVelocity.size(), sizeof(float)) +
+         bytes(3 * H.wallIndex.size(), sizeof(double));            // wall tables and FP64 force accumulators
+    const size_t m = H.openCells.size();
+    size_t sources = 0;
+    for (const auto& ob : H.openBCs) sources += ob.source.size();
+    b += bytes(m, sizeof(int)) * 2 + bytes(m, sizeof(int4)) + bytes(m, sizeof(float4)) + bytes(m, sizeof(float)) +
+         bytes(sources, sizeof(int)) + bytes(4 * m, sizeof(float));  // cell, info, nbr, target, beta, source, refs
+    b += bytes(openChunkCount(H), sizeof(int4)) + (m ? bytes(LBM_MBBC_NORMALS, mbbcTableBytes(storage)) : 0);
+    if (H.info.gridID == 0) b += bytes(8, sizeof(double)) + bytes(1, sizeof(int));
     return b;
 }
 
@@ -442,8 +479,8 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
             d.wallData = own(upload(H.wallData, s));
             d.linkLength = own(upload(H.linkLength, s));
             d.wallVel = own(upload(H.wallVelocity, s));
-            d.wallForce = own(devAlloc<float>(3 * H.wallIndex.size()));
-            if (d.wallForce) ck(cudaMemsetAsync(d.wallForce, 0, 3 * H.wallIndex.size() * sizeof(float), s), "memset");
+            d.wallForce = own(devAlloc<double>(3 * H.wallIndex.size()));
+            if (d.wallForce) ck(cudaMemsetAsync(d.wallForce, 0, 3 * H.wallIndex.size() * sizeof(double), s), "memset");
             {
                 // open boundaries.  The device keeps the per-cell records in
                 // kernel order: cells grouped by outer normal (table row) into
@@ -494,7 +531,13 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
                 d.trackOpen = c->track_open_boundaries ? 1 : 0;
                 d.obChunk = own(upload(chunks, s));
                 d.obChunkCount = static_cast<int>(chunks.size());
-                d.obTables = m ? own(upload(tables, s)) : nullptr;
+                if (m && c->storage == LBM_STORE_F64) {
+                    std::vector<lbm::MbbcDirT<double>> wide(LBM_MBBC_NORMALS);
+                    for (int t = 0; t < LBM_MBBC_NORMALS; ++t) wide[t] = lbm::mbbcDirFromTable<double>(kLbmMbbc[t]);
+                    d.obTables = own(upload(wide, s));
+                } else {
+                    d.obTables = m ? own(upload(tables, s)) : nullptr;
+                }
             }
             d.trackWallForce = c->track_wall_force ? 1 : 0;
             d.useIBB = c->use_ibb ? 1 : 0;
@@ -504,6 +547,7 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
             lbm::BC bc;
             lbm::evalLocalBC(*c, bc);
             d.coll = lbm::makeCollisionConsts(H.info.nu, bc.nuMultiplier, bc.collisionLimiter);
+            d.coll64 = lbm::makeCollisionConstsT<double>(H.info.nu, bc.nuMultiplier, bc.collisionLimiter);
             // memory accounting as the reference prints it (gridBuilderFunctions.h:1630-1649),
             // scaled by the population storage size
             L.memBytes = levelBytes(H, c->storage);
@@ -687,7 +731,7 @@ int lbm_read_array(lbm_grids* g, int level, int which, void* host, size_t bytes)
         case LBM_ARRAY_WALL_INDEX: src = d.wallIndex; need = size_t(d.wallCount) * 4; break;
         case LBM_ARRAY_WALL_DATA: src = d.wallData; need = size_t(d.wallCount) * 4; break;
         case LBM_ARRAY_LINK_LENGTH: src = d.linkLength; need = size_t(d.wallCount) * 7 * 4; break;
-        case LBM_ARRAY_WALL_FORCE: src = d.wallForce; need = size_t(d.wallCount) * 3 * 4; break;
+        case LBM_ARRAY_WALL_FORCE: need = size_t(d.wallCount) * 3 * 4; break;  // FP64 on the device
         case LBM_ARRAY_WALL_VELOCITY: src = d.wallVel; need = size_t(d.wallCount) * 3 * 4; break;
         case LBM_ARRAY_OPEN_INDEX: src = d.obCell; need = size_t(d.obCount) * 4; break;
         case LBM_ARRAY_OPEN_SOURCE: src = L.obSource; need = size_t(d.obCount) * 4; break;
@@ -712,7 +756,14 @@ int lbm_read_array(lbm_grids* g, int level, int which, void* host, size_t bytes)
                                          std::to_string(need) + ")");
     return guarded("lbm_read_array", [&] {
         if (need == 0) return;
-        if (which == LBM_ARRAY_F || which == LBM_ARRAY_MACRO) {
+        if (which == LBM_ARRAY_WALL_FORCE) {
+            std::vector<double> tmp(need / 4);
+            ck(cudaMemcpyAsync(tmp.data(), d.wallForce, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                               g->stream), "copy");
+            ck(cudaStreamSynchronize(g->stream), "sync");
+            float* out = static_cast<float*>(host);
+            for (size_t q = 0; q < tmp.size(); ++q) out[q] = static_cast<float>(tmp[q]);
+        } else if (which == LBM_ARRAY_F || which == LBM_ARRAY_MACRO) {
             float* tmp = devAlloc<float>(need / 4);
             try {
                 if (which == LBM_ARRAY_F) lbm::launchGatherF(d, g->stream, tmp);
@@ -767,7 +818,7 @@ int lbm_write_f(lbm_grids* g, int level, const float* host, size_t bytes) {
 static void resetTracker(lbm_grids* g) {
     for (LevelState& L : g->levels) {
         const lbm::DevLevel& d = L.dev;
-        if (d.wallForce) ck(cudaMemsetAsync(d.wallForce, 0, 3 * size_t(d.wallCount) * sizeof(float), g->stream), "memset");
+        if (d.wallForce) ck(cudaMemsetAsync(d.wallForce, 0, 3 * size_t(d.wallCount) * sizeof(double), g->stream), "memset");
         if (d.obRhoCum) ck(cudaMemsetAsync(d.obRhoCum, 0, 2 * size_t(d.obCount) * sizeof(float), g->stream), "memset");
         for (int r = 0; r < d.rotorCount; ++r)
             if (d.rotor[r].force)
@@ -795,6 +846,31 @@ int lbm_kinetic_energy(lbm_grids* g, float uRefPhys, float domainLength, double*
         }
         const double len = double(domainLength) / 1000.0;
         *out = energy / (len * len * len);
+    });
+}
+
+int lbm_global_sums(lbm_grids* g, double* out) {
+    if (!g || !out) return fail(LBM_ERR_INVALID, "lbm_global_sums: bad argument");
+    return guarded("lbm_global_sums", [&] {
+        double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (LevelState& L : g->levels) {
+            ck(cudaMemsetAsync(g->scratch, 0, 6 * sizeof(double), g->stream), "memset");
+            lbm::launchGlobalSums(L.dev, L.info.esotwistFlipper, g->stream, g->scratch);
+            ck(cudaGetLastError(), "global sums launch");
+            double sum[6];
+            ck(cudaMemcpyAsync(sum, g->scratch, sizeof(sum), cudaMemcpyDeviceToHost, g->stream), "copy");
+            ck(cudaStreamSynchronize(g->stream), "sync");
+            const double dx = double(L.info.res) / 1000.0;                // m
+            const double cellMass = double(g->c.rho_phys) * dx * dx * dx;  // kg per unit lattice density
+            const double vel = dx / double(L.info.dtPhys);                 // m/s per lattice velocity
+            acc[0] += cellMass * sum[0];
+            acc[1] += cellMass * sum[1];
+            for (int a = 0; a < 3; ++a) acc[2 + a] += cellMass * vel * sum[2 + a];
+            acc[5] += sum[5];
+            acc[6] += sum[0];
+            acc[7] += sum[1];
+        }
+        for (int q = 0; q < 8; ++q) out[q] = acc[q];
     });
 }
 
@@ -916,6 +992,135 @@ int lbm_rotor_force(lbm_grids* g, int rotor, int reset, double* out) {
     });
 }
 
+int lbm_export_vtk(lbm_grids* g, const char* filename) {
+    if (!g || !filename) return fail(LBM_ERR_INVALID, "lbm_export_vtk: null argument");
+    return guarded("lbm_export_vtk", [&] {
+        // per level: cell centres (mm), wall flag, velocity (m/s), pressure
+        // (Pa), interface overlap flag, all computed as the reference does
+        struct LevelFields {
+            std::vector<float> x, y, z, ux, uy, uz, p;
+            std::vector<unsigned char> wall, overlap;
+            int gridID = 0;
+            float res = 0.f;
+        };
+        std::vector<LevelFields> lf(g->levels.size());
+        size_t total = 0;
+        const float invSqrt3 = 0.57735026918962576f;
+        for (size_t l = 0; l < g->levels.size(); ++l) {
+            LevelState& L = g->levels[l];
+            const lbm::DevLevel& d = L.dev;
+            const size_t n = static_cast<size_t>(d.cellCount);
+            const size_t rows = static_cast<size_t>(L.rowCount);
+            auto fetch = [&](const void* src, size_t bytes, void* dst) {
+                if (bytes) ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, g->stream), "copy");
+            };
+            std::vector<int> shifter(n), rI(rows), rJ(rows), rK(rows), wallMap(n);
+            std::vector<unsigned> wallData(static_cast<size_t>(d.wallCount));
+            fetch(d.shifter, n * 4, shifter.data());
+            fetch(d.rowI, rows * 4, rI.data());
+            fetch(d.rowJ, rows * 4, rJ.data());
+            fetch(d.rowK, rows * 4, rK.data());
+            fetch(d.wallMap, n * 4, wallMap.data());
+            fetch(d.wallData, wallData.size() * 4, wallData.data());
+            std::vector<float> macro(4 * n);
+            if (n) {
+                float* tmp = devAlloc<float>(4 * n);
+                try {
+                    lbm::launchMacro(d, L.info.esotwistFlipper, g->stream, tmp);
+                    ck(cudaGetLastError(), "macro launch");
+                    fetch(tmp, 4 * n * 4, macro.data());
+                    ck(cudaStreamSynchronize(g->stream), "sync");
+                } catch (...) {
+                    cudaFree(tmp);
+                    throw;
+                }
+                cudaFree(tmp);
+            }
+            ck(cudaStreamSynchronize(g->stream), "sync");
+            LevelFields& F = lf[l];
+            F.gridID = L.info.gridID;
+            F.res = L.info.res;
+            for (auto* v : {&F.x, &F.y, &F.z, &F.ux, &F.uy, &F.uz, &F.p}) v->assign(n, 0.f);
+            F.wall.assign(n, 0);
+            F.overlap.assign(n, 0);
+            const lbm::Info& in = L.info;
+            const float scale = (in.res / 1000.f);
+            const float cs = invSqrt3 * (in.res / 1000.f) / in.dtPhys;
+            for (size_t c = 0; c < n; ++c) {
+                // getCompressedIJK (include/cellFunctions.h:51-72)
+                const int sh = shifter[c];
+                const int head = sh >= 0 ? static_cast<int>(c) : static_cast<int>(c) + sh;
+                const int row = shifter[static_cast<size_t>(head)];
+                const int i = rI[row] + (static_cast<int>(c) - head), j = rJ[row], k = rK[row];
+                F.x[c] = i * in.res + in.ox;
+                F.y[c] = j * in.res + in.oy;
+                F.z[c] = k * in.res + in.oz;
+                const int wm = wallMap[c];
+                if (wm == -3) {
+                    F.wall[c] = 1;
+                    continue;
+                }
+                F.overlap[c] = (wm == -2 || (wm >= 0 && (wallData[static_cast<size_t>(wm)] & 1u))) ? 1 : 0;
+                // convertToPhysicalVelocity / convertToPhysicalPressure (include/cellFunctions.h:281-294)
+                F.ux[c] = macro[n + c] * scale / in.dtPhys;
+                F.uy[c] = macro[2 * n + c] * scale / in.dtPhys;
+                F.uz[c] = macro[3 * n + c] * scale / in.dtPhys;
+                F.p[c] = macro[c] * g->c.rho_phys * cs * cs;
+            }
+            total += n;
+        }
+        FILE* fp = std::fopen(filename, "w");
+        if (!fp) throw std::runtime_error(std::string("cannot open VTK file: ") + filename);
+        std::string buf;
+        buf.reserve(1 << 22);
+        char tmp[128];
+        auto flush = [&](bool force) {
+            if (force || buf.size() > (1u << 21)) {
+                if (std::fwrite(buf.data(), 1, buf.size(), fp) != buf.size()) {
+                    std::fclose(fp);
+                    throw std::runtime_error(std::string("failed writing VTK file: ") + filename);
+                }
+                buf.clear();
+            }
+        };
+        auto add = [&](const char* fmt, auto... v) {
+            const int k = std::snprintf(tmp, sizeof(tmp), fmt, v...);
+            buf.append(tmp, static_cast<size_t>(k));
+            flush(false);
+        };
+        // legacy VTK POLYDATA, one vertex per cell (include/exportVTK.h:17-158);
+        // floats with 9 significant digits (max_digits10 of float)
+        add("# vtk DataFile Version 3.0\nLBM snapshot; coordinates in mm; grid count %zu\nASCII\nDATASET POLYDATA\n",
+            lf.size());
+        add("POINTS %zu float\n", total);
+        for (const auto& F : lf)
+            for (size_t c = 0; c < F.x.size(); ++c) add("%.9g %.9g %.9g\n", double(F.x[c]), double(F.y[c]), double(F.z[c]));
+        add("VERTICES %zu %zu\n", total, 2 * total);
+        for (size_t c = 0; c < total; ++c) add("1 %zu\n", c);
+        add("POINT_DATA %zu\nSCALARS wall int 1\nLOOKUP_TABLE default\n", total);
+        for (const auto& F : lf)
+            for (unsigned char w : F.wall) add("%d\n", int(w));
+        add("VECTORS velocity_m_s float\n");
+        for (const auto& F : lf)
+            for (size_t c = 0; c < F.ux.size(); ++c)
+                add("%.9g %.9g %.9g\n", double(F.ux[c]), double(F.uy[c]), double(F.uz[c]));
+        add("SCALARS pressure_Pa float 1\nLOOKUP_TABLE default\n");
+        for (const auto& F : lf)
+            for (float v : F.p) add("%.9g\n", double(v));
+        add("SCALARS grid_id int 1\nLOOKUP_TABLE default\n");
+        for (const auto& F : lf)
+            for (size_t c = 0; c < F.x.size(); ++c) add("%d\n", F.gridID);
+        add("SCALARS grid_resolution_mm float 1\nLOOKUP_TABLE default\n");
+        for (const auto& F : lf)
+            for (size_t c = 0; c < F.x.size(); ++c) add("%.9g\n", double(F.res));
+        add("SCALARS interface_overlap int 1\nLOOKUP_TABLE default\n");
+        for (const auto& F : lf)
+            for (unsigned char o : F.overlap) add("%d\n", int(o));
+        flush(true);
+        if (std::fclose(fp) != 0) throw std::runtime_error(std::string("failed writing VTK file: ") + filename);
+    });
+}
+
 int lbm_flow_report(lbm_grids* g, int plane, float cut, const float* bounds, double* out) {
     if (!g || !out || plane < 0 || plane > 2) return fail(LBM_ERR_INVALID, "lbm_flow_report: bad argument");
     if (g->levels.size() != 1) return fail(LBM_ERR_UNSUPPORTED, "lbm_flow_report: single-level grids only");
@@ -980,7 +1185,7 @@ std::vector<StateRegion> stateRegions(LevelState& L) {
         r.push_back({d.obRhoRef, 2ULL * d.obCount * sizeof(float)});
         r.push_back({d.obRhoCum, 2ULL * d.obCount * sizeof(float)});
     }
-    if (d.wallCount) r.push_back({d.wallForce, 3ULL * d.wallCount * sizeof(float)});
+    if (d.wallCount) r.push_back({d.wallForce, 3ULL * d.wallCount * sizeof(double)});
     for (int q = 0; q < d.rotorCount; ++q)
         if (d.rotor[q].nonzero) r.push_back({d.rotor[q].force, 3ULL * 27 * d.rotor[q].nonzero * sizeof(float)});
     return r;

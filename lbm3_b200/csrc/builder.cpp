@@ -102,7 +102,8 @@ void validateCase(const lbm_case& c) {
         if (kind != LBM_BC_PERIODIC && c.face[f].open_bc_id < 0)
             throw std::runtime_error("open_bc_id must be >= 0");
     }
-    if (c.storage != LBM_STORE_F32 && c.storage != LBM_STORE_F16 && c.storage != LBM_STORE_BF16)
+    if (c.storage != LBM_STORE_F32 && c.storage != LBM_STORE_F16 && c.storage != LBM_STORE_BF16 &&
+        c.storage != LBM_STORE_F64)
         throw std::runtime_error("unknown storage precision");
     if (c.body_count < 0 || c.body_count > LBM_MAX_BODIES)
         throw std::runtime_error("body_count must be in [0, LBM_MAX_BODIES]");

@@ -40,7 +40,9 @@ std::mutex gScratchMutex;
 double* gScratchPtr[kMaxDevices] = {};
 
 // Device address of gEnergyScratch on the current device (set-up on the first
-// call per device).
+// call per device).  The address is cached for the life of the process: a
+// cudaDeviceReset destroys the context that owns it, so a process that resets
+// a device must not call lbm_kinetic_energy_noalloc on that device afterwards.
 cudaError_t scratchPointer(double** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -91,9 +93,9 @@ __global__ void __launch_bounds__(kNoAllocEnergyBlock) energyPartials(DevLevel g
         if (wm != -3 && wm != -2 && !overlap) {
             int nb[8];
             decodeNbr(g, cell, nb, nullptr);
-            float f[27];
+            Real<S> f[27];
             readPre<F, S>(g, nb, f);
-            float dRho, ux, uy, uz;
+            Real<S> dRho, ux, uy, uz;
             macroFromF(f, dRho, ux, uy, uz);
             e = 0.5 * (1.0 + double(dRho)) * (double(ux) * ux + double(uy) * uy + double(uz) * uz);
         }
@@ -134,6 +136,10 @@ cudaError_t kineticEnergyNoAlloc(const DevLevel& g, bool flip, cudaStream_t s, d
         case LBM_STORE_BF16:
             flip ? launchPartials<true, __nv_bfloat16>(g, s, blocks, scratch)
                  : launchPartials<false, __nv_bfloat16>(g, s, blocks, scratch);
+            break;
+        case LBM_STORE_F64:
+            flip ? launchPartials<true, double>(g, s, blocks, scratch)
+                 : launchPartials<false, double>(g, s, blocks, scratch);
             break;
         default:
             flip ? launchPartials<true, float>(g, s, blocks, scratch)

@@ -57,6 +57,14 @@ LBM_HD constexpr float weight(int d) {
                                                                  : 1.f / 216.f;
 }
 
+// Weight in the arithmetic type T (exact fraction rounded once).
+template <class T> LBM_HD constexpr T weightT(int d) {
+    return (cx(d) * cx(d) + cy(d) * cy(d) + cz(d) * cz(d)) == 0 ? T(8) / T(27)
+         : (cx(d) * cx(d) + cy(d) * cy(d) + cz(d) * cz(d)) == 1 ? T(2) / T(27)
+         : (cx(d) * cx(d) + cy(d) * cy(d) + cz(d) * cz(d)) == 2 ? T(1) / T(54)
+                                                                 : T(1) / T(216);
+}
+
 // Esotwist neighbour used by a direction: the cell offset by max(0, -c) on
 // every axis holds the pre-collision value (include/esotwistStreamingFunctions.h:17-74);
 // the post-collision value goes to the cell offset by max(0, +c) (:76-127).

@@ -16,24 +16,30 @@
 
 namespace lbm {
 
-struct MbbcDir {
-    float smf[LBM_MBBC_MAX_UNKNOWN][27];  // S Mfk: weight of population d in equation i
-    float inv[27][LBM_MBBC_MAX_UNKNOWN];  // row of (S Mfu)^-1 producing unknown population d
-    float rhoMfk[27];                     // restoreRho numerator weights
-    float uMfk[3][27];                    // restoreUxUyUz (edges, corners)
-    float uInv[3][3];
-    float uQ[3];
-    float rhoQ, rhoQu[3];
+// T: the arithmetic type of the kernel (the FP64 build holds the same
+// coefficients, the generated float values, widened to double).
+template <class T> struct MbbcDirT {
+    T smf[LBM_MBBC_MAX_UNKNOWN][27];  // S Mfk: weight of population d in equation i
+    T inv[27][LBM_MBBC_MAX_UNKNOWN];  // row of (S Mfu)^-1 producing unknown population d
+    T rhoMfk[27];                     // restoreRho numerator weights
+    T uMfk[3][27];                    // restoreUxUyUz (edges, corners)
+    T uInv[3][3];
+    T uQ[3];
+    T rhoQ, rhoQu[3];
     signed char moment[LBM_MBBC_MAX_UNKNOWN];  // equilibrium moment of equation i
     int nu;                                    // unknown count
     int face;                                  // 1: velocity from the face closed form
     unsigned unknownMask;                      // bit d: population d is unknown
     int nx, ny, nz;                            // outer normal
 };
+using MbbcDir = MbbcDirT<float>;
+
+LBM_HD float mfma(float a, float b, float c) { return fmaf(a, b, c); }
+LBM_HD double mfma(double a, double b, double c) { return fma(a, b, c); }
 
 // Direction-indexed form of one generated table (host, at grid build).
-inline MbbcDir mbbcDirFromTable(const LbmMbbcTable& T) {
-    MbbcDir D{};
+template <class V = float> inline MbbcDirT<V> mbbcDirFromTable(const LbmMbbcTable& T) {
+    MbbcDirT<V> D{};
     D.nu = T.nu;
     D.face = T.face;
     D.nx = T.code / 100 - 5;
@@ -41,7 +47,7 @@ inline MbbcDir mbbcDirFromTable(const LbmMbbcTable& T) {
     D.nz = T.code % 10 - 5;
     for (int i = 0; i < T.nu; ++i) {
         D.moment[i] = T.moment[i];
-        for (int k = 0; k < T.nk; ++k) D.smf[i][T.known[k]] = float(T.smfk[i][k]);
+        for (int k = 0; k < T.nk; ++k) D.smf[i][T.known[k]] = V(T.smfk[i][k]);
     }
     for (int r = 0; r < T.nu; ++r) {
         D.unknownMask |= 1u << T.unknown[r];
@@ -61,8 +67,8 @@ inline MbbcDir mbbcDirFromTable(const LbmMbbcTable& T) {
 }
 
 // Equilibrium value of moment m (the 23 moments in table order).
-LBM_HD float mbbcMomentEq(int m, float rho, float ux, float uy, float uz) {
-    const float t = 1.f / 3.f, n = 1.f / 9.f;
+template <class V> LBM_HD V mbbcMomentEq(int m, V rho, V ux, V uy, V uz) {
+    const V t = V(1) / V(3), n = V(1) / V(9);
     switch (m) {
         case 0: return rho;
         case 1: return rho * ux;
@@ -74,7 +80,7 @@ LBM_HD float mbbcMomentEq(int m, float rho, float ux, float uy, float uz) {
         case 7: return rho * uy * uz;
         case 8: return rho * ux * uz;
         case 9: return rho * ux * uy;
-        case 10: return 0.f;
+        case 10: return V(0);
         case 11: return t * rho * uy + rho * ux * ux * uy;
         case 12: return t * rho * uz + rho * ux * ux * uz;
         case 13: return t * rho * ux + rho * ux * uy * uy;
@@ -91,53 +97,56 @@ LBM_HD float mbbcMomentEq(int m, float rho, float ux, float uy, float uz) {
 }
 
 // applyMBBC: overwrite the unknown populations of f.
-LBM_HD void mbbcApply(const MbbcDir& T, float rho, float ux, float uy, float uz, float (&f)[27]) {
-    float s[LBM_MBBC_MAX_UNKNOWN];
+template <class V>
+LBM_HD void mbbcApply(const MbbcDirT<V>& T, V rho, V ux, V uy, V uz, V (&f)[27]) {
+    V s[LBM_MBBC_MAX_UNKNOWN];
 #pragma unroll
     for (int i = 0; i < LBM_MBBC_MAX_UNKNOWN; ++i) {
-        s[i] = 0.f;
+        s[i] = V(0);
         if (i >= T.nu) continue;
-        float smf = 0.f;
+        V smf = V(0);
 #pragma unroll
-        for (int d = 0; d < 27; ++d) smf = fmaf(T.smf[i][d], f[d], smf);
+        for (int d = 0; d < 27; ++d) smf = mfma(T.smf[i][d], f[d], smf);
         s[i] = mbbcMomentEq(T.moment[i], rho, ux, uy, uz) - smf;
     }
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         if (!(T.unknownMask >> d & 1u)) continue;
-        float v = 0.f;
+        V v = V(0);
 #pragma unroll
-        for (int j = 0; j < LBM_MBBC_MAX_UNKNOWN; ++j) v = fmaf(T.inv[d][j], s[j], v);
+        for (int j = 0; j < LBM_MBBC_MAX_UNKNOWN; ++j) v = mfma(T.inv[d][j], s[j], v);
         f[d] = v;
     }
 }
 
 // restoreRho: density from the known populations and the velocity.
-LBM_HD float mbbcRestoreRho(const MbbcDir& T, float ux, float uy, float uz, const float (&f)[27]) {
-    const float scqu = T.rhoQu[0] * ux + T.rhoQu[1] * uy + T.rhoQu[2] * uz;
-    const float s = T.rhoQ + scqu;
-    float scmf = 0.f;
+template <class V>
+LBM_HD V mbbcRestoreRho(const MbbcDirT<V>& T, V ux, V uy, V uz, const V (&f)[27]) {
+    const V scqu = T.rhoQu[0] * ux + T.rhoQu[1] * uy + T.rhoQu[2] * uz;
+    const V s = T.rhoQ + scqu;
+    V scmf = V(0);
 #pragma unroll
-    for (int d = 0; d < 27; ++d) scmf = fmaf(T.rhoMfk[d], f[d], scmf);
+    for (int d = 0; d < 27; ++d) scmf = mfma(T.rhoMfk[d], f[d], scmf);
     return scmf / s;
 }
 
 // restoreUxUyUz: faces by the closed form (normal velocity from the
 // known-population density, tangential velocity from a vanishing k_nnt),
 // edges and corners from three moment relations free of the unknowns.
-LBM_HD void mbbcRestoreU(const MbbcDir& T, float rho, const float (&f)[27], float& ux, float& uy, float& uz) {
+template <class V>
+LBM_HD void mbbcRestoreU(const MbbcDirT<V>& T, V rho, const V (&f)[27], V& ux, V& uy, V& uz) {
     const int nx = T.nx, ny = T.ny, nz = T.nz;
     if (T.face) {
-        float fZero = 0.f, fPlus = 0.f;
+        V fZero = V(0), fPlus = V(0);
 #pragma unroll
         for (int d = 0; d < 27; ++d) {
             const int cn = cx(d) * nx + cy(d) * ny + cz(d) * nz;
             if (cn == 0) fZero = fZero + f[d];
             else if (cn == 1) fPlus = fPlus + f[d];
         }
-        const float uNormal = (fZero + 2.f * fPlus) / rho - 1.f;
-        const float den = fZero + 2.f * (uNormal + 1.f) * rho * uNormal;
-        float u[3];
+        const V uNormal = (fZero + V(2) * fPlus) / rho - V(1);
+        const V den = fZero + V(2) * (uNormal + V(1)) * rho * uNormal;
+        V u[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const int na = a == 0 ? nx : a == 1 ? ny : nz;
@@ -145,7 +154,7 @@ LBM_HD void mbbcRestoreU(const MbbcDir& T, float rho, const float (&f)[27], floa
                 u[a] = na > 0 ? uNormal : -uNormal;
                 continue;
             }
-            float jZero = 0.f, jPlus = 0.f;
+            V jZero = V(0), jPlus = V(0);
 #pragma unroll
             for (int d = 0; d < 27; ++d) {
                 const int cn = cx(d) * nx + cy(d) * ny + cz(d) * nz;
@@ -154,27 +163,27 @@ LBM_HD void mbbcRestoreU(const MbbcDir& T, float rho, const float (&f)[27], floa
                 if (cn == 0) jZero = ca > 0 ? jZero + f[d] : jZero - f[d];
                 else if (cn == 1) jPlus = ca > 0 ? jPlus + f[d] : jPlus - f[d];
             }
-            u[a] = ((2.f * uNormal + 1.f) * jZero + 4.f * uNormal * jPlus) / den;
+            u[a] = ((V(2) * uNormal + V(1)) * jZero + V(4) * uNormal * jPlus) / den;
         }
         ux = u[0];
         uy = u[1];
         uz = u[2];
         return;
     }
-    float s[3];
+    V s[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-        float acc = 0.f;
+        V acc = V(0);
 #pragma unroll
-        for (int d = 0; d < 27; ++d) acc = fmaf(T.uMfk[i][d], f[d], acc);
+        for (int d = 0; d < 27; ++d) acc = mfma(T.uMfk[i][d], f[d], acc);
         s[i] = acc / rho - T.uQ[i];
     }
-    float u[3];
+    V u[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        float v = 0.f;
+        V v = V(0);
 #pragma unroll
-        for (int j = 0; j < 3; ++j) v = fmaf(T.uInv[a][j], s[j], v);
+        for (int j = 0; j < 3; ++j) v = mfma(T.uInv[a][j], s[j], v);
         u[a] = v;
     }
     ux = u[0];

@@ -27,7 +27,34 @@
 #include <string>
 #include <type_traits>
 
+// One storage type per translation unit (compiled three times), so the
+// kernels of the three population formats build in parallel.
+#ifndef LBM3_STEP_STORAGE
+#define LBM3_STEP_STORAGE 0
+#endif
+#if LBM3_STEP_STORAGE == 1
+#define LBM3_STEP_SUFFIX F16
+#elif LBM3_STEP_STORAGE == 2
+#define LBM3_STEP_SUFFIX BF16
+#elif LBM3_STEP_STORAGE == 3
+#define LBM3_STEP_SUFFIX F64
+#else
+#define LBM3_STEP_SUFFIX F32
+#endif
+#define LBM3_STEP_JOIN2(a, b) a##b
+#define LBM3_STEP_JOIN(a, b) LBM3_STEP_JOIN2(a, b)
+
 namespace lbm {
+
+#if LBM3_STEP_STORAGE == 1
+using StepStore = __half;
+#elif LBM3_STEP_STORAGE == 2
+using StepStore = __nv_bfloat16;
+#elif LBM3_STEP_STORAGE == 3
+using StepStore = double;  // the FP64 build: FP64 storage and arithmetic
+#else
+using StepStore = float;
+#endif
 
 namespace {
 
@@ -42,10 +69,10 @@ constexpr int kBlock = 256;
 // rho (u_rotor - u) times the smoothstep of the fraction, the fractions of
 // all rotors capped at 1 in total.  The collision limiter is scaled by
 // 1 - total fraction.  uxPre.. is the velocity after the local body force.
-__device__ __forceinline__ void rotorForcing(const DevLevel& g, float x, float y, float z, float rho, float uxPre,
-                                             float uyPre, float uzPre, bool trackForce, float& gx, float& gy,
-                                             float& gz, float& lambda) {
-    float cum = 0.f;
+template <class T>
+__device__ __forceinline__ void rotorForcing(const DevLevel& g, float x, float y, float z, T rho, T uxPre, T uyPre,
+                                             T uzPre, bool trackForce, T& gx, T& gy, T& gz, T& lambda) {
+    T cum = T(0);
     for (int r = 0; r < g.rotorCount; ++r) {
         const DevRotor& R = g.rotor[r];
         const float dx = x - R.ox, dy = y - R.oy, dz = z - R.oz;
@@ -88,11 +115,11 @@ __device__ __forceinline__ void rotorForcing(const DevLevel& g, float x, float y
         if (R.axis == 0) { ut[1] = -R.scale * dz; ut[2] = R.scale * dy; }
         else if (R.axis == 1) { ut[0] = R.scale * dz; ut[2] = -R.scale * dx; }
         else { ut[0] = -R.scale * dy; ut[1] = R.scale * dx; }
-        float gxR = rho * (ut[0] - uxPre), gyR = rho * (ut[1] - uyPre), gzR = rho * (ut[2] - uzPre);
-        float ff = frac * frac * (3.f - 2.f * frac);
-        if (cum + ff > 1.f) {
-            ff = 1.f - cum;
-            cum = 1.f;
+        T gxR = rho * (T(ut[0]) - uxPre), gyR = rho * (T(ut[1]) - uyPre), gzR = rho * (T(ut[2]) - uzPre);
+        T ff = T(frac) * T(frac) * (T(3) - T(2) * T(frac));
+        if (cum + ff > T(1)) {
+            ff = T(1) - cum;
+            cum = T(1);
         } else {
             cum += ff;
         }
@@ -104,7 +131,7 @@ __device__ __forceinline__ void rotorForcing(const DevLevel& g, float x, float y
         gz += gzR;
         if (g.trackRotorForce && trackForce) {
             // the force in the rotor frame, binned 3x3x3 per block
-            float fx = gxR, fy = gyR, fz = gzR;
+            T fx = gxR, fy = gyR, fz = gzR;
             if (R.axis == 0) { fy = R.c * gyR + R.s * gzR; fz = -R.s * gyR + R.c * gzR; }
             else if (R.axis == 1) { fx = R.c * gxR - R.s * gzR; fz = R.s * gxR + R.c * gzR; }
             else { fx = R.c * gxR + R.s * gyR; fy = -R.s * gxR + R.c * gyR; }
@@ -113,26 +140,26 @@ __device__ __forceinline__ void rotorForcing(const DevLevel& g, float x, float y
             const int kF = max(0, min(2, static_cast<int>(0.75f * ((kk % 4) + zw))));
             const int bin = map * 27 + kF * 9 + jF * 3 + iF;
             const int nb = 27 * R.nonzero;
-            atomicAdd(R.force + bin, fx);
-            atomicAdd(R.force + nb + bin, fy);
-            atomicAdd(R.force + 2 * nb + bin, fz);
+            atomicAdd(R.force + bin, static_cast<float>(fx));
+            atomicAdd(R.force + nb + bin, static_cast<float>(fy));
+            atomicAdd(R.force + 2 * nb + bin, static_cast<float>(fz));
         }
-        if (cum >= 1.f) break;
+        if (cum >= T(1)) break;
     }
-    if (cum > 0.f) lambda *= 1.f - fminf(fmaxf(cum, 0.f), 1.f);
+    if (cum > T(0)) lambda *= T(1) - (cum < T(0) ? T(0) : cum > T(1) ? T(1) : cum);
 }
 
 // Rotor forcing of one cell before its collision (needs the cell's indices).
-template <bool F, class S>
-__device__ __forceinline__ void cellRotorForcing(const DevLevel& g, const int (&ijk)[3], int wm, const float (&f)[27],
-                                                 float& gx, float& gy, float& gz, float& lambda) {
-    float dRho, ux, uy, uz;
+template <bool F, class S, class T>
+__device__ __forceinline__ void cellRotorForcing(const DevLevel& g, const int (&ijk)[3], int wm, const T (&f)[27],
+                                                 T& gx, T& gy, T& gz, T& lambda) {
+    T dRho, ux, uy, uz;
     macroFromF(f, dRho, ux, uy, uz);
-    const float rho = dRho + 1.f;
-    const float rhoInv = 1.f / rho;
-    const float uxPre = (ux * rho + gx) * rhoInv;
-    const float uyPre = (uy * rho + gy) * rhoInv;
-    const float uzPre = (uz * rho + gz) * rhoInv;
+    const T rho = dRho + T(1);
+    const T rhoInv = T(1) / rho;
+    const T uxPre = (ux * rho + gx) * rhoInv;
+    const T uyPre = (uy * rho + gy) * rhoInv;
+    const T uzPre = (uz * rho + gz) * rhoInv;
     bool track = wm != -2;
     if (wm >= 0 && (__ldg(g.wallData + wm) & 1u)) track = false;
     const float x = ijk[0] * g.res + g.ox, y = ijk[1] * g.res + g.oy, z = ijk[2] * g.res + g.oz;
@@ -147,11 +174,12 @@ __global__ void __launch_bounds__(kBlock) collideStream(DevLevel g) {
     if (wm == -3) return;  // the cell itself is a wall
     int nb[8], ijk[3];
     decodeNbr(g, cell, nb, g.rotorCount > 0 ? ijk : nullptr);
-    float f[27];
+    using T = Real<S>;
+    T f[27];
     readPre<F, S>(g, nb, f);
-    float gx = g.gx, gy = g.gy, gz = g.gz, lambda = g.coll.lambda;
+    T gx = g.gx, gy = g.gy, gz = g.gz, lambda = collConsts<T>(g).lambda;
     if (g.rotorCount > 0) cellRotorForcing<F, S>(g, ijk, wm, f, gx, gy, gz, lambda);
-    collideCumulant(f, g.coll, lambda, gx, gy, gz);
+    collideCumulantT(f, collConsts<T>(g), lambda, gx, gy, gz);
     writePost<F, S>(g, nb, f);
 }
 
@@ -440,14 +468,15 @@ __global__ void __launch_bounds__(kTile, LBM3_TMA_MIN_BLOCKS) collideBulkTma(Dev
                 int nb[8];
                 segNbr(g, d[k], t, nb);
                 const unsigned char* st = smem + k * stageBytes<S>();
-                float f[27];
+                Real<S> f[27];
 #pragma unroll
                 for (int q = 0; q < 27; ++q) {
                     const int off = static_cast<int>((runStart<F>(g, d[k], q) * (long long)sizeof(S)) & 15) /
                                     int(sizeof(S));
                     f[q] = Store<S>::ld(reinterpret_cast<const S*>(st + q * runBytes<S>()) + off + t);
                 }
-                collideCumulant(f, g.coll, g.coll.lambda, g.gx, g.gy, g.gz);
+                collideCumulantT(f, collConsts<Real<S>>(g), collConsts<Real<S>>(g).lambda, Real<S>(g.gx),
+                                 Real<S>(g.gy), Real<S>(g.gz));
                 writePost<F, S>(g, nb, f);
             }
         }
@@ -476,24 +505,25 @@ __device__ __forceinline__ void collideSpecialCell(const DevLevel& g, int cell) 
     const int wm = __ldg(g.wallMap + cell);
     int nb[8], ijk[3];
     decodeNbr(g, cell, nb, kRotors ? ijk : nullptr);
-    float f[27];
+    using T = Real<S>;
+    T f[27];
     readPre<F, S>(g, nb, f);
-    float gx = g.gx, gy = g.gy, gz = g.gz, lambda = g.coll.lambda;
+    T gx = g.gx, gy = g.gy, gz = g.gz, lambda = collConsts<T>(g).lambda;
     if (kRotors) cellRotorForcing<F, S>(g, ijk, wm, f, gx, gy, gz, lambda);
-    collideCumulant(f, g.coll, lambda, gx, gy, gz);
+    collideCumulantT(f, collConsts<T>(g), lambda, gx, gy, gz);
     if (wm < 0) {
         writePost<F, S>(g, nb, f);
         return;
     }
     const unsigned wallData = __ldg(g.wallData + wm);
     const int nw = g.wallCount;
-    const float uwx = __ldg(g.wallVel + wm), uwy = __ldg(g.wallVel + nw + wm), uwz = __ldg(g.wallVel + 2 * nw + wm);
-    float dRho, ux, uy, uz;
+    const T uwx = __ldg(g.wallVel + wm), uwy = __ldg(g.wallVel + nw + wm), uwz = __ldg(g.wallVel + 2 * nw + wm);
+    T dRho, ux, uy, uz;
     macroFromF(f, dRho, ux, uy, uz);
-    float out[27];
+    T out[27];
 #pragma unroll
     for (int d = 0; d < 27; ++d) out[d] = f[d];
-    float fx = 0.f, fy = 0.f, fz = 0.f;
+    T fx = T(0), fy = T(0), fz = T(0);
     int link = 0;
     unsigned code = 0u;
     const S* base = static_cast<const S*>(g.f);
@@ -501,23 +531,24 @@ __device__ __forceinline__ void collideSpecialCell(const DevLevel& g, int cell) 
     for (int d = 1; d < 27; ++d) {
         if (!((wallData >> d) & 1u)) continue;
         const int id = inv(d);
-        const float eu = float(cx(id)) * uwx + float(cy(id)) * uwy + float(cz(id)) * uwz;
-        const float wallTerm = 6.f * weight(id) * (1.f + dRho) * eu;
-        float gamma = 0.5f;
+        const T eu = T(cx(id)) * uwx + T(cy(id)) * uwy + T(cz(id)) * uwz;
+        const T wallTerm = T(6) * weightT<T>(id) * (T(1) + dRho) * eu;
+        T gamma = T(0.5);
         if (g.useIBB) {
             if ((link & 3) == 0) code = __ldg(g.linkLength + (link >> 2) * nw + wm);
             const unsigned c8 = (code >> (8 * (link & 3))) & 255u;
-            gamma = fminf(fmaxf(static_cast<float>(c8) / 254.f, 0.01f), 1.f);
+            const T q = static_cast<T>(c8) / T(254);
+            gamma = q < T(0.01f) ? T(0.01f) : q > T(1) ? T(1) : q;
             ++link;
         }
         // pre-collision value of direction d, still unchanged in memory
-        const float fPre = Store<S>::ld(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
-        const float invDen = 1.f / (1.f + gamma);
-        const float r = ((1.f - gamma) * invDen) * fPre + (gamma * invDen) * f[id] + (gamma * invDen) * f[d] +
-                        invDen * wallTerm;
-        fx += -f[d] * (float(cx(d)) - uwx) + r * (float(cx(id)) - uwx);
-        fy += -f[d] * (float(cy(d)) - uwy) + r * (float(cy(id)) - uwy);
-        fz += -f[d] * (float(cz(d)) - uwz) + r * (float(cz(id)) - uwz);
+        const T fPre = Store<S>::ld(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
+        const T invDen = T(1) / (T(1) + gamma);
+        const T r = ((T(1) - gamma) * invDen) * fPre + (gamma * invDen) * f[id] + (gamma * invDen) * f[d] +
+                    invDen * wallTerm;
+        fx += -f[d] * (T(cx(d)) - uwx) + r * (T(cx(id)) - uwx);
+        fy += -f[d] * (T(cy(d)) - uwy) + r * (T(cy(id)) - uwy);
+        fz += -f[d] * (T(cz(d)) - uwz) + r * (T(cz(id)) - uwz);
         out[d] = r;
     }
     // writes: a linked direction goes to the next pre-collision slot of its
@@ -530,9 +561,9 @@ __device__ __forceinline__ void collideSpecialCell(const DevLevel& g, int cell) 
         Store<S>::st(wbase + (long long)slot * g.stride + nb[postNbr(d)], out[d]);
     }
     if (g.trackWallForce && !(wallData & 1u)) {
-        g.wallForce[wm] += fx;
-        g.wallForce[nw + wm] += fy;
-        g.wallForce[2 * nw + wm] += fz;
+        g.wallForce[wm] += double(fx);
+        g.wallForce[nw + wm] += double(fy);
+        g.wallForce[2 * nw + wm] += double(fz);
     }
 }
 
@@ -583,20 +614,22 @@ __global__ void __launch_bounds__(kTile, LBM3_PREFETCH_MIN_BLOCKS) collidePrefet
     loadDesc(g, fetch() - nSpecial, dNext, lNext);
     int nb[8];
     segNbr(g, dCur, t, nb);
-    float fn[27];
+    using T = Real<S>;
+    const CollisionConstsT<T>& P = collConsts<T>(g);
+    T fn[27];
     if (t < lCur) readPre<F, S>(g, nb, fn);
     while (lCur > 0) {  // CTA-uniform: lengths come from the shared descriptors
         int4 dAfter;
         int lAfter;
         loadDesc(g, fetch() - nSpecial, dAfter, lAfter);
-        float f[27];
+        T f[27];
 #pragma unroll
         for (int q = 0; q < 27; ++q) f[q] = fn[q];
         int nbn[8];
         segNbr(g, dNext, t, nbn);
         if (t < lNext) readPre<F, S>(g, nbn, fn);
         if (t < lCur) {
-            collideCumulant(f, g.coll, g.coll.lambda, g.gx, g.gy, g.gz);
+            collideCumulantT(f, P, P.lambda, T(g.gx), T(g.gy), T(g.gz));
             writePost<F, S>(g, nb, f);
         }
 #pragma unroll
@@ -604,6 +637,128 @@ __global__ void __launch_bounds__(kTile, LBM3_PREFETCH_MIN_BLOCKS) collidePrefet
         lCur = lNext;
         dNext = dAfter;
         lNext = lAfter;
+    }
+    if (t == 0) {
+        __threadfence();
+        if (atomicAdd(g.work + 1, 1) == int(gridDim.x) - 1) {
+            g.work[0] = 0;
+            g.work[1] = 0;
+            __threadfence();
+        }
+    }
+}
+
+// ---- paired bulk collide-stream ---------------------------------------------
+// collidePair (default): CTAs of kHalf threads; thread t collides cells t and
+// t + kHalf of a 128-cell segment as one Pair, so every add/mul/fma of the
+// cumulant transform is one packed FP32x2 instruction for both cells (the
+// kernel is bounded by instruction issue, not by the FMA pipe), and the
+// second cell's 27 loads and 27 stores reuse the first cell's address with
+// an immediate offset.  Population offsets are 32-bit element indices
+// (27 x stride < 2^31; larger grids take collidePrefetch).  The CTA fetches
+// its next work item while the current tile's loads are in flight; with
+// LBM3_PAIR_PREFETCH the next tile's populations are also loaded into
+// registers during the current tile's collision.
+constexpr int kHalf = kTile / 2;
+
+#ifndef LBM3_PAIR_MIN_BLOCKS
+#define LBM3_PAIR_MIN_BLOCKS 8
+#endif
+#ifndef LBM3_PAIR_PREFETCH
+#define LBM3_PAIR_PREFETCH 0
+#endif
+
+// Element offset of direction q's pre- (Pre) or post-collision run for the
+// tile with descriptor d: slot x stride + the neighbour row start.
+template <bool F, bool Pre>
+__device__ __forceinline__ int runOffset32(const DevLevel& g, const int4& d, int q) {
+    const int k = Pre ? preNbr(q) : postNbr(q);
+    const int b = (k >> 1) == 0 ? d.x : (k >> 1) == 1 ? d.y : (k >> 1) == 2 ? d.z : d.w;
+    const int slot = Pre ? preSlot<F>(q) : postSlot<F>(q);
+    return slot * static_cast<int>(g.stride) + b + (k & 1);
+}
+
+// Load the 27 pre-collision values of lanes t and t + kHalf.  A partial tile
+// clamps lane A to the last cell (its store is masked) and skips lane B.
+template <bool F, class S, bool kFull>
+__device__ __forceinline__ void loadPair(const DevLevel& g, const int4& d, int t, int len, Pair (&f)[27]) {
+    const S* base = static_cast<const S*>(g.f);
+    const int tA = kFull ? t : min(t, len - 1);
+    const bool okB = kFull || t + kHalf < len;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const S* p = base + (runOffset32<F, true>(g, d, q) + tA);
+        const float a = Store<S>::ld(p);
+        const float b = okB ? Store<S>::ld(p + kHalf) : 0.f;
+        f[q] = mkPair(a, b);
+    }
+}
+
+template <bool F, class S>
+__device__ __forceinline__ void storePair(const DevLevel& g, const int4& d, int t, int len, const Pair (&f)[27]) {
+    S* base = static_cast<S*>(g.f);
+    const bool okA = t < len, okB = t + kHalf < len;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        S* p = base + (runOffset32<F, false>(g, d, q) + t);
+        if (okA) Store<S>::st(p, f[q].v.x);
+        if (okB) Store<S>::st(p + kHalf, f[q].v.y);
+    }
+}
+
+template <bool F, class S>
+__device__ __forceinline__ void loadTilePair(const DevLevel& g, const int4& d, int t, int len, Pair (&f)[27]) {
+    if (len == kTile) loadPair<F, S, true>(g, d, t, len, f);
+    else if (len > 0) loadPair<F, S, false>(g, d, t, len, f);
+}
+
+template <bool F, class S>
+__global__ void __launch_bounds__(kHalf, LBM3_PAIR_MIN_BLOCKS) collidePair(DevLevel g) {
+    __shared__ int slot[2];
+    const int nSpecial = (g.specialCount + kTile - 1) / kTile;
+    const int t = threadIdx.x;
+    int parity = 0;
+    auto fetch = [&]() {
+        if (t == 0) slot[parity] = atomicAdd(g.work, 1);
+        __syncthreads();
+        const int v = slot[parity];
+        parity ^= 1;
+        return v;
+    };
+    int item = fetch();
+    while (item < nSpecial) {
+        const int q = item * kTile + t;
+        if (q < g.specialCount) collideSpecialCell<F, S>(g, __ldg(g.special + q));
+        if (q + kHalf < g.specialCount) collideSpecialCell<F, S>(g, __ldg(g.special + q + kHalf));
+        item = fetch();
+    }
+    int4 dCur;
+    int lCur;
+    loadDesc(g, item - nSpecial, dCur, lCur);
+    int next = fetch();
+#if LBM3_PAIR_PREFETCH
+    Pair fn[27];
+    loadTilePair<F, S>(g, dCur, t, lCur, fn);
+#endif
+    while (lCur > 0) {  // CTA-uniform: lengths come from the shared descriptors
+        Pair f[27];
+#if LBM3_PAIR_PREFETCH
+#pragma unroll
+        for (int q = 0; q < 27; ++q) f[q] = fn[q];
+#else
+        loadTilePair<F, S>(g, dCur, t, lCur, f);
+#endif
+        int4 dNext;
+        int lNext;
+        loadDesc(g, next - nSpecial, dNext, lNext);
+        next = fetch();  // the atomic's latency overlaps the loads in flight
+#if LBM3_PAIR_PREFETCH
+        loadTilePair<F, S>(g, dNext, t, lNext, fn);
+#endif
+        collideCumulantT(f, g.coll, g.coll.lambda, g.gx, g.gy, g.gz);
+        storePair<F, S>(g, dCur, t, lCur, f);
+        dCur = dNext;
+        lCur = lNext;
     }
     if (t == 0) {
         __threadfence();
@@ -734,7 +889,7 @@ __global__ void __launch_bounds__(kBlock) periodicCopy(DevLevel g) {
     const int cell = __ldg(g.perIndex + idx);
     const int src = __ldg(g.perSource + idx);
     int nb[8];
-    float f[27];
+    Real<S> f[27];
     decodeNbr(g, src, nb, nullptr);
     readPre<F, S>(g, nb, f);
     decodeNbr(g, cell, nb, nullptr);
@@ -744,13 +899,14 @@ __global__ void __launch_bounds__(kBlock) periodicCopy(DevLevel g) {
 // Characteristic (non-reflective) normal velocity of a face cell: the
 // outgoing Riemann invariant of the streamed state against the reference
 // values (include/updateGrid.h:268-308).
-__device__ __forceinline__ float nonReflectiveUNormal(float uTarget, float dRhoZ, float dRhoRef) {
-    const float cs = 0.57735026918962576f;  // 1/sqrt(3)
-    const float rhoRef = dRhoRef + 1.f;
-    const float rhoTerm = (dRhoZ - dRhoRef) / rhoRef;
-    const float numerator = 2.f * (uTarget + cs * rhoTerm);
-    const float root = (1.f + cs - uTarget) * (1.f + cs - uTarget) + 4.f * (uTarget + cs * rhoTerm);
-    const float denominator = 1.f + cs - uTarget + sqrtf(root);
+template <class V>
+__device__ __forceinline__ V nonReflectiveUNormal(V uTarget, V dRhoZ, V dRhoRef) {
+    const V cs = V(0.57735026918962576);  // 1/sqrt(3)
+    const V rhoRef = dRhoRef + V(1);
+    const V rhoTerm = (dRhoZ - dRhoRef) / rhoRef;
+    const V numerator = V(2) * (uTarget + cs * rhoTerm);
+    const V root = (V(1) + cs - uTarget) * (V(1) + cs - uTarget) + V(4) * (uTarget + cs * rhoTerm);
+    const V denominator = V(1) + cs - uTarget + sqrt(root);
     return numerator / denominator;
 }
 
@@ -765,14 +921,18 @@ __device__ __forceinline__ float nonReflectiveUNormal(float uTarget, float dRhoZ
 // cell's own pre-collision slots.  All open-boundary IDs go in one launch:
 // their cells are disjoint and a cell touches only its own 27 slots, so the
 // reference's loop over IDs gives the same result in any order.
+#ifndef LBM3_OPEN_MIN_BLOCKS
+#define LBM3_OPEN_MIN_BLOCKS 8
+#endif
 template <bool F, class S>
-__global__ void __launch_bounds__(kOpenChunk) openBoundary(DevLevel g, int iterationsFinished) {
-    __shared__ MbbcDir T;
+__global__ void __launch_bounds__(kOpenChunk, LBM3_OPEN_MIN_BLOCKS) openBoundary(DevLevel g, int iterationsFinished) {
+    using V = Real<S>;
+    __shared__ MbbcDirT<V> T;
     const int4 chunk = __ldg(g.obChunk + blockIdx.x);  // {first, count, normal row, unknown mask}
     {
-        const int* src = reinterpret_cast<const int*>(g.obTables + chunk.z);
+        const int* src = reinterpret_cast<const int*>(static_cast<const MbbcDirT<V>*>(g.obTables) + chunk.z);
         int* dst = reinterpret_cast<int*>(&T);
-        for (int q = threadIdx.x; q < int(sizeof(MbbcDir) / 4); q += kOpenChunk) dst[q] = __ldg(src + q);
+        for (int q = threadIdx.x; q < int(sizeof(MbbcDirT<V>) / 4); q += kOpenChunk) dst[q] = __ldg(src + q);
     }
     // everything that does not need the tables is loaded before the barrier,
     // so the population gathers overlap the table staging
@@ -780,6 +940,11 @@ __global__ void __launch_bounds__(kOpenChunk) openBoundary(DevLevel g, int itera
     const int idx = chunk.x + (active ? int(threadIdx.x) : 0);
     const int info = __ldg(g.obInfo + idx);
     const int4 rows = __ldg(g.obNbr + idx);
+    // per-cell records: one round of independent loads with the gathers
+    const float dRhoRef = g.obRhoRef[idx];
+    const float uNormalRef = g.obUnRef[idx];
+    const float4 target = __ldg(g.obTarget + idx);
+    const float beta = __ldg(g.obBeta + idx);
     const int nx = ((info >> 3) & 3) - 1, ny = ((info >> 5) & 3) - 1, nz = ((info >> 7) & 3) - 1;
     const unsigned unknown = static_cast<unsigned>(chunk.w);
     const int n = g.cellCount;
@@ -793,58 +958,54 @@ __global__ void __launch_bounds__(kOpenChunk) openBoundary(DevLevel g, int itera
     nb[6] = rows.w;
     nb[7] = rows.w + 1 < n ? rows.w + 1 : 0;
     S* base = static_cast<S*>(g.f);
-    float f[27];
+    V f[27];
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
-        f[d] = 0.f;
+        f[d] = V(0);
         if (active && !(unknown >> d & 1u))
             f[d] = Store<S>::ld(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
     }
     __syncthreads();
     if (!active) return;
-    float dRhoZ = 0.f;
+    V dRhoZ = V(0);
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         if (unknown >> d & 1u) continue;
         if (nx * cx(d) + ny * cy(d) + nz * cz(d) == 0) dRhoZ += f[d];
-        else dRhoZ += 2.f * f[d];
-        f[d] += weight(d);  // the closure is ill-conditioned on shifted populations
+        else dRhoZ += V(2) * f[d];
+        f[d] += weightT<V>(d);  // the closure is ill-conditioned on shifted populations
     }
-    const float dRhoRef = g.obRhoRef[idx];
-    const float uNormalRef = g.obUnRef[idx];
-    const float4 target = __ldg(g.obTarget + idx);
-    float dRho = target.x, ux = target.y, uy = target.z, uz = target.w;
+    V dRho = target.x, ux = target.y, uy = target.z, uz = target.w;
     const bool nonReflective = info & 4;
     if ((info & 3) == 2) {  // pressure: density given, velocity restored
         if (nonReflective) {
-            const float uNormal = nonReflectiveUNormal(uNormalRef, dRhoZ, dRho);
-            dRho = (dRhoZ - uNormal) / (1.f + uNormal);
+            const V uNormal = nonReflectiveUNormal<V>(uNormalRef, dRhoZ, dRho);
+            dRho = (dRhoZ - uNormal) / (V(1) + uNormal);
         }
-        mbbcRestoreU(T, dRho + 1.f, f, ux, uy, uz);
+        mbbcRestoreU(T, dRho + V(1), f, ux, uy, uz);
     } else if ((info & 3) == 1) {  // velocity: velocity given, density restored
         if (nonReflective) {
-            float uTarget = 0.f;
+            V uTarget = V(0);
             if (nx != 0) uTarget = nx > 0 ? ux : -ux;
             if (ny != 0) uTarget = ny > 0 ? uy : -uy;
             if (nz != 0) uTarget = nz > 0 ? uz : -uz;
-            const float uNormal = nonReflectiveUNormal(uTarget, dRhoZ, dRhoRef);
+            const V uNormal = nonReflectiveUNormal<V>(uTarget, dRhoZ, dRhoRef);
             if (nx != 0) ux = nx > 0 ? uNormal : -uNormal;
             if (ny != 0) uy = ny > 0 ? uNormal : -uNormal;
             if (nz != 0) uz = nz > 0 ? uNormal : -uNormal;
         }
-        dRho = mbbcRestoreRho(T, ux, uy, uz, f) - 1.f;
+        dRho = mbbcRestoreRho(T, ux, uy, uz, f) - V(1);
     }
-    mbbcApply(T, dRho + 1.f, ux, uy, uz, f);
+    mbbcApply(T, dRho + V(1), ux, uy, uz, f);
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         if (!(unknown >> d & 1u)) continue;
-        Store<S>::st(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)], f[d] - weight(d));
+        Store<S>::st(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)], f[d] - weightT<V>(d));
     }
     // reference values: exponential average whose weight decays with the
     // iteration count; below 1e-5 the weight is tripled and the update runs
     // every 3^k iterations instead (include/updateGrid.h:325-347)
-    const float uNormal = (float)nx * ux + (float)ny * uy + (float)nz * uz;
-    const float beta = __ldg(g.obBeta + idx);
+    const float uNormal = float(V(nx) * ux + V(ny) * uy + V(nz) * uz);
     float alpha = beta / ((float)iterationsFinished + beta + 10.f);
     int updateEvery = 1;
     while (alpha < 1.e-5f) {
@@ -852,11 +1013,11 @@ __global__ void __launch_bounds__(kOpenChunk) openBoundary(DevLevel g, int itera
         updateEvery *= 3;
     }
     if (iterationsFinished % updateEvery == 0) {
-        g.obRhoRef[idx] = fmaf(alpha, dRho - dRhoRef, dRhoRef);
+        g.obRhoRef[idx] = fmaf(alpha, float(dRho) - dRhoRef, dRhoRef);
         g.obUnRef[idx] = fmaf(alpha, uNormal - uNormalRef, uNormalRef);
     }
     if (g.trackOpen && (info & 512)) {
-        g.obRhoCum[idx] += dRho;
+        g.obRhoCum[idx] += float(dRho);
         g.obUnCum[idx] += uNormal;
     }
 }
@@ -871,12 +1032,13 @@ __global__ void __launch_bounds__(kBlock) openBoundaryInit(DevLevel g) {
     const int nx = ((info >> 3) & 3) - 1, ny = ((info >> 5) & 3) - 1, nz = ((info >> 7) & 3) - 1;
     int nb[8];
     decodeNbr(g, cell, nb, nullptr);
-    float f[27];
+    using V = Real<S>;
+    V f[27];
     readPre<F, S>(g, nb, f);
-    float dRho, ux, uy, uz;
+    V dRho, ux, uy, uz;
     macroFromF(f, dRho, ux, uy, uz);
-    g.obRhoRef[idx] = dRho;
-    g.obUnRef[idx] = (float)nx * ux + (float)ny * uy + (float)nz * uz;
+    g.obRhoRef[idx] = float(dRho);
+    g.obUnRef[idx] = float(V(nx) * ux + V(ny) * uy + V(nz) * uz);
 }
 
 // getFeq (include/cellFunctions.h:125-148) with rounding-exact intrinsics so
@@ -898,6 +1060,21 @@ __device__ __forceinline__ void feqExact(float dRho, float ux, float uy, float u
     }
 }
 
+// getFeq in double for the FP64 build (the same expression, FP64 throughout).
+__device__ __forceinline__ void feqExact(double dRho, double ux, double uy, double uz, double (&feq)[27]) {
+    const double ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const double X = cx(q), Y = cy(q), Z = cz(q);
+        const double dx = 3.0 * X * ux + (4.5 * X * X - 1.5) * ux2;
+        const double dy = 3.0 * Y * uy + (4.5 * Y * Y - 1.5) * uy2;
+        const double dz = 3.0 * Z * uz + (4.5 * Z * Z - 1.5) * uz2;
+        const double xy = dx + dy + dx * dy;
+        const double corr = xy + dz + xy * dz;
+        feq[q] = weightT<double>(q) * (dRho + corr + dRho * corr);
+    }
+}
+
 template <bool F, class S>
 __global__ void __launch_bounds__(kBlock) initFeq(DevLevel g, const float4* macro, float4 uniform) {
     const int cell = blockIdx.x * kBlock + threadIdx.x;
@@ -905,8 +1082,9 @@ __global__ void __launch_bounds__(kBlock) initFeq(DevLevel g, const float4* macr
     const float4 m = macro ? macro[cell] : uniform;
     int nb[8];
     decodeNbr(g, cell, nb, nullptr);
-    float f[27];
-    feqExact(m.x, m.y, m.z, m.w, f);
+    using V = Real<S>;
+    V f[27];
+    feqExact(V(m.x), V(m.y), V(m.z), V(m.w), f);
     writePre<F, S>(g, nb, f);
 }
 
@@ -928,9 +1106,9 @@ __global__ void __launch_bounds__(kBlock) kineticEnergy(DevLevel g, double* out)
         if (wm != -3 && wm != -2 && !overlap) {
             int nb[8];
             decodeNbr(g, cell, nb, nullptr);
-            float f[27];
+            Real<S> f[27];
             readPre<F, S>(g, nb, f);
-            float dRho, ux, uy, uz;
+            Real<S> dRho, ux, uy, uz;
             macroFromF(f, dRho, ux, uy, uz);
             e = 0.5 * (1.0 + double(dRho)) *
                 (double(ux) * ux + double(uy) * uy + double(uz) * uz);
@@ -947,21 +1125,71 @@ __global__ void __launch_bounds__(kBlock) kineticEnergy(DevLevel g, double* out)
     }
 }
 
+// FP64 global sums over the fluid cells (walls, periodic ghosts and
+// interface duplicates excluded, as in the kinetic energy): out[0] sum of rho,
+// out[1] sum of dRho, out[2..4] sum of rho u (momentum), out[5] cell count.
+// The populations are read in the kernel's arithmetic type and each cell's
+// contribution is formed in FP64.
+template <bool F, class S>
+__global__ void __launch_bounds__(kBlock) globalSums(DevLevel g, double* out) {
+    const int cell = blockIdx.x * kBlock + threadIdx.x;
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    if (cell < g.cellCount) {
+        const int wm = __ldg(g.wallMap + cell);
+        const bool overlap = wm >= 0 && (__ldg(g.wallData + wm) & 1u);
+        if (wm != -3 && wm != -2 && !overlap) {
+            int nb[8];
+            decodeNbr(g, cell, nb, nullptr);
+            Real<S> f[27];
+            readPre<F, S>(g, nb, f);
+            double dRho = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+#pragma unroll
+            for (int d = 0; d < 27; ++d) {
+                const double fd = f[d];
+                dRho += fd;
+                mx += cx(d) * fd;
+                my += cy(d) * fd;
+                mz += cz(d) * fd;
+            }
+            v[0] = 1.0 + dRho;
+            v[1] = dRho;
+            v[2] = mx;
+            v[3] = my;
+            v[4] = mz;
+            v[5] = 1.0;
+        }
+    }
+    __shared__ double part[6][kBlock / 32];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        double a = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+        if ((threadIdx.x & 31) == 0) part[q][threadIdx.x >> 5] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double a = 0.0;
+        for (int k = 0; k < kBlock / 32; ++k) a += part[threadIdx.x][k];
+        atomicAdd(out + threadIdx.x, a);
+    }
+}
+
 template <bool F, class S>
 __global__ void __launch_bounds__(kBlock) macroFields(DevLevel g, float* out) {
     const int cell = blockIdx.x * kBlock + threadIdx.x;
     if (cell >= g.cellCount) return;
     int nb[8];
     decodeNbr(g, cell, nb, nullptr);
-    float f[27];
+    Real<S> f[27];
     readPre<F, S>(g, nb, f);
-    float dRho, ux, uy, uz;
+    Real<S> dRho, ux, uy, uz;
     macroFromF(f, dRho, ux, uy, uz);
     const long long n = g.cellCount;
-    out[cell] = dRho;
-    out[n + cell] = ux;
-    out[2 * n + cell] = uy;
-    out[3 * n + cell] = uz;
+    out[cell] = float(dRho);
+    out[n + cell] = float(ux);
+    out[2 * n + cell] = float(uy);
+    out[3 * n + cell] = float(uz);
 }
 
 template <bool F, class S>
@@ -998,42 +1226,44 @@ __global__ void __launch_bounds__(kBlock) collideBatch(float* f, int n, Collisio
 
 inline unsigned blocksFor(long long n) { return static_cast<unsigned>((n + kBlock - 1) / kBlock); }
 
-// Dispatch on (flipper, storage type).
+// Dispatch on the flipper; this translation unit holds the kernels of one
+// storage type (LBM3_STEP_STORAGE), step_dispatch.cu picks the unit.
 template <template <bool, class> class K, class... A>
 void dispatch(const DevLevel& g, bool flip, A&&... args) {
-    switch (g.storage) {
-        case LBM_STORE_F16:
-            flip ? K<true, __half>::run(g, args...) : K<false, __half>::run(g, args...);
-            break;
-        case LBM_STORE_BF16:
-            flip ? K<true, __nv_bfloat16>::run(g, args...) : K<false, __nv_bfloat16>::run(g, args...);
-            break;
-        default:
-            flip ? K<true, float>::run(g, args...) : K<false, float>::run(g, args...);
-    }
+    flip ? K<true, StepStore>::run(g, args...) : K<false, StepStore>::run(g, args...);
 }
 
-// Persistent grid size: SMs x resident CTAs of the kernel.
-template <class K> int persistentGrid(K kernel, int smem) {
-    int dev = 0, sms = 0, perSm = 0;
+// Persistent grid size of a kernel on the current device: SMs x resident
+// CTAs.  Cached per device and kernel (devices may differ in SM count).
+template <class K> int persistentGrid(K kernel, int block, int smem) {
+    constexpr int kMaxDevices = 64;
+    static int cache[kMaxDevices] = {};
+    int dev = 0;
     cudaGetDevice(&dev);
+    if (dev >= 0 && dev < kMaxDevices && cache[dev] > 0) return cache[dev];
+    int sms = 0, perSm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (smem > 0) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, kTile, smem);
-    return sms * (perSm > 0 ? perSm : 1);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, block, smem);
+    const int grid = (sms > 0 ? sms : 1) * (perSm > 0 ? perSm : 1);
+    if (dev >= 0 && dev < kMaxDevices) cache[dev] = grid;
+    return grid;
 }
 
-enum class CollideVariant { Tma, Prefetch, Simple };
+enum class CollideVariant { Tma, Prefetch, Simple, Pair };
 
 CollideVariant collideVariant() {
     static int v = -1;
     if (v < 0) {
         const char* e = std::getenv("LBM3_COLLIDE_KERNEL");
         const std::string s = e ? e : "";
-        v = s == "simple" ? 2 : s == "tma" ? 0 : 1;
+        v = s == "simple" ? 2 : s == "tma" ? 0 : s == "prefetch" ? 1 : 3;
     }
     return static_cast<CollideVariant>(v);
 }
+
+// The paired kernel indexes populations with 32-bit element offsets.
+bool pairFits(const DevLevel& g) { return 27LL * g.stride + kTile < (1LL << 31); }
 
 template <bool F, class S> struct RunCollide {
     static void run(const DevLevel& g, cudaStream_t s) {
@@ -1044,21 +1274,27 @@ template <bool F, class S> struct RunCollide {
         }
         if (g.segCount > 0) {
             if (v == CollideVariant::Tma) {
-                static int grid = 0;
-                if (grid == 0) {
-                    grid = persistentGrid(collideBulkTma<F, S>, tmaSmemBytes<S>());
-                    persistentGrid(collideBulkTma<!F, S>, tmaSmemBytes<S>());
-                }
+                const int grid = persistentGrid(collideBulkTma<F, S>, kTile, tmaSmemBytes<S>());
+                persistentGrid(collideBulkTma<!F, S>, kTile, tmaSmemBytes<S>());
                 collideBulkTma<F, S><<<std::min(grid, g.segCount), kTile, tmaSmemBytes<S>(), s>>>(g);
             }
         }
-        if (v == CollideVariant::Prefetch) {
+        // the paired kernel packs two FP32 cells; the FP64 build collides one cell per thread
+        const bool pair = v == CollideVariant::Pair && pairFits(g) && !std::is_same<S, double>::value;
+        if (v == CollideVariant::Prefetch || (v == CollideVariant::Pair && !pair)) {
             // bulk segments and listed cells in one persistent launch
             const int items = g.segCount + (g.specialCount + kTile - 1) / kTile;
             if (items > 0) {
-                static int grid = 0;
-                if (grid == 0) grid = persistentGrid(collidePrefetch<F, S>, 0);
+                const int grid = persistentGrid(collidePrefetch<F, S>, kTile, 0);
                 collidePrefetch<F, S><<<std::min(grid, items), kTile, 0, s>>>(g);
+            }
+        } else if (pair) {
+            if constexpr (!std::is_same<S, double>::value) {
+                const int items = g.segCount + (g.specialCount + kTile - 1) / kTile;
+                if (items > 0) {
+                    const int grid = persistentGrid(collidePair<F, S>, kHalf, 0);
+                    collidePair<F, S><<<std::min(grid, items), kHalf, 0, s>>>(g);
+                }
             }
         } else if (g.specialCount > 0) {
             collideList<F, S><<<blocksFor(g.specialCount), kBlock, 0, s>>>(g);
@@ -1098,6 +1334,11 @@ template <bool F, class S> struct RunEnergy {
         kineticEnergy<F, S><<<blocksFor(g.cellCount), kBlock, 0, s>>>(g, out);
     }
 };
+template <bool F, class S> struct RunGlobalSums {
+    static void run(const DevLevel& g, cudaStream_t s, double* out) {
+        globalSums<F, S><<<blocksFor(g.cellCount), kBlock, 0, s>>>(g, out);
+    }
+};
 template <bool F, class S> struct RunMacro {
     static void run(const DevLevel& g, cudaStream_t s, float* out) {
         macroFields<F, S><<<blocksFor(g.cellCount), kBlock, 0, s>>>(g, out);
@@ -1116,35 +1357,44 @@ template <bool F, class S> struct RunScatter {
 
 }  // namespace
 
-void launchCollideStream(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunCollide>(g, flip, s); }
+#define LBM3_FN(name) LBM3_STEP_JOIN(name, LBM3_STEP_SUFFIX)
+
+void LBM3_FN(launchCollideStream)(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunCollide>(g, flip, s); }
+void LBM3_FN(launchPeriodic)(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunPeriodic>(g, flip, s); }
+void LBM3_FN(launchOpenBoundary)(const DevLevel& g, bool flip, cudaStream_t s, int iterationsFinished) {
+    dispatch<RunOpen>(g, flip, s, iterationsFinished);
+}
+void LBM3_FN(launchOpenBoundaryInit)(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunOpenInit>(g, flip, s); }
+void LBM3_FN(launchInit)(const DevLevel& g, bool flip, cudaStream_t s, const float4* macro, float4 uniform) {
+    dispatch<RunInit>(g, flip, s, macro, uniform);
+}
+void LBM3_FN(launchKineticEnergy)(const DevLevel& g, bool flip, cudaStream_t s, double* out) {
+    dispatch<RunEnergy>(g, flip, s, out);
+}
+void LBM3_FN(launchMacro)(const DevLevel& g, bool flip, cudaStream_t s, float* out) { dispatch<RunMacro>(g, flip, s, out); }
+void LBM3_FN(launchGlobalSums)(const DevLevel& g, bool flip, cudaStream_t s, double* out) {
+    dispatch<RunGlobalSums>(g, flip, s, out);
+}
+void LBM3_FN(launchGatherF)(const DevLevel& g, cudaStream_t s, float* out) { dispatch<RunGather>(g, false, s, out); }
+void LBM3_FN(launchScatterF)(const DevLevel& g, cudaStream_t s, const float* in) { dispatch<RunScatter>(g, false, s, in); }
+void LBM3_FN(launchFlowReport)(const DevLevel& g, bool flip, cudaStream_t s, int plane, int layer, int h0, int h1,
+                               int v0, int v1, double* out) {
+    dispatch<RunFlowReport>(g, flip, s, plane, layer, h0, h1, v0, v1, out);
+}
+
+#if LBM3_STEP_STORAGE == 0
+// storage-independent launchers live in the FP32 unit
 int stepLaunchCount(const DevLevel& g) {
     int n = 0;
     const CollideVariant v = collideVariant();
     if (v == CollideVariant::Simple) n += g.cellCount > 0;
-    else if (v == CollideVariant::Prefetch) n += ((g.segCount + g.specialCount) > 0) + (g.rotorCellCount > 0);
+    else if (v == CollideVariant::Prefetch || v == CollideVariant::Pair)
+        n += ((g.segCount + g.specialCount) > 0) + (g.rotorCellCount > 0);
     else n += (g.segCount > 0) + (g.specialCount > 0) + (g.rotorCellCount > 0);
     return n + (g.obCount > 0) + (g.perCount > 0);
 }
-void launchPeriodic(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunPeriodic>(g, flip, s); }
-void launchOpenBoundary(const DevLevel& g, bool flip, cudaStream_t s, int iterationsFinished) {
-    dispatch<RunOpen>(g, flip, s, iterationsFinished);
-}
-void launchOpenBoundaryInit(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunOpenInit>(g, flip, s); }
-void launchInit(const DevLevel& g, bool flip, cudaStream_t s, const float4* macro, float4 uniform) {
-    dispatch<RunInit>(g, flip, s, macro, uniform);
-}
-void launchKineticEnergy(const DevLevel& g, bool flip, cudaStream_t s, double* out) {
-    dispatch<RunEnergy>(g, flip, s, out);
-}
-void launchMacro(const DevLevel& g, bool flip, cudaStream_t s, float* out) { dispatch<RunMacro>(g, flip, s, out); }
-void launchGatherF(const DevLevel& g, cudaStream_t s, float* out) { dispatch<RunGather>(g, false, s, out); }
-void launchScatterF(const DevLevel& g, cudaStream_t s, const float* in) { dispatch<RunScatter>(g, false, s, in); }
 void launchWallForce(const DevLevel& g, int wallID, cudaStream_t s, double* out) {
     if (g.wallCount > 0) wallForceSum<<<blocksFor(g.wallCount), kBlock, 0, s>>>(g, wallID, out);
-}
-void launchFlowReport(const DevLevel& g, bool flip, cudaStream_t s, int plane, int layer, int h0, int h1, int v0,
-                      int v1, double* out) {
-    dispatch<RunFlowReport>(g, flip, s, plane, layer, h0, h1, v0, v1, out);
 }
 void launchRotorForce(const DevRotor& R, const int* index, cudaStream_t s, double* out) {
     if (R.nonzero > 0) rotorForceSum<<<blocksFor(R.nonzero), kBlock, 0, s>>>(R, index, out);
@@ -1156,5 +1406,6 @@ void launchCollideBatch(float* f, int n, const CollisionConsts& P, float gx, flo
                         cudaStream_t s) {
     collideBatch<<<blocksFor(n), kBlock, 0, s>>>(f, n, P, gx, gy, gz);
 }
+#endif
 
 }  // namespace lbm

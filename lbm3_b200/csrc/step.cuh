@@ -15,7 +15,6 @@ namespace lbm {
 // open-boundary cells per CTA of the boundary kernel
 constexpr int kOpenChunk = 128;
 
-struct MbbcDir;
 
 // One forcing rotor as the collide kernels see it (RotorViewStruct,
 // include/types.h:217-219), with this step's angle as cosine and sine.
@@ -63,7 +62,7 @@ struct DevLevel {
     const unsigned* wallData;      // [wallCount]
     const unsigned* linkLength;    // [7][wallCount] packed 8-bit link codes
     const float* wallVel;          // [3][wallCount] wall velocity, lattice units
-    float* wallForce;              // [3][wallCount] momentum-exchange force accumulators
+    double* wallForce;             // [3][wallCount] momentum-exchange force accumulators (FP64)
     const int* wallIndex;          // [wallCount] cell of each entry
     int wallCount;
     int trackWallForce;
@@ -85,16 +84,27 @@ struct DevLevel {
     // unknown-direction mask} is one CTA of the boundary kernel
     const int4* obChunk;
     int obChunkCount;
-    const MbbcDir* obTables;          // [26] direction-indexed closure tables
+    const void* obTables;             // [26] direction-indexed closure tables (MbbcDirT of the
+                                      // arithmetic type)
     int nx, ny, nz;
     float res, ox, oy, oz;
     CollisionConsts coll;
+    CollisionConstsT<double> coll64;  // the same constants for the FP64 build
     DevRotor rotor[kMaxRotors];
     int rotorCount;
     const int* rotorCells;         // cells inside a rotor's swept cylinder
     int rotorCellCount;
     int trackRotorForce;
 };
+
+// Collision constants in the arithmetic type T.
+template <class T> __device__ __forceinline__ const CollisionConstsT<T>& collConsts(const DevLevel& g);
+template <> __device__ __forceinline__ const CollisionConstsT<float>& collConsts<float>(const DevLevel& g) {
+    return g.coll;
+}
+template <> __device__ __forceinline__ const CollisionConstsT<double>& collConsts<double>(const DevLevel& g) {
+    return g.coll64;
+}
 
 // Neighbour cells of `cell` in the order self, +i, +j, +ij, +k, +ik, +jk, +ijk
 // (bit 0 = i, bit 1 = j, bit 2 = k), from the compressed rows
@@ -130,8 +140,18 @@ __device__ __forceinline__ void decodeNbr(const DevLevel& g, int cell, int (&nb)
 }
 
 // Typed population storage.  Half and bfloat16 hold the shifted value
-// f_i - w_i directly (the reference already stores shifted FP32).
+// f_i - w_i directly (the reference already stores shifted FP32).  Arithmetic
+// is FP32 for every storage type except double, which is the FP64 build of
+// the kernels (FP64 storage and arithmetic).
+template <class S> struct Compute { using type = float; };
+template <> struct Compute<double> { using type = double; };
+template <class S> using Real = typename Compute<S>::type;
+
 template <class S> struct Store;
+template <> struct Store<double> {
+    static __device__ __forceinline__ double ld(const double* p) { return *p; }
+    static __device__ __forceinline__ void st(double* p, double v) { *p = v; }
+};
 template <> struct Store<float> {
     static __device__ __forceinline__ float ld(const float* p) { return *p; }
     static __device__ __forceinline__ void st(float* p, float v) { *p = v; }
@@ -152,16 +172,16 @@ template <> struct Store<__nv_bfloat16> {
 template <bool F> __device__ __forceinline__ constexpr int preSlot(int d) { return F ? inv(d) : d; }
 template <bool F> __device__ __forceinline__ constexpr int postSlot(int d) { return F ? d : inv(d); }
 
-template <bool F, class S>
-__device__ __forceinline__ void readPre(const DevLevel& g, const int (&nb)[8], float (&f)[27]) {
+template <bool F, class S, class T>
+__device__ __forceinline__ void readPre(const DevLevel& g, const int (&nb)[8], T (&f)[27]) {
     const S* base = static_cast<const S*>(g.f);
 #pragma unroll
     for (int d = 0; d < 27; ++d)
         f[d] = Store<S>::ld(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
 }
 
-template <bool F, class S>
-__device__ __forceinline__ void writePost(const DevLevel& g, const int (&nb)[8], const float (&f)[27]) {
+template <bool F, class S, class T>
+__device__ __forceinline__ void writePost(const DevLevel& g, const int (&nb)[8], const T (&f)[27]) {
     S* base = static_cast<S*>(g.f);
 #pragma unroll
     for (int d = 0; d < 27; ++d)
@@ -170,8 +190,8 @@ __device__ __forceinline__ void writePost(const DevLevel& g, const int (&nb)[8],
 
 // Write f as pre-collision values of the cell (used by initial condition and
 // periodic ghost copies, which both write with getPreCollisionIndex).
-template <bool F, class S>
-__device__ __forceinline__ void writePre(const DevLevel& g, const int (&nb)[8], const float (&f)[27]) {
+template <bool F, class S, class T>
+__device__ __forceinline__ void writePre(const DevLevel& g, const int (&nb)[8], const T (&f)[27]) {
     S* base = static_cast<S*>(g.f);
 #pragma unroll
     for (int d = 0; d < 27; ++d)
@@ -184,21 +204,21 @@ namespace lbm {
 
 // Density deviation and velocity from shifted populations with the
 // reference's pairwise summation (getDRhoUxUyUz, include/cellFunctions.h:257-279).
-__host__ __device__ __forceinline__ void macroFromF(const float (&f)[27], float& dRho, float& ux,
-                                                    float& uy, float& uz) {
+template <class T>
+__host__ __device__ __forceinline__ void macroFromF(const T (&f)[27], T& dRho, T& ux, T& uy, T& uz) {
     dRho = (((f[PPP] + f[MMM]) + (f[PMP] + f[MPM])) + ((f[PPM] + f[MMP]) + (f[PMM] + f[MPP]))) +
            (((f[OPP] + f[OMM]) + (f[OPM] + f[OMP])) + ((f[POP] + f[MOM]) + (f[POM] + f[MOP])) +
             ((f[PPO] + f[MMO]) + (f[PMO] + f[MPO]))) +
            ((f[POO] + f[MOO]) + (f[OPO] + f[OMO]) + (f[OOP] + f[OOM])) + f[OOO];
-    const float rhoInv = 1.f / (dRho + 1.f);
-    const float a = f[PPP] - f[MMM], b = f[PMP] - f[MPM], c = f[PPM] - f[MMP], d = f[PMM] - f[MPP];
-    const float mx = (((a + b) + (c + d)) + (((f[POP] - f[MOM]) + (f[POM] - f[MOP])) +
+    const T rhoInv = T(1) / (dRho + T(1));
+    const T a = f[PPP] - f[MMM], b = f[PMP] - f[MPM], c = f[PPM] - f[MMP], d = f[PMM] - f[MPP];
+    const T mx = (((a + b) + (c + d)) + (((f[POP] - f[MOM]) + (f[POM] - f[MOP])) +
                                              ((f[PPO] - f[MMO]) + (f[PMO] - f[MPO])))) +
                      (f[POO] - f[MOO]);
-    const float my = (((a - b) + (c - d)) + (((f[OPP] - f[OMM]) + (f[OPM] - f[OMP])) +
+    const T my = (((a - b) + (c - d)) + (((f[OPP] - f[OMM]) + (f[OPM] - f[OMP])) +
                                              ((f[PPO] - f[MMO]) - (f[PMO] - f[MPO])))) +
                      (f[OPO] - f[OMO]);
-    const float mz = (((a + b) - (c + d)) + (((f[OPP] - f[OMM]) - (f[OPM] - f[OMP])) +
+    const T mz = (((a + b) - (c + d)) + (((f[OPP] - f[OMM]) - (f[OPM] - f[OMP])) +
                                              ((f[POP] - f[MOM]) - (f[POM] - f[MOP])))) +
                      (f[OOP] - f[OOM]);
     ux = mx * rhoInv;

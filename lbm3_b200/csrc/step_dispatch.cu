@@ -1,0 +1,42 @@
+// Storage dispatch of the level launchers: step.cu is compiled once per
+// population storage type, and these entry points forward to its unit.
+#include "step_launch.h"
+
+namespace lbm {
+
+#define LBM3_BY_STORAGE(name, ...)                                          \
+    switch (g.storage) {                                                    \
+        case LBM_STORE_F16: name##F16(__VA_ARGS__); break;                  \
+        case LBM_STORE_BF16: name##BF16(__VA_ARGS__); break;                \
+        case LBM_STORE_F64: name##F64(__VA_ARGS__); break;                  \
+        default: name##F32(__VA_ARGS__);                                    \
+    }
+
+void launchCollideStream(const DevLevel& g, bool flip, cudaStream_t s) { LBM3_BY_STORAGE(launchCollideStream, g, flip, s) }
+void launchPeriodic(const DevLevel& g, bool flip, cudaStream_t s) { LBM3_BY_STORAGE(launchPeriodic, g, flip, s) }
+void launchOpenBoundary(const DevLevel& g, bool flip, cudaStream_t s, int iterationsFinished) {
+    LBM3_BY_STORAGE(launchOpenBoundary, g, flip, s, iterationsFinished)
+}
+void launchOpenBoundaryInit(const DevLevel& g, bool flip, cudaStream_t s) {
+    LBM3_BY_STORAGE(launchOpenBoundaryInit, g, flip, s)
+}
+void launchInit(const DevLevel& g, bool flip, cudaStream_t s, const float4* macro, float4 uniform) {
+    LBM3_BY_STORAGE(launchInit, g, flip, s, macro, uniform)
+}
+void launchKineticEnergy(const DevLevel& g, bool flip, cudaStream_t s, double* out) {
+    LBM3_BY_STORAGE(launchKineticEnergy, g, flip, s, out)
+}
+void launchMacro(const DevLevel& g, bool flip, cudaStream_t s, float* out) { LBM3_BY_STORAGE(launchMacro, g, flip, s, out) }
+void launchGlobalSums(const DevLevel& g, bool flip, cudaStream_t s, double* out) {
+    LBM3_BY_STORAGE(launchGlobalSums, g, flip, s, out)
+}
+void launchGatherF(const DevLevel& g, cudaStream_t s, float* out) { LBM3_BY_STORAGE(launchGatherF, g, s, out) }
+void launchScatterF(const DevLevel& g, cudaStream_t s, const float* in) { LBM3_BY_STORAGE(launchScatterF, g, s, in) }
+void launchFlowReport(const DevLevel& g, bool flip, cudaStream_t s, int plane, int layer, int h0, int h1, int v0,
+                      int v1, double* out) {
+    LBM3_BY_STORAGE(launchFlowReport, g, flip, s, plane, layer, h0, h1, v0, v1, out)
+}
+
+#undef LBM3_BY_STORAGE
+
+}  // namespace lbm

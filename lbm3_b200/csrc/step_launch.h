@@ -1,4 +1,6 @@
-// Host-callable launchers of the level kernels (implemented in step.cu).
+// Host-callable launchers of the level kernels.  step.cu is compiled once per
+// population storage type (launchers suffixed F32, F16, BF16, F64);
+// step_dispatch.cu selects the unit by DevLevel::storage.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -17,6 +19,8 @@ void launchOpenBoundaryInit(const DevLevel& g, bool flip, cudaStream_t s);
 void launchInit(const DevLevel& g, bool flip, cudaStream_t s, const float4* macro, float4 uniform);
 void launchKineticEnergy(const DevLevel& g, bool flip, cudaStream_t s, double* out);
 void launchMacro(const DevLevel& g, bool flip, cudaStream_t s, float* out);
+// FP64 sums over the fluid cells: {rho, dRho, rho ux, rho uy, rho uz, cells}
+void launchGlobalSums(const DevLevel& g, bool flip, cudaStream_t s, double* out);
 void launchGatherF(const DevLevel& g, cudaStream_t s, float* out);
 void launchScatterF(const DevLevel& g, cudaStream_t s, const float* in);
 void launchWallForce(const DevLevel& g, int wallID, cudaStream_t s, double* out);
@@ -26,5 +30,25 @@ void launchRotorForce(const DevRotor& R, const int* index, cudaStream_t s, doubl
 void launchOpenFlow(const DevLevel& g, int openBCID, float invSpan, cudaStream_t s, double* out);
 void launchCollideBatch(float* f, int n, const CollisionConsts& P, float gx, float gy, float gz,
                         cudaStream_t s);
+
+// per-storage launchers (one set per step.cu unit)
+#define LBM3_DECLARE_STORAGE_LAUNCHERS(SUF)                                                                      \
+    void launchCollideStream##SUF(const DevLevel& g, bool flip, cudaStream_t s);                               \
+    void launchPeriodic##SUF(const DevLevel& g, bool flip, cudaStream_t s);                                    \
+    void launchOpenBoundary##SUF(const DevLevel& g, bool flip, cudaStream_t s, int iterationsFinished);        \
+    void launchOpenBoundaryInit##SUF(const DevLevel& g, bool flip, cudaStream_t s);                            \
+    void launchInit##SUF(const DevLevel& g, bool flip, cudaStream_t s, const float4* macro, float4 uniform);   \
+    void launchKineticEnergy##SUF(const DevLevel& g, bool flip, cudaStream_t s, double* out);                  \
+    void launchMacro##SUF(const DevLevel& g, bool flip, cudaStream_t s, float* out);                           \
+    void launchGlobalSums##SUF(const DevLevel& g, bool flip, cudaStream_t s, double* out);                     \
+    void launchGatherF##SUF(const DevLevel& g, cudaStream_t s, float* out);                                    \
+    void launchScatterF##SUF(const DevLevel& g, cudaStream_t s, const float* in);                              \
+    void launchFlowReport##SUF(const DevLevel& g, bool flip, cudaStream_t s, int plane, int layer, int h0,     \
+                               int h1, int v0, int v1, double* out);
+LBM3_DECLARE_STORAGE_LAUNCHERS(F32)
+LBM3_DECLARE_STORAGE_LAUNCHERS(F16)
+LBM3_DECLARE_STORAGE_LAUNCHERS(BF16)
+LBM3_DECLARE_STORAGE_LAUNCHERS(F64)
+#undef LBM3_DECLARE_STORAGE_LAUNCHERS
 
 }  // namespace lbm

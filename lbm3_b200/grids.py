@@ -217,6 +217,15 @@ class Grids:
         A.check(A.lib().lbm_kinetic_energy(self._h, u_ref_phys, domain_length, C.byref(out)))
         return out.value
 
+    def global_sums(self) -> dict:
+        """FP64 accumulators over the fluid cells: mass, mass deviation,
+        momentum (SI), fluid cell count, and the lattice sums of rho and dRho."""
+        out = (C.c_double * 8)()
+        A.check(A.lib().lbm_global_sums(self._h, out))
+        keys = ("mass", "mass_deviation", "momentum_x", "momentum_y", "momentum_z", "cells", "sum_rho",
+                "sum_drho")
+        return dict(zip(keys, out[:]))
+
     def wall_force(self, wall_id: int, reset: bool = False) -> np.ndarray:
         """{Fx, Fy, Fz [N], Tx, Ty, Tz [N m]} on a body, averaged since the last reset."""
         out = (C.c_double * 6)()
@@ -234,6 +243,10 @@ class Grids:
         keys = ("normal_velocity", "mass_flow", "momentum_thrust", "pressure", "pressure_power",
                 "normal_kinetic_power", "area_mm2")
         return dict(zip(keys, out[:]))
+
+    def export_vtk(self, path) -> None:
+        """exportVTK: every cell of every level as a legacy ASCII VTK file."""
+        A.check(A.lib().lbm_export_vtk(self._h, str(path).encode()))
 
     def save_state(self) -> bytes:
         """Checkpoint of everything the run carries between steps."""

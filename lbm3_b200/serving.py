@@ -2,11 +2,15 @@
 
 Requests (a case and a step count) arrive over time.  A request is admitted
 as soon as a slot is free and its device footprint (the plan's
-grid_memory_bytes) fits the remaining HBM budget; admitted domains keep their
-populations and tables resident and advance together with update_batch, one
-stream each, in chunks of steps, so that work of requests that arrived at
-different times overlaps on the GPU.  A finished domain reads its result,
-frees its memory and its slot, and the next waiting request is admitted.
+grid_memory_bytes, every device array the build allocates) fits the
+remaining HBM budget.  Its grids are then built on a builder thread (host
+voxelization and tables, upload, initial condition) while the domains
+already resident keep stepping; once built, a domain joins the active set.
+Active domains keep their populations and tables resident and advance
+together with update_batch, one stream each, in chunks of steps, so that
+work of requests that arrived at different times overlaps on the GPU.  A
+finished domain reads its result, frees its memory and its slot, and the
+next waiting request is admitted.
 
 Each result is the one the request gets when run alone: batched stepping is
 bit-identical to stepping a domain by itself.
@@ -14,6 +18,7 @@ bit-identical to stepping a domain by itself.
 from __future__ import annotations
 
 import time
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -28,9 +33,10 @@ class Request:
     case: A.LbmCase
     steps: int
     arrival: float = 0.0        # seconds after the server starts
-    wall_id: int = 0            # body whose force is the result (-1: kinetic energy)
+    wall_id: int = 0            # body whose force is the result; -1: the kinetic energy instead
     footprint: int = 0          # device bytes, if known at submission (else planned at admission)
     updates: int = 0            # fluid cell updates per step, with footprint
+    energy_ref: tuple = (1.0, 1000.0)  # (u_ref m/s, domain length mm) normalising the kinetic energy
 
 
 @dataclass
@@ -42,6 +48,7 @@ class Result:
     finished: float
     arrival: float
     force: np.ndarray | None = None
+    energy: float | None = None
     macro: np.ndarray | None = None
 
     @property
@@ -52,74 +59,110 @@ class Result:
 @dataclass
 class _Active:
     req: Request
-    grids: Grids
+    grids: Grids | None
     stream: object
     remaining: int
     footprint: int
     admitted: float
     updates: int
+    build: object = None        # future of the grid build while it runs
+
+
+def _footprint(req: Request):
+    if req.footprint > 0:
+        return req.footprint, req.updates * req.steps
+    plan = Plan(req.case)
+    try:
+        return int(plan.info().grid_memory_bytes), int(plan.fluid_updates_per_iteration) * req.steps
+    finally:
+        plan.close()
 
 
 @dataclass
 class Server:
     """`hbm_budget` bytes of device memory for resident domains, at most
-    `max_slots` of them, stepped in chunks of up to `chunk_steps`."""
+    `max_slots` of them, stepped in chunks of up to `chunk_steps`; grids are
+    built by `builders` host threads."""
     hbm_budget: int
     max_slots: int = 16
     chunk_steps: int = 100
     keep_fields: bool = False
+    builders: int = 2
     results: list = field(default_factory=list)
 
     def run(self, requests) -> list:
         import torch
         pending = sorted(requests, key=lambda r: r.arrival)
+        device = torch.cuda.current_device()
         active: list[_Active] = []
         used = 0
+        pool = ThreadPoolExecutor(max_workers=max(1, self.builders))
+
+        def build(case):
+            torch.cuda.set_device(device)
+            return Grids(case)
+
         t0 = time.perf_counter()
-        while pending or active:
-            now = time.perf_counter() - t0
-            # admission: arrived, a free slot, and the footprint fits
-            while pending and pending[0].arrival <= now and len(active) < self.max_slots:
-                req = pending[0]
-                if req.footprint > 0:
-                    footprint, updates = req.footprint, req.updates * req.steps
-                else:
-                    plan = Plan(req.case)
-                    footprint = int(plan.info().grid_memory_bytes)
-                    updates = int(plan.fluid_updates_per_iteration) * req.steps
-                    plan.close()
-                if footprint > self.hbm_budget:
-                    raise ValueError(f"request {req.rid} needs {footprint} bytes, more than the whole budget")
-                if used + footprint > self.hbm_budget:
-                    break
-                pending.pop(0)
-                g = Grids(req.case)
-                stream = torch.cuda.Stream()
-                g.set_stream(stream.cuda_stream)
-                active.append(_Active(req, g, stream, req.steps, footprint, time.perf_counter() - t0, updates))
-                used += footprint
-            if not active:
-                # idle until the next arrival
-                time.sleep(max(0.0, min(0.01, pending[0].arrival - (time.perf_counter() - t0))))
-                continue
-            chunk = min(self.chunk_steps, min(a.remaining for a in active))
-            update_batch([a.grids for a in active], chunk)
+        try:
+            while pending or active:
+                now = time.perf_counter() - t0
+                # admission: arrived, a free slot, and the footprint fits
+                while pending and pending[0].arrival <= now and len(active) < self.max_slots:
+                    req = pending[0]
+                    footprint, updates = _footprint(req)
+                    if footprint > self.hbm_budget:
+                        raise ValueError(f"request {req.rid} needs {footprint} bytes, more than the whole budget")
+                    if used + footprint > self.hbm_budget:
+                        break
+                    pending.pop(0)
+                    active.append(_Active(req, None, None, req.steps, footprint, time.perf_counter() - t0,
+                                          updates, pool.submit(build, req.case)))
+                    used += footprint
+                # domains whose build finished join the stepping set
+                for a in active:
+                    if a.build is not None and a.build.done():
+                        a.grids = a.build.result()
+                        a.build = None
+                        a.stream = torch.cuda.Stream()
+                        a.grids.set_stream(a.stream.cuda_stream)
+                ready = [a for a in active if a.grids is not None]
+                if not ready:
+                    # idle until the next arrival or build completion
+                    wait = 0.002 if active else max(0.0, pending[0].arrival - (time.perf_counter() - t0))
+                    time.sleep(min(0.01, wait))
+                    continue
+                chunk = min(self.chunk_steps, min(a.remaining for a in ready))
+                update_batch([a.grids for a in ready], chunk)
+                for a in ready:
+                    a.remaining -= chunk
+                done = [a for a in ready if a.remaining == 0]
+                for a in done:
+                    g = a.grids
+                    g.synchronize()
+                    res = Result(a.req.rid, a.req.steps, a.updates, a.admitted, 0.0, a.req.arrival)
+                    if a.req.wall_id >= 0:
+                        res.force = g.wall_force(a.req.wall_id)
+                    else:
+                        res.energy = g.kinetic_energy(*a.req.energy_ref)
+                    if self.keep_fields:
+                        res.macro = g.macro()
+                    res.finished = time.perf_counter() - t0
+                    g.close()
+                    a.grids = None
+                    used -= a.footprint
+                    self.results.append(res)
+                active = [a for a in active if a.remaining > 0]
+        finally:
+            # on an error, release everything admitted so far
             for a in active:
-                a.remaining -= chunk
-            done = [a for a in active if a.remaining == 0]
-            for a in done:
-                g = a.grids
-                g.synchronize()
-                res = Result(a.req.rid, a.req.steps, a.updates, a.admitted, 0.0, a.req.arrival)
-                if a.req.wall_id >= 0:
-                    res.force = g.wall_force(a.req.wall_id)
-                if self.keep_fields:
-                    res.macro = g.macro()
-                res.finished = time.perf_counter() - t0
-                g.close()
-                used -= a.footprint
-                self.results.append(res)
-            active = [a for a in active if a.remaining > 0]
+                if a.build is not None:
+                    try:
+                        a.grids = a.build.result()
+                    except Exception:
+                        a.grids = None
+                if a.grids is not None:
+                    a.grids.close()
+            pool.shutdown(wait=True)
         return self.results
 
 

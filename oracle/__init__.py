@@ -91,6 +91,7 @@ def lib() -> C.CDLL:
         h.oracle_kinetic_energy.argtypes = [C.POINTER(OGrid), C.c_float, C.c_float]
         h.oracle_kinetic_energy.restype = C.c_double
         h.oracle_macro.argtypes = [C.POINTER(OGrid), C.POINTER(C.c_float)]
+        h.oracle_global_sums.argtypes = [C.POINTER(OGrid), C.POINTER(C.c_double)]
         h.oracle_threads.restype = C.c_int
         h.oracle_collide_range.argtypes = [C.POINTER(OGrid), C.c_int, C.c_int]
         h.oracle_from_tables.argtypes = [C.c_void_p, C.POINTER(OGrid), C.c_int, C.c_int] + [C.c_void_p] * 8 + \
@@ -262,6 +263,12 @@ class OracleGrid:
 
     def kinetic_energy(self, u_ref_phys: float, domain_length: float) -> float:
         return lib().oracle_kinetic_energy(C.byref(self.g), u_ref_phys, domain_length)
+
+    def global_sums(self) -> np.ndarray:
+        """{sum rho, sum dRho, momentum x, y, z, cells} in lattice units (FP64)."""
+        out = (C.c_double * 6)()
+        lib().oracle_global_sums(C.byref(self.g), out)
+        return np.array(out[:])
 
     def macro(self) -> np.ndarray:
         out = np.empty((4, self.g.cellCount), dtype=np.float32)

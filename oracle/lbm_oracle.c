@@ -1748,6 +1748,36 @@ void oracle_collide_range(ogrid* g, int c0, int c1) {
     }
 }
 
+/* FP64 sums over the fluid cells (walls, periodic ghosts and interface
+ * duplicates excluded): out = {sum rho, sum dRho, sum c_x f, sum c_y f,
+ * sum c_z f, cells}, lattice units. */
+void oracle_global_sums(const ogrid* g, double* out) {
+    for (int q = 0; q < 6; ++q) out[q] = 0.0;
+    const int n = g->cellCount;
+    for (int c = 0; c < n; ++c) {
+        const int wm = g->wallMap[c];
+        if (wm == -3 || wm == -2) continue;
+        if (wm >= 0 && (g->wallData[wm] & 1u)) continue;
+        int nb[8];
+        get_nbr(g, c, nb);
+        double dRho = 0.0, m[3] = {0.0, 0.0, 0.0};
+        for (int d = 0; d < 27; ++d) {
+            const int slot = g->flip ? INV[d] : d;
+            const double f = g->f[(size_t)slot * n + nb[pre_nbr(d)]];
+            dRho += f;
+            m[0] += CX[d] * f;
+            m[1] += CY[d] * f;
+            m[2] += CZ[d] * f;
+        }
+        out[0] += 1.0 + dRho;
+        out[1] += dRho;
+        out[2] += m[0];
+        out[3] += m[1];
+        out[4] += m[2];
+        out[5] += 1.0;
+    }
+}
+
 double oracle_kinetic_energy(const ogrid* g, float uRefPhys, float domainLength) {
     const long long n = g->cellCount;
     double sum = 0.0;

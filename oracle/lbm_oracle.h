@@ -120,6 +120,9 @@ void oracle_collide_range(ogrid* g, int c0, int c1);
 /* getKineticEnergy (cases/taylorGreenVortex/taylorGreenVortexMain.cu:116-180). */
 double oracle_kinetic_energy(const ogrid* g, float uRefPhys, float domainLength);
 
+/* FP64 sums over the fluid cells: {sum rho, sum dRho, momentum x, y, z, cells}. */
+void oracle_global_sums(const ogrid* g, double* out);
+
 /* dRho,ux,uy,uz of every cell: out[4][cellCount]. */
 void oracle_macro(const ogrid* g, float* out);
 

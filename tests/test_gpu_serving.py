@@ -38,6 +38,23 @@ def test_results_in_the_mix_equal_results_alone():
     assert summary["requests"] == 5 and summary["p99_s"] >= summary["p50_s"] > 0
 
 
+def test_energy_result_and_builds_off_the_stepping_thread():
+    """A request with wall_id -1 returns its kinetic energy, equal to the
+    request run alone; grids are built on builder threads."""
+    rng = np.random.default_rng(3)
+    reqs = [S.channel_request(q, 16, rng, 50 + 10 * q, arrival=0.01 * q) for q in range(4)]
+    for r in reqs:
+        r.wall_id = -1
+    server = S.Server(hbm_budget=1 << 34, max_slots=4, chunk_steps=25, builders=2)
+    results = {r.rid: r for r in server.run(reqs)}
+    for req in reqs:
+        with L.build_grids(req.case) as g:
+            g.update_all_grids(req.steps)
+            assert results[req.rid].force is None
+            # FP64 block partials are summed with atomics: equal up to ordering
+            assert results[req.rid].energy == pytest.approx(g.kinetic_energy(*req.energy_ref), rel=1e-12)
+
+
 def test_request_larger_than_the_budget_is_rejected():
     req = requests()[2]
     server = S.Server(hbm_budget=1000, max_slots=2)
