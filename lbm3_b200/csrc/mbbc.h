@@ -4,11 +4,16 @@
 // indices (populations stay in registers) and plain FMA chains (zero
 // coefficients of unknown or unused populations add nothing).
 //
-// Sums run in ascending direction order, which is the order of the known
-// populations in the generated tables and in the reference's generated code
-// (include/boundaryConditions/{restoreRho,restoreUxUyUz,applyMBBC}.h), so the
-// results agree with it to rounding.  Populations are full (weight-
-// compensated) f, as at the reference's call site (include/updateGrid.h:223-240).
+// The closure (applyMBBC) solves S Mfu f_u = m_eq - S Mfk f_k for the unknown
+// populations.  The host folds the two steps of the generated code into one
+// row per unknown population u:
+//   f_u = sum_m E[u][m] m_eq[m] + sum_d C[u][d] f_d,
+// E = (S Mfu)^-1 grouped by equilibrium moment and C = -(S Mfu)^-1 S Mfk,
+// formed in double and rounded once, so the kernel runs one short loop over
+// the unknowns (equal to the generated code to rounding).  Populations are
+// full (weight-compensated) f, as at the reference's call site
+// (include/updateGrid.h:223-240); restoreRho and restoreUxUyUz keep the
+// generated sums in ascending direction order.
 #pragma once
 
 #include "lattice.h"
@@ -18,15 +23,20 @@ namespace lbm {
 
 // T: the arithmetic type of the kernel (the FP64 build holds the same
 // coefficients, the generated float values, widened to double).
+constexpr int kMbbcMoments = 23;  // equilibrium moments of the closure, in table order
+
 template <class T> struct MbbcDirT {
-    T smf[LBM_MBBC_MAX_UNKNOWN][27];  // S Mfk: weight of population d in equation i
-    T inv[27][LBM_MBBC_MAX_UNKNOWN];  // row of (S Mfu)^-1 producing unknown population d
+    T E[LBM_MBBC_MAX_UNKNOWN][kMbbcMoments];  // unknown row r: weights of the equilibrium moments
+    T C[LBM_MBBC_MAX_UNKNOWN][27];            // unknown row r: weights of the known populations
     T rhoMfk[27];                     // restoreRho numerator weights
     T uMfk[3][27];                    // restoreUxUyUz (edges, corners)
     T uInv[3][3];
     T uQ[3];
     T rhoQ, rhoQu[3];
-    signed char moment[LBM_MBBC_MAX_UNKNOWN];  // equilibrium moment of equation i
+    signed char unknownDir[LBM_MBBC_MAX_UNKNOWN];  // population d of unknown row r
+    signed char unknownInv[LBM_MBBC_MAX_UNKNOWN];  // its inverse direction
+    signed char unknownNbr[LBM_MBBC_MAX_UNKNOWN];  // esotwist pre-collision neighbour of d
+    T unknownW[LBM_MBBC_MAX_UNKNOWN];              // lattice weight of d
     int nu;                                    // unknown count
     int face;                                  // 1: velocity from the face closed form
     unsigned unknownMask;                      // bit d: population d is unknown
@@ -45,13 +55,20 @@ template <class V = float> inline MbbcDirT<V> mbbcDirFromTable(const LbmMbbcTabl
     D.nx = T.code / 100 - 5;
     D.ny = (T.code / 10) % 10 - 5;
     D.nz = T.code % 10 - 5;
-    for (int i = 0; i < T.nu; ++i) {
-        D.moment[i] = T.moment[i];
-        for (int k = 0; k < T.nk; ++k) D.smf[i][T.known[k]] = V(T.smfk[i][k]);
-    }
     for (int r = 0; r < T.nu; ++r) {
         D.unknownMask |= 1u << T.unknown[r];
-        for (int j = 0; j < T.nu; ++j) D.inv[T.unknown[r]][j] = T.inv[r][j];
+        D.unknownDir[r] = T.unknown[r];
+        D.unknownInv[r] = static_cast<signed char>(inv(T.unknown[r]));
+        D.unknownNbr[r] = static_cast<signed char>(preNbr(T.unknown[r]));
+        D.unknownW[r] = weightT<V>(T.unknown[r]);
+        double e[kMbbcMoments] = {};
+        double c[27] = {};
+        for (int j = 0; j < T.nu; ++j) {
+            e[T.moment[j]] += double(T.inv[r][j]);
+            for (int k = 0; k < T.nk; ++k) c[T.known[k]] -= double(T.inv[r][j]) * double(T.smfk[j][k]);
+        }
+        for (int m = 0; m < kMbbcMoments; ++m) D.E[r][m] = V(e[m]);
+        for (int d = 0; d < 27; ++d) D.C[r][d] = V(c[d]);
     }
     for (int k = 0; k < T.nk; ++k) {
         D.rhoMfk[T.known[k]] = T.rhoMfk[k];
@@ -66,57 +83,43 @@ template <class V = float> inline MbbcDirT<V> mbbcDirFromTable(const LbmMbbcTabl
     return D;
 }
 
-// Equilibrium value of moment m (the 23 moments in table order).
-template <class V> LBM_HD V mbbcMomentEq(int m, V rho, V ux, V uy, V uz) {
+// The 23 equilibrium moments of the closure, in table order.
+template <class V> LBM_HD void mbbcMomentsEq(V rho, V ux, V uy, V uz, V (&m)[kMbbcMoments]) {
     const V t = V(1) / V(3), n = V(1) / V(9);
-    switch (m) {
-        case 0: return rho;
-        case 1: return rho * ux;
-        case 2: return rho * uy;
-        case 3: return rho * uz;
-        case 4: return t * rho + rho * ux * ux;
-        case 5: return t * rho + rho * uy * uy;
-        case 6: return t * rho + rho * uz * uz;
-        case 7: return rho * uy * uz;
-        case 8: return rho * ux * uz;
-        case 9: return rho * ux * uy;
-        case 10: return V(0);
-        case 11: return t * rho * uy + rho * ux * ux * uy;
-        case 12: return t * rho * uz + rho * ux * ux * uz;
-        case 13: return t * rho * ux + rho * ux * uy * uy;
-        case 14: return t * rho * uz + rho * uy * uy * uz;
-        case 15: return t * rho * ux + rho * ux * uz * uz;
-        case 16: return t * rho * uy + rho * uy * uz * uz;
-        case 17: return n * rho + t * rho * uy * uy + t * rho * uz * uz + rho * uy * uy * uz * uz;
-        case 18: return n * rho + t * rho * ux * ux + t * rho * uz * uz + rho * ux * ux * uz * uz;
-        case 19: return n * rho + t * rho * ux * ux + t * rho * uy * uy + rho * ux * ux * uy * uy;
-        case 20: return t * rho * uy * uz;
-        case 21: return t * rho * ux * uz;
-        default: return t * rho * ux * uy;
-    }
+    m[0] = rho;
+    m[1] = rho * ux;
+    m[2] = rho * uy;
+    m[3] = rho * uz;
+    m[4] = t * rho + rho * ux * ux;
+    m[5] = t * rho + rho * uy * uy;
+    m[6] = t * rho + rho * uz * uz;
+    m[7] = rho * uy * uz;
+    m[8] = rho * ux * uz;
+    m[9] = rho * ux * uy;
+    m[10] = V(0);
+    m[11] = t * rho * uy + rho * ux * ux * uy;
+    m[12] = t * rho * uz + rho * ux * ux * uz;
+    m[13] = t * rho * ux + rho * ux * uy * uy;
+    m[14] = t * rho * uz + rho * uy * uy * uz;
+    m[15] = t * rho * ux + rho * ux * uz * uz;
+    m[16] = t * rho * uy + rho * uy * uz * uz;
+    m[17] = n * rho + t * rho * uy * uy + t * rho * uz * uz + rho * uy * uy * uz * uz;
+    m[18] = n * rho + t * rho * ux * ux + t * rho * uz * uz + rho * ux * ux * uz * uz;
+    m[19] = n * rho + t * rho * ux * ux + t * rho * uy * uy + rho * ux * ux * uy * uy;
+    m[20] = t * rho * uy * uz;
+    m[21] = t * rho * ux * uz;
+    m[22] = t * rho * ux * uy;
 }
 
-// applyMBBC: overwrite the unknown populations of f.
+// applyMBBC for unknown row r: the closed (full) population T.unknownDir[r].
 template <class V>
-LBM_HD void mbbcApply(const MbbcDirT<V>& T, V rho, V ux, V uy, V uz, V (&f)[27]) {
-    V s[LBM_MBBC_MAX_UNKNOWN];
+LBM_HD V mbbcUnknown(const MbbcDirT<V>& T, int r, const V (&meq)[kMbbcMoments], const V (&f)[27]) {
+    V v = V(0);
 #pragma unroll
-    for (int i = 0; i < LBM_MBBC_MAX_UNKNOWN; ++i) {
-        s[i] = V(0);
-        if (i >= T.nu) continue;
-        V smf = V(0);
+    for (int m = 0; m < kMbbcMoments; ++m) v = mfma(T.E[r][m], meq[m], v);
 #pragma unroll
-        for (int d = 0; d < 27; ++d) smf = mfma(T.smf[i][d], f[d], smf);
-        s[i] = mbbcMomentEq(T.moment[i], rho, ux, uy, uz) - smf;
-    }
-#pragma unroll
-    for (int d = 0; d < 27; ++d) {
-        if (!(T.unknownMask >> d & 1u)) continue;
-        V v = V(0);
-#pragma unroll
-        for (int j = 0; j < LBM_MBBC_MAX_UNKNOWN; ++j) v = mfma(T.inv[d][j], s[j], v);
-        f[d] = v;
-    }
+    for (int d = 0; d < 27; ++d) v = mfma(T.C[r][d], f[d], v);
+    return v;
 }
 
 // restoreRho: density from the known populations and the velocity.
