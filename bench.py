@@ -27,6 +27,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 BYTES_PER_POP = {"f32": 4, "f16": 2, "bf16": 2, "f64": 8}
+A_STORE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3}  # LBM_STORE_* of include/lbm3_b200.h
 
 
 def peaks():
@@ -279,11 +280,15 @@ def run_ours(args):
     torch.cuda.synchronize()
     with ClockSampler(uuid) as clk:
         clk.start()
-        ms = g.time_steps(args.steps)          # CUDA events on the grid stream
+        # the step schedule replayed as CUDA graphs, CUDA events on the grid stream
+        ms = g.time_steps_graph(args.steps)
         clk.stop()
     torch.cuda.synchronize()
+    # collide-stream kernel time: a pass of direct launches, each bracketed by events
+    kt_steps = max(2, min(args.steps, 400))
+    g.time_steps(kt_steps)
     kernel_ms, launches = g.last_kernel_time()
-    all_launches = g.last_launch_count()
+    all_launches = int(round(g.last_launch_count() / kt_steps * args.steps))
     if dist:
         dist.barrier()
     ms_max = max_over_ranks(ms, dist, "cuda")
@@ -327,6 +332,8 @@ def run_ours(args):
     e2e_value = whole_job_rate(updates, e2e_steps, world, max_over_ranks(e2e_s, dist, "cuda"))
     del np
 
+    extras = storage_comparison(args, value, torch) if (rank == 0 and world == 1 and not args.no_extras) else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         mlups, steps, el, thr = time_oracle(case, target_s=args.cpu_seconds)
@@ -359,11 +366,81 @@ def run_ours(args):
             "gpu_launches": all_launches,
             "clocks": clocks,
         }
+        if extras:
+            line.update(extras)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def time_batch(cases, steps: int, warmup: int, torch) -> float:
+    """MLUPS of independent domains advanced together by update_batch, one
+    stream each, device-timed from a start event all streams wait on to an
+    end event that waits on all of them."""
+    import lbm3_b200 as L
+    grids = [L.build_grids(c) for c in cases]
+    streams = [torch.cuda.Stream() for _ in grids]
+    for g, s in zip(grids, streams):
+        g.set_stream(s.cuda_stream)
+    L.update_batch(grids, warmup)
+    torch.cuda.synchronize()
+    main = torch.cuda.current_stream()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(main)
+    for s in streams:
+        s.wait_event(start)
+    L.update_batch(grids, steps)
+    for s in streams:
+        ev = torch.cuda.Event()
+        ev.record(s)
+        main.wait_event(ev)
+    end.record(main)
+    end.synchronize()
+    ms = start.elapsed_time(end)
+    updates = sum(g.fluid_updates_per_iteration for g in grids)
+    for g in grids:
+        g.close()
+    return updates * steps / (ms * 1e-3) / 1e6
+
+
+def storage_comparison(args, f32_value: float, torch) -> dict:
+    """The metric's comparison: the same workload with FP16-shifted storage,
+    and the FP16-shifted batched form (8 Taylor-Green 64^3 domains, the plain
+    method's configuration, one stream each) against the plain FP32 kernel
+    on one domain of that configuration and on this workload."""
+    import lbm3_b200 as L
+    out = {}
+    if args.storage == "f32":
+        c16, _, _ = make_case(args.workload, "f16")
+        g = L.build_grids(c16)
+        s = torch.cuda.Stream()
+        g.set_stream(s.cuda_stream)
+        g.update_all_grids(args.warmup)
+        steps = max(2, min(args.steps, 2000))
+        ms = g.time_steps_graph(steps)
+        v16 = g.fluid_updates_per_iteration * steps / (ms * 1e-3) / 1e6
+        g.close()
+        out["storage_f16"] = {"value": round(v16, 2), "unit": "MLUPS", "ratio_vs_f32": round(v16 / f32_value, 4),
+                              "workload": "same workload, FP16-shifted populations, FP32 arithmetic"}
+    tgv32 = L.tgv_plain_method().case
+    g = L.build_grids(tgv32)
+    s = torch.cuda.Stream()
+    g.set_stream(s.cuda_stream)
+    g.update_all_grids(args.warmup)
+    ms = g.time_steps_graph(1000)
+    plain = g.fluid_updates_per_iteration * 1000 / (ms * 1e-3) / 1e6
+    g.close()
+    batched = time_batch([L.tgv_plain_method(storage=A_STORE["f16"]).case for _ in range(8)], 500, args.warmup, torch)
+    out["batched_f16"] = {
+        "value": round(batched, 2), "unit": "MLUPS",
+        "workload": "8 Taylor-Green 64^3 domains (66^3 with ghosts), FP16-shifted, one stream each, step pairs "
+                    "replayed as CUDA graphs",
+        "plain_f32_single_domain": round(plain, 2),
+        "ratio_vs_plain_f32_same_configuration": round(batched / plain, 4),
+        "ratio_vs_plain_f32_this_workload": round(batched / f32_value, 4)}
+    return out
 
 
 def run_batch(args, copies: int, base: str):
@@ -540,6 +617,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=90.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the FP16 and batched comparisons")
     ap.add_argument("--requests", type=int, default=48, help="serving: requests in the measured stream")
     ap.add_argument("--calibration-requests", type=int, default=12, help="serving: saturated capacity sample")
     ap.add_argument("--hbm-budget-gb", type=float, default=120.0, help="serving: device memory for resident domains")

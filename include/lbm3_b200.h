@@ -158,6 +158,22 @@ typedef struct lbm_body {
     float radians_per_second;   /* signed angular speed                        */
 } lbm_body;
 
+/* BCStruct (include/types.h:131-136) as a hook fills it.  A hook receives it
+ * with the reference's defaults (lbm_default_bc) and the cell's wallID. */
+typedef struct lbm_bc {
+    float dRho, ux, uy, uz;     /* target / initial / wall values              */
+    float gx, gy, gz;           /* body force                                  */
+    int   wallID, openBCID;
+    int   useIBB, dirichletU, dirichletRho, periodic, nonReflective;
+    float nonReflectiveBeta, collisionLimiter, nuMultiplier;
+} lbm_bc;
+
+struct lbm_grid_info;
+/* A per-cell hook of a reference driver (getOpenBC, getInitialCondition,
+ * getLocalBC, include/updateGrid.h:95,256), called on the host while the grid
+ * is built, with the cell's (i, j, k) on its level and the level's info. */
+typedef void (*lbm_cell_hook)(void* user, lbm_bc* bc, int i, int j, int k, const struct lbm_grid_info* info);
+
 typedef struct lbm_case {
     /* compile-time constants of a reference driver */
     int   grid_level_count;     /* GRID_LEVEL_COUNT (1 in this build)          */
@@ -196,7 +212,22 @@ typedef struct lbm_case {
     int       rotor_count;
     lbm_rotor rotor[LBM_MAX_ROTORS];
     int       track_rotor_force;  /* TRACK_ROTOR_FORCE                         */
+
+    /* Per-cell hooks; NULL keeps the tables above.  open_bc_hook replaces the
+     * face table for every boundary cell (getOpenBC); initial_condition_hook
+     * gives dRho, ux, uy, uz of every cell (getInitialCondition);
+     * local_bc_hook gives the wall velocity (bc.ux, uy, uz) of every
+     * wall-adjacent cell, called with bc.wallID = its body (the per-wallID
+     * branch of getLocalBC).  The kernels keep the collision limiter, nu
+     * multiplier and body force uniform (the fields above). */
+    lbm_cell_hook open_bc_hook;
+    lbm_cell_hook initial_condition_hook;
+    lbm_cell_hook local_bc_hook;
+    void*         hook_user;
 } lbm_case;
+
+/* The reference's BCStruct defaults (include/types.h:131-136). */
+void lbm_default_bc(lbm_bc* bc);
 
 /* Per-level summary (InfoStruct, include/types.h:120-129, plus table sizes). */
 typedef struct lbm_grid_info {
@@ -267,6 +298,20 @@ int lbm_update_all_grids(lbm_grids* g, int coarse_steps);
  * domain's result is the one it gets when stepped alone.
  * No counterpart in the reference (one domain per driver process). */
 int lbm_update_batch(lbm_grids* const* grids, int count, int coarse_steps);
+
+/* Graph replay of the step schedule.  lbm_update_all_grids and
+ * lbm_update_batch advance step pairs by launching a CUDA graph of two steps
+ * (captured on first use, one per starting esotwist parity) instead of the
+ * individual kernels; domains with rotors, whose rotating frame is host
+ * state, launch directly.  Results are identical either way.  `enabled` = 0
+ * turns replay off for these grids (LBM3_GRAPHS=0 turns it off everywhere).
+ * No counterpart in the reference. */
+int lbm_set_graphs(lbm_grids* g, int enabled);
+
+/* Time `steps` coarse steps as replayed graphs (graphs captured before the
+ * timed region), device time in *ms; no per-kernel events.
+ * No counterpart in the reference. */
+int lbm_time_steps_graph(lbm_grids* g, int steps, float* ms);
 
 /* Block until the grid stream is idle; returns a pending CUDA error, if any. */
 int lbm_synchronize(lbm_grids* g);

@@ -6,7 +6,7 @@ package is the host-side mirror of the reference driver API.
 """
 from . import _abi
 from ._abi import LbmCase, LbmError, LbmFaceBC, LbmGridInfo, lib
-from .cases import flow_around_sphere, open_channel, periodic_box, taylor_green, tgv_plain_method
+from .cases import flow_around_sphere, open_channel, periodic_box, set_hooks, taylor_green, tgv_plain_method
 from .grids import Grids, Plan, apply_collision_batch, build_grids, update_batch
 
 __all__ = [

@@ -120,6 +120,20 @@ class LbmCase(C.Structure):
         ("body_count", C.c_int), ("body", LbmBody * LBM_MAX_BODIES),
         ("storage", C.c_int),
         ("rotor_count", C.c_int), ("rotor", LbmRotor * LBM_MAX_ROTORS), ("track_rotor_force", C.c_int),
+        ("open_bc_hook", C.c_void_p), ("initial_condition_hook", C.c_void_p), ("local_bc_hook", C.c_void_p),
+        ("hook_user", C.c_void_p),
+    ]
+
+
+class LbmBC(C.Structure):
+    """lbm_bc: BCStruct as a per-cell hook fills it."""
+    _fields_ = [
+        ("dRho", C.c_float), ("ux", C.c_float), ("uy", C.c_float), ("uz", C.c_float),
+        ("gx", C.c_float), ("gy", C.c_float), ("gz", C.c_float),
+        ("wallID", C.c_int), ("openBCID", C.c_int),
+        ("useIBB", C.c_int), ("dirichletU", C.c_int), ("dirichletRho", C.c_int),
+        ("periodic", C.c_int), ("nonReflective", C.c_int),
+        ("nonReflectiveBeta", C.c_float), ("collisionLimiter", C.c_float), ("nuMultiplier", C.c_float),
     ]
 
 
@@ -138,11 +152,15 @@ class LbmGridInfo(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+# lbm_cell_hook: void (*)(void* user, lbm_bc* bc, int i, int j, int k, const lbm_grid_info* info)
+CELL_HOOK = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(LbmBC), C.c_int, C.c_int, C.c_int, C.POINTER(LbmGridInfo))
+
 # (name, restype, argtypes) of every exported function
 _P = C.c_void_p
 SIGNATURES = [
     ("lbm_last_error", C.c_char_p, []),
     ("lbm_device_count", C.c_int, []),
+    ("lbm_default_bc", None, [C.POINTER(LbmBC)]),
     ("lbm_plan_grids", C.c_int, [C.POINTER(LbmCase), C.POINTER(_P), C.POINTER(C.c_longlong)]),
     ("lbm_free_plan", None, [_P]),
     ("lbm_plan_level_count", C.c_int, [_P]),
@@ -154,6 +172,8 @@ SIGNATURES = [
     ("lbm_update_all_grids", C.c_int, [_P, C.c_int]),
     ("lbm_update_batch", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int]),
     ("lbm_synchronize", C.c_int, [_P]),
+    ("lbm_set_graphs", C.c_int, [_P, C.c_int]),
+    ("lbm_time_steps_graph", C.c_int, [_P, C.c_int, C.POINTER(C.c_float)]),
     ("lbm_time_steps", C.c_int, [_P, C.c_int, C.POINTER(C.c_float)]),
     ("lbm_last_kernel_time", C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     ("lbm_last_launch_count", C.c_int, [_P, C.POINTER(C.c_longlong)]),

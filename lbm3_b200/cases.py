@@ -8,6 +8,7 @@ lattice viscosity are bit-identical to what the driver's compiler computes.
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 from dataclasses import dataclass
 
@@ -209,3 +210,29 @@ def flow_around_sphere(nx: int = 256, ny: int = 128, nz: int = 128, diameter: fl
     tris = icosphere(subdivisions, 0.5 * diameter, center)
     set_bodies(c, [tris])
     return SphereSetup(c, float(diameter), float(u_in), 1.0, float(c.rho_phys), float(diameter) / 1000.0)
+
+
+def set_hooks(case: A.LbmCase, open_bc=None, initial_condition=None, local_bc=None) -> A.LbmCase:
+    """Attach per-cell driver hooks (getOpenBC, getInitialCondition, getLocalBC)
+    written in Python: each is called as hook(bc, i, j, k, info) with an
+    lbm_bc to fill (the reference's BCStruct defaults, bc.wallID set for
+    getLocalBC) and the level's lbm_grid_info, on the host while the grid is
+    built.  The callbacks are kept alive on the case object."""
+    keep = []
+
+    def wrap(fn):
+        if fn is None:
+            return None
+
+        def tramp(user, bc, i, j, k, info):
+            fn(bc.contents, i, j, k, info.contents)
+        cb = A.CELL_HOOK(tramp)
+        keep.append(cb)
+        return C.cast(cb, C.c_void_p).value
+
+    case.open_bc_hook = wrap(open_bc)
+    case.initial_condition_hook = wrap(initial_condition)
+    case.local_bc_hook = wrap(local_bc)
+    case.hook_user = None
+    case._hook_refs = keep
+    return case

@@ -99,6 +99,12 @@ struct lbm_grids {
     lbm_case c{};
     std::vector<LevelState> levels;
     cudaStream_t stream = nullptr;
+    // CUDA graphs of two consecutive steps, one per starting esotwist parity,
+    // replayed by lbm_update_all_grids / lbm_update_batch (domains without
+    // rotors: their per-step frame is host state); captured on captureStream
+    bool graphsEnabled = true;
+    cudaStream_t captureStream = nullptr;
+    cudaGraphExec_t pairExec[2] = {nullptr, nullptr};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double* scratch = nullptr;
     int* errorFlag = nullptr;  // device word the kernels set when a bounded wait gives up
@@ -118,6 +124,9 @@ struct lbm_grids {
         if (errorFlag) cudaFree(errorFlag);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        for (cudaGraphExec_t e : pairExec)
+            if (e) cudaGraphExecDestroy(e);
+        if (captureStream) cudaStreamDestroy(captureStream);
     }
 };
 
@@ -164,6 +173,7 @@ unsigned long long levelBytes(const lbm::HostLevel& H, int storage) {
     b += bytes(m, sizeof(int)) * 2 + bytes(m, sizeof(int4)) + bytes(m, sizeof(float4)) + bytes(m, sizeof(float)) +
          bytes(sources, sizeof(int)) + bytes(4 * m, sizeof(float));  // cell, info, nbr, target, beta, source, refs
     b += bytes(openChunkCount(H), sizeof(int4)) + (m ? bytes(LBM_MBBC_NORMALS, mbbcTableBytes(storage)) : 0);
+    b += m ? bytes(2, sizeof(int)) : 0;                             // device iteration counter
     if (H.info.gridID == 0) b += bytes(8, sizeof(double)) + bytes(1, sizeof(int));
     return b;
 }
@@ -229,8 +239,15 @@ void updateSingleGrid(lbm_grids* g, LevelState& L) {
         lbm::launchCollideStream(L.dev, flip, g->stream);
     }
     L.info.esotwistFlipper = !flip;  // applyStreaming
-    lbm::launchOpenBoundary(L.dev, L.info.esotwistFlipper, g->stream, L.info.iterationsFinished);
+    lbm::launchOpenBoundary(L.dev, L.info.esotwistFlipper, g->stream);
     lbm::launchPeriodic(L.dev, L.info.esotwistFlipper, g->stream);
+    L.info.iterationsFinished++;
+    L.iterationsSinceTrackerReset++;
+}
+
+// Host bookkeeping of one step whose kernels ran inside a replayed graph.
+void advanceHostState(LevelState& L) {
+    L.info.esotwistFlipper = !L.info.esotwistFlipper;
     L.info.iterationsFinished++;
     L.iterationsSinceTrackerReset++;
 }
@@ -238,6 +255,73 @@ void updateSingleGrid(lbm_grids* g, LevelState& L) {
 void updateAllGrids(lbm_grids* g, int level) {
     updateSingleGrid(g, g->levels[level]);
     // single-level build: no finer level to recurse into (updateGrid.h:391-395)
+}
+
+// Graph replay applies when no level has rotors (their frame is advanced
+// on the host every step) and LBM3_GRAPHS is not "0".
+bool graphable(const lbm_grids* g) {
+    static const bool env = [] {
+        const char* e = std::getenv("LBM3_GRAPHS");
+        return !(e && std::string(e) == "0");
+    }();
+    if (!env || !g->graphsEnabled) return false;
+    for (const LevelState& L : g->levels)
+        if (!L.rotors.empty()) return false;
+    return true;
+}
+
+// The instantiated graph of two steps starting at esotwist parity `parity`
+// (captured on first use; kernel arguments are fixed per grids object).
+cudaGraphExec_t pairGraph(lbm_grids* g, int parity) {
+    if (g->pairExec[parity]) return g->pairExec[parity];
+    if (!g->captureStream) ck(cudaStreamCreateWithFlags(&g->captureStream, cudaStreamNonBlocking), "stream");
+    // capture changes no host state: save and restore the step bookkeeping
+    std::vector<lbm::Info> saved;
+    std::vector<int> savedReset;
+    for (LevelState& L : g->levels) {
+        saved.push_back(L.info);
+        savedReset.push_back(L.iterationsSinceTrackerReset);
+        L.info.esotwistFlipper = parity != 0;
+    }
+    cudaStream_t user = g->stream;
+    g->stream = g->captureStream;
+    cudaGraph_t graph = nullptr;
+    ck(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+        updateAllGrids(g, 0);
+        updateAllGrids(g, 0);
+    } catch (...) {
+        cudaStreamEndCapture(g->stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        g->stream = user;
+        for (size_t l = 0; l < g->levels.size(); ++l) {
+            g->levels[l].info = saved[l];
+            g->levels[l].iterationsSinceTrackerReset = savedReset[l];
+        }
+        throw;
+    }
+    const cudaError_t e = cudaStreamEndCapture(g->stream, &graph);
+    g->stream = user;
+    for (size_t l = 0; l < g->levels.size(); ++l) {
+        g->levels[l].info = saved[l];
+        g->levels[l].iterationsSinceTrackerReset = savedReset[l];
+    }
+    ck(e, "end capture");
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    ck(ei, "graph instantiate");
+    g->pairExec[parity] = exec;
+    return exec;
+}
+
+// Launch two steps of a grids object from its graph, on its stream.
+void launchPair(lbm_grids* g) {
+    const int parity = g->levels[0].info.esotwistFlipper ? 1 : 0;
+    cudaGraphExec_t exec = pairGraph(g, parity);
+    ck(cudaGraphLaunch(exec, g->stream), "graph launch");
+    for (int k = 0; k < 2; ++k)
+        for (LevelState& L : g->levels) advanceHostState(L);
 }
 
 struct DeviceWaitError : std::runtime_error {
@@ -381,6 +465,18 @@ int lbm_plan_read_array(lbm_plan* p, int level, int which, void* host, size_t by
                                          std::to_string(v->size() * sizeof(int)) + ")");
     if (bytes) std::memcpy(host, v->data(), bytes);
     return LBM_OK;
+}
+
+void lbm_default_bc(lbm_bc* bc) {
+    if (!bc) return;
+    const lbm::BC d;
+    bc->dRho = d.dRho; bc->ux = d.ux; bc->uy = d.uy; bc->uz = d.uz;
+    bc->gx = d.gx; bc->gy = d.gy; bc->gz = d.gz;
+    bc->wallID = d.wallID; bc->openBCID = d.openBCID;
+    bc->useIBB = d.useIBB; bc->dirichletU = d.dirichletU; bc->dirichletRho = d.dirichletRho;
+    bc->periodic = d.periodic; bc->nonReflective = d.nonReflective;
+    bc->nonReflectiveBeta = d.nonReflectiveBeta; bc->collisionLimiter = d.collisionLimiter;
+    bc->nuMultiplier = d.nuMultiplier;
 }
 
 int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates) {
@@ -530,6 +626,8 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
                 if (m) ck(cudaMemsetAsync(d.obRhoCum, 0, 2 * m * sizeof(float), s), "memset");
                 d.trackOpen = c->track_open_boundaries ? 1 : 0;
                 d.obChunk = own(upload(chunks, s));
+                d.obCounter = m ? own(devAlloc<int>(2)) : nullptr;
+                if (m) ck(cudaMemsetAsync(d.obCounter, 0, 2 * sizeof(int), s), "memset");
                 d.obChunkCount = static_cast<int>(chunks.size());
                 if (m && c->storage == LBM_STORE_F64) {
                     std::vector<lbm::MbbcDirT<double>> wide(LBM_MBBC_NORMALS);
@@ -556,7 +654,7 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
             // getInitialCondition hook), equilibrium populations on the device
             float4 uni = make_float4(c->ic_dRho, c->ic_ux, c->ic_uy, c->ic_uz);
             float4* dm = nullptr;
-            if (c->ic_kind != LBM_IC_UNIFORM) {
+            if (c->ic_kind != LBM_IC_UNIFORM || c->initial_condition_hook) {
                 std::vector<float4> macro(n);
                 for (long long q = 0; q < n; ++q) {
                     const lbm::BC ic = lbm::evalInitialCondition(*c, H.info, H.I[q], H.J[q], H.K[q]);
@@ -575,6 +673,11 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
         }
         ck(cudaStreamSynchronize(s), "build sync");
         if (fluidUpdates) *fluidUpdates = host.fluidUpdatesPerIteration;
+        // the driver's hooks are evaluated during the build only
+        g->c.open_bc_hook = nullptr;
+        g->c.initial_condition_hook = nullptr;
+        g->c.local_bc_hook = nullptr;
+        g->c.hook_user = nullptr;
     });
     if (rc != LBM_OK) {
         delete g;
@@ -599,7 +702,10 @@ int lbm_set_stream(lbm_grids* g, void* stream) {
 int lbm_update_all_grids(lbm_grids* g, int steps) {
     if (!g || steps < 0) return fail(LBM_ERR_INVALID, "lbm_update_all_grids: bad argument");
     return guarded("lbm_update_all_grids", [&] {
-        for (int s = 0; s < steps; ++s) updateAllGrids(g, 0);
+        int s = 0;
+        if (graphable(g))
+            for (; s + 2 <= steps; s += 2) launchPair(g);
+        for (; s < steps; ++s) updateAllGrids(g, 0);
         ck(cudaGetLastError(), "step launch");
     });
 }
@@ -609,9 +715,47 @@ int lbm_update_batch(lbm_grids* const* grids, int count, int steps) {
     for (int q = 0; q < count; ++q)
         if (!grids[q]) return fail(LBM_ERR_INVALID, "lbm_update_batch: null grids in the batch");
     return guarded("lbm_update_batch", [&] {
-        for (int s = 0; s < steps; ++s)
+        // step pairs from each domain's graph, interleaved across domains;
+        // domains without graphs (rotors) and a trailing odd step launch directly
+        int s = 0;
+        for (; s + 2 <= steps; s += 2)
+            for (int q = 0; q < count; ++q) {
+                if (graphable(grids[q])) {
+                    launchPair(grids[q]);
+                } else {
+                    updateAllGrids(grids[q], 0);
+                    updateAllGrids(grids[q], 0);
+                }
+            }
+        for (; s < steps; ++s)
             for (int q = 0; q < count; ++q) updateAllGrids(grids[q], 0);
         ck(cudaGetLastError(), "step launch");
+    });
+}
+
+int lbm_set_graphs(lbm_grids* g, int enabled) {
+    if (!g) return fail(LBM_ERR_INVALID, "lbm_set_graphs: null grids");
+    g->graphsEnabled = enabled != 0;
+    return LBM_OK;
+}
+
+int lbm_time_steps_graph(lbm_grids* g, int steps, float* ms) {
+    if (!g || !ms || steps < 0) return fail(LBM_ERR_INVALID, "lbm_time_steps_graph: bad argument");
+    return guarded("lbm_time_steps_graph", [&] {
+        // capture outside the timed region
+        if (graphable(g) && steps >= 2) {
+            pairGraph(g, 0);
+            pairGraph(g, 1);
+        }
+        ck(cudaEventRecord(g->ev0, g->stream), "event");
+        int s = 0;
+        if (graphable(g))
+            for (; s + 2 <= steps; s += 2) launchPair(g);
+        for (; s < steps; ++s) updateAllGrids(g, 0);
+        ck(cudaEventRecord(g->ev1, g->stream), "event");
+        ck(cudaEventSynchronize(g->ev1), "event sync");
+        checkDeviceFlag(g);
+        ck(cudaEventElapsedTime(ms, g->ev0, g->ev1), "elapsed");
     });
 }
 
@@ -1294,6 +1438,12 @@ int lbm_load_state(lbm_grids* g, const void* host, size_t bytes) {
             for (const StateRegion& r : stateRegions(L)) {
                 ck(cudaMemcpyAsync(r.ptr, p, r.bytes, cudaMemcpyHostToDevice, g->stream), "copy");
                 p += r.bytes;
+            }
+            if (L.dev.obCounter) {
+                const int counter[2] = {L.info.iterationsFinished, 0};
+                ck(cudaMemcpyAsync(L.dev.obCounter, counter, sizeof(counter), cudaMemcpyHostToDevice, g->stream),
+                   "copy");
+                ck(cudaStreamSynchronize(g->stream), "sync");
             }
         }
         ck(cudaStreamSynchronize(g->stream), "sync");

@@ -35,7 +35,62 @@ int winningFace(const lbm_case& c, const Info& info, int i, int j, int k) {
 
 }  // namespace
 
+namespace {
+
+lbm_bc toHookBC(const BC& b) {
+    lbm_bc h;
+    h.dRho = b.dRho; h.ux = b.ux; h.uy = b.uy; h.uz = b.uz;
+    h.gx = b.gx; h.gy = b.gy; h.gz = b.gz;
+    h.wallID = b.wallID; h.openBCID = b.openBCID;
+    h.useIBB = b.useIBB; h.dirichletU = b.dirichletU; h.dirichletRho = b.dirichletRho;
+    h.periodic = b.periodic; h.nonReflective = b.nonReflective;
+    h.nonReflectiveBeta = b.nonReflectiveBeta; h.collisionLimiter = b.collisionLimiter;
+    h.nuMultiplier = b.nuMultiplier;
+    return h;
+}
+
+BC fromHookBC(const lbm_bc& h) {
+    BC b;
+    b.dRho = h.dRho; b.ux = h.ux; b.uy = h.uy; b.uz = h.uz;
+    b.gx = h.gx; b.gy = h.gy; b.gz = h.gz;
+    b.wallID = h.wallID; b.openBCID = h.openBCID;
+    b.useIBB = h.useIBB != 0; b.dirichletU = h.dirichletU != 0; b.dirichletRho = h.dirichletRho != 0;
+    b.periodic = h.periodic != 0; b.nonReflective = h.nonReflective != 0;
+    b.nonReflectiveBeta = h.nonReflectiveBeta; b.collisionLimiter = h.collisionLimiter;
+    b.nuMultiplier = h.nuMultiplier;
+    return b;
+}
+
+// The level's InfoStruct as a hook sees it.
+lbm_grid_info hookInfo(const Info& in) {
+    lbm_grid_info g{};
+    g.grid_id = in.gridID;
+    g.cell_count = in.cellCount;
+    g.cell_count_x = in.nx;
+    g.cell_count_y = in.ny;
+    g.cell_count_z = in.nz;
+    g.res = in.res;
+    g.ox = in.ox;
+    g.oy = in.oy;
+    g.oz = in.oz;
+    g.nu = in.nu;
+    g.dt_phys = in.dtPhys;
+    g.iterations_finished = in.iterationsFinished;
+    return g;
+}
+
+// Call a driver hook on a BCStruct that starts from `start`.
+BC callHook(const lbm_case& c, lbm_cell_hook hook, const BC& start, const Info& info, int i, int j, int k) {
+    lbm_bc h = toHookBC(start);
+    const lbm_grid_info gi = hookInfo(info);
+    hook(c.hook_user, &h, i, j, k, &gi);
+    return fromHookBC(h);
+}
+
+}  // namespace
+
 BC evalOpenBC(const lbm_case& c, const Info& info, int i, int j, int k) {
+    if (c.open_bc_hook) return callHook(c, c.open_bc_hook, BC{}, info, i, j, k);
     BC bc;
     const int f = winningFace(c, info, i, j, k);
     if (f < 0) return bc;
@@ -64,6 +119,7 @@ void evalLocalBC(const lbm_case& c, BC& bc) {
 }
 
 BC evalInitialCondition(const lbm_case& c, const Info& info, int i, int j, int k) {
+    if (c.initial_condition_hook) return callHook(c, c.initial_condition_hook, BC{}, info, i, j, k);
     BC bc;
     if (c.ic_kind == LBM_IC_TAYLOR_GREEN) {
         // cases/taylorGreenVortex/taylorGreenVortexMain.cu:66-87
@@ -658,7 +714,15 @@ void buildWalls(const lbm_case& c, HostLevel& L, const std::vector<Triangles>& b
         L.wallData[w] = data;
         // getLocalBC wall velocity of the body (evaluated at the fluid cell centre)
         const lbm_body& body = c.body[ids[w]];
-        if (body.motion == LBM_WALL_ROTATING) {
+        if (c.local_bc_hook) {
+            const int cell = L.wallIndex[w];
+            BC start;
+            start.wallID = ids[w];
+            const BC bc = callHook(c, c.local_bc_hook, start, in, L.I[cell], L.J[cell], L.K[cell]);
+            L.wallVelocity[static_cast<size_t>(0) * nw + w] = bc.ux;
+            L.wallVelocity[static_cast<size_t>(1) * nw + w] = bc.uy;
+            L.wallVelocity[static_cast<size_t>(2) * nw + w] = bc.uz;
+        } else if (body.motion == LBM_WALL_ROTATING) {
             const int cell = L.wallIndex[w];
             const float x = L.I[cell] * in.res + in.ox - body.origin[0];
             const float y = L.J[cell] * in.res + in.oy - body.origin[1];
@@ -832,7 +896,11 @@ void buildSegments(HostLevel& L) {
 void buildDomain(const lbm_case& c, HostDomain& out) {
     validateCase(c);
     out.c = c;
-    out.c.body_count = 0;  // triangle pointers are not kept past this call
+    out.c.body_count = 0;  // triangle pointers and hooks are not kept past this call
+    out.c.open_bc_hook = nullptr;
+    out.c.initial_condition_hook = nullptr;
+    out.c.local_bc_hook = nullptr;
+    out.c.hook_user = nullptr;
     for (int r = 0; r < LBM_MAX_ROTORS; ++r) out.c.rotor[r].triangles = nullptr;
     out.levels.assign(1, HostLevel{});
     HostLevel& L = out.levels[0];

@@ -924,9 +924,25 @@ __device__ __forceinline__ V nonReflectiveUNormal(V uTarget, V dRhoZ, V dRhoRef)
 #ifndef LBM3_OPEN_MIN_BLOCKS
 #define LBM3_OPEN_MIN_BLOCKS 8
 #endif
+// The open-boundary launch's last CTA advances the device iteration count.
+__device__ __forceinline__ void openBoundaryDone(const DevLevel& g) {
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(g.obCounter + 1, 1) == int(gridDim.x) - 1) {
+            g.obCounter[1] = 0;
+            g.obCounter[0] += 1;
+            __threadfence();
+        }
+    }
+}
+
 template <bool F, class S>
-__global__ void __launch_bounds__(kOpenChunk, LBM3_OPEN_MIN_BLOCKS) openBoundary(DevLevel g, int iterationsFinished) {
+__global__ void __launch_bounds__(kOpenChunk, LBM3_OPEN_MIN_BLOCKS) openBoundary(DevLevel g) {
     using V = Real<S>;
+    // the level's finished iterations live on the device (obCounter[0]), so
+    // a captured step graph replays with the right count; the last CTA of the
+    // launch advances it once every CTA has read it
+    const int iterationsFinished = __ldcg(g.obCounter);
     __shared__ MbbcDirT<V> T;
     const int4 chunk = __ldg(g.obChunk + blockIdx.x);  // {first, count, normal row, unknown mask}
     {
@@ -996,11 +1012,19 @@ __global__ void __launch_bounds__(kOpenChunk, LBM3_OPEN_MIN_BLOCKS) openBoundary
         }
         dRho = mbbcRestoreRho(T, ux, uy, uz, f) - V(1);
     }
-    mbbcApply(T, dRho + V(1), ux, uy, uz, f);
-#pragma unroll
-    for (int d = 0; d < 27; ++d) {
-        if (!(unknown >> d & 1u)) continue;
-        Store<S>::st(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)], f[d] - weightT<V>(d));
+    // closure: one row per unknown population, written to its pre-collision
+    // slot (F ? inv(d) : d) in the neighbour offset by max(0, -c_d)
+    V meq[kMbbcMoments];
+    mbbcMomentsEq(dRho + V(1), ux, uy, uz, meq);
+#pragma unroll 1
+    for (int r = 0; r < T.nu; ++r) {
+        const V v = mbbcUnknown(T, r, meq, f);
+        const int k = T.unknownNbr[r];
+        const int sel = k >> 1;
+        int c = sel == 0 ? rows.x : sel == 1 ? rows.y : sel == 2 ? rows.z : rows.w;
+        if (k & 1) c = c + 1 < n ? c + 1 : 0;
+        const int slot = F ? T.unknownInv[r] : T.unknownDir[r];
+        Store<S>::st(base + (long long)slot * g.stride + c, v - T.unknownW[r]);
     }
     // reference values: exponential average whose weight decays with the
     // iteration count; below 1e-5 the weight is tripled and the update runs
@@ -1020,7 +1044,9 @@ __global__ void __launch_bounds__(kOpenChunk, LBM3_OPEN_MIN_BLOCKS) openBoundary
         g.obRhoCum[idx] += float(dRho);
         g.obUnCum[idx] += uNormal;
     }
+    openBoundaryDone(g);  // thread 0 is always active
 }
+
 
 // Initial reference values of the open boundary (applyInitialCondition.h:43-81).
 template <bool F, class S>
@@ -1309,8 +1335,8 @@ template <bool F, class S> struct RunPeriodic {
     }
 };
 template <bool F, class S> struct RunOpen {
-    static void run(const DevLevel& g, cudaStream_t s, int iterationsFinished) {
-        if (g.obChunkCount > 0) openBoundary<F, S><<<g.obChunkCount, kOpenChunk, 0, s>>>(g, iterationsFinished);
+    static void run(const DevLevel& g, cudaStream_t s) {
+        if (g.obChunkCount > 0) openBoundary<F, S><<<g.obChunkCount, kOpenChunk, 0, s>>>(g);
     }
 };
 template <bool F, class S> struct RunOpenInit {
@@ -1361,8 +1387,8 @@ template <bool F, class S> struct RunScatter {
 
 void LBM3_FN(launchCollideStream)(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunCollide>(g, flip, s); }
 void LBM3_FN(launchPeriodic)(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunPeriodic>(g, flip, s); }
-void LBM3_FN(launchOpenBoundary)(const DevLevel& g, bool flip, cudaStream_t s, int iterationsFinished) {
-    dispatch<RunOpen>(g, flip, s, iterationsFinished);
+void LBM3_FN(launchOpenBoundary)(const DevLevel& g, bool flip, cudaStream_t s) {
+    dispatch<RunOpen>(g, flip, s);
 }
 void LBM3_FN(launchOpenBoundaryInit)(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunOpenInit>(g, flip, s); }
 void LBM3_FN(launchInit)(const DevLevel& g, bool flip, cudaStream_t s, const float4* macro, float4 uniform) {

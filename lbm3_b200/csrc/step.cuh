@@ -83,6 +83,7 @@ struct DevLevel {
     // cells are grouped by outer normal; each chunk {first, count, normal row,
     // unknown-direction mask} is one CTA of the boundary kernel
     const int4* obChunk;
+    int* obCounter;                   // [2] iterations finished, CTAs done in the running launch
     int obChunkCount;
     const void* obTables;             // [26] direction-indexed closure tables (MbbcDirT of the
                                       // arithmetic type)

@@ -14,8 +14,8 @@ namespace lbm {
 
 void launchCollideStream(const DevLevel& g, bool flip, cudaStream_t s) { LBM3_BY_STORAGE(launchCollideStream, g, flip, s) }
 void launchPeriodic(const DevLevel& g, bool flip, cudaStream_t s) { LBM3_BY_STORAGE(launchPeriodic, g, flip, s) }
-void launchOpenBoundary(const DevLevel& g, bool flip, cudaStream_t s, int iterationsFinished) {
-    LBM3_BY_STORAGE(launchOpenBoundary, g, flip, s, iterationsFinished)
+void launchOpenBoundary(const DevLevel& g, bool flip, cudaStream_t s) {
+    LBM3_BY_STORAGE(launchOpenBoundary, g, flip, s)
 }
 void launchOpenBoundaryInit(const DevLevel& g, bool flip, cudaStream_t s) {
     LBM3_BY_STORAGE(launchOpenBoundaryInit, g, flip, s)

@@ -14,7 +14,8 @@ void launchCollideStream(const DevLevel& g, bool flip, cudaStream_t s);
 // kernels one updateSingleGrid launches for this level
 int stepLaunchCount(const DevLevel& g);
 void launchPeriodic(const DevLevel& g, bool flip, cudaStream_t s);
-void launchOpenBoundary(const DevLevel& g, bool flip, cudaStream_t s, int iterationsFinished);
+// K2; reads and advances the device iteration count (DevLevel::obCounter)
+void launchOpenBoundary(const DevLevel& g, bool flip, cudaStream_t s);
 void launchOpenBoundaryInit(const DevLevel& g, bool flip, cudaStream_t s);
 void launchInit(const DevLevel& g, bool flip, cudaStream_t s, const float4* macro, float4 uniform);
 void launchKineticEnergy(const DevLevel& g, bool flip, cudaStream_t s, double* out);
@@ -35,7 +36,7 @@ void launchCollideBatch(float* f, int n, const CollisionConsts& P, float gx, flo
 #define LBM3_DECLARE_STORAGE_LAUNCHERS(SUF)                                                                      \
     void launchCollideStream##SUF(const DevLevel& g, bool flip, cudaStream_t s);                               \
     void launchPeriodic##SUF(const DevLevel& g, bool flip, cudaStream_t s);                                    \
-    void launchOpenBoundary##SUF(const DevLevel& g, bool flip, cudaStream_t s, int iterationsFinished);        \
+    void launchOpenBoundary##SUF(const DevLevel& g, bool flip, cudaStream_t s);                                \
     void launchOpenBoundaryInit##SUF(const DevLevel& g, bool flip, cudaStream_t s);                            \
     void launchInit##SUF(const DevLevel& g, bool flip, cudaStream_t s, const float4* macro, float4 uniform);   \
     void launchKineticEnergy##SUF(const DevLevel& g, bool flip, cudaStream_t s, double* out);                  \

@@ -165,6 +165,15 @@ class Grids:
         A.check(A.lib().lbm_time_steps(self._h, int(steps), C.byref(ms)))
         return ms.value
 
+    def time_steps_graph(self, steps: int) -> float:
+        """Run `steps` coarse steps as replayed CUDA graphs; returns device ms."""
+        ms = C.c_float()
+        A.check(A.lib().lbm_time_steps_graph(self._h, int(steps), C.byref(ms)))
+        return ms.value
+
+    def set_graphs(self, enabled: bool):
+        A.check(A.lib().lbm_set_graphs(self._h, int(bool(enabled))))
+
     def last_launch_count(self) -> int:
         """Every kernel launch of the last time_steps call."""
         n = C.c_longlong()

@@ -59,6 +59,7 @@ class OGrid(C.Structure):
         ("face", FaceBC * 6), ("openCount", C.c_int), ("openIndex", _IP),
         ("openRef", C.POINTER(C.c_float)), ("openCum", C.POINTER(C.c_float)), ("trackOpen", C.c_int),
         ("rotorCount", C.c_int), ("rotors", C.c_void_p), ("trackRotorForce", C.c_int),
+        ("openHook", C.c_void_p), ("hookUser", C.c_void_p),
     ]
 
 

@@ -510,8 +510,49 @@ static obc open_bc_faces(const lbm_face_bc* face, const ogrid* g, int i, int j, 
     return bc;
 }
 
+/* A driver hook (getOpenBC / getInitialCondition / getLocalBC) on a
+ * BCStruct that starts from `bc`, with the level's info. */
+static obc call_hook(lbm_cell_hook hook, void* user, obc bc, const ogrid* g, int i, int j, int k) {
+    lbm_bc h;
+    h.dRho = bc.dRho; h.ux = bc.ux; h.uy = bc.uy; h.uz = bc.uz;
+    h.gx = bc.gx; h.gy = bc.gy; h.gz = bc.gz;
+    h.wallID = bc.wallID; h.openBCID = bc.openBCID;
+    h.useIBB = bc.useIBB; h.dirichletU = bc.dirichletU; h.dirichletRho = bc.dirichletRho;
+    h.periodic = bc.periodic; h.nonReflective = bc.nonReflective;
+    h.nonReflectiveBeta = bc.nonReflectiveBeta; h.collisionLimiter = bc.collisionLimiter;
+    h.nuMultiplier = bc.nuMultiplier;
+    lbm_grid_info info;
+    memset(&info, 0, sizeof(info));
+    info.grid_id = g->gridID;
+    info.cell_count = g->cellCount;
+    info.cell_count_x = g->nx; info.cell_count_y = g->ny; info.cell_count_z = g->nz;
+    info.res = g->res; info.ox = g->ox; info.oy = g->oy; info.oz = g->oz;
+    info.nu = g->nu; info.dt_phys = g->dtPhys;
+    info.iterations_finished = g->iterationsFinished;
+    hook(user, &h, i, j, k, &info);
+    obc r;
+    r.dRho = h.dRho; r.ux = h.ux; r.uy = h.uy; r.uz = h.uz;
+    r.gx = h.gx; r.gy = h.gy; r.gz = h.gz;
+    r.wallID = h.wallID; r.openBCID = h.openBCID;
+    r.useIBB = h.useIBB != 0; r.dirichletU = h.dirichletU != 0; r.dirichletRho = h.dirichletRho != 0;
+    r.periodic = h.periodic != 0; r.nonReflective = h.nonReflective != 0;
+    r.nonReflectiveBeta = h.nonReflectiveBeta; r.collisionLimiter = h.collisionLimiter;
+    r.nuMultiplier = h.nuMultiplier;
+    return r;
+}
+
+static obc open_bc_of(const ogrid* g, int i, int j, int k) {
+    if (g->openHook) {
+        obc bc;
+        oracle_default_bc(&bc);
+        return call_hook(g->openHook, g->hookUser, bc, g, i, j, k);
+    }
+    return open_bc_faces(g->face, g, i, j, k);
+}
+
 static obc open_bc(const lbm_case* c, const ogrid* g, int i, int j, int k) {
-    return open_bc_faces(c->face, g, i, j, k);
+    (void)c;
+    return open_bc_of(g, i, j, k);
 }
 
 static int cmp_kji(const void* a, const void* b) {
@@ -838,8 +879,16 @@ static void build_walls(const lbm_case* c, ogrid* g, const ostl* bodies, const o
         g->wallData[w] = data;
         const int cell = g->wallIndex[w];
         float u[3];
-        body_wall_velocity(&c->body[ids[w]], g->I[cell] * g->res + g->ox, g->J[cell] * g->res + g->oy,
-                           g->K[cell] * g->res + g->oz, g->dtPhys, g->res, u);
+        if (c->local_bc_hook) {
+            obc bc;
+            oracle_default_bc(&bc);
+            bc.wallID = ids[w];
+            bc = call_hook(c->local_bc_hook, c->hook_user, bc, g, g->I[cell], g->J[cell], g->K[cell]);
+            u[0] = bc.ux; u[1] = bc.uy; u[2] = bc.uz;
+        } else {
+            body_wall_velocity(&c->body[ids[w]], g->I[cell] * g->res + g->ox, g->J[cell] * g->res + g->oy,
+                               g->K[cell] * g->res + g->oz, g->dtPhys, g->res, u);
+        }
         for (int a = 0; a < 3; ++a) g->wallVel[(size_t)a * nw + w] = u[a];
     }
     free(ids);
@@ -1055,6 +1104,8 @@ static void init_info(const lbm_case* c, ogrid* g) {
     g->trackOpen = c->track_open_boundaries;
     g->trackRotorForce = c->track_rotor_force;
     memcpy(g->face, c->face, sizeof(g->face));
+    g->openHook = c->open_bc_hook;
+    g->hookUser = c->hook_user;
 }
 
 /* Open-boundary lists (gridBuilderFunctions.h:1276-1330): boundary cells that
@@ -1070,7 +1121,7 @@ static void build_open_list(ogrid* g) {
         int i, j, k;
         get_ijk(g, q, &i, &j, &k);
         if (!(i == 0 || i == g->nx - 1 || j == 0 || j == g->ny - 1 || k == 0 || k == g->nz - 1)) continue;
-        const obc bc = open_bc_faces(g->face, g, i, j, k);
+        const obc bc = open_bc_of(g, i, j, k);
         if (bc.periodic) continue;
         id[q] = bc.openBCID;
         if (id[q] > maxId) maxId = id[q];
@@ -1114,7 +1165,9 @@ static void apply_initial_condition(const lbm_case* c, ogrid* g) {
         oracle_default_bc(&bc);
         int ci, cj, ck;
         get_ijk(g, q, &ci, &cj, &ck);
-        if (c->ic_kind == LBM_IC_TAYLOR_GREEN) {
+        if (c->initial_condition_hook) {
+            bc = call_hook(c->initial_condition_hook, c->hook_user, bc, g, ci, cj, ck);
+        } else if (c->ic_kind == LBM_IC_TAYLOR_GREEN) {
             const float x = ci * g->res + g->ox, y = cj * g->res + g->oy, z = ck * g->res + g->oz;
             const float X = x / c->tgv_length, Y = y / c->tgv_length, Z = z / c->tgv_length;
             const float u0 = c->tgv_u0;

@@ -86,6 +86,9 @@ typedef struct ogrid {
     int rotorCount;
     void* rotors;                    /* orotor[4], private to lbm_oracle.c */
     int trackRotorForce;
+    /* the case's getOpenBC hook (NULL: the face table) */
+    lbm_cell_hook openHook;
+    void* hookUser;
 } ogrid;
 
 /* buildGrids (include/gridBuilderFunctions.h:1577-1670) for one level,
