@@ -37,7 +37,10 @@ def test_sphere_configuration_fields_and_drag():
 
 def test_tgv64_plain_method_full_run():
     """The plain-method configuration for its 1000 steps: fields to the FP32
-    bar and the kinetic-energy history to 1e-6."""
+    bar, and the kinetic-energy history to twice that bar (the energy is
+    quadratic in the velocity, so a relative velocity error e moves it by at
+    most about 2e; the GPU contracts multiply-adds and the oracle does not, so
+    the two drift apart by rounding)."""
     s = L.tgv_plain_method()
     o = O.OracleGrid(s.case)
     with L.build_grids(s.case) as g:
@@ -51,7 +54,7 @@ def test_tgv64_plain_method_full_run():
         assert e_rho < FIELD_REL_L2 and e_u < FIELD_REL_L2, (e_rho, e_u)
         assert g.info().iterations_finished == 1000
     eg, eo = np.array(eg), np.array(eo)
-    assert np.max(np.abs(eg - eo) / eo) < 1e-6
+    assert np.max(np.abs(eg - eo) / eo) < 2 * FIELD_REL_L2
     # the vortex decays
     assert eg[-1] < eg[0]
     o.close()
