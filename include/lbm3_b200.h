@@ -96,6 +96,18 @@ extern "C" {
 #define LBM_ARRAY_ROTOR_BASE   32
 #define LBM_ARRAY_OPEN_CUMULATIVE 20 /* float [2][openBCCount] dRhoCumulativeArray,
                                      uNormalCumulativeArray since the last tracker reset */
+/* Interfaces between a level (coarse) and the next finer one, read on the
+ * coarse level (InterfaceStruct, include/types.h:198-200): */
+#define LBM_ARRAY_F2C_INDEX      21 /* int32 [f2cCount] FineToCoarseInterface.indexArray (coarse cells) */
+#define LBM_ARRAY_F2C_CHILD      22 /* int32 [f2cCount] childMapArray (fine cell (2i,2j,2k))          */
+#define LBM_ARRAY_C2F_INDEX      23 /* int32 [c2fCount] CoarseToFineInterface.indexArray: coarse
+                                       stencil corner (the block's -x,-y,-z coarse cell)           */
+#define LBM_ARRAY_C2F_CHILD      24 /* int32 [c2fCount] childMapArray: fine cell (2i+1,2j+1,2k+1)   */
+#define LBM_ARRAY_LEFTOVER_INDEX 25 /* int32 [leftoverCount] leftoverIndexArray (fine cells)        */
+#define LBM_ARRAY_LEFTOVER_PARENT 26 /* int32 [leftoverCount] leftoverParentMapArray (coarse cells)  */
+#define LBM_ARRAY_LEFTOVER_NBR   27 /* int32 [3][leftoverCount] leftoverNbrI/J/KArray: the coarse
+                                       neighbour on the fine cell's side, or -(cell)-1 for the
+                                       opposite side                                               */
 
 /* A rotor forced towards rigid rotation (RotorStruct, include/types.h:206-219):
  * triangles of its surface at angle 0 (mm), the axis it turns about (parallel
@@ -147,6 +159,8 @@ typedef struct lbm_face_bc {
 
 #define LBM_MAX_BODIES 16     /* wallID is packed into 5 bits of wallData      */
 
+#define LBM_MAX_LEVELS 4      /* grid levels of one domain, refinement ratio 2  */
+
 /* One static body: a triangle soup in mm (the reference's gridStaticSTLs
  * entry; its index is the body's wallID). */
 typedef struct lbm_body {
@@ -173,10 +187,15 @@ struct lbm_grid_info;
  * getLocalBC, include/updateGrid.h:95,256), called on the host while the grid
  * is built, with the cell's (i, j, k) on its level and the level's info. */
 typedef void (*lbm_cell_hook)(void* user, lbm_bc* bc, int i, int j, int k, const struct lbm_grid_info* info);
+/* getRefinementModifier (include/markerFunctions.h:254-271), called on the host
+ * for every cell of every level but the finest while the grids are built:
+ * `*mark` arrives as the deep-refinement marker from the walls (and from
+ * lbm_case.refine_box) and the hook may set it (1) or clear it (0). */
+typedef void (*lbm_refinement_hook)(void* user, int i, int j, int k, int* mark, const struct lbm_grid_info* info);
 
 typedef struct lbm_case {
     /* compile-time constants of a reference driver */
-    int   grid_level_count;     /* GRID_LEVEL_COUNT (1 in this build)          */
+    int   grid_level_count;     /* GRID_LEVEL_COUNT, 1 .. LBM_MAX_LEVELS       */
     int   wall_refinement_count;/* WALL_REFINEMENT_COUNT                       */
     float res_global;           /* RES_GLOBAL, mm                              */
     float nu_phys;              /* NU_PHYS, m^2/s                              */
@@ -219,11 +238,23 @@ typedef struct lbm_case {
      * local_bc_hook gives the wall velocity (bc.ux, uy, uz) of every
      * wall-adjacent cell, called with bc.wallID = its body (the per-wallID
      * branch of getLocalBC).  The kernels keep the collision limiter, nu
-     * multiplier and body force uniform (the fields above). */
+     * multiplier, body force and IBB switch uniform over a level: the fields
+     * above, or, with a local_bc_hook, what the hook returns for them when it
+     * is called once per level for a fluid cell (wallID -1) at the level's
+     * first cell (so a hook may, e.g., pick another limiter on level 0). */
     lbm_cell_hook open_bc_hook;
     lbm_cell_hook initial_condition_hook;
     lbm_cell_hook local_bc_hook;
     void*         hook_user;
+
+    /* Refinement (getRefinementModifier) on a level L < grid_level_count - 1:
+     * a cell whose centre lies strictly inside refine_box[L] (xMin, yMin, zMin,
+     * xMax, yMax, zMax in mm; a box with min >= max on some axis marks
+     * nothing) is deep-refined, in addition to the cells the walls mark
+     * (WALL_REFINEMENT_COUNT spreads around every finer level's walls);
+     * refinement_hook, if set, then sees the marker and may change it. */
+    float refine_box[LBM_MAX_LEVELS][6];
+    lbm_refinement_hook refinement_hook;
 } lbm_case;
 
 /* The reference's BCStruct defaults (include/types.h:131-136). */
@@ -243,6 +274,10 @@ typedef struct lbm_grid_info {
     int   storage;
     float res, ox, oy, oz, nu, dt_phys;
     unsigned long long grid_memory_bytes;
+    /* interfaces to the next finer level (0 on the finest) */
+    int   f2c_count;            /* FineToCoarseInterface.interfaceCount        */
+    int   c2f_count;            /* CoarseToFineInterface.interfaceCount (blocks) */
+    int   leftover_count;       /* CoarseToFineInterface.leftoverCount         */
 } lbm_grid_info;
 
 typedef struct lbm_grids lbm_grids;   /* opaque: all levels of one domain */

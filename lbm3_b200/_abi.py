@@ -75,6 +75,14 @@ ARRAY_OPEN_INDEX = 17
 ARRAY_OPEN_SOURCE = 18
 ARRAY_OPEN_REFERENCE = 19
 ARRAY_OPEN_CUMULATIVE = 20
+ARRAY_F2C_INDEX = 21
+ARRAY_F2C_CHILD = 22
+ARRAY_C2F_INDEX = 23
+ARRAY_C2F_CHILD = 24
+ARRAY_LEFTOVER_INDEX = 25
+ARRAY_LEFTOVER_PARENT = 26
+ARRAY_LEFTOVER_NBR = 27
+LBM_MAX_LEVELS = 4
 LBM_ERR_DEVICE_WAIT = -7
 
 
@@ -122,6 +130,7 @@ class LbmCase(C.Structure):
         ("rotor_count", C.c_int), ("rotor", LbmRotor * LBM_MAX_ROTORS), ("track_rotor_force", C.c_int),
         ("open_bc_hook", C.c_void_p), ("initial_condition_hook", C.c_void_p), ("local_bc_hook", C.c_void_p),
         ("hook_user", C.c_void_p),
+        ("refine_box", (C.c_float * 6) * LBM_MAX_LEVELS), ("refinement_hook", C.c_void_p),
     ]
 
 
@@ -146,6 +155,7 @@ class LbmGridInfo(C.Structure):
         ("esotwist_flipper", C.c_int), ("iterations_finished", C.c_int), ("storage", C.c_int),
         ("res", C.c_float), ("ox", C.c_float), ("oy", C.c_float), ("oz", C.c_float),
         ("nu", C.c_float), ("dt_phys", C.c_float), ("grid_memory_bytes", C.c_ulonglong),
+        ("f2c_count", C.c_int), ("c2f_count", C.c_int), ("leftover_count", C.c_int),
     ]
 
     def as_dict(self) -> dict:
@@ -154,6 +164,9 @@ class LbmGridInfo(C.Structure):
 
 # lbm_cell_hook: void (*)(void* user, lbm_bc* bc, int i, int j, int k, const lbm_grid_info* info)
 CELL_HOOK = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(LbmBC), C.c_int, C.c_int, C.c_int, C.POINTER(LbmGridInfo))
+# lbm_refinement_hook: void (*)(void* user, int i, int j, int k, int* mark, const lbm_grid_info* info)
+REFINEMENT_HOOK = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int),
+                              C.POINTER(LbmGridInfo))
 
 # (name, restype, argtypes) of every exported function
 _P = C.c_void_p

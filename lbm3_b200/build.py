@@ -30,7 +30,7 @@ SOURCES = [
     ("geometry.cpp", "geometry.o", []),
     ("energy_noalloc.cu", "energy_noalloc.o", []),
 ]
-HEADERS = ["lattice.h", "cumulant.cuh", "step.cuh", "step_launch.h", "builder.h", "geometry.h", "mbbc.h",
+HEADERS = ["lattice.h", "cumulant.cuh", "interface.cuh", "step.cuh", "step_launch.h", "builder.h", "geometry.h", "mbbc.h",
            "mbbc_tables.h", "energy_noalloc.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [

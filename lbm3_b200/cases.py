@@ -103,6 +103,26 @@ def taylor_green(cells_per_domain: int = 128, reynolds: float = 1600.0, mach: fl
                     float(ref_time), float(dt), iters)
 
 
+def set_refine_box(case: A.LbmCase, level: int, lo, hi) -> A.LbmCase:
+    """Refine the cells of `level` whose centres lie strictly inside the box
+    [lo, hi] (mm) to the next level (getRefinementModifier as a table)."""
+    for a in range(3):
+        case.refine_box[level][a] = f32(lo[a])
+        case.refine_box[level][a + 3] = f32(hi[a])
+    return case
+
+
+def taylor_green_refined(cells_per_domain: int = 128, storage: int = A.LBM_STORE_F32, **kw) -> TGVSetup:
+    """The refined Taylor–Green run of the reference driver: two levels, the
+    central cube [-pi L/2, pi L/2]^3 on the fine level
+    (cases/taylorGreenVortex/taylorGreenVortexMain.cu:8-12, :53-67)."""
+    s = taylor_green(cells_per_domain, storage=storage, **kw)
+    s.case.grid_level_count = 2
+    half = f32(f32(0.25) * f32(s.domain_length))
+    set_refine_box(s.case, 0, (-half,) * 3, (half,) * 3)
+    return s
+
+
 def tgv_plain_method(storage: int = A.LBM_STORE_F32) -> TGVSetup:
     """Plain-method Taylor–Green: periodic 64^3, u0 = 0.05, nu = 0.01, 1000 steps."""
     s = taylor_green(64, u_lattice=0.05, nu_lattice=0.01, storage=storage)
@@ -212,12 +232,61 @@ def flow_around_sphere(nx: int = 256, ny: int = 128, nz: int = 128, diameter: fl
     return SphereSetup(c, float(diameter), float(u_in), 1.0, float(c.rho_phys), float(diameter) / 1000.0)
 
 
-def set_hooks(case: A.LbmCase, open_bc=None, initial_condition=None, local_bc=None) -> A.LbmCase:
+@dataclass
+class MultilevelSphereSetup:
+    case: A.LbmCase
+    diameter_finest: float    # sphere diameter in finest-level cells
+    u_in: float
+    reynolds: float
+
+
+def multilevel_sphere(nx: int = 128, ny: int = 64, nz: int = 64, levels: int = 3, diameter_finest: float = 48.0,
+                      reynolds: float = 300.0, u_in: float = 0.04, wall_refinement_count: int = 2,
+                      subdivisions: int = 5, storage: int = A.LBM_STORE_F32,
+                      fine_boxes=((96, 64, 64), (112, 80, 80))) -> MultilevelSphereSetup:
+    """Flow around a sphere on nested refinement levels (ratio 2): an
+    nx*ny*nz base channel (see :func:`open_channel`), the sphere of
+    `diameter_finest` finest-level cells with its centre at a quarter of the
+    channel length, and per level below the finest a refinement box around
+    it of fine_boxes[level] cells of the next level, starting one third of
+    its length upstream of the centre.  The sphere's own cells are refined to
+    the finest level by its walls (markAllFinerWalls + WALL_REFINEMENT_COUNT).
+    nu is set on the base level so that Re = u_in D / nu on every level.
+    Level 0 collides with AllOne (limiter 0) and the finer levels with K17
+    at limiter 0.1, as the reference's sphere driver does
+    (cases/flowAroundSphere/flowAroundSphereMain.cu:136-149)."""
+    from .geometry import icosphere, set_bodies
+    scale = 2 ** (levels - 1)
+    d0 = float(diameter_finest) / scale            # diameter in base cells
+    nu0 = u_in * d0 / reynolds
+    c = open_channel(nx, ny, nz, u_in=u_in, nu_lattice=nu0, collision_limiter=0.1, storage=storage)
+    centre = (nx / 4.0, ny / 2.0, nz / 2.0)
+    set_bodies(c, [icosphere(subdivisions, 0.5 * d0, centre)])
+    c.grid_level_count = levels
+    c.wall_refinement_count = wall_refinement_count
+    c.track_wall_force = 1
+    for l in range(levels - 1):
+        cells = fine_boxes[l]
+        size = [v / 2.0 ** (l + 1) for v in cells]       # in base cells
+        lo = (centre[0] - size[0] / 3.0, centre[1] - size[1] / 2.0, centre[2] - size[2] / 2.0)
+        set_refine_box(c, l, lo, (lo[0] + size[0], lo[1] + size[1], lo[2] + size[2]))
+
+    def local(bc, i, j, k, info):
+        if bc.wallID < 0:
+            bc.collisionLimiter = 0.0 if info.grid_id == 0 else 0.1
+    set_hooks(c, local_bc=local)
+    return MultilevelSphereSetup(c, float(diameter_finest), float(u_in), float(reynolds))
+
+
+def set_hooks(case: A.LbmCase, open_bc=None, initial_condition=None, local_bc=None,
+              refinement=None) -> A.LbmCase:
     """Attach per-cell driver hooks (getOpenBC, getInitialCondition, getLocalBC)
     written in Python: each is called as hook(bc, i, j, k, info) with an
     lbm_bc to fill (the reference's BCStruct defaults, bc.wallID set for
     getLocalBC) and the level's lbm_grid_info, on the host while the grid is
-    built.  The callbacks are kept alive on the case object."""
+    built.  `refinement(i, j, k, mark, info)` (getRefinementModifier)
+    returns the refinement marker of a cell of a level below the finest.
+    The callbacks are kept alive on the case object."""
     keep = []
 
     def wrap(fn):
@@ -233,6 +302,15 @@ def set_hooks(case: A.LbmCase, open_bc=None, initial_condition=None, local_bc=No
     case.open_bc_hook = wrap(open_bc)
     case.initial_condition_hook = wrap(initial_condition)
     case.local_bc_hook = wrap(local_bc)
+    if refinement is None:
+        case.refinement_hook = None
+    else:
+        # refinement(i, j, k, mark, info) -> new mark (getRefinementModifier)
+        def rtramp(user, i, j, k, mark, info):
+            mark[0] = int(bool(refinement(i, j, k, bool(mark[0]), info.contents)))
+        rcb = A.REFINEMENT_HOOK(rtramp)
+        keep.append(rcb)
+        case.refinement_hook = C.cast(rcb, C.c_void_p).value
     case.hook_user = None
     case._hook_refs = keep
     return case

@@ -92,6 +92,10 @@ struct LevelState {
     std::vector<int*> rotorIndex;        // device indexArray per rotor
     unsigned long long memBytes = 0;
     lbm::DevLevel dev{};
+    // interface to the next finer level (empty on the finest): device lists
+    // and host copies for readback
+    lbm::DevInterface itf{};
+    std::vector<int> f2cIndex, f2cChild, c2fIndex, c2fChild, leftIndex, leftParent, leftNbr;
     std::vector<void*> owned;
 };
 
@@ -174,6 +178,8 @@ unsigned long long levelBytes(const lbm::HostLevel& H, int storage) {
          bytes(sources, sizeof(int)) + bytes(4 * m, sizeof(float));  // cell, info, nbr, target, beta, source, refs
     b += bytes(openChunkCount(H), sizeof(int4)) + (m ? bytes(LBM_MBBC_NORMALS, mbbcTableBytes(storage)) : 0);
     b += m ? bytes(2, sizeof(int)) : 0;                             // device iteration counter
+    b += bytes(H.f2cIndex.size() + H.f2cChild.size() + H.c2fIndex.size() + H.c2fChild.size(), sizeof(int));
+    b += bytes(H.leftIndex.size() + H.leftParent.size() + H.leftNbr.size(), sizeof(int));  // interface lists
     if (H.info.gridID == 0) b += bytes(8, sizeof(double)) + bytes(1, sizeof(int));
     return b;
 }
@@ -202,6 +208,9 @@ void fillInfo(const lbm::HostLevel& H, int storage, lbm_grid_info* out) {
     out->nu = H.info.nu;
     out->dt_phys = H.info.dtPhys;
     out->grid_memory_bytes = levelBytes(H, storage);
+    out->f2c_count = static_cast<int>(H.f2cIndex.size());
+    out->c2f_count = static_cast<int>(H.c2fIndex.size());
+    out->leftover_count = static_cast<int>(H.leftIndex.size());
 }
 
 }  // namespace
@@ -252,9 +261,23 @@ void advanceHostState(LevelState& L) {
     L.iterationsSinceTrackerReset++;
 }
 
+// updateAllGrids (include/updateGrid.h:388-396): a level steps once, the
+// next finer level twice (recursively), then the interface between them.
 void updateAllGrids(lbm_grids* g, int level) {
     updateSingleGrid(g, g->levels[level]);
-    // single-level build: no finer level to recurse into (updateGrid.h:391-395)
+    if (level + 1 < static_cast<int>(g->levels.size())) {
+        for (int i = 0; i < 2; ++i) updateAllGrids(g, level + 1);
+        LevelState& C = g->levels[level];
+        LevelState& F = g->levels[level + 1];
+        lbm::launchInterface(C.dev, F.dev, C.itf, C.info.esotwistFlipper, F.info.esotwistFlipper, g->stream);
+    }
+}
+
+// Host bookkeeping of one coarse step whose kernels ran inside a replayed
+// graph: level L advances 2^L substeps.
+void advanceHostStep(lbm_grids* g) {
+    for (LevelState& L : g->levels)
+        for (int k = 0; k < (1 << L.info.gridID); ++k) advanceHostState(L);
 }
 
 // Graph replay applies when no level has rotors (their frame is advanced
@@ -281,8 +304,8 @@ cudaGraphExec_t pairGraph(lbm_grids* g, int parity) {
     for (LevelState& L : g->levels) {
         saved.push_back(L.info);
         savedReset.push_back(L.iterationsSinceTrackerReset);
-        L.info.esotwistFlipper = parity != 0;
     }
+    g->levels[0].info.esotwistFlipper = parity != 0;
     cudaStream_t user = g->stream;
     g->stream = g->captureStream;
     cudaGraph_t graph = nullptr;
@@ -320,8 +343,7 @@ void launchPair(lbm_grids* g) {
     const int parity = g->levels[0].info.esotwistFlipper ? 1 : 0;
     cudaGraphExec_t exec = pairGraph(g, parity);
     ck(cudaGraphLaunch(exec, g->stream), "graph launch");
-    for (int k = 0; k < 2; ++k)
-        for (LevelState& L : g->levels) advanceHostState(L);
+    for (int k = 0; k < 2; ++k) advanceHostStep(g);
 }
 
 struct DeviceWaitError : std::runtime_error {
@@ -428,6 +450,17 @@ int lbm_plan_read_array(lbm_plan* p, int level, int which, void* host, size_t by
         if (bytes != need) return fail(LBM_ERR_INVALID, "lbm_plan_read_array: byte count does not match array size");
         if (bytes) std::memcpy(host, src, bytes);
         return LBM_OK;
+    }
+    {
+        const std::vector<int>* lists[7] = {&H.f2cIndex, &H.f2cChild, &H.c2fIndex, &H.c2fChild,
+                                            &H.leftIndex, &H.leftParent, &H.leftNbr};
+        if (which >= LBM_ARRAY_F2C_INDEX && which <= LBM_ARRAY_LEFTOVER_NBR) {
+            const std::vector<int>& v = *lists[which - LBM_ARRAY_F2C_INDEX];
+            if (bytes != v.size() * sizeof(int))
+                return fail(LBM_ERR_INVALID, "lbm_plan_read_array: byte count does not match array size");
+            if (bytes) std::memcpy(host, v.data(), bytes);
+            return LBM_OK;
+        }
     }
     if (which == LBM_ARRAY_WALL_VELOCITY) {
         const size_t need = H.wallVelocity.size() * sizeof(float);
@@ -638,12 +671,11 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
                 }
             }
             d.trackWallForce = c->track_wall_force ? 1 : 0;
-            d.useIBB = c->use_ibb ? 1 : 0;
-            d.gx = c->gx;
-            d.gy = c->gy;
-            d.gz = c->gz;
-            lbm::BC bc;
-            lbm::evalLocalBC(*c, bc);
+            const lbm::BC bc = lbm::levelLocalBC(*c, H);
+            d.useIBB = bc.useIBB ? 1 : 0;
+            d.gx = bc.gx;
+            d.gy = bc.gy;
+            d.gz = bc.gz;
             d.coll = lbm::makeCollisionConsts(H.info.nu, bc.nuMultiplier, bc.collisionLimiter);
             d.coll64 = lbm::makeCollisionConstsT<double>(H.info.nu, bc.nuMultiplier, bc.collisionLimiter);
             // memory accounting as the reference prints it (gridBuilderFunctions.h:1630-1649),
@@ -670,6 +702,33 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
             // reference values of the open boundary from the initial state
             lbm::launchOpenBoundaryInit(d, L.info.esotwistFlipper, s);
             ck(cudaGetLastError(), "init launch");
+        }
+        // interface lists between consecutive levels (owned by the coarse level)
+        for (size_t l = 0; l + 1 < host.levels.size(); ++l) {
+            const lbm::HostLevel& H = host.levels[l];
+            LevelState& L = g->levels[l];
+            auto own = [&](auto* p) { if (p) L.owned.push_back(p); return p; };
+            L.f2cIndex = H.f2cIndex; L.f2cChild = H.f2cChild;
+            L.c2fIndex = H.c2fIndex; L.c2fChild = H.c2fChild;
+            L.leftIndex = H.leftIndex; L.leftParent = H.leftParent; L.leftNbr = H.leftNbr;
+            lbm::DevInterface& I = L.itf;
+            I.f2cIndex = own(upload(H.f2cIndex, s));
+            I.f2cChild = own(upload(H.f2cChild, s));
+            I.f2cCount = static_cast<int>(H.f2cIndex.size());
+            I.c2fIndex = own(upload(H.c2fIndex, s));
+            I.c2fChild = own(upload(H.c2fChild, s));
+            I.c2fCount = static_cast<int>(H.c2fIndex.size());
+            I.leftIndex = own(upload(H.leftIndex, s));
+            I.leftParent = own(upload(H.leftParent, s));
+            I.leftNbr = own(upload(H.leftNbr, s));
+            I.leftCount = static_cast<int>(H.leftIndex.size());
+            // omega1 = 1 / (3 nu + 1/2) of each level, in the arithmetic type
+            auto omega = [&](float nu) {
+                return c->storage == LBM_STORE_F64 ? 1.0 / (3.0 * static_cast<double>(nu) + 0.5)
+                                                   : static_cast<double>(1.f / (3.f * nu + 0.5f));
+            };
+            I.omegaCoarse = omega(H.info.nu);
+            I.omegaFine = omega(host.levels[l + 1].info.nu);
         }
         ck(cudaStreamSynchronize(s), "build sync");
         if (fluidUpdates) *fluidUpdates = host.fluidUpdatesPerIteration;
@@ -801,8 +860,13 @@ int lbm_time_steps(lbm_grids* g, int steps, float* ms) {
         g->lastKernelMs = kernel;
         g->lastLaunches = g->kernelEventsUsed / 2;
         g->lastStepKernels = 0;
-        for (const LevelState& L : g->levels)
+        for (size_t l = 0; l < g->levels.size(); ++l) {
+            const LevelState& L = g->levels[l];
             g->lastStepKernels += (static_cast<long long>(steps) << L.info.gridID) * lbm::stepLaunchCount(L.dev);
+            const lbm::DevInterface& I = L.itf;
+            if (l + 1 < g->levels.size() && I.f2cCount + I.c2fCount + I.leftCount > 0)
+                g->lastStepKernels += static_cast<long long>(steps) << L.info.gridID;
+        }
     });
 }
 
@@ -849,6 +913,9 @@ int lbm_get_grid_info(lbm_grids* g, int level, lbm_grid_info* out) {
     out->nu = L.info.nu;
     out->dt_phys = L.info.dtPhys;
     out->grid_memory_bytes = L.memBytes;
+    out->f2c_count = L.itf.f2cCount;
+    out->c2f_count = L.itf.c2fCount;
+    out->leftover_count = L.itf.leftCount;
     return LBM_OK;
 }
 
@@ -883,6 +950,15 @@ int lbm_read_array(lbm_grids* g, int level, int which, void* host, size_t bytes)
         case LBM_ARRAY_OPEN_CUMULATIVE: src = d.obRhoCum; need = size_t(d.obCount) * 2 * 4; break;
         case LBM_ARRAY_F: need = 27 * n * 4; break;
         default:
+            if (which >= LBM_ARRAY_F2C_INDEX && which <= LBM_ARRAY_LEFTOVER_NBR) {
+                const std::vector<int>* lists[7] = {&L.f2cIndex, &L.f2cChild, &L.c2fIndex, &L.c2fChild,
+                                                    &L.leftIndex, &L.leftParent, &L.leftNbr};
+                const std::vector<int>& v = *lists[which - LBM_ARRAY_F2C_INDEX];
+                if (bytes != v.size() * sizeof(int))
+                    return fail(LBM_ERR_INVALID, "lbm_read_array: byte count does not match array size");
+                if (bytes) std::memcpy(host, v.data(), bytes);
+                return LBM_OK;
+            }
             if (which >= LBM_ARRAY_ROTOR_BASE && (which - LBM_ARRAY_ROTOR_BASE) / 4 < d.rotorCount) {
                 const int r = (which - LBM_ARRAY_ROTOR_BASE) / 4, part = (which - LBM_ARRAY_ROTOR_BASE) % 4;
                 const lbm::HostRotor& R = L.rotors[r];

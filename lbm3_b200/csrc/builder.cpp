@@ -118,6 +118,18 @@ void evalLocalBC(const lbm_case& c, BC& bc) {
     bc.nuMultiplier = c.nu_multiplier;
 }
 
+BC levelLocalBC(const lbm_case& c, const HostLevel& L) {
+    BC bc;
+    evalLocalBC(c, bc);
+    bc.gx = c.gx;
+    bc.gy = c.gy;
+    bc.gz = c.gz;
+    bc.useIBB = c.use_ibb != 0;
+    bc.wallID = -1;
+    if (c.local_bc_hook && L.info.cellCount > 0) bc = callHook(c, c.local_bc_hook, bc, L.info, L.I[0], L.J[0], L.K[0]);
+    return bc;
+}
+
 BC evalInitialCondition(const lbm_case& c, const Info& info, int i, int j, int k) {
     if (c.initial_condition_hook) return callHook(c, c.initial_condition_hook, BC{}, info, i, j, k);
     BC bc;
@@ -143,8 +155,9 @@ BC evalInitialCondition(const lbm_case& c, const Info& info, int i, int j, int k
 namespace {
 
 void validateCase(const lbm_case& c) {
-    if (c.grid_level_count != 1)
-        throw std::runtime_error("grid_level_count must be 1 in this build");
+    if (c.grid_level_count < 1 || c.grid_level_count > LBM_MAX_LEVELS)
+        throw std::runtime_error("grid_level_count must be in [1, LBM_MAX_LEVELS]");
+    if (c.wall_refinement_count < 0) throw std::runtime_error("wall_refinement_count must be >= 0");
     if (!(c.res_global > 0.f)) throw std::runtime_error("res_global must be > 0");
     if (!(c.dt_phys_global > 0.f)) throw std::runtime_error("dt_phys_global must be > 0");
     if (!(c.nu_phys > 0.f)) throw std::runtime_error("nu_phys must be > 0");
@@ -329,8 +342,10 @@ void buildBoundaryLists(const lbm_case& c, HostLevel& L) {
     const int n = in.cellCount;
     L.wallMap.assign(n, -1);
     L.wallCellCount = 0;
-    for (int cidx = 0; cidx < n; ++cidx)
+    for (int cidx = 0; cidx < n; ++cidx) {
         if (L.wallMarker[cidx]) { L.wallMap[cidx] = -3; ++L.wallCellCount; }
+        else if (!L.interfaceOverlap.empty() && L.interfaceOverlap[cidx]) L.wallMap[cidx] = -2;
+    }
     L.wallAdjacentCount = static_cast<int>(L.wallIndex.size());
     for (int w = 0; w < L.wallAdjacentCount; ++w) L.wallMap[L.wallIndex[w]] = w;
 
@@ -373,7 +388,8 @@ void buildBoundaryLists(const lbm_case& c, HostLevel& L) {
         ob.trackFlowCount = 0;
         for (size_t q = 0; q < ob.index.size(); ++q) {
             const int cidx = ob.index[q];
-            if (L.wallMap[cidx] != -2) ++ob.trackFlowCount;
+            const int wmap = L.wallMap[cidx];
+            if (wmap != -2 && !(wmap >= 0 && (L.wallData[wmap] & 1u))) ++ob.trackFlowCount;
             const int i = L.I[cidx], j = L.J[cidx], k = L.K[cidx];
             const int onx = i == 0 ? -1 : (i == in.nx - 1 ? 1 : 0);
             const int ony = j == 0 ? -1 : (j == in.ny - 1 ? 1 : 0);
@@ -566,8 +582,11 @@ void fullNbrList(const HostLevel& L, int c, int (&nb)[27]) {
 }
 
 // Links of one wall-adjacent cell (buildLinkExistenceMarkerArray,
-// interpolatedBouncebackFunctions.h:181-398, single level: no interface links).
-uint32_t linkBits(const HostLevel& L, int c) {
+// interpolatedBouncebackFunctions.h:181-398).  `iface` marks the cells of an
+// interface band (a parent on the coarser level, or fine-to-coarse /
+// coarse-to-fine on this one; empty on a single level); a link from or to such
+// a cell is returned in `pierce` and later gets length 1/2.
+uint32_t linkBits(const HostLevel& L, int c, const std::vector<uint8_t>& iface, uint32_t& pierce) {
     const Info& in = L.info;
     int nb[27];
     fullNbrList(L, c, nb);
@@ -590,40 +609,72 @@ uint32_t linkBits(const HostLevel& L, int c) {
         if (cz(d) < 0) km = false;
     }
     uint32_t bits = 0;
+    pierce = 0;
+    const bool meInterface = !iface.empty() && iface[c];
+    auto add = [&](int d) {
+        bits |= 1u << d;
+        if (meInterface || (!iface.empty() && iface[nb[d]])) pierce |= 1u << d;
+    };
     const bool interior = i != 0 && i != in.nx - 1 && j != 0 && j != in.ny - 1 && k != 0 && k != in.nz - 1;
     if (interior) {
         if (!all) return 0;
         for (int d = 1; d < 27; ++d)
-            if (L.wallMarker[nb[d]]) bits |= 1u << d;
+            if (L.wallMarker[nb[d]]) add(d);
         return bits;
     }
     for (int d = 1; d < 27; ++d) {
         if (!geom[d] || !L.wallMarker[nb[d]]) continue;
         if ((cx(d) > 0 && !ip) || (cy(d) > 0 && !jp) || (cz(d) > 0 && !kp)) continue;
         if ((cx(d) < 0 && !im) || (cy(d) < 0 && !jm) || (cz(d) < 0 && !km)) continue;
-        bits |= 1u << d;
+        add(d);
     }
     return bits;
 }
+
+// Markers of one level that live only while the domain is built
+// (GridBuilderStruct, include/types.h:181-190).
+struct LevelMarks {
+    std::vector<uint8_t> deep, f2c, c2f, refine;  // levels with a finer one
+    std::vector<int> parent;                        // levels with a coarser one: parent cell or -1
+    std::vector<uint8_t> parentInterface, parentF2C, needValues;
+    std::vector<int> wallIDFull;                    // wallIDArrayFull: body of a wall-adjacent cell or -1
+};
 
 // Wall markers, wall IDs, wall-adjacent list, link existence and link lengths
 // (buildWallMarkers, include/gridBuilderFunctions.h:590-739, and
 // buildLinkLengthArray, interpolatedBouncebackFunctions.h:482-660), then the
 // packed wallData / linkLength words (packWallData, :662-695).
-void buildWalls(const lbm_case& c, HostLevel& L, const std::vector<Triangles>& bodies,
-                const std::vector<RayMap>& maps, const RayMap& total) {
+// On a finer level (`coarse` set) cells with a parent inherit the parent's
+// wall state and body marks, and a wall-adjacent cell takes its parent's
+// wallID when the parent has one (buildWallMarkers steps 1-2).
+void buildWalls(const lbm_case& c, HostLevel& L, LevelMarks& M, const HostLevel* coarse, const LevelMarks* CM,
+                const std::vector<Triangles>& bodies, const std::vector<RayMap>& maps, const RayMap& total,
+                const std::vector<RayMap>* coarseMaps, const std::vector<uint8_t>& iface) {
     const Info& in = L.info;
     const int n = in.cellCount;
     L.wallMarker.assign(n, 0);
     for (int q = 0; q < n; ++q) L.wallMarker[q] = isSolid(total, L.I[q], L.J[q], L.K[q]) ? 1 : 0;
+    if (coarse)
+        for (int q = 0; q < n; ++q)
+            if (M.parent[q] >= 0) L.wallMarker[q] = coarse->wallMarker[M.parent[q]];
     std::vector<int> wallID(n, -1);
     for (size_t b = 0; b < maps.size(); ++b) {
         std::vector<uint8_t> body(n, 0);
         for (int q = 0; q < n; ++q) body[q] = isSolid(maps[b], L.I[q], L.J[q], L.K[q]) ? 1 : 0;
+        if (coarse)
+            for (int q = 0; q < n; ++q) {
+                const int p = M.parent[q];
+                if (p >= 0) body[q] = isSolid((*coarseMaps)[b], coarse->I[p], coarse->J[p], coarse->K[p]) ? 1 : 0;
+            }
         body = spreadCells(L, body);
-        for (int q = 0; q < n; ++q)
-            if (body[q] && !L.wallMarker[q]) wallID[q] = static_cast<int>(b);  // last body wins
+        for (int q = 0; q < n; ++q) {
+            if (!body[q] || L.wallMarker[q]) continue;
+            int id = static_cast<int>(b);  // last body wins
+            if (coarse && M.parent[q] >= 0 && CM->wallIDFull[M.parent[q]] >= 0) id = CM->wallIDFull[M.parent[q]];
+            wallID[q] = id;
+        }
     }
+    M.wallIDFull = wallID;
     L.wallIndex.clear();
     std::vector<int> ids;
     for (int q = 0; q < n; ++q)
@@ -632,8 +683,8 @@ void buildWalls(const lbm_case& c, HostLevel& L, const std::vector<Triangles>& b
             ids.push_back(wallID[q]);
         }
     const int nw = static_cast<int>(L.wallIndex.size());
-    std::vector<uint32_t> links(nw, 0);
-    for (int w = 0; w < nw; ++w) links[w] = linkBits(L, L.wallIndex[w]);
+    std::vector<uint32_t> links(nw, 0), pierce(nw, 0);
+    for (int w = 0; w < nw; ++w) links[w] = linkBits(L, L.wallIndex[w], iface, pierce[w]);
 
     // link lengths: nearest triangle crossing of each link, per body bins
     std::vector<float> len(static_cast<size_t>(nw) * 27, 2.f);
@@ -659,7 +710,7 @@ void buildWalls(const lbm_case& c, HostLevel& L, const std::vector<Triangles>& b
                 const float bx = t.bx[tri] - x, by = t.by[tri] - y, bz = t.bz[tri] - z;
                 const float cxv = t.cx[tri] - x, cyv = t.cy[tri] - y, czv = t.cz[tri] - z;
                 for (int d = 1; d < 27; ++d) {
-                    if (!((links[w] >> d) & 1u)) continue;
+                    if (!((links[w] >> d) & 1u) || ((pierce[w] >> d) & 1u)) continue;
                     float tHit;
                     if (!intersectRayTriangle(ax, ay, az, bx, by, bz, cxv, cyv, czv, float(cx(d)), float(cy(d)),
                                               float(cz(d)), edgeTol, tHit))
@@ -688,7 +739,9 @@ void buildWalls(const lbm_case& c, HostLevel& L, const std::vector<Triangles>& b
             if (!((links[w] >> d) & 1u)) continue;
             ++L.linksTotal;
             float& slot = len[static_cast<size_t>(w) * 27 + d];
-            if (slot > 1.f) {
+            if ((pierce[w] >> d) & 1u) {
+                slot = 0.5f;  // crosses an interface: the same length on both levels
+            } else if (slot > 1.f) {
                 slot = 0.5f;  // no crossing found: safe fallback
                 ++L.linksNotFound;
             } else if (slot < 0.f) {
@@ -702,6 +755,7 @@ void buildWalls(const lbm_case& c, HostLevel& L, const std::vector<Triangles>& b
     L.wallVelocity.assign(static_cast<size_t>(3) * nw, 0.f);
     for (int w = 0; w < nw; ++w) {
         uint32_t data = static_cast<uint32_t>(ids[w]) << 27;
+        if (!L.interfaceOverlap.empty() && L.interfaceOverlap[L.wallIndex[w]]) data |= 1u;
         int li = 0;
         for (int d = 1; d < 27; ++d) {
             if (!((links[w] >> d) & 1u)) continue;
@@ -893,6 +947,284 @@ void buildSegments(HostLevel& L) {
     }
 }
 
+namespace {
+
+size_t denseIndex(const Info& in, int i, int j, int k) {
+    return (static_cast<size_t>(k) * in.ny + j) * in.nx + i;
+}
+
+// initializeGridInfo for a finer level (include/gridBuilderFunctions.h:50-62):
+// half the spacing, twice the cells per axis, origin shifted by half a fine
+// cell, half the time step.
+void initFinerInfo(const lbm_case& c, const Info& coarse, Info& fine, int level) {
+    fine.gridID = level;
+    fine.res = coarse.res * 0.5f;
+    fine.nx = coarse.nx * 2;
+    fine.ny = coarse.ny * 2;
+    fine.nz = coarse.nz * 2;
+    fine.ox = coarse.ox - fine.res * 0.5f;
+    fine.oy = coarse.oy - fine.res * 0.5f;
+    fine.oz = coarse.oz - fine.res * 0.5f;
+    fine.dtPhys = coarse.dtPhys * 0.5f;
+    fine.nu = (fine.dtPhys * c.nu_phys) / ((fine.res / 1000.f) * (fine.res / 1000.f));
+}
+
+// Keep the marked cells of a level (deleteExcessCells steps 7-13): the cell
+// list is re-emitted in k-j-i order with fresh neighbours; returns the new
+// index of every old cell (-1 when deleted).
+std::vector<int> compactLevel(HostLevel& L, const std::vector<uint8_t>& keepCell) {
+    const Info& in = L.info;
+    std::vector<uint8_t> dense(static_cast<size_t>(in.nx) * in.ny * in.nz, 0);
+    std::vector<int> remap(keepCell.size(), -1);
+    int n = 0;
+    for (size_t q = 0; q < keepCell.size(); ++q)
+        if (keepCell[q]) {
+            dense[denseIndex(in, L.I[q], L.J[q], L.K[q])] = 1;
+            remap[q] = n++;
+        }
+    buildCellsAndNBR(L, dense);
+    return remap;
+}
+
+template <class T>
+std::vector<T> remapCells(const std::vector<T>& v, const std::vector<int>& remap, int n) {
+    std::vector<T> out(n);
+    if (v.empty()) return {};
+    for (size_t q = 0; q < remap.size(); ++q)
+        if (remap[q] >= 0) out[remap[q]] = v[q];
+    return out;
+}
+
+std::vector<uint8_t> andNot(std::vector<uint8_t> a, const std::vector<uint8_t>& b) {
+    for (size_t q = 0; q < a.size(); ++q) a[q] = a[q] && !b[q];
+    return a;
+}
+
+// markRefinementCells (include/markerFunctions.h:419-450) on a level with a
+// finer one: keep marks (cells that cover fluid on any finer level, spread
+// once, plus the parent interface), deep refinement (cells that cover a wall
+// on any finer level, spread WALL_REFINEMENT_COUNT times, then the user
+// modification), the fine-to-coarse ring (one layer) and the coarse-to-fine
+// band (two layers) around it.
+void markRefinement(const lbm_case& c, const HostLevel& L, LevelMarks& M, const std::vector<RayMap>& total) {
+    const Info& in = L.info;
+    const int n = in.cellCount, lv = in.gridID, NL = c.grid_level_count;
+    std::vector<uint8_t> keep(n, 0), deep(n, 0);
+    for (int q = 0; q < n; ++q) {
+        bool fluid = false, wall = false;
+        for (int m = lv; m < NL; ++m) {
+            const int down = 1 << (m - lv);
+            fluid = fluid || coarseHasFluid(total[m], down, L.I[q], L.J[q], L.K[q]);
+            wall = wall || coarseHasWall(total[m], down, L.I[q], L.J[q], L.K[q]);
+        }
+        keep[q] = fluid;
+        deep[q] = wall;
+    }
+    keep = spreadCells(L, keep);
+    if (lv > 0)
+        for (int q = 0; q < n; ++q) keep[q] = keep[q] || M.parentInterface[q];
+    for (int r = 0; r < c.wall_refinement_count; ++r) deep = spreadCells(L, deep);
+    // applyUserRefinementModification (:254-271): the refinement box of this
+    // level, then the driver's hook
+    const float* box = c.refine_box[lv];
+    const bool useBox = box[0] < box[3] && box[1] < box[4] && box[2] < box[5];
+    lbm_grid_info hi = hookInfo(in);
+    hi.cell_count = n;
+    for (int q = 0; q < n; ++q) {
+        int mark = deep[q];
+        if (useBox) {
+            const float x = L.I[q] * in.res + in.ox, y = L.J[q] * in.res + in.oy, z = L.K[q] * in.res + in.oz;
+            if (x > box[0] && x < box[3] && y > box[1] && y < box[4] && z > box[2] && z < box[5]) mark = 1;
+        }
+        if (c.refinement_hook) c.refinement_hook(c.hook_user, L.I[q], L.J[q], L.K[q], &mark, &hi);
+        deep[q] = mark != 0;
+    }
+    if (lv > 0) deep = andNot(deep, M.parentInterface);
+    for (int q = 0; q < n; ++q) deep[q] = deep[q] && keep[q];
+    std::vector<uint8_t> f2c = spreadCells(L, deep);
+    for (int q = 0; q < n; ++q) f2c[q] = f2c[q] && keep[q] && !deep[q];
+    std::vector<uint8_t> c2f = spreadCells(L, spreadCells(L, f2c));
+    for (int q = 0; q < n; ++q) c2f[q] = c2f[q] && keep[q] && !deep[q] && !f2c[q];
+    M.refine.assign(n, 0);
+    for (int q = 0; q < n; ++q) M.refine[q] = deep[q] || f2c[q] || c2f[q];
+    M.deep = std::move(deep);
+    M.f2c = std::move(f2c);
+    M.c2f = std::move(c2f);
+}
+
+// buildFinerGridBuilder (include/gridBuilderFunctions.h:134-201) + sortIJK:
+// the 2x2x2 children of every refinement-marked coarse cell, emitted in k-j-i
+// order; then the parent map and the parent-interface marks (buildIJKFull
+// steps 6-7).
+void buildFinerLevel(const HostLevel& C, const LevelMarks& CM, HostLevel& F, LevelMarks& FM) {
+    const Info& fin = F.info;
+    std::vector<uint8_t> dense(static_cast<size_t>(fin.nx) * fin.ny * fin.nz, 0);
+    for (int q = 0; q < C.info.cellCount; ++q) {
+        if (!CM.refine[q]) continue;
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b)
+                for (int e = 0; e < 2; ++e)
+                    dense[denseIndex(fin, 2 * C.I[q] + e, 2 * C.J[q] + b, 2 * C.K[q] + a)] = 1;
+    }
+    buildCellsAndNBR(F, dense);
+    const int n = F.info.cellCount;
+    FM.parent.assign(n, -1);
+    FM.parentInterface.assign(n, 0);
+    FM.parentF2C.assign(n, 0);
+    for (int q = 0; q < n; ++q) {
+        const int p = findCell(C, F.I[q] / 2, F.J[q] / 2, F.K[q] / 2);
+        FM.parent[q] = p;
+        if (p < 0) continue;
+        FM.parentInterface[q] = CM.c2f[p] || CM.f2c[p];
+        FM.parentF2C[q] = CM.f2c[p];
+    }
+}
+
+// deleteExcessCells (include/gridBuilderFunctions.h:402-588) for one level,
+// after its coarser level has been compacted.
+void deleteExcess(const lbm_case& c, HostLevel& L, LevelMarks& M, const HostLevel* coarse, const RayMap& total) {
+    const int NL = c.grid_level_count;
+    const int lv = L.info.gridID;
+    const int n = L.info.cellCount;
+    if (coarse) {
+        for (int q = 0; q < n; ++q) {
+            M.parent[q] = findCell(*coarse, L.I[q] / 2, L.J[q] / 2, L.K[q] / 2);
+            M.parentInterface[q] = M.parent[q] >= 0;
+        }
+    }
+    std::vector<uint8_t> keep(n, 0);
+    for (int q = 0; q < n; ++q) keep[q] = !isSolid(total, L.I[q], L.J[q], L.K[q]);
+    if (coarse)
+        for (int q = 0; q < n; ++q) keep[q] = keep[q] || M.parentInterface[q];
+    keep = spreadCells(L, keep);
+    if (lv < NL - 1) keep = andNot(keep, M.deep);
+    if (coarse) {
+        // the outermost layer of the parent interface goes: the coarse-to-fine
+        // blocks reach the fine cells between coarse centres only
+        const std::vector<uint8_t> s1 = spreadCells(L, M.parentF2C);
+        const std::vector<uint8_t> s3 = spreadCells(L, spreadCells(L, s1));
+        for (int q = 0; q < n; ++q)
+            if (M.parentInterface[q] && !s3[q]) keep[q] = 0;
+        M.needValues.assign(n, 0);
+        for (int q = 0; q < n; ++q) M.needValues[q] = M.parentInterface[q] && keep[q] && !s1[q];
+    }
+    const std::vector<int> remap = compactLevel(L, keep);
+    const int m = L.info.cellCount;
+    if (coarse) {
+        M.parent = remapCells(M.parent, remap, m);
+        M.needValues = remapCells(M.needValues, remap, m);
+        M.parentInterface = remapCells(M.parentInterface, remap, m);
+        M.parentF2C = remapCells(M.parentF2C, remap, m);
+    }
+    if (lv < NL - 1) {
+        M.f2c = remapCells(M.f2c, remap, m);
+        M.c2f = remapCells(M.c2f, remap, m);
+    }
+    M.deep.clear();
+    M.refine.clear();
+}
+
+// The 8 plus neighbours of a builder cell in the order self, +i, +j, +ij, +k,
+// +ik, +jk, +ijk (finishNBRPlus, include/NBRFunctions.h:5-11).
+void blockNbrs(const HostLevel& L, int c, int (&nb)[8]) {
+    const int n = L.info.cellCount;
+    auto wrap = [n](int v) { return v + 1 < n ? v + 1 : 0; };
+    nb[0] = c;
+    nb[1] = wrap(c);
+    nb[2] = L.jPlus[c];
+    nb[3] = wrap(nb[2]);
+    nb[4] = L.kPlus[c];
+    nb[5] = wrap(nb[4]);
+    nb[6] = L.jPlus[nb[4]];
+    nb[7] = wrap(nb[6]);
+}
+
+// Interface lists of a coarse level towards the next finer one
+// (gridBuilderToGrid step 6, include/gridBuilderFunctions.h:1192-1231, with
+// fillFineToCoarseInterface :741-769 and fillCoarseToFineInterface :771-1030).
+void buildInterfaces(HostLevel& C, const LevelMarks& CM, const HostLevel& F, const LevelMarks& FM) {
+    const int nc = C.info.cellCount, nf = F.info.cellCount;
+    // childMapArrayGlobal: the (2i,2j,2k) child of every coarse cell
+    std::vector<int> child(nc, -1);
+    for (int q = 0; q < nf; ++q) {
+        const int p = FM.parent[q];
+        if (p >= 0 && F.I[q] % 2 == 0 && F.J[q] % 2 == 0 && F.K[q] % 2 == 0) child[p] = q;
+    }
+    C.f2cIndex.clear(); C.f2cChild.clear();
+    for (int q = 0; q < nc; ++q)
+        if (CM.f2c[q] && !C.wallMarker[q]) {
+            C.f2cIndex.push_back(q);
+            C.f2cChild.push_back(child[q]);
+        }
+    // coarse-to-fine: full 2x2x2 coarse stencils whose centre block of fine
+    // cells exists in full
+    std::vector<uint8_t> mark(nc, 0);
+    for (int q = 0; q < nc; ++q) mark[q] = CM.c2f[q] && !C.wallMarker[q];
+    C.c2fIndex.clear(); C.c2fChild.clear();
+    std::vector<uint8_t> received(nf, 0);
+    for (int q = 0; q < nc; ++q) {
+        if (!mark[q]) continue;
+        int nb[8];
+        blockNbrs(C, q, nb);
+        bool ok = true;
+        for (int t = 1; t < 8 && ok; ++t) {
+            const int r = nb[t];
+            ok = mark[r] && C.I[r] == C.I[q] + (t & 1) && C.J[r] == C.J[q] + ((t >> 1) & 1) &&
+                 C.K[r] == C.K[q] + ((t >> 2) & 1);
+        }
+        if (!ok) continue;
+        const int top = child[nb[7]];
+        if (top < 0) continue;
+        // walk back from the top child: jkPlus = top - 1, kPlus = jMinus,
+        // self = kMinus
+        int jk = top - 1;
+        if (jk < 0) jk = nf - 1;
+        const int kp = F.jMinus[jk];
+        const int self = F.kMinus[kp];
+        int fb[8];
+        blockNbrs(F, self, fb);
+        for (int t = 0; t < 8 && ok; ++t) {
+            const int r = fb[t];
+            ok = F.I[r] == 2 * C.I[q] + 1 + (t & 1) && F.J[r] == 2 * C.J[q] + 1 + ((t >> 1) & 1) &&
+                 F.K[r] == 2 * C.K[q] + 1 + ((t >> 2) & 1);
+        }
+        if (!ok) continue;
+        C.c2fIndex.push_back(q);
+        C.c2fChild.push_back(self);
+        for (int t = 0; t < 8; ++t) received[fb[t]] = 1;
+    }
+    // leftovers: fine cells that need coarse values and no block reached
+    C.leftIndex.clear(); C.leftParent.clear();
+    std::vector<int> nbI, nbJ, nbK;
+    for (int q = 0; q < nf; ++q) {
+        if (!(FM.needValues[q] && !F.wallMarker[q] && !received[q])) continue;
+        const int p = FM.parent[q];
+        const int ic = C.I[p], jc = C.J[p], kc = C.K[p];
+        auto at = [&](int r, int di, int dj, int dk) {
+            return mark[r] && C.I[r] == ic + di && C.J[r] == jc + dj && C.K[r] == kc + dk;
+        };
+        auto pick = [&](bool plusFirst, int plusCell, int minusCell, int di, int dj, int dk) {
+            const int first = plusFirst ? plusCell : minusCell, second = plusFirst ? minusCell : plusCell;
+            const int s = plusFirst ? 1 : -1;
+            if (at(first, s * di, s * dj, s * dk)) return first;
+            if (at(second, -s * di, -s * dj, -s * dk)) return -second - 1;
+            return p;
+        };
+        const int iPlus = p + 1 >= nc ? 0 : p + 1, iMinus = p - 1 < 0 ? nc - 1 : p - 1;
+        nbI.push_back(pick(F.I[q] % 2 == 1, iPlus, iMinus, 1, 0, 0));
+        nbJ.push_back(pick(F.J[q] % 2 == 1, C.jPlus[p], C.jMinus[p], 0, 1, 0));
+        nbK.push_back(pick(F.K[q] % 2 == 1, C.kPlus[p], C.kMinus[p], 0, 0, 1));
+        C.leftIndex.push_back(q);
+        C.leftParent.push_back(p);
+    }
+    C.leftNbr.clear();
+    C.leftNbr.insert(C.leftNbr.end(), nbI.begin(), nbI.end());
+    C.leftNbr.insert(C.leftNbr.end(), nbJ.begin(), nbJ.end());
+    C.leftNbr.insert(C.leftNbr.end(), nbK.begin(), nbK.end());
+}
+
+}  // namespace
+
 void buildDomain(const lbm_case& c, HostDomain& out) {
     validateCase(c);
     out.c = c;
@@ -900,73 +1232,120 @@ void buildDomain(const lbm_case& c, HostDomain& out) {
     out.c.open_bc_hook = nullptr;
     out.c.initial_condition_hook = nullptr;
     out.c.local_bc_hook = nullptr;
+    out.c.refinement_hook = nullptr;
     out.c.hook_user = nullptr;
     for (int r = 0; r < LBM_MAX_ROTORS; ++r) out.c.rotor[r].triangles = nullptr;
-    out.levels.assign(1, HostLevel{});
-    HostLevel& L = out.levels[0];
+    const int NL = c.grid_level_count;
+    out.levels.assign(NL, HostLevel{});
     Info skel;
-    initLevel0(c, L.info, skel);
-    const Info& in = L.info;
+    initLevel0(c, out.levels[0].info, skel);
+    for (int l = 1; l < NL; ++l) initFinerInfo(c, out.levels[l - 1].info, out.levels[l].info, l);
 
-    // bodies: triangles, bins and one ray map each, plus their union
-    // (readSTL/sortSTLToBins, initializeVoxelizers: voxelizerFunctions.h:692-728)
+    // bodies: triangles and bins once, a ray map per body and level plus
+    // their union (readSTL/sortSTLToBins, initializeVoxelizers:
+    // voxelizerFunctions.h:692-728)
     std::vector<Triangles> bodies(c.body_count);
-    std::vector<RayMap> maps(c.body_count);
-    RayMap total;
-    total.nx = in.nx;
-    total.ny = in.ny;
-    total.scan.assign(static_cast<size_t>(in.nx) * in.ny + 1, 0);
     for (int b = 0; b < c.body_count; ++b) {
         loadTriangles(c.body[b].triangles, c.body[b].triangle_count, bodies[b]);
         sortToBins(bodies[b], c.res_global);
-        voxelize(bodies[b], in.ox, in.oy, in.oz, in.res, in.nx, in.ny, maps[b]);
-        if (b == 0) total = maps[0];
-        else unionRayMaps(total, maps[b]);
+    }
+    std::vector<std::vector<RayMap>> maps(NL, std::vector<RayMap>(c.body_count));
+    std::vector<RayMap> total(NL);
+    for (int l = 0; l < NL; ++l) {
+        const Info& in = out.levels[l].info;
+        total[l].nx = in.nx;
+        total[l].ny = in.ny;
+        total[l].scan.assign(static_cast<size_t>(in.nx) * in.ny + 1, 0);
+        for (int b = 0; b < c.body_count; ++b) {
+            voxelize(bodies[b], in.ox, in.oy, in.oz, in.res, in.nx, in.ny, maps[l][b]);
+            if (b == 0) total[l] = maps[l][0];
+            else unionRayMaps(total[l], maps[l][b]);
+        }
     }
 
-    // markKeepCells on the skeleton: keep a skeleton cell that covers fluid,
-    // plus one layer (markerFunctions.h:401-409)
-    const int snx = skel.nx, sny = skel.ny, snz = skel.nz;
-    std::vector<uint8_t> keepSkel(static_cast<size_t>(snx) * sny * snz, 1);
-    if (c.body_count > 0) {
-        for (int k = 0; k < snz; ++k)
-            for (int j = 0; j < sny; ++j)
-                for (int i = 0; i < snx; ++i)
-                    keepSkel[(static_cast<size_t>(k) * sny + j) * snx + i] = coarseHasFluid(total, 2, i, j, k) ? 1 : 0;
-        keepSkel = spreadDense(keepSkel, snx, sny, snz);
+    // buildIJKFull (include/gridBuilderFunctions.h:299-400).  Level 0 from the
+    // skeleton: a skeleton cell is kept when it covers fluid on any level,
+    // plus one layer (markKeepCells, markerFunctions.h:401-409), and
+    // contributes its 2x2x2 children.
+    std::vector<LevelMarks> marks(NL);
+    {
+        HostLevel& L0 = out.levels[0];
+        const Info& in = L0.info;
+        const int snx = skel.nx, sny = skel.ny, snz = skel.nz;
+        std::vector<uint8_t> keepSkel(static_cast<size_t>(snx) * sny * snz, 1);
+        if (c.body_count > 0) {
+            for (int k = 0; k < snz; ++k)
+                for (int j = 0; j < sny; ++j)
+                    for (int i = 0; i < snx; ++i) {
+                        bool fluid = false;
+                        for (int m = 0; m < NL && !fluid; ++m) fluid = coarseHasFluid(total[m], 2 << m, i, j, k);
+                        keepSkel[(static_cast<size_t>(k) * sny + j) * snx + i] = fluid ? 1 : 0;
+                    }
+            keepSkel = spreadDense(keepSkel, snx, sny, snz);
+        }
+        std::vector<uint8_t> keep(static_cast<size_t>(in.nx) * in.ny * in.nz, 0);
+        for (int k = 0; k < in.nz; ++k)
+            for (int j = 0; j < in.ny; ++j)
+                for (int i = 0; i < in.nx; ++i)
+                    keep[denseIndex(in, i, j, k)] = keepSkel[(static_cast<size_t>(k / 2) * sny + j / 2) * snx + i / 2];
+        buildCellsAndNBR(L0, keep);
     }
-    const size_t full = static_cast<size_t>(in.nx) * in.ny * in.nz;
-    std::vector<uint8_t> keep(full, 0);
-    for (int k = 0; k < in.nz; ++k)
-        for (int j = 0; j < in.ny; ++j)
-            for (int i = 0; i < in.nx; ++i)
-                keep[(static_cast<size_t>(k) * in.ny + j) * in.nx + i] =
-                    keepSkel[(static_cast<size_t>(k / 2) * sny + j / 2) * snx + i / 2];
-    buildCellsAndNBR(L, keep);
+    // finer levels: refinement marks on the coarser level, then its children
+    for (int l = 0; l + 1 < NL; ++l) {
+        markRefinement(c, out.levels[l], marks[l], total);
+        buildFinerLevel(out.levels[l], marks[l], out.levels[l + 1], marks[l + 1]);
+    }
+    // deleteExcessCells, coarse to fine
+    for (int l = 0; l < NL; ++l)
+        deleteExcess(c, out.levels[l], marks[l], l > 0 ? &out.levels[l - 1] : nullptr, total[l]);
 
-    if (c.body_count > 0) {
-        // deleteExcessCells (gridBuilderFunctions.h:402-588): keep fluid plus
-        // one layer of wall cells
-        std::vector<uint8_t> fluid(L.info.cellCount, 0);
-        for (int q = 0; q < L.info.cellCount; ++q)
-            fluid[q] = isSolid(total, L.I[q], L.J[q], L.K[q]) ? 0 : 1;
-        fluid = spreadCells(L, fluid);
-        std::fill(keep.begin(), keep.end(), 0);
-        for (int q = 0; q < L.info.cellCount; ++q)
-            if (fluid[q]) keep[(static_cast<size_t>(L.K[q]) * in.ny + L.J[q]) * in.nx + L.I[q]] = 1;
-        buildCellsAndNBR(L, keep);
-        buildWalls(c, L, bodies, maps, total);
-    } else {
-        L.wallMarker.assign(L.info.cellCount, 0);
-        L.wallIndex.clear();
-        L.wallData.clear();
-        L.linkLength.clear();
-        L.wallVelocity.clear();
+    // buildWallMarkers (include/gridBuilderFunctions.h:590-739), coarse to fine
+    for (int l = 0; l < NL; ++l) {
+        HostLevel& L = out.levels[l];
+        LevelMarks& M = marks[l];
+        const int n = L.info.cellCount;
+        // interface overlap (step 7): this level's fine-to-coarse cells and
+        // the cells under the parent's coarse-to-fine band
+        L.interfaceOverlap.assign(n, 0);
+        std::vector<uint8_t> iface;
+        if (NL > 1) {
+            iface.assign(n, 0);
+            for (int q = 0; q < n; ++q) {
+                bool ov = false, in = false;
+                if (l + 1 < NL) {
+                    ov = M.f2c[q];
+                    in = M.f2c[q] || M.c2f[q];
+                }
+                if (l > 0 && M.parent[q] >= 0) {
+                    in = true;
+                    if (marks[l - 1].c2f[M.parent[q]]) ov = true;
+                }
+                L.interfaceOverlap[q] = ov;
+                iface[q] = in;
+            }
+        }
+        if (c.body_count > 0) {
+            buildWalls(c, L, M, l > 0 ? &out.levels[l - 1] : nullptr, l > 0 ? &marks[l - 1] : nullptr, bodies,
+                       maps[l], total[l], l > 0 ? &maps[l - 1] : nullptr, iface);
+        } else {
+            L.wallMarker.assign(n, 0);
+            M.wallIDFull.assign(n, -1);
+            L.wallIndex.clear();
+            L.wallData.clear();
+            L.linkLength.clear();
+            L.wallVelocity.clear();
+        }
     }
-    compressRows(L);
-    buildBoundaryLists(c, L);
-    buildRotors(c, L);
-    buildSegments(L);
+
+    // gridBuilderToGrid (include/gridBuilderFunctions.h:1032-1564) per level
+    for (int l = 0; l < NL; ++l) {
+        HostLevel& L = out.levels[l];
+        compressRows(L);
+        buildBoundaryLists(c, L);
+        if (l + 1 < NL) buildInterfaces(L, marks[l], out.levels[l + 1], marks[l + 1]);
+        buildRotors(c, L);
+        buildSegments(L);
+    }
 
     out.fluidUpdatesPerIteration = 0;
     for (const HostLevel& lv : out.levels)

@@ -105,6 +105,19 @@ struct HostLevel {
     std::vector<HostRotor> rotors;
     std::vector<uint8_t> rotorCell;
     std::vector<int> rotorCells;          // collided by the rotor kernel
+    // cells whose values another level supplies: this level's fine-to-coarse
+    // cells and the cells under the parent's coarse-to-fine band (no force or
+    // flow tracking, wallMap -2 / wallData bit 0)
+    std::vector<uint8_t> interfaceOverlap;
+    // Interfaces to the next finer level, owned by the coarse level
+    // (InterfaceStruct, include/types.h:198-200).  Fine-to-coarse: coarse cell
+    // and its fine child (2i,2j,2k).  Coarse-to-fine: the -x-y-z coarse corner
+    // of a full 2x2x2 coarse stencil and the fine cell (2i+1,2j+1,2k+1) that
+    // starts the 2x2x2 fine block at its centre.  Leftovers: fine cells of the
+    // band no full block covers, their coarse parent and the coarse neighbour
+    // per axis on the fine cell's side (-cell-1: the opposite side).
+    std::vector<int> f2cIndex, f2cChild, c2fIndex, c2fChild;
+    std::vector<int> leftIndex, leftParent, leftNbr;  // leftNbr [3][leftoverCount]
 };
 
 constexpr int kSegmentCells = 128;
@@ -122,6 +135,14 @@ void evalLocalBC(const lbm_case& c, BC& bc);
 // getInitialCondition.
 BC evalInitialCondition(const lbm_case& c, const Info& info, int i, int j, int k);
 
+struct HostLevel;
+// getLocalBC as the collide kernels use it, uniform over a level: the case's
+// limiter, nu multiplier, body force and IBB switch; with a local_bc_hook,
+// what the hook makes of them for a fluid cell (wallID -1) at the level's
+// first cell (a driver may, e.g., use another limiter on the coarsest level,
+// cases/flowAroundSphere/flowAroundSphereMain.cu:136-149).
+BC levelLocalBC(const lbm_case& c, const HostLevel& L);
+
 // buildRotors (include/rotorFunctions.h:315-585) for one level, plus the
 // rotorCell marks of the cells inside any rotor's swept cylinder.
 void buildRotors(const lbm_case& c, HostLevel& L);
@@ -129,8 +150,8 @@ void buildRotors(const lbm_case& c, HostLevel& L);
 // Split the compressed rows into bulk segments (needs wallMap and rotorCell).
 void buildSegments(HostLevel& L);
 
-// Build all tables; throws std::runtime_error on an invalid case (the
-// reference's setup throws at the same points).
+// Build all tables of every level; throws std::runtime_error on an invalid
+// case (the reference's setup throws at the same points).
 void buildDomain(const lbm_case& c, HostDomain& out);
 
 }  // namespace lbm

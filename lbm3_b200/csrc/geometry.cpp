@@ -294,6 +294,22 @@ bool coarseHasFluid(const RayMap& fine, int down, int i, int j, int k) {
     return false;
 }
 
+bool coarseHasWall(const RayMap& fine, int down, int i, int j, int k) {
+    const int kFirst = k * down, kLast = kFirst + down - 1;
+    for (int jAdd = 0; jAdd < down; ++jAdd)
+        for (int iAdd = 0; iAdd < down; ++iAdd) {
+            const size_t r = static_cast<size_t>(fine.nx) * (j * down + jAdd) + (i * down + iAdd);
+            for (long long s = fine.scan[r]; s < fine.scan[r + 1]; s += 2) {
+                const int kStart = fine.hits[s];
+                if (kStart > kLast) break;            // intervals above the coarse cell
+                if (kStart >= kFirst) return true;    // solid starts inside it
+                if (fine.hits[s + 1] <= kFirst) continue;  // interval ends below it
+                return true;                          // interval covers its bottom
+            }
+        }
+    return false;
+}
+
 bool intersectRayTriangle(float ax, float ay, float az, float bx, float by, float bz, float cx, float cy,
                           float cz, float ex, float ey, float ez, float edgeTol, float& t) {
     const float e1x = bx - ax, e1y = by - ay, e1z = bz - az;

@@ -57,6 +57,10 @@ bool isSolid(const RayMap& m, int i, int j, int k);
 // cell (i, j, k) cover at least one fluid cell of the `downsample`x finer map?
 bool coarseHasFluid(const RayMap& fine, int downsample, int i, int j, int k);
 
+// markSingleFinerWall (include/markerFunctions.h:174-220): does the coarse
+// cell (i, j, k) cover at least one solid cell of the `downsample`x finer map?
+bool coarseHasWall(const RayMap& fine, int downsample, int i, int j, int k);
+
 // intersectRayTriangle (include/boundaryConditions/interpolatedBouncebackFunctions.h:400-480),
 // ray from the origin along e; returns the ray parameter t.
 bool intersectRayTriangle(float ax, float ay, float az, float bx, float by, float bz, float cx, float cy,

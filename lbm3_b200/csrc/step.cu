@@ -4,6 +4,8 @@
 //                  (updateSingleGrid cell lambda, include/updateGrid.h:51-178)
 //   openBoundary   K2: moment-based open boundary on the streamed state (:181-355)
 //   periodicCopy   K3: ghost <- interior pre-collision copy (:358-382)
+//   interfaceExchange  K4-K6: fine-to-coarse, coarse-to-fine and leftover
+//                  interface updates between two levels (updateInterface.h)
 //   initFeq        equilibrium initial condition (applyInitialCondition.h:23-41)
 //   kineticEnergy  FP64 reduction of the Taylor–Green driver's energy
 //   macroFields    dRho, ux, uy, uz of every cell
@@ -17,6 +19,7 @@
 // synchronisation between cells.
 #define LBM_MBBC_TYPES_ONLY
 #include "builder.h"
+#include "interface.cuh"
 #include "mbbc.h"
 #include "step_launch.h"
 
@@ -896,6 +899,109 @@ __global__ void __launch_bounds__(kBlock) periodicCopy(DevLevel g) {
     writePre<F, S>(g, nb, f);
 }
 
+// K4-K6 (updateInterface, include/updateInterface.h:155-891): the interface
+// between coarse level C and fine level Fn after the fine level's two
+// substeps; FC and FF are the two levels' flippers after streaming.  Work
+// units of 8 lanes: fine-to-coarse items, then coarse-to-fine blocks, then
+// the leftover fine cells, 8 per unit (one per lane).  Reads and writes are
+// disjoint: fine-to-coarse reads fine cells under fine-to-coarse coarse cells
+// and writes those coarse cells; coarse-to-fine reads coarse-to-fine coarse
+// cells and writes fine cells between their centres.
+template <bool FC, bool FF, class S>
+__global__ void __launch_bounds__(kBlock) interfaceExchange(DevLevel C, DevLevel Fn, DevInterface I) {
+    using T = Real<S>;
+    const int lane = threadIdx.x & 7;
+    const unsigned mask = 0xFFu << (threadIdx.x & 24);
+    const int unit = (blockIdx.x * kBlock + threadIdx.x) >> 3;
+    const T omegaC = static_cast<T>(I.omegaCoarse), omegaF = static_cast<T>(I.omegaFine);
+    if (unit < I.f2cCount) {
+        // fine to coarse: the 8 children of the coarse cell, fitted at their centre
+        int nb[8], nr[8];
+        decodeNbr(Fn, __ldg(I.f2cChild + unit), nb, nullptr);
+        decodeNbr(Fn, nb[lane], nr, nullptr);
+        T f[27];
+        readPre<FF, S>(Fn, nr, f);
+        const itf::Fit<T> fit = itf::fitStencil(itf::cellMoments(f, omegaF), lane, mask, false);
+        T out[27];
+        itf::populationsFromGradient(out, fit.d0, fit.c0[0], fit.c0[1], fit.c0[2], fit.g, T(2) / omegaC);
+        decodeNbr(C, __ldg(I.f2cIndex + unit), nb, nullptr);
+        S* base = static_cast<S*>(C.f);
+#pragma unroll
+        for (int d = 0; d < 27; ++d)
+            if ((d & 7) == lane) Store<S>::st(base + (long long)preSlot<FC>(d) * C.stride + nb[preNbr(d)], out[d]);
+        return;
+    }
+    if (unit < I.f2cCount + I.c2fCount) {
+        // coarse to fine: the 8 coarse cells around a block of 8 fine cells
+        const int u = unit - I.f2cCount;
+        int nb[8], nr[8];
+        decodeNbr(C, __ldg(I.c2fIndex + u), nb, nullptr);
+        decodeNbr(C, nb[lane], nr, nullptr);
+        T f[27];
+        readPre<FC, S>(C, nr, f);
+        const itf::Fit<T> fit = itf::fitStencil(itf::cellMoments(f, omegaC), lane, mask, true);
+        // this lane's fine cell sits at +-1/4 coarse spacing from the centre
+        const T x = itf::sgnX<T>(lane) * T(0.25), y = itf::sgnY<T>(lane) * T(0.25), z = itf::sgnZ<T>(lane) * T(0.25);
+        T dRho, uv[3], G[3][3];
+        itf::evalFit(fit, x, y, z, dRho, uv, G);
+        T out[27];
+        itf::populationsFromGradient(out, dRho, uv[0], uv[1], uv[2], G, T(0.5) / omegaF);
+        decodeNbr(Fn, __ldg(I.c2fChild + u), nb, nullptr);
+        decodeNbr(Fn, nb[lane], nr, nullptr);
+        writePre<FF, S>(Fn, nr, out);
+        return;
+    }
+    // leftovers: the parent plus one coarse neighbour per axis, linear
+    // (include/updateInterface.h:694-884)
+    const int idx = (unit - I.f2cCount - I.c2fCount) * 8 + lane;
+    if (idx >= I.leftCount) return;
+    const int parent = __ldg(I.leftParent + idx);
+    int nb[8];
+    T f[27];
+    decodeNbr(C, parent, nb, nullptr);
+    readPre<FC, S>(C, nb, f);
+    const itf::CellMoments<T> mc = itf::cellMoments(f, omegaC);
+    const int wm = __ldg(C.wallMap + parent);
+    const unsigned wallData = wm >= 0 ? __ldg(C.wallData + wm) : 0u;
+    T uw[3] = {mc.ux, mc.uy, mc.uz};
+    if (wm >= 0)
+        for (int a = 0; a < 3; ++a) uw[a] = static_cast<T>(__ldg(C.wallVel + (long long)a * C.wallCount + wm));
+    T r[9] = {mc.d, mc.ux, mc.uy, mc.uz, mc.kxy, mc.kyz, mc.kxz, mc.kxxMyy, mc.kxxMzz};
+    const T cen[9] = {mc.d, mc.ux, mc.uy, mc.uz, mc.kxy, mc.kyz, mc.kxz, mc.kxxMyy, mc.kxxMzz};
+#pragma unroll 1
+    for (int a = 0; a < 3; ++a) {
+        int cell = __ldg(I.leftNbr + (long long)a * I.leftCount + idx);
+        const bool opposite = cell < 0;
+        if (opposite) cell = -cell - 1;
+        decodeNbr(C, cell, nb, nullptr);
+        readPre<FC, S>(C, nb, f);
+        const itf::CellMoments<T> m = itf::cellMoments(f, omegaC);
+        const T v[9] = {m.d, m.ux, m.uy, m.uz, m.kxy, m.kyz, m.kxz, m.kxxMyy, m.kxxMzz};
+        if (!opposite) {
+#pragma unroll
+            for (int t = 0; t < 9; ++t) r[t] += T(0.25) * (v[t] - cen[t]);
+            continue;
+        }
+        // extrapolate from the opposite side: density and moments always;
+        // the velocity towards a wall bends to the wall velocity instead
+        r[0] -= T(0.25) * (v[0] - cen[0]);
+#pragma unroll
+        for (int t = 4; t < 9; ++t) r[t] -= T(0.25) * (v[t] - cen[t]);
+        const int dir = a == 0 ? POO : a == 1 ? OPO : OOP;
+        const bool wall = (wallData & (1u << dir)) || (wallData & (1u << inv(dir)));
+#pragma unroll
+        for (int t = 1; t < 4; ++t)
+            r[t] = wall ? r[t] + (T(1) / T(24)) * (T(10) * uw[t - 1] - T(9) * cen[t] - v[t]) : r[t] - T(0.25) * (v[t] - cen[t]);
+    }
+    // the moments are strain estimates: (kxy, kyz, kxz) = off-diagonal
+    // gradient sums, kxxMyy / kxxMzz = diagonal differences
+    const T G[3][3] = {{T(0), r[4], r[6]}, {T(0), -r[7], r[5]}, {T(0), T(0), -r[8]}};
+    T out[27];
+    itf::populationsFromGradient(out, r[0], r[1], r[2], r[3], G, T(0.5) / omegaF);
+    decodeNbr(Fn, __ldg(I.leftIndex + idx), nb, nullptr);
+    writePre<FF, S>(Fn, nb, out);
+}
+
 // Characteristic (non-reflective) normal velocity of a face cell: the
 // outgoing Riemann invariant of the streamed state against the reference
 // values (include/updateGrid.h:268-308).
@@ -1329,6 +1435,19 @@ template <bool F, class S> struct RunCollide {
     }
 };
 
+template <class S> void runInterface(const DevLevel& c, const DevLevel& f, const DevInterface& I, bool flipC,
+                                     bool flipF, cudaStream_t s) {
+    const long long units = static_cast<long long>(I.f2cCount) + I.c2fCount + (I.leftCount + 7) / 8;
+    if (units <= 0) return;
+    const unsigned blocks = static_cast<unsigned>((units * 8 + kBlock - 1) / kBlock);
+    if (flipC)
+        flipF ? interfaceExchange<true, true, S><<<blocks, kBlock, 0, s>>>(c, f, I)
+              : interfaceExchange<true, false, S><<<blocks, kBlock, 0, s>>>(c, f, I);
+    else
+        flipF ? interfaceExchange<false, true, S><<<blocks, kBlock, 0, s>>>(c, f, I)
+              : interfaceExchange<false, false, S><<<blocks, kBlock, 0, s>>>(c, f, I);
+}
+
 template <bool F, class S> struct RunPeriodic {
     static void run(const DevLevel& g, cudaStream_t s) {
         if (g.perCount > 0) periodicCopy<F, S><<<blocksFor(g.perCount), kBlock, 0, s>>>(g);
@@ -1387,6 +1506,10 @@ template <bool F, class S> struct RunScatter {
 
 void LBM3_FN(launchCollideStream)(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunCollide>(g, flip, s); }
 void LBM3_FN(launchPeriodic)(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunPeriodic>(g, flip, s); }
+void LBM3_FN(launchInterface)(const DevLevel& coarse, const DevLevel& fine, const DevInterface& I, bool flipCoarse,
+                              bool flipFine, cudaStream_t s) {
+    runInterface<StepStore>(coarse, fine, I, flipCoarse, flipFine, s);
+}
 void LBM3_FN(launchOpenBoundary)(const DevLevel& g, bool flip, cudaStream_t s) {
     dispatch<RunOpen>(g, flip, s);
 }

@@ -98,6 +98,22 @@ struct DevLevel {
     int trackRotorForce;
 };
 
+// Interface lists between a coarse level and the next finer one
+// (InterfaceStruct, include/types.h:198-200) and the two levels' omega1.
+struct DevInterface {
+    const int* f2cIndex;     // [f2cCount] coarse cell
+    const int* f2cChild;     // [f2cCount] its fine child (2i, 2j, 2k)
+    int f2cCount;
+    const int* c2fIndex;     // [c2fCount] -x-y-z coarse corner of a full stencil
+    const int* c2fChild;     // [c2fCount] fine cell (2i+1, 2j+1, 2k+1)
+    int c2fCount;
+    const int* leftIndex;    // [leftCount] fine cell
+    const int* leftParent;   // [leftCount] its coarse parent
+    const int* leftNbr;      // [3][leftCount] coarse neighbour per axis (-cell-1: opposite side)
+    int leftCount;
+    double omegaCoarse, omegaFine;  // 1 / (3 nu + 1/2) of each level
+};
+
 // Collision constants in the arithmetic type T.
 template <class T> __device__ __forceinline__ const CollisionConstsT<T>& collConsts(const DevLevel& g);
 template <> __device__ __forceinline__ const CollisionConstsT<float>& collConsts<float>(const DevLevel& g) {

@@ -14,6 +14,11 @@ namespace lbm {
 
 void launchCollideStream(const DevLevel& g, bool flip, cudaStream_t s) { LBM3_BY_STORAGE(launchCollideStream, g, flip, s) }
 void launchPeriodic(const DevLevel& g, bool flip, cudaStream_t s) { LBM3_BY_STORAGE(launchPeriodic, g, flip, s) }
+void launchInterface(const DevLevel& coarse, const DevLevel& fine, const DevInterface& I, bool flipCoarse,
+                     bool flipFine, cudaStream_t s) {
+    const DevLevel& g = coarse;
+    LBM3_BY_STORAGE(launchInterface, coarse, fine, I, flipCoarse, flipFine, s)
+}
 void launchOpenBoundary(const DevLevel& g, bool flip, cudaStream_t s) {
     LBM3_BY_STORAGE(launchOpenBoundary, g, flip, s)
 }

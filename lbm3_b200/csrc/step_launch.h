@@ -14,6 +14,11 @@ void launchCollideStream(const DevLevel& g, bool flip, cudaStream_t s);
 // kernels one updateSingleGrid launches for this level
 int stepLaunchCount(const DevLevel& g);
 void launchPeriodic(const DevLevel& g, bool flip, cudaStream_t s);
+// K4-K6: fine-to-coarse, coarse-to-fine and leftover interface updates
+// between a level and the next finer one, after the finer level's substeps;
+// the flippers are the two levels' after streaming
+void launchInterface(const DevLevel& coarse, const DevLevel& fine, const DevInterface& I, bool flipCoarse,
+                     bool flipFine, cudaStream_t s);
 // K2; reads and advances the device iteration count (DevLevel::obCounter)
 void launchOpenBoundary(const DevLevel& g, bool flip, cudaStream_t s);
 void launchOpenBoundaryInit(const DevLevel& g, bool flip, cudaStream_t s);
@@ -36,6 +41,8 @@ void launchCollideBatch(float* f, int n, const CollisionConsts& P, float gx, flo
 #define LBM3_DECLARE_STORAGE_LAUNCHERS(SUF)                                                                      \
     void launchCollideStream##SUF(const DevLevel& g, bool flip, cudaStream_t s);                               \
     void launchPeriodic##SUF(const DevLevel& g, bool flip, cudaStream_t s);                                    \
+    void launchInterface##SUF(const DevLevel& coarse, const DevLevel& fine, const DevInterface& I, bool flipC,  \
+                              bool flipF, cudaStream_t s);                                                     \
     void launchOpenBoundary##SUF(const DevLevel& g, bool flip, cudaStream_t s);                                \
     void launchOpenBoundaryInit##SUF(const DevLevel& g, bool flip, cudaStream_t s);                            \
     void launchInit##SUF(const DevLevel& g, bool flip, cudaStream_t s, const float4* macro, float4 uniform);   \

@@ -19,6 +19,10 @@ _INT_ARRAYS = {
     "row_jkplus": A.ARRAY_ROW_JKPLUS, "wall_map": A.ARRAY_WALL_MAP,
     "periodic_index": A.ARRAY_PERIODIC_INDEX, "periodic_source": A.ARRAY_PERIODIC_SOURCE,
     "wall_index": A.ARRAY_WALL_INDEX, "open_index": A.ARRAY_OPEN_INDEX, "open_source": A.ARRAY_OPEN_SOURCE,
+    # interfaces towards the next finer level, read on the coarse level
+    "f2c_index": A.ARRAY_F2C_INDEX, "f2c_child": A.ARRAY_F2C_CHILD, "c2f_index": A.ARRAY_C2F_INDEX,
+    "c2f_child": A.ARRAY_C2F_CHILD, "leftover_index": A.ARRAY_LEFTOVER_INDEX,
+    "leftover_parent": A.ARRAY_LEFTOVER_PARENT, "leftover_nbr": A.ARRAY_LEFTOVER_NBR,
 }
 _UINT_ARRAYS = {"wall_data": A.ARRAY_WALL_DATA, "link_length": A.ARRAY_LINK_LENGTH}
 
@@ -34,6 +38,14 @@ def _int_len(info: A.LbmGridInfo, which: int) -> int:
         return 7 * info.wall_adjacent_count
     if which in (A.ARRAY_OPEN_INDEX, A.ARRAY_OPEN_SOURCE):
         return info.open_bc_count
+    if which in (A.ARRAY_F2C_INDEX, A.ARRAY_F2C_CHILD):
+        return info.f2c_count
+    if which in (A.ARRAY_C2F_INDEX, A.ARRAY_C2F_CHILD):
+        return info.c2f_count
+    if which in (A.ARRAY_LEFTOVER_INDEX, A.ARRAY_LEFTOVER_PARENT):
+        return info.leftover_count
+    if which == A.ARRAY_LEFTOVER_NBR:
+        return 3 * info.leftover_count
     return info.row_count
 
 

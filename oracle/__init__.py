@@ -63,6 +63,19 @@ class OGrid(C.Structure):
     ]
 
 
+class OInterface(C.Structure):
+    _fields_ = [("f2cCount", C.c_int), ("c2fCount", C.c_int), ("leftCount", C.c_int),
+                ("f2cIndex", _IP), ("f2cChild", _IP), ("c2fIndex", _IP), ("c2fChild", _IP),
+                ("leftIndex", _IP), ("leftParent", _IP), ("leftNbr", _IP)]
+
+
+MAX_LEVELS = 4
+
+
+class ODomain(C.Structure):
+    _fields_ = [("levelCount", C.c_int), ("level", OGrid * MAX_LEVELS), ("itf", OInterface * MAX_LEVELS)]
+
+
 _lib = None
 
 
@@ -111,6 +124,13 @@ def lib() -> C.CDLL:
         h.oracle_mbbc_apply.argtypes = [C.c_int] + [C.c_float] * 4 + [C.POINTER(C.c_float)]
         h.oracle_mbbc_restore_rho.argtypes = [C.c_int] + [C.c_float] * 3 + [C.POINTER(C.c_float)] * 2
         h.oracle_mbbc_restore_u.argtypes = [C.c_int, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        h.oracle_domain_build.argtypes = [C.c_void_p, C.POINTER(ODomain)]
+        h.oracle_domain_build.restype = C.c_int
+        h.oracle_domain_free.argtypes = [C.POINTER(ODomain)]
+        h.oracle_domain_step.argtypes = [C.POINTER(ODomain), C.c_int]
+        h.oracle_domain_kinetic_energy.argtypes = [C.POINTER(ODomain), C.c_float, C.c_float]
+        h.oracle_domain_kinetic_energy.restype = C.c_double
+        h.oracle_fit_check.argtypes = [C.POINTER(C.c_float), C.c_float, C.c_float, C.c_float, C.POINTER(C.c_float)]
         _lib = h
     return _lib
 
@@ -353,3 +373,78 @@ class OracleGrid:
         if n == 0:
             return np.empty(0, dtype=np.int32)
         return np.ctypeslib.as_array(ptr, shape=(n,)).copy()
+
+
+class OracleLevel(OracleGrid):
+    """One level of an :class:`OracleDomain` (a view; the domain owns it)."""
+
+    def __init__(self, view: OGrid, owner):
+        self.g = view
+        self._owner = owner
+        self._rotor_nonzero = [self.rotor_tables(r)["nonzero"] for r in range(self.g.rotorCount)]
+
+    def close(self):
+        pass
+
+    def step(self, steps: int = 1):
+        raise RuntimeError("step a multilevel domain with OracleDomain.step")
+
+
+class OracleDomain:
+    """Every level of a domain run by the oracle: its own multilevel build
+    (refinement markers, finer grids, interfaces) and the recursive time step
+    with the interface exchange."""
+
+    def __init__(self, case):
+        self.d = ODomain()
+        rc = lib().oracle_domain_build(C.cast(C.byref(case), C.c_void_p), C.byref(self.d))
+        if rc != 0:
+            raise RuntimeError(f"oracle_domain_build failed with status {rc}")
+        self.levels = [OracleLevel(self.d.level[l], self) for l in range(self.d.levelCount)]
+
+    def level(self, l: int) -> OracleLevel:
+        return self.levels[l]
+
+    @property
+    def level_count(self) -> int:
+        return self.d.levelCount
+
+    def step(self, coarse_steps: int = 1):
+        lib().oracle_domain_step(C.byref(self.d), int(coarse_steps))
+
+    def kinetic_energy(self, u_ref_phys: float, domain_length: float) -> float:
+        return lib().oracle_domain_kinetic_energy(C.byref(self.d), u_ref_phys, domain_length)
+
+    def macro(self, l: int = 0) -> np.ndarray:
+        return self.levels[l].macro()
+
+    def interface(self, l: int) -> dict:
+        """Interface lists of level l towards level l + 1."""
+        it = self.d.itf[l]
+
+        def arr(ptr, n):
+            return np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n else np.empty(0, np.int32)
+        return {"f2c_index": arr(it.f2cIndex, it.f2cCount), "f2c_child": arr(it.f2cChild, it.f2cCount),
+                "c2f_index": arr(it.c2fIndex, it.c2fCount), "c2f_child": arr(it.c2fChild, it.c2fCount),
+                "leftover_index": arr(it.leftIndex, it.leftCount),
+                "leftover_parent": arr(it.leftParent, it.leftCount),
+                "leftover_nbr": arr(it.leftNbr, 3 * it.leftCount)}
+
+    def close(self):
+        if self.d.levelCount:
+            self.levels = []
+            lib().oracle_domain_free(C.byref(self.d))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def fit_check(corners: np.ndarray, x: float, y: float, z: float) -> np.ndarray:
+    """The interface fit of 8 corner records [8][9] at (x, y, z): {dRho, u, G}."""
+    c = np.ascontiguousarray(corners, dtype=np.float32).reshape(-1)
+    out = np.empty(13, dtype=np.float32)
+    lib().oracle_fit_check(_fp(c), x, y, z, _fp(out))
+    return out

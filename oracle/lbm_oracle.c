@@ -112,6 +112,55 @@ static float kw_y(int x, int zord) {
     return x == 1 ? 2.f / 9.f : 1.f / 18.f;
 }
 
+/* Back transform of the well-conditioned scheme (applyCollision.h:390-490):
+ * central moments s[order x][order y][order z] about u -> shifted populations. */
+static void back_transform(float s[3][3][3], float ux, float uy, float uz, float f[27]) {
+    const float ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;
+    /* back transform x (:390-418): X[x line][order y][order z] */
+    float X[3][3][3];
+    for (int m = 0; m < 3; ++m)
+        for (int n = 0; n < 3; ++n) {
+            const float s0 = s[0][m][n], s1 = s[1][m][n], s2 = s[2][m][n];
+            float K = 0.f, centre = s0 * (1.f - ux2) - 2.f * ux * s1 - s2;
+            if (m == 0 && n == 0) { K = 1.f; centre = centre - ux2; }
+            else if ((m == 0 && n == 2) || (m == 2 && n == 0)) { K = 1.f / 3.f; centre = centre - ux2 / 3.f; }
+            else if (m == 2 && n == 2) { K = 1.f / 9.f; centre = centre - ux2 / 9.f; }
+            X[1][m][n] = centre;
+            if (K != 0.f) {
+                X[0][m][n] = ((s0 + K) * (ux2 - ux) + s1 * (2.f * ux - 1.f) + s2) * 0.5f;
+                X[2][m][n] = ((s0 + K) * (ux2 + ux) + s1 * (2.f * ux + 1.f) + s2) * 0.5f;
+            } else {
+                X[0][m][n] = (s0 * (ux2 - ux) + s1 * (2.f * ux - 1.f) + s2) * 0.5f;
+                X[2][m][n] = (s0 * (ux2 + ux) + s1 * (2.f * ux + 1.f) + s2) * 0.5f;
+            }
+        }
+    /* back transform y (:420-448): V[x line][y line][order z] */
+    float V[3][3][3];
+    for (int x = 0; x < 3; ++x)
+        for (int n = 0; n < 3; ++n) {
+            const float s0 = X[x][0][n], s1 = X[x][1][n], s2 = X[x][2][n];
+            if (n == 1) {
+                V[x][1][n] = s0 * (1.f - uy2) - 2.f * uy * s1 - s2;
+                V[x][0][n] = (s0 * (uy2 - uy) + s1 * (2.f * uy - 1.f) + s2) * 0.5f;
+                V[x][2][n] = (s0 * (uy2 + uy) + s1 * (2.f * uy + 1.f) + s2) * 0.5f;
+            } else {
+                const float K = kw_y(x, n);
+                V[x][1][n] = s0 * (1.f - uy2) - 2.f * uy * s1 - s2 - K * uy2;
+                V[x][0][n] = ((s0 + K) * (uy2 - uy) + s1 * (2.f * uy - 1.f) + s2) * 0.5f;
+                V[x][2][n] = ((s0 + K) * (uy2 + uy) + s1 * (2.f * uy + 1.f) + s2) * 0.5f;
+            }
+        }
+    /* back transform z (:450-490) */
+    for (int x = 0; x < 3; ++x)
+        for (int y = 0; y < 3; ++y) {
+            const float s0 = V[x][y][0], s1 = V[x][y][1], s2 = V[x][y][2];
+            const float K = kw_z(x, y);
+            f[pidx(x, y, 1)] = s0 * (1.f - uz2) - 2.f * uz * s1 - s2 - K * uz2;
+            f[pidx(x, y, 0)] = ((s0 + K) * (uz2 - uz) + s1 * (2.f * uz - 1.f) + s2) * 0.5f;
+            f[pidx(x, y, 2)] = ((s0 + K) * (uz2 + uz) + s1 * (2.f * uz + 1.f) + s2) * 0.5f;
+        }
+}
+
 void oracle_apply_collision(float f[27], const obc* bc, float nu) {
     const float gx = bc->gx, gy = bc->gy, gz = bc->gz;
     float A0[3][3]; /* zeroth z moment of line (x,y): k_xy0 */
@@ -302,49 +351,7 @@ void oracle_apply_collision(float f[27], const obc* bc, float nu) {
     s[0][1][0] = -k[0][1][0];
     s[0][0][1] = -k[0][0][1];
 
-    /* back transform x (:390-418): X[x line][order y][order z] */
-    float X[3][3][3];
-    for (int m = 0; m < 3; ++m)
-        for (int n = 0; n < 3; ++n) {
-            const float s0 = s[0][m][n], s1 = s[1][m][n], s2 = s[2][m][n];
-            float K = 0.f, centre = s0 * (1.f - ux2) - 2.f * ux * s1 - s2;
-            if (m == 0 && n == 0) { K = 1.f; centre = centre - ux2; }
-            else if ((m == 0 && n == 2) || (m == 2 && n == 0)) { K = 1.f / 3.f; centre = centre - ux2 / 3.f; }
-            else if (m == 2 && n == 2) { K = 1.f / 9.f; centre = centre - ux2 / 9.f; }
-            X[1][m][n] = centre;
-            if (K != 0.f) {
-                X[0][m][n] = ((s0 + K) * (ux2 - ux) + s1 * (2.f * ux - 1.f) + s2) * 0.5f;
-                X[2][m][n] = ((s0 + K) * (ux2 + ux) + s1 * (2.f * ux + 1.f) + s2) * 0.5f;
-            } else {
-                X[0][m][n] = (s0 * (ux2 - ux) + s1 * (2.f * ux - 1.f) + s2) * 0.5f;
-                X[2][m][n] = (s0 * (ux2 + ux) + s1 * (2.f * ux + 1.f) + s2) * 0.5f;
-            }
-        }
-    /* back transform y (:420-448): V[x line][y line][order z] */
-    float V[3][3][3];
-    for (int x = 0; x < 3; ++x)
-        for (int n = 0; n < 3; ++n) {
-            const float s0 = X[x][0][n], s1 = X[x][1][n], s2 = X[x][2][n];
-            if (n == 1) {
-                V[x][1][n] = s0 * (1.f - uy2) - 2.f * uy * s1 - s2;
-                V[x][0][n] = (s0 * (uy2 - uy) + s1 * (2.f * uy - 1.f) + s2) * 0.5f;
-                V[x][2][n] = (s0 * (uy2 + uy) + s1 * (2.f * uy + 1.f) + s2) * 0.5f;
-            } else {
-                const float K = kw_y(x, n);
-                V[x][1][n] = s0 * (1.f - uy2) - 2.f * uy * s1 - s2 - K * uy2;
-                V[x][0][n] = ((s0 + K) * (uy2 - uy) + s1 * (2.f * uy - 1.f) + s2) * 0.5f;
-                V[x][2][n] = ((s0 + K) * (uy2 + uy) + s1 * (2.f * uy + 1.f) + s2) * 0.5f;
-            }
-        }
-    /* back transform z (:450-490) */
-    for (int x = 0; x < 3; ++x)
-        for (int y = 0; y < 3; ++y) {
-            const float s0 = V[x][y][0], s1 = V[x][y][1], s2 = V[x][y][2];
-            const float K = kw_z(x, y);
-            f[pidx(x, y, 1)] = s0 * (1.f - uz2) - 2.f * uz * s1 - s2 - K * uz2;
-            f[pidx(x, y, 0)] = ((s0 + K) * (uz2 - uz) + s1 * (2.f * uz - 1.f) + s2) * 0.5f;
-            f[pidx(x, y, 2)] = ((s0 + K) * (uz2 + uz) + s1 * (2.f * uz + 1.f) + s2) * 0.5f;
-        }
+    back_transform(s, ux, uy, uz, f);
 }
 
 void oracle_apply_collision_batch(float* f, int n, float nu, float limiter, float nuMultiplier, float gx,
@@ -735,10 +742,12 @@ static void full_nbrs(const ogrid* g, const int* jMinus, const int* kMinus, int 
     nb[PMM] = kMinus[jMinus[iP]]; nb[MPP] = jP[kP[iM]]; nb[MMM] = kMinus[jMinus[iM]]; nb[PPP] = jP[kP[iP]];
 }
 
-/* buildLinkExistenceMarkerArray for one wall-adjacent cell, single level (no
- * interface links): interpolatedBouncebackFunctions.h:181-398.  Bit d set =
- * link towards a wall cell in direction d. */
-static unsigned link_bits(const ogrid* g, const int* jMinus, const int* kMinus, int cell) {
+/* buildLinkExistenceMarkerArray for one wall-adjacent cell:
+ * interpolatedBouncebackFunctions.h:181-398.  Bit d set = link towards a wall
+ * cell in direction d; `pierce` gets the links that start or end on an
+ * interface cell (iface, NULL on a single level). */
+static unsigned link_bits(const ogrid* g, const int* jMinus, const int* kMinus, int cell, const unsigned char* iface,
+                          unsigned* pierce) {
     int nb[27];
     full_nbrs(g, jMinus, kMinus, cell, nb);
     const int i = g->I[cell], j = g->J[cell], k = g->K[cell];
@@ -760,10 +769,15 @@ static unsigned link_bits(const ogrid* g, const int* jMinus, const int* kMinus, 
         if (CZ[d] < 0) km = 0;
     }
     unsigned bits = 0;
+    *pierce = 0;
+    const int me = iface && iface[cell];
     if (i != 0 && i != g->nx - 1 && j != 0 && j != g->ny - 1 && k != 0 && k != g->nz - 1) {
         if (!all) return 0;
         for (int d = 1; d < 27; ++d)
-            if (g->wallMarker[nb[d]]) bits |= 1u << d;
+            if (g->wallMarker[nb[d]]) {
+                bits |= 1u << d;
+                if (me || (iface && iface[nb[d]])) *pierce |= 1u << d;
+            }
         return bits;
     }
     for (int d = 1; d < 27; ++d) {
@@ -771,27 +785,58 @@ static unsigned link_bits(const ogrid* g, const int* jMinus, const int* kMinus, 
         if ((CX[d] > 0 && !ip) || (CY[d] > 0 && !jp) || (CZ[d] > 0 && !kp)) continue;
         if ((CX[d] < 0 && !im) || (CY[d] < 0 && !jm) || (CZ[d] < 0 && !km)) continue;
         bits |= 1u << d;
+        if (me || (iface && iface[nb[d]])) *pierce |= 1u << d;
     }
     return bits;
 }
 
-/* buildWallMarkers (include/gridBuilderFunctions.h:590-739), single level,
- * then buildLinkLengthArray (interpolatedBouncebackFunctions.h:471-660) and
+/* The coarser level of a level under construction: its grid, the parent of
+ * every cell here (-1: none), its wallIDArrayFull and its body ray maps. */
+typedef struct oparent {
+    const ogrid* grid;
+    const int* parent;
+    const int* wallIDFull;
+    const oraymap* maps;
+} oparent;
+
+/* buildWallMarkers (include/gridBuilderFunctions.h:590-739), then
+ * buildLinkLengthArray (interpolatedBouncebackFunctions.h:471-660) and
  * packWallData (:662-695).  Fills wallMarker, the wall-adjacent list in cell
- * order, wallData, linkLength and the wall velocities. */
-static void build_walls(const lbm_case* c, ogrid* g, const ostl* bodies, const oraymap* maps, const oraymap* total) {
+ * order, wallData, linkLength and the wall velocities.  On a finer level
+ * (`up` set) a cell with a parent inherits the parent's wall state and body
+ * marks, and the parent's wallID wins (steps 1-2); `iface` marks interface
+ * cells (links from or to them get length 1/2), `overlap` the cells whose
+ * wallData carries the overlap bit; `wallIDFull` (may be NULL) receives the
+ * wallID of every cell. */
+static void build_walls(const lbm_case* c, ogrid* g, const ostl* bodies, const oraymap* maps, const oraymap* total,
+                        const oparent* up, const unsigned char* iface, const unsigned char* overlap,
+                        int* wallIDFull) {
     const int n = g->cellCount;
     for (int q = 0; q < n; ++q) g->wallMarker[q] = (unsigned char)oray_solid(total, g->I[q], g->J[q], g->K[q]);
+    if (up)
+        for (int q = 0; q < n; ++q)
+            if (up->parent[q] >= 0) g->wallMarker[q] = up->grid->wallMarker[up->parent[q]];
     int* wallID = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
     unsigned char* src = (unsigned char*)malloc((size_t)(n > 0 ? n : 1));
     unsigned char* bw = (unsigned char*)malloc((size_t)(n > 0 ? n : 1));
     for (int q = 0; q < n; ++q) wallID[q] = -1;
     for (int b = 0; b < c->body_count; ++b) {
         for (int q = 0; q < n; ++q) src[q] = (unsigned char)oray_solid(&maps[b], g->I[q], g->J[q], g->K[q]);
+        if (up)
+            for (int q = 0; q < n; ++q) {
+                const int pc = up->parent[q];
+                if (pc >= 0)
+                    src[q] = (unsigned char)oray_solid(&up->maps[b], up->grid->I[pc], up->grid->J[pc], up->grid->K[pc]);
+            }
         spread_cells(g, src, bw);
-        for (int q = 0; q < n; ++q)
-            if (bw[q] && !g->wallMarker[q]) wallID[q] = b;  /* the last body wins */
+        for (int q = 0; q < n; ++q) {
+            if (!bw[q] || g->wallMarker[q]) continue;
+            int id = b;  /* the last body wins, a parent's wallID above all */
+            if (up && up->parent[q] >= 0 && up->wallIDFull[up->parent[q]] >= 0) id = up->wallIDFull[up->parent[q]];
+            wallID[q] = id;
+        }
     }
+    if (wallIDFull) memcpy(wallIDFull, wallID, sizeof(int) * (size_t)n);
     free(src);
     free(bw);
     int nw = 0;
@@ -808,7 +853,8 @@ static void build_walls(const lbm_case* c, ogrid* g, const ostl* bodies, const o
     int* kMinus = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
     for (int q = 0; q < n; ++q) { jMinus[g->jPlus[q]] = q; kMinus[g->kPlus[q]] = q; }
     unsigned* links = (unsigned*)malloc(sizeof(unsigned) * (size_t)(nw > 0 ? nw : 1));
-    for (int w = 0; w < nw; ++w) links[w] = link_bits(g, jMinus, kMinus, g->wallIndex[w]);
+    unsigned* pierce = (unsigned*)malloc(sizeof(unsigned) * (size_t)(nw > 0 ? nw : 1));
+    for (int w = 0; w < nw; ++w) links[w] = link_bits(g, jMinus, kMinus, g->wallIndex[w], iface, &pierce[w]);
     free(jMinus);
     free(kMinus);
 
@@ -836,7 +882,7 @@ static void build_walls(const lbm_case* c, ogrid* g, const ostl* bodies, const o
                 const float bx = t->bx[tri] - x, by = t->by[tri] - y, bz = t->bz[tri] - z;
                 const float cx = t->cx[tri] - x, cy = t->cy[tri] - y, cz = t->cz[tri] - z;
                 for (int d = 1; d < 27; ++d) {
-                    if (!((links[w] >> d) & 1u)) continue;
+                    if (!((links[w] >> d) & 1u) || ((pierce[w] >> d) & 1u)) continue;
                     float tHit;
                     if (!oray_triangle(ax, ay, az, bx, by, bz, cx, cy, cz, (float)CX[d], (float)CY[d], (float)CZ[d],
                                        edgeTol, &tHit))
@@ -864,11 +910,13 @@ static void build_walls(const lbm_case* c, ogrid* g, const ostl* bodies, const o
     g->wallForce = (float*)calloc(3 * (size_t)(nw > 0 ? nw : 1), sizeof(float));
     for (int w = 0; w < nw; ++w) {
         unsigned data = (unsigned)ids[w] << 27;
+        if (overlap && overlap[g->wallIndex[w]]) data |= 1u;
         int li = 0;
         for (int d = 1; d < 27; ++d) {
             if (!((links[w] >> d) & 1u)) continue;
             float qv = len[(size_t)w * 27 + d];
-            if (qv > 1.f) qv = 0.5f;           /* no crossing found: safe fallback */
+            if ((pierce[w] >> d) & 1u) qv = 0.5f;  /* through an interface: as on the other level */
+            else if (qv > 1.f) qv = 0.5f;      /* no crossing found: safe fallback */
             else if (qv < 0.f) qv = -qv;       /* near miss kept */
             qv = qv < 0.f ? 0.f : (qv > 1.f ? 1.f : qv);
             data |= 1u << d;
@@ -893,10 +941,12 @@ static void build_walls(const lbm_case* c, ogrid* g, const ostl* bodies, const o
     }
     free(ids);
     free(links);
+    free(pierce);
     free(len);
 }
 
 static int build_rotor(ogrid* g, int r, const lbm_rotor* rt);
+static int finish_level(const lbm_case* c, ogrid* g, const unsigned char* overlap);
 
 int oracle_build(const lbm_case* c, ogrid* g) {
     memset(g, 0, sizeof(*g));
@@ -986,16 +1036,40 @@ int oracle_build(const lbm_case* c, ogrid* g) {
     }
     const int n = g->cellCount;
     g->wallMarker = (unsigned char*)calloc((size_t)(n > 0 ? n : 1), 1);
-    build_walls(c, g, bodies, maps, &total);
+    build_walls(c, g, bodies, maps, &total, NULL, NULL, NULL, NULL);
     for (int b = 0; b < nb; ++b) { ostl_free(&bodies[b]); oray_free(&maps[b]); }
     free(bodies);
     free(maps);
     oray_free(&total);
 
+    return finish_level(c, g, NULL);
+}
+
+/* gridBuilderToGrid (include/gridBuilderFunctions.h:1032-1564) for one level
+ * whose cells, NBR and walls are built, then buildRotors and
+ * applyInitialCondition.  `overlap` (NULL: none) marks the cells under an
+ * interface overlap (wallMap -2).  The level's uniform getLocalBC is the
+ * case's, or the local hook's answer for a fluid cell at the first cell. */
+static int finish_level(const lbm_case* c, ogrid* g, const unsigned char* overlap) {
+    const int n = g->cellCount;
+    if (c->local_bc_hook && n > 0) {
+        obc bc;
+        oracle_default_bc(&bc);
+        bc.collisionLimiter = g->limiter;
+        bc.nuMultiplier = g->nuMultiplier;
+        bc.gx = g->gx; bc.gy = g->gy; bc.gz = g->gz;
+        bc.useIBB = g->useIBB;
+        bc.wallID = -1;
+        bc = call_hook(c->local_bc_hook, c->hook_user, bc, g, g->I[0], g->J[0], g->K[0]);
+        g->limiter = bc.collisionLimiter;
+        g->nuMultiplier = bc.nuMultiplier;
+        g->gx = bc.gx; g->gy = bc.gy; g->gz = bc.gz;
+        g->useIBB = bc.useIBB;
+    }
     /* gridBuilderToGrid (:1032-1126): first-in-row marks, inclusive max scan,
      * exclusive sum scan, compressed arrays */
-    int* firstInRow = (int*)malloc(sizeof(int) * n);
-    int* scan = (int*)malloc(sizeof(int) * n);
+    int* firstInRow = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    int* scan = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
     for (int q = 0; q < n; ++q) {
         if (q == 0) { firstInRow[q] = 0; scan[q] = 1; continue; }
         const int jk = g->jPlus[g->kPlus[q]], jkPrev = g->jPlus[g->kPlus[q - 1]];
@@ -1026,8 +1100,8 @@ int oracle_build(const lbm_case* c, ogrid* g) {
     free(firstInRow); free(scan);
 
     /* wallMap (:1128-1149) and the periodic overlap (:1232-1274) */
-    g->wallMap = (int*)malloc(sizeof(int) * n);
-    for (int q = 0; q < n; ++q) g->wallMap[q] = g->wallMarker[q] ? -3 : -1;
+    g->wallMap = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    for (int q = 0; q < n; ++q) g->wallMap[q] = g->wallMarker[q] ? -3 : (overlap && overlap[q] ? -2 : -1);
     for (int w = 0; w < g->wallCount; ++w) g->wallMap[g->wallIndex[w]] = w;
     const int layers = 1 << g->gridID;
     for (int q = 0; q < n; ++q) {
@@ -1863,4 +1937,692 @@ void oracle_macro(const ogrid* g, float* out) {
         oracle_get_drho_u(f, m);
         for (int q = 0; q < 4; ++q) out[q * n + cell] = m[q];
     }
+}
+
+/* ---- multilevel domains ------------------------------------------------------
+ * buildGrids over several levels (include/gridBuilderFunctions.h:9-64,
+ * :66-201, :299-739, :741-1231), the recursive time step (updateAllGrids,
+ * include/updateGrid.h:388-396) and the interface exchange (updateInterface,
+ * include/updateInterface.h:29-891). */
+
+static unsigned char* ucalloc(int n) { return (unsigned char*)calloc((size_t)(n > 0 ? n : 1), 1); }
+static int* imalloc(int n) { return (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1)); }
+
+/* initializeGridInfo for a finer level (gridBuilderFunctions.h:50-62) */
+static void finer_info(const lbm_case* c, const ogrid* cg, ogrid* fg, int level) {
+    init_info(c, fg);
+    fg->gridID = level;
+    fg->res = cg->res * 0.5f;
+    fg->nx = cg->nx * 2; fg->ny = cg->ny * 2; fg->nz = cg->nz * 2;
+    fg->ox = cg->ox - fg->res * 0.5f;
+    fg->oy = cg->oy - fg->res * 0.5f;
+    fg->oz = cg->oz - fg->res * 0.5f;
+    fg->dtPhys = cg->dtPhys * 0.5f;
+    fg->nu = (fg->dtPhys * c->nu_phys) / ((fg->res / 1000.f) * (fg->res / 1000.f));
+}
+
+/* GridBuilderStruct markers of one level while the domain is built
+ * (include/types.h:181-190) */
+typedef struct omarks {
+    unsigned char *deep, *f2c, *c2f, *refine;
+    int* parent;
+    unsigned char *parentInterface, *parentF2C, *needValues;
+    int* wallIDFull;
+} omarks;
+
+static void omarks_free(omarks* M) {
+    free(M->deep); free(M->f2c); free(M->c2f); free(M->refine); free(M->parent);
+    free(M->parentInterface); free(M->parentF2C); free(M->needValues); free(M->wallIDFull);
+    memset(M, 0, sizeof(*M));
+}
+
+/* spreadMarkers in place: the result replaces `m` */
+static void spread_in_place(const ogrid* g, unsigned char* m) {
+    unsigned char* t = ucalloc(g->cellCount);
+    spread_cells(g, m, t);
+    memcpy(m, t, (size_t)g->cellCount);
+    free(t);
+}
+
+/* markRefinementCells (include/markerFunctions.h:419-450) with markKeepCells
+ * (:411-417), markAllFinerFluids/Walls (:222-252) and
+ * applyUserRefinementModification (:254-271) */
+static void mark_refinement(const lbm_case* c, const ogrid* g, omarks* M, const oraymap* total, int NL) {
+    const int n = g->cellCount, lv = g->gridID;
+    unsigned char* keep = ucalloc(n);
+    M->deep = ucalloc(n);
+    for (int q = 0; q < n; ++q)
+        for (int m = lv; m < NL; ++m) {
+            if (oray_block_has_fluid(&total[m], g->I[q], g->J[q], g->K[q], 1 << (m - lv))) keep[q] = 1;
+            if (oray_block_has_wall(&total[m], g->I[q], g->J[q], g->K[q], 1 << (m - lv))) M->deep[q] = 1;
+        }
+    spread_in_place(g, keep);
+    if (lv > 0)
+        for (int q = 0; q < n; ++q) keep[q] = keep[q] || M->parentInterface[q];
+    for (int r = 0; r < c->wall_refinement_count; ++r) spread_in_place(g, M->deep);
+    const float* box = c->refine_box[lv];
+    const int useBox = box[0] < box[3] && box[1] < box[4] && box[2] < box[5];
+    lbm_grid_info info;
+    memset(&info, 0, sizeof(info));
+    info.grid_id = g->gridID;
+    info.cell_count = n;
+    info.cell_count_x = g->nx; info.cell_count_y = g->ny; info.cell_count_z = g->nz;
+    info.res = g->res; info.ox = g->ox; info.oy = g->oy; info.oz = g->oz;
+    info.nu = g->nu; info.dt_phys = g->dtPhys;
+    for (int q = 0; q < n; ++q) {
+        int mark = M->deep[q];
+        if (useBox) {
+            const float x = g->I[q] * g->res + g->ox, y = g->J[q] * g->res + g->oy, z = g->K[q] * g->res + g->oz;
+            if (x > box[0] && x < box[3] && y > box[1] && y < box[4] && z > box[2] && z < box[5]) mark = 1;
+        }
+        if (c->refinement_hook) c->refinement_hook(c->hook_user, g->I[q], g->J[q], g->K[q], &mark, &info);
+        M->deep[q] = mark != 0;
+    }
+    for (int q = 0; q < n; ++q) {
+        if (lv > 0 && M->parentInterface[q]) M->deep[q] = 0;
+        M->deep[q] = M->deep[q] && keep[q];
+    }
+    M->f2c = ucalloc(n);
+    spread_cells(g, M->deep, M->f2c);
+    for (int q = 0; q < n; ++q) M->f2c[q] = M->f2c[q] && keep[q] && !M->deep[q];
+    M->c2f = ucalloc(n);
+    memcpy(M->c2f, M->f2c, (size_t)n);
+    spread_in_place(g, M->c2f);
+    spread_in_place(g, M->c2f);
+    for (int q = 0; q < n; ++q) M->c2f[q] = M->c2f[q] && keep[q] && !M->deep[q] && !M->f2c[q];
+    M->refine = ucalloc(n);
+    for (int q = 0; q < n; ++q) M->refine[q] = M->deep[q] || M->f2c[q] || M->c2f[q];
+    free(keep);
+}
+
+/* buildFinerGridBuilder (gridBuilderFunctions.h:134-201): 8 children of every
+ * refinement-marked coarse cell, then sortIJK (:204-234), buildNBRPlus, and
+ * buildIJKFull steps 6-7 (parent map, parent-interface marks) */
+static void build_finer(const ogrid* cg, const omarks* CM, ogrid* fg, omarks* FM) {
+    int count = 0;
+    for (int q = 0; q < cg->cellCount; ++q) count += CM->refine[q];
+    const int n = 8 * count;
+    int* ijk = imalloc(3 * n);
+    int w = 0;
+    for (int q = 0; q < cg->cellCount; ++q) {
+        if (!CM->refine[q]) continue;
+        for (int ka = 0; ka < 2; ++ka)
+            for (int ja = 0; ja < 2; ++ja)
+                for (int ia = 0; ia < 2; ++ia) {
+                    ijk[3 * w] = 2 * cg->I[q] + ia;
+                    ijk[3 * w + 1] = 2 * cg->J[q] + ja;
+                    ijk[3 * w + 2] = 2 * cg->K[q] + ka;
+                    ++w;
+                }
+    }
+    qsort(ijk, (size_t)n, 3 * sizeof(int), cmp_kji);
+    fg->cellCount = n;
+    fg->I = imalloc(n); fg->J = imalloc(n); fg->K = imalloc(n);
+    for (int q = 0; q < n; ++q) { fg->I[q] = ijk[3 * q]; fg->J[q] = ijk[3 * q + 1]; fg->K[q] = ijk[3 * q + 2]; }
+    free(ijk);
+    nbr_plus(fg);
+    FM->parent = imalloc(n);
+    FM->parentInterface = ucalloc(n);
+    FM->parentF2C = ucalloc(n);
+    for (int q = 0; q < n; ++q) {
+        const int pc = find_cell(cg, fg->I[q] / 2, fg->J[q] / 2, fg->K[q] / 2);
+        FM->parent[q] = pc;
+        if (pc < 0) continue;
+        FM->parentInterface[q] = CM->c2f[pc] || CM->f2c[pc];
+        FM->parentF2C[q] = CM->f2c[pc];
+    }
+}
+
+/* deleteExcessCells (gridBuilderFunctions.h:402-588) for one level */
+static void delete_excess(ogrid* g, omarks* M, const ogrid* cg, const oraymap* total, int finest) {
+    const int n = g->cellCount;
+    if (cg)
+        for (int q = 0; q < n; ++q) {
+            M->parent[q] = find_cell(cg, g->I[q] / 2, g->J[q] / 2, g->K[q] / 2);
+            M->parentInterface[q] = M->parent[q] >= 0;
+        }
+    unsigned char* keep = ucalloc(n);
+    for (int q = 0; q < n; ++q) {
+        keep[q] = !oray_solid(total, g->I[q], g->J[q], g->K[q]);
+        if (cg && M->parentInterface[q]) keep[q] = 1;
+    }
+    spread_in_place(g, keep);
+    if (!finest)
+        for (int q = 0; q < n; ++q) keep[q] = keep[q] && !M->deep[q];
+    if (cg) {
+        unsigned char* s1 = ucalloc(n);
+        unsigned char* s3 = ucalloc(n);
+        spread_cells(g, M->parentF2C, s1);
+        memcpy(s3, s1, (size_t)n);
+        spread_in_place(g, s3);
+        spread_in_place(g, s3);
+        M->needValues = ucalloc(n);
+        for (int q = 0; q < n; ++q) {
+            if (M->parentInterface[q] && !s3[q]) keep[q] = 0;
+            M->needValues[q] = M->parentInterface[q] && keep[q] && !s1[q];
+        }
+        free(s1);
+        free(s3);
+    }
+    /* fullToKeep scan and compaction of the per-cell arrays */
+    int w = 0;
+    for (int q = 0; q < n; ++q) {
+        if (!keep[q]) continue;
+        g->I[w] = g->I[q]; g->J[w] = g->J[q]; g->K[w] = g->K[q];
+        if (cg) { M->parent[w] = M->parent[q]; M->needValues[w] = M->needValues[q]; }
+        if (!finest) { M->f2c[w] = M->f2c[q]; M->c2f[w] = M->c2f[q]; }
+        ++w;
+    }
+    g->cellCount = w;
+    nbr_plus(g);
+    free(keep);
+}
+
+/* fillFineToCoarseInterface and fillCoarseToFineInterface
+ * (gridBuilderFunctions.h:741-1030) with the child map of :1192-1222 */
+static void build_interface(const ogrid* cg, const omarks* CM, const ogrid* fg, const omarks* FM, ointerface* I) {
+    const int nc = cg->cellCount, nf = fg->cellCount;
+    int* child = imalloc(nc);
+    for (int q = 0; q < nc; ++q) child[q] = -1;
+    for (int q = 0; q < nf; ++q) {
+        const int pc = FM->parent[q];
+        if (pc >= 0 && fg->I[q] % 2 == 0 && fg->J[q] % 2 == 0 && fg->K[q] % 2 == 0) child[pc] = q;
+    }
+    /* fine to coarse: marked coarse cells that are not walls */
+    I->f2cCount = 0;
+    for (int q = 0; q < nc; ++q) I->f2cCount += CM->f2c[q] && !cg->wallMarker[q];
+    I->f2cIndex = imalloc(I->f2cCount);
+    I->f2cChild = imalloc(I->f2cCount);
+    for (int q = 0, t = 0; q < nc; ++q)
+        if (CM->f2c[q] && !cg->wallMarker[q]) { I->f2cIndex[t] = q; I->f2cChild[t] = child[q]; ++t; }
+    /* coarse to fine: cells that see a full block of marked coarse cells
+     * around the centre of 8 existing fine cells */
+    unsigned char* mark = ucalloc(nc);
+    for (int q = 0; q < nc; ++q) mark[q] = CM->c2f[q] && !cg->wallMarker[q];
+    int* jMinusF = imalloc(nf);
+    int* kMinusF = imalloc(nf);
+    for (int q = 0; q < nf; ++q) { jMinusF[fg->jPlus[q]] = q; kMinusF[fg->kPlus[q]] = q; }
+    int* jMinusC = imalloc(nc);
+    int* kMinusC = imalloc(nc);
+    for (int q = 0; q < nc; ++q) { jMinusC[cg->jPlus[q]] = q; kMinusC[cg->kPlus[q]] = q; }
+    int* sees = imalloc(nc);
+    I->c2fCount = 0;
+    for (int q = 0; q < nc; ++q) {
+        sees[q] = -1;
+        if (!mark[q]) continue;
+        /* NBR of the coarse cell (finishNBRPlus, NBRFunctions.h:5-11) */
+        const int iP = q + 1 < nc ? q + 1 : 0, jP = cg->jPlus[q], kP = cg->kPlus[q], jkP = cg->jPlus[kP];
+        const int ijP = jP + 1 < nc ? jP + 1 : 0, ikP = kP + 1 < nc ? kP + 1 : 0, ijkP = jkP + 1 < nc ? jkP + 1 : 0;
+        const int nb[7] = {iP, jP, ijP, kP, ikP, jkP, ijkP};
+        const int di[7] = {1, 0, 1, 0, 1, 0, 1}, dj[7] = {0, 1, 1, 0, 0, 1, 1}, dk[7] = {0, 0, 0, 1, 1, 1, 1};
+        int ok = 1;
+        for (int t = 0; t < 7; ++t) if (!mark[nb[t]]) ok = 0;
+        for (int t = 0; t < 7 && ok; ++t)
+            if (cg->I[nb[t]] != cg->I[q] + di[t] || cg->J[nb[t]] != cg->J[q] + dj[t] || cg->K[nb[t]] != cg->K[q] + dk[t])
+                ok = 0;
+        if (!ok) continue;
+        const int top = child[ijkP];
+        if (top < 0) continue;
+        int fjk = top - 1;
+        if (fjk < 0) fjk = nf - 1;
+        const int fk = jMinusF[fjk];
+        const int fs = kMinusF[fk];
+        const int fj = fg->jPlus[fs];
+        const int fiP = fs + 1 < nf ? fs + 1 : 0, fijP = fj + 1 < nf ? fj + 1 : 0, fikP = fk + 1 < nf ? fk + 1 : 0;
+        const int fijkP = fjk + 1 < nf ? fjk + 1 : 0;
+        const int fb[8] = {fs, fiP, fj, fijP, fk, fikP, fjk, fijkP};
+        const int ei[8] = {1, 2, 1, 2, 1, 2, 1, 2}, ej[8] = {1, 1, 2, 2, 1, 1, 2, 2}, ek[8] = {1, 1, 1, 1, 2, 2, 2, 2};
+        for (int t = 0; t < 8 && ok; ++t)
+            if (fg->I[fb[t]] != 2 * cg->I[q] + ei[t] || fg->J[fb[t]] != 2 * cg->J[q] + ej[t] ||
+                fg->K[fb[t]] != 2 * cg->K[q] + ek[t])
+                ok = 0;
+        if (!ok) continue;
+        sees[q] = fs;
+        I->c2fCount++;
+    }
+    I->c2fIndex = imalloc(I->c2fCount);
+    I->c2fChild = imalloc(I->c2fCount);
+    unsigned char* received = ucalloc(nf);
+    for (int q = 0, t = 0; q < nc; ++q) {
+        if (sees[q] < 0) continue;
+        I->c2fIndex[t] = q;
+        I->c2fChild[t] = sees[q];
+        ++t;
+        const int fs = sees[q], fj = fg->jPlus[fs], fk = fg->kPlus[fs], fjk = fg->jPlus[fk];
+        const int cells[8] = {fs, fs + 1 < nf ? fs + 1 : 0, fj, fj + 1 < nf ? fj + 1 : 0,
+                              fk, fk + 1 < nf ? fk + 1 : 0, fjk, fjk + 1 < nf ? fjk + 1 : 0};
+        for (int u = 0; u < 8; ++u) received[cells[u]] = 1;
+    }
+    /* leftovers (:919-1029): fine cells that need coarse values and got none */
+    I->leftCount = 0;
+    for (int q = 0; q < nf; ++q) I->leftCount += FM->needValues[q] && !fg->wallMarker[q] && !received[q];
+    const int m = I->leftCount;
+    I->leftIndex = imalloc(m);
+    I->leftParent = imalloc(m);
+    I->leftNbr = imalloc(3 * m);
+    for (int q = 0, t = 0; q < nf; ++q) {
+        if (!(FM->needValues[q] && !fg->wallMarker[q] && !received[q])) continue;
+        const int pc = FM->parent[q];
+        const int ic = cg->I[pc], jc = cg->J[pc], kc = cg->K[pc];
+        /* per axis: the neighbour on the fine cell's side if it is marked and
+         * in place, else the opposite one coded as -cell-1, else the parent */
+        const int plus[3] = {pc + 1 >= nc ? 0 : pc + 1, cg->jPlus[pc], cg->kPlus[pc]};
+        const int minus[3] = {pc - 1 < 0 ? nc - 1 : pc - 1, jMinusC[pc], kMinusC[pc]};
+        const int odd[3] = {fg->I[q] % 2 == 1, fg->J[q] % 2 == 1, fg->K[q] % 2 == 1};
+        for (int a = 0; a < 3; ++a) {
+            const int e[3] = {a == 0, a == 1, a == 2};
+            int pick = pc;
+            const int first = odd[a] ? plus[a] : minus[a], second = odd[a] ? minus[a] : plus[a];
+            const int sf = odd[a] ? 1 : -1;
+            if (mark[first] && cg->I[first] == ic + sf * e[0] && cg->J[first] == jc + sf * e[1] &&
+                cg->K[first] == kc + sf * e[2])
+                pick = first;
+            else if (mark[second] && cg->I[second] == ic - sf * e[0] && cg->J[second] == jc - sf * e[1] &&
+                     cg->K[second] == kc - sf * e[2])
+                pick = -second - 1;
+            I->leftNbr[(size_t)a * m + t] = pick;
+        }
+        I->leftIndex[t] = q;
+        I->leftParent[t] = pc;
+        ++t;
+    }
+    free(child); free(mark); free(jMinusF); free(kMinusF); free(jMinusC); free(kMinusC); free(sees); free(received);
+}
+
+int oracle_domain_build(const lbm_case* c, odomain* d) {
+    memset(d, 0, sizeof(*d));
+    const int NL = c->grid_level_count;
+    if (NL < 1 || NL > LBM_MAX_LEVELS) return LBM_ERR_INVALID;
+    if (NL == 1) {
+        d->levelCount = 1;
+        return oracle_build(c, &d->level[0]);
+    }
+    if (c->body_count < 0 || c->body_count > LBM_MAX_BODIES || c->rotor_count < 0 || c->rotor_count > 4)
+        return LBM_ERR_INVALID;
+    d->levelCount = NL;
+    init_info(c, &d->level[0]);
+    for (int l = 1; l < NL; ++l) finer_info(c, &d->level[l - 1], &d->level[l], l);
+    /* bodies on every level (initializeVoxelizers, voxelizerFunctions.h:692-728) */
+    const int nb = c->body_count;
+    ostl* bodies = (ostl*)calloc((size_t)(nb > 0 ? nb : 1), sizeof(ostl));
+    oraymap* maps = (oraymap*)calloc((size_t)NL * (nb > 0 ? nb : 1), sizeof(oraymap));
+    oraymap total[LBM_MAX_LEVELS];
+    for (int b = 0; b < nb; ++b) {
+        if (!c->body[b].triangles || ostl_load(&bodies[b], c->body[b].triangles, c->body[b].triangle_count) == 0) {
+            for (int q = 0; q <= b; ++q) ostl_free(&bodies[q]);
+            free(bodies); free(maps);
+            return LBM_ERR_BUILD;
+        }
+        ostl_bins(&bodies[b], c->res_global);
+    }
+    for (int l = 0; l < NL; ++l) {
+        const ogrid* g = &d->level[l];
+        for (int b = 0; b < nb; ++b) oray_voxelize(&maps[l * nb + b], &bodies[b], g->ox, g->oy, g->oz, g->res, g->nx, g->ny);
+        if (nb > 0) {
+            oray_copy(&total[l], &maps[l * nb]);
+            for (int b = 1; b < nb; ++b) oray_union(&total[l], &maps[l * nb + b]);
+        } else {
+            oray_empty(&total[l], g->nx, g->ny);
+        }
+    }
+    /* buildIJKFull (:299-400): level 0 from the skeleton (a skeleton cell is
+     * kept when it covers fluid on any level, plus one layer) */
+    {
+        ogrid* g = &d->level[0];
+        const int snx = g->nx / 2, sny = g->ny / 2, snz = g->nz / 2;
+        const size_t sc = (size_t)snx * sny * snz;
+        unsigned char* keepS = (unsigned char*)calloc(sc, 1);
+        unsigned char* keepT = (unsigned char*)calloc(sc, 1);
+        for (size_t sIdx = 0; sIdx < sc; ++sIdx) {
+            const int ks = (int)(sIdx / ((size_t)snx * sny)), rem = (int)(sIdx % ((size_t)snx * sny));
+            for (int m = 0; m < NL && !keepS[sIdx]; ++m)
+                keepS[sIdx] = (unsigned char)oray_block_has_fluid(&total[m], rem % snx, rem / snx, ks, 2 << m);
+        }
+        spread_dense(keepS, keepT, snx, sny, snz);
+        int kept = 0;
+        for (size_t q = 0; q < sc; ++q) kept += keepT[q];
+        const int n0 = 8 * kept;
+        int* ijk = imalloc(3 * n0);
+        int cf = 0;
+        for (size_t sIdx = 0; sIdx < sc; ++sIdx) {
+            if (!keepT[sIdx]) continue;
+            const int ks = (int)(sIdx / ((size_t)snx * sny)), rem = (int)(sIdx % ((size_t)snx * sny));
+            for (int ka = 0; ka < 2; ++ka)
+                for (int ja = 0; ja < 2; ++ja)
+                    for (int ia = 0; ia < 2; ++ia) {
+                        ijk[3 * cf] = 2 * (rem % snx) + ia;
+                        ijk[3 * cf + 1] = 2 * (rem / snx) + ja;
+                        ijk[3 * cf + 2] = 2 * ks + ka;
+                        ++cf;
+                    }
+        }
+        free(keepS); free(keepT);
+        qsort(ijk, (size_t)n0, 3 * sizeof(int), cmp_kji);
+        g->cellCount = n0;
+        g->I = imalloc(n0); g->J = imalloc(n0); g->K = imalloc(n0);
+        for (int q = 0; q < n0; ++q) { g->I[q] = ijk[3 * q]; g->J[q] = ijk[3 * q + 1]; g->K[q] = ijk[3 * q + 2]; }
+        free(ijk);
+        nbr_plus(g);
+    }
+    omarks marks[LBM_MAX_LEVELS];
+    memset(marks, 0, sizeof(marks));
+    for (int l = 0; l + 1 < NL; ++l) {
+        mark_refinement(c, &d->level[l], &marks[l], total, NL);
+        build_finer(&d->level[l], &marks[l], &d->level[l + 1], &marks[l + 1]);
+    }
+    for (int l = 0; l < NL; ++l)
+        delete_excess(&d->level[l], &marks[l], l > 0 ? &d->level[l - 1] : NULL, &total[l], l == NL - 1);
+    /* buildWallMarkers (:590-739) with the interface overlap (step 7) */
+    int rc = 0;
+    for (int l = 0; l < NL && rc == 0; ++l) {
+        ogrid* g = &d->level[l];
+        omarks* M = &marks[l];
+        const int n = g->cellCount;
+        unsigned char* overlap = ucalloc(n);
+        unsigned char* iface = ucalloc(n);
+        for (int q = 0; q < n; ++q) {
+            if (l + 1 < NL) {
+                overlap[q] = M->f2c[q];
+                iface[q] = M->f2c[q] || M->c2f[q];
+            }
+            if (l > 0 && M->parent[q] >= 0) {
+                iface[q] = 1;
+                if (marks[l - 1].c2f[M->parent[q]]) overlap[q] = 1;
+            }
+        }
+        g->wallMarker = ucalloc(n);
+        M->wallIDFull = imalloc(n);
+        oparent up = {l > 0 ? &d->level[l - 1] : NULL, M->parent, l > 0 ? marks[l - 1].wallIDFull : NULL,
+                      l > 0 ? &maps[(l - 1) * nb] : NULL};
+        build_walls(c, g, bodies, &maps[l * nb], &total[l], l > 0 ? &up : NULL, iface, overlap, M->wallIDFull);
+        rc = finish_level(c, g, overlap);
+        free(overlap);
+        free(iface);
+    }
+    for (int l = 0; rc == 0 && l + 1 < NL; ++l)
+        build_interface(&d->level[l], &marks[l], &d->level[l + 1], &marks[l + 1], &d->itf[l]);
+    for (int l = 0; l < NL; ++l) omarks_free(&marks[l]);
+    for (int b = 0; b < nb; ++b) ostl_free(&bodies[b]);
+    for (int q = 0; q < NL * nb; ++q) oray_free(&maps[q]);
+    for (int l = 0; l < NL; ++l) oray_free(&total[l]);
+    free(bodies);
+    free(maps);
+    if (rc != 0) oracle_domain_free(d);
+    return rc;
+}
+
+void oracle_domain_free(odomain* d) {
+    for (int l = 0; l < d->levelCount; ++l) {
+        oracle_free(&d->level[l]);
+        ointerface* I = &d->itf[l];
+        free(I->f2cIndex); free(I->f2cChild); free(I->c2fIndex); free(I->c2fChild);
+        free(I->leftIndex); free(I->leftParent); free(I->leftNbr);
+    }
+    memset(d, 0, sizeof(*d));
+}
+
+/* pre-collision populations of a cell in the current esotwist state */
+static void read_pre(const ogrid* g, int cell, float f[27]) {
+    int nb[8];
+    get_nbr(g, cell, nb);
+    const size_t n = (size_t)g->cellCount;
+    for (int dd = 0; dd < 27; ++dd) f[dd] = g->f[(size_t)(g->flip ? INV[dd] : dd) * n + nb[pre_nbr(dd)]];
+}
+
+static void write_pre(ogrid* g, int cell, const float f[27]) {
+    int nb[8];
+    get_nbr(g, cell, nb);
+    const size_t n = (size_t)g->cellCount;
+    for (int dd = 0; dd < 27; ++dd) g->f[(size_t)(g->flip ? INV[dd] : dd) * n + nb[pre_nbr(dd)]] = f[dd];
+}
+
+/* Density deviation, velocity and the five velocity-gradient estimates of a
+ * cell from its populations (the stencil loops of updateInterface.h:204-239):
+ * out = {dRho, ux, uy, uz, kxy, kyz, kxz, kxx-kyy, kxx-kzz}; sums of the
+ * second moments run over the directions in index order. */
+static void interface_moments(const float f[27], float omega, float out[9]) {
+    float m[4];
+    oracle_get_drho_u(f, m);
+    const float rho = 1.f + m[0];
+    float pxy = 0.f, pyz = 0.f, pxz = 0.f, pmy = 0.f, pmz = 0.f;
+    for (int dd = 1; dd < 27; ++dd) {
+        const int xy = CX[dd] * CY[dd], yz = CY[dd] * CZ[dd], xz = CX[dd] * CZ[dd];
+        const int my = CX[dd] * CX[dd] - CY[dd] * CY[dd], mz = CX[dd] * CX[dd] - CZ[dd] * CZ[dd];
+        if (xy > 0) pxy = pxy + f[dd]; else if (xy < 0) pxy = pxy - f[dd];
+        if (yz > 0) pyz = pyz + f[dd]; else if (yz < 0) pyz = pyz - f[dd];
+        if (xz > 0) pxz = pxz + f[dd]; else if (xz < 0) pxz = pxz - f[dd];
+        if (my > 0) pmy = pmy + f[dd]; else if (my < 0) pmy = pmy - f[dd];
+        if (mz > 0) pmz = pmz + f[dd]; else if (mz < 0) pmz = pmz - f[dd];
+    }
+    out[0] = m[0]; out[1] = m[1]; out[2] = m[2]; out[3] = m[3];
+    out[4] = -3.f * omega * (pxy / rho - m[1] * m[2]);
+    out[5] = -3.f * omega * (pyz / rho - m[2] * m[3]);
+    out[6] = -3.f * omega * (pxz / rho - m[1] * m[3]);
+    out[7] = -1.5f * omega * (pmy / rho - (m[1] * m[1] - m[2] * m[2]));
+    out[8] = -1.5f * omega * (pmz / rho - (m[1] * m[1] - m[3] * m[3]));
+}
+
+/* reconstructInterpolatedF (updateInterface.h:29-153): populations from
+ * dRho, u and the second-order central moments, every other central moment
+ * at its rest value; the back transform x, y, z of applyCollision
+ * (applyCollision.h:390-490). */
+static void reconstruct_f(float f[27], float dRho, float ux, float uy, float uz, float k011, float k101, float k110,
+                          float k200, float k020, float k002) {
+    float s[3][3][3];
+    memset(s, 0, sizeof(s));
+    s[0][0][0] = dRho;
+    s[2][0][0] = k200; s[0][2][0] = k020; s[0][0][2] = k002;
+    s[1][1][0] = k110; s[1][0][1] = k101; s[0][1][1] = k011;
+    s[2][2][0] = dRho / 9.f; s[0][2][2] = dRho / 9.f; s[2][0][2] = dRho / 9.f;
+    s[2][2][2] = dRho / 27.f;
+    back_transform(s, ux, uy, uz, f);
+}
+
+/* Quadratic fit over a 2x2x2 stencil (Schoenherr 2015, the coefficient set
+ * of updateInterface.h:262-306 and :443-545): corners q = self, +i, +j, +ij,
+ * +k, +ik, +jk, +ijk at (+-1/2)^3; v[q] = interface_moments of corner q.
+ * Each coefficient is the signed corner sum of updateInterface.h, formed
+ * corner by corner. */
+typedef struct ofit {
+    float d[8];                /* 1, x, y, z, xy, xz, yz, xyz */
+    float u[3][11];            /* 1, x, y, z, xy, xz, yz, xyz, xx, yy, zz */
+} ofit;
+
+static float corner_sum(const float v[8][9], int field, int px, int py, int pz) {
+    float s = 0.f;
+    for (int q = 0; q < 8; ++q) {
+        const int sx = (q & 1) ? 1 : -1, sy = (q & 2) ? 1 : -1, sz = (q & 4) ? 1 : -1;
+        const int sign = (px ? sx : 1) * (py ? sy : 1) * (pz ? sz : 1);
+        s = sign > 0 ? s + v[q][field] : s - v[q][field];
+    }
+    return s;
+}
+
+static void fit_stencil(const float v[8][9], ofit* F) {
+    enum { D = 0, UX = 1, KXY = 4, KYZ = 5, KXZ = 6, KMY = 7, KMZ = 8 };
+    F->d[0] = 0.125f * corner_sum(v, D, 0, 0, 0);
+    F->d[1] = 0.25f * corner_sum(v, D, 1, 0, 0);
+    F->d[2] = 0.25f * corner_sum(v, D, 0, 1, 0);
+    F->d[3] = 0.25f * corner_sum(v, D, 0, 0, 1);
+    F->d[4] = 0.5f * corner_sum(v, D, 1, 1, 0);
+    F->d[5] = 0.5f * corner_sum(v, D, 1, 0, 1);
+    F->d[6] = 0.5f * corner_sum(v, D, 0, 1, 1);
+    F->d[7] = corner_sum(v, D, 1, 1, 1);
+    for (int a = 0; a < 3; ++a) {
+        F->u[a][1] = 0.25f * corner_sum(v, UX + a, 1, 0, 0);
+        F->u[a][2] = 0.25f * corner_sum(v, UX + a, 0, 1, 0);
+        F->u[a][3] = 0.25f * corner_sum(v, UX + a, 0, 0, 1);
+        F->u[a][4] = 0.5f * corner_sum(v, UX + a, 1, 1, 0);
+        F->u[a][5] = 0.5f * corner_sum(v, UX + a, 1, 0, 1);
+        F->u[a][6] = 0.5f * corner_sum(v, UX + a, 0, 1, 1);
+        F->u[a][7] = corner_sum(v, UX + a, 1, 1, 1);
+    }
+    const float sux = corner_sum(v, UX, 0, 0, 0), suy = corner_sum(v, UX + 1, 0, 0, 0), suz = corner_sum(v, UX + 2, 0, 0, 0);
+    const float uxXY = corner_sum(v, UX, 1, 1, 0), uxXZ = corner_sum(v, UX, 1, 0, 1);
+    const float uyXY = corner_sum(v, UX + 1, 1, 1, 0), uyYZ = corner_sum(v, UX + 1, 0, 1, 1);
+    const float uzXZ = corner_sum(v, UX + 2, 1, 0, 1), uzYZ = corner_sum(v, UX + 2, 0, 1, 1);
+    const float kxyX = corner_sum(v, KXY, 1, 0, 0), kxyY = corner_sum(v, KXY, 0, 1, 0);
+    const float kxzX = corner_sum(v, KXZ, 1, 0, 0), kxzZ = corner_sum(v, KXZ, 0, 0, 1);
+    const float kyzY = corner_sum(v, KYZ, 0, 1, 0), kyzZ = corner_sum(v, KYZ, 0, 0, 1);
+    const float myX = corner_sum(v, KMY, 1, 0, 0), myY = corner_sum(v, KMY, 0, 1, 0), myZ = corner_sum(v, KMY, 0, 0, 1);
+    const float mzX = corner_sum(v, KMZ, 1, 0, 0), mzY = corner_sum(v, KMZ, 0, 1, 0), mzZ = corner_sum(v, KMZ, 0, 0, 1);
+    /* a000, b000, c000 */
+    F->u[0][0] = 0.015625f * (2.f * (uyXY + uzXZ - kxyY - kxzZ) + 8.f * sux - myX - mzX);
+    F->u[1][0] = 0.015625f * (2.f * (uxXY + uzYZ + myY - kxyX - kyzZ) + 8.f * suy - mzY);
+    F->u[2][0] = 0.015625f * (2.f * (uxXZ + uyYZ + mzZ - kxzX - kyzY) + 8.f * suz - myZ);
+    /* a200 .. c002 */
+    F->u[0][8] = 0.0625f * (2.f * (uyXY + uzXZ) + myX + mzX);
+    F->u[1][8] = 0.125f * (kxyX - 2.f * uxXY);
+    F->u[2][8] = 0.125f * (kxzX - 2.f * uxXZ);
+    F->u[0][9] = 0.125f * (kxyY - 2.f * uyXY);
+    F->u[1][9] = 0.0625f * (2.f * (uxXY + uzYZ - myY) + mzY);
+    F->u[2][9] = 0.125f * (kyzY - 2.f * uyYZ);
+    F->u[0][10] = 0.125f * (kxzZ - 2.f * uzXZ);
+    F->u[1][10] = 0.125f * (kyzZ - 2.f * uzYZ);
+    F->u[2][10] = 0.0625f * (2.f * (uxXZ + uyYZ - mzZ) + myZ);
+}
+
+/* velocity gradient of the fit at (x, y, z): G[a][b] = d u_a / d x_b */
+static void fit_gradient(const ofit* F, float x, float y, float z, float G[3][3]) {
+    for (int a = 0; a < 3; ++a) {
+        const float* c = F->u[a];
+        G[a][0] = c[1] + c[4] * y + c[5] * z + c[7] * y * z + 2.f * c[8] * x;
+        G[a][1] = c[2] + c[4] * x + c[6] * z + c[7] * x * z + 2.f * c[9] * y;
+        G[a][2] = c[3] + c[5] * x + c[6] * y + c[7] * x * y + 2.f * c[10] * z;
+    }
+}
+
+/* second-order central moments from the strain rate, rescaled by
+ * sigma / omega of the target level (updateInterface.h:334-346, :645-660) */
+static void populations_from_gradient(float f[27], float dRho, const float u[3], const float G[3][3], float sigma,
+                                      float omega) {
+    const float rho = 1.f + dRho;
+    const float k011 = -(1.f / 3.f) * (G[1][2] + G[2][1]) * sigma / omega * rho;
+    const float k101 = -(1.f / 3.f) * (G[0][2] + G[2][0]) * sigma / omega * rho;
+    const float k110 = -(1.f / 3.f) * (G[0][1] + G[1][0]) * sigma / omega * rho;
+    const float mxxMyy = -(2.f / 3.f) * (G[0][0] - G[1][1]) * sigma / omega * rho;
+    const float mxxMzz = -(2.f / 3.f) * (G[0][0] - G[2][2]) * sigma / omega * rho;
+    const float k200 = (1.f / 3.f) * (mxxMyy + mxxMzz + dRho);
+    const float k020 = (1.f / 3.f) * (-2.f * mxxMyy + mxxMzz + dRho);
+    const float k002 = (1.f / 3.f) * (mxxMyy - 2.f * mxxMzz + dRho);
+    reconstruct_f(f, dRho, u[0], u[1], u[2], k011, k101, k110, k200, k020, k002);
+}
+
+/* updateInterface (updateInterface.h:155-891) between level c and level c+1 */
+static void interface_update(ogrid* cg, ogrid* fg, const ointerface* I) {
+    const float omegaC = 1.f / (3.f * cg->nu + 0.5f), omegaF = 1.f / (3.f * fg->nu + 0.5f);
+    /* fine to coarse (:155-359) */
+#pragma omp parallel for schedule(static)
+    for (int t = 0; t < I->f2cCount; ++t) {
+        int nb[8];
+        get_nbr(fg, I->f2cChild[t], nb);
+        float v[8][9], f[27];
+        for (int q = 0; q < 8; ++q) { read_pre(fg, nb[q], f); interface_moments(f, omegaF, v[q]); }
+        ofit F;
+        fit_stencil(v, &F);
+        float G[3][3], u[3] = {F.u[0][0], F.u[1][0], F.u[2][0]};
+        fit_gradient(&F, 0.f, 0.f, 0.f, G);
+        populations_from_gradient(f, F.d[0], u, G, 2.f, omegaC);
+        write_pre(cg, I->f2cIndex[t], f);
+    }
+    /* coarse to fine blocks (:362-676) */
+#pragma omp parallel for schedule(static)
+    for (int t = 0; t < I->c2fCount; ++t) {
+        int nb[8], fb[8];
+        get_nbr(cg, I->c2fIndex[t], nb);
+        float v[8][9], f[27];
+        for (int q = 0; q < 8; ++q) { read_pre(cg, nb[q], f); interface_moments(f, omegaC, v[q]); }
+        ofit F;
+        fit_stencil(v, &F);
+        get_nbr(fg, I->c2fChild[t], fb);
+        for (int q = 0; q < 8; ++q) {
+            const float x = (q & 1) ? 0.25f : -0.25f, y = (q & 2) ? 0.25f : -0.25f, z = (q & 4) ? 0.25f : -0.25f;
+            const float dRho = F.d[0] + F.d[1] * x + F.d[2] * y + F.d[3] * z + F.d[4] * x * y + F.d[5] * x * z +
+                               F.d[6] * y * z + F.d[7] * x * y * z;
+            float u[3], G[3][3];
+            for (int a = 0; a < 3; ++a) {
+                const float* c = F.u[a];
+                u[a] = c[0] + c[1] * x + c[2] * y + c[3] * z + c[4] * x * y + c[5] * x * z + c[6] * y * z +
+                       c[7] * x * y * z + c[8] * x * x + c[9] * y * y + c[10] * z * z;
+            }
+            fit_gradient(&F, x, y, z, G);
+            populations_from_gradient(f, dRho, u, G, 0.5f, omegaF);
+            write_pre(fg, fb[q], f);
+        }
+    }
+    /* leftovers (:678-884) */
+#pragma omp parallel for schedule(static)
+    for (int t = 0; t < I->leftCount; ++t) {
+        const int pc = I->leftParent[t];
+        float f[27], cen[9], r[9], uw[3];
+        read_pre(cg, pc, f);
+        interface_moments(f, omegaC, cen);
+        const int wm = cg->wallMap[pc];
+        const unsigned wallData = wm >= 0 ? cg->wallData[wm] : 0u;
+        for (int a = 0; a < 3; ++a) uw[a] = wm >= 0 ? cg->wallVel[(size_t)a * cg->wallCount + wm] : cen[1 + a];
+        for (int q = 0; q < 9; ++q) r[q] = cen[q];
+        const int dirs[3] = {1, 6, 4}; /* POO, OPO, OOP */
+        for (int a = 0; a < 3; ++a) {
+            int cell = I->leftNbr[(size_t)a * I->leftCount + t];
+            const int opposite = cell < 0;
+            if (opposite) cell = -cell - 1;
+            float v[9];
+            read_pre(cg, cell, f);
+            interface_moments(f, omegaC, v);
+            if (!opposite) {
+                for (int q = 0; q < 9; ++q) r[q] += 0.25f * (v[q] - cen[q]);
+                continue;
+            }
+            r[0] -= 0.25f * (v[0] - cen[0]);
+            for (int q = 4; q < 9; ++q) r[q] -= 0.25f * (v[q] - cen[q]);
+            const int wall = (wallData & (1u << dirs[a])) || (wallData & (1u << INV[dirs[a]]));
+            for (int q = 1; q < 4; ++q) {
+                if (!wall) r[q] -= 0.25f * (v[q] - cen[q]);
+                else r[q] += (1.f / 24.f) * (10.f * uw[q - 1] - 9.f * cen[q] - v[q]);
+            }
+        }
+        const float G[3][3] = {{0.f, r[4], r[6]}, {0.f, -r[7], r[5]}, {0.f, 0.f, -r[8]}};
+        const float u[3] = {r[1], r[2], r[3]};
+        populations_from_gradient(f, r[0], u, G, 0.5f, omegaF);
+        write_pre(fg, I->leftIndex[t], f);
+    }
+}
+
+static void domain_update(odomain* d, int level) {
+    oracle_step(&d->level[level], 1);
+    if (level + 1 < d->levelCount && level + 1 < LBM_MAX_LEVELS) {
+        for (int i = 0; i < 2; ++i) domain_update(d, level + 1);
+        interface_update(&d->level[level], &d->level[level + 1], &d->itf[level]);
+    }
+}
+
+void oracle_domain_step(odomain* d, int coarseSteps) {
+    for (int s = 0; s < coarseSteps; ++s) domain_update(d, 0);
+}
+
+double oracle_domain_kinetic_energy(const odomain* d, float uRefPhys, float domainLength) {
+    double e = 0.0;
+    for (int l = 0; l < d->levelCount; ++l) e += oracle_kinetic_energy(&d->level[l], uRefPhys, domainLength);
+    return e;
+}
+
+void oracle_fit_check(const float* corners, float x, float y, float z, float* out) {
+    /* test hook: the fit of 8 corner records {dRho, ux, uy, uz, kxy, kyz, kxz,
+     * kxx-kyy, kxx-kzz} evaluated at (x, y, z): out = {dRho, ux, uy, uz, G} */
+    float v[8][9];
+    for (int q = 0; q < 8; ++q)
+        for (int t = 0; t < 9; ++t) v[q][t] = corners[q * 9 + t];
+    ofit F;
+    fit_stencil(v, &F);
+    out[0] = F.d[0] + F.d[1] * x + F.d[2] * y + F.d[3] * z + F.d[4] * x * y + F.d[5] * x * z + F.d[6] * y * z +
+             F.d[7] * x * y * z;
+    for (int a = 0; a < 3; ++a) {
+        const float* c = F.u[a];
+        out[1 + a] = c[0] + c[1] * x + c[2] * y + c[3] * z + c[4] * x * y + c[5] * x * z + c[6] * y * z +
+                     c[7] * x * y * z + c[8] * x * x + c[9] * y * y + c[10] * z * z;
+    }
+    float G[3][3];
+    fit_gradient(&F, x, y, z, G);
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) out[4 + 3 * a + b] = G[a][b];
 }

@@ -160,6 +160,40 @@ void oracle_flow_sums(const ogrid* g, int plane, int layer, int h0, int h1, int 
 /* number of OpenMP threads the oracle uses */
 int oracle_threads(void);
 
+/* Interface lists between a level and the next finer one (InterfaceStruct,
+ * include/types.h:198-200). */
+typedef struct ointerface {
+    int f2cCount, c2fCount, leftCount;
+    int *f2cIndex, *f2cChild, *c2fIndex, *c2fChild, *leftIndex, *leftParent, *leftNbr; /* leftNbr [3][leftCount] */
+} ointerface;
+
+/* Every level of a domain (std::vector<GridStruct>) and the interfaces
+ * between consecutive levels, owned by the coarser one. */
+typedef struct odomain {
+    int levelCount;
+    ogrid level[LBM_MAX_LEVELS];
+    ointerface itf[LBM_MAX_LEVELS];
+} odomain;
+
+/* buildGrids over all levels (include/gridBuilderFunctions.h:1577-1670):
+ * refinement markers, finer grids, excess-cell deletion, walls with parent
+ * inheritance, interfaces, then applyInitialCondition on every level.  A
+ * single-level case builds exactly as oracle_build.  Returns 0 or a negative
+ * LBM_ERR_* code. */
+int oracle_domain_build(const lbm_case* c, odomain* d);
+void oracle_domain_free(odomain* d);
+/* updateAllGrids(grids, 0) `coarseSteps` times (include/updateGrid.h:388-396):
+ * level L steps 2^L times per coarse step, each finer pair followed by
+ * updateInterface (include/updateInterface.h:887-891). */
+void oracle_domain_step(odomain* d, int coarseSteps);
+/* getKineticEnergy over every level (cases/taylorGreenVortex/taylorGreenVortexMain.cu:116-180) */
+double oracle_domain_kinetic_energy(const odomain* d, float uRefPhys, float domainLength);
+/* The interface fit of 8 corner records {dRho, ux, uy, uz, kxy, kyz, kxz,
+ * kxx-kyy, kxx-kzz} (corners self, +i, +j, +ij, +k, +ik, +jk, +ijk at
+ * (+-1/2)^3) evaluated at (x, y, z): out[13] = {dRho, ux, uy, uz, the
+ * velocity gradient G[a][b] = d u_a / d x_b row by row}. */
+void oracle_fit_check(const float* corners, float x, float y, float z, float* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -355,6 +355,24 @@ int oray_block_has_fluid(const oraymap* m, int ic, int jc, int kc, int down) {
     return 0;
 }
 
+/* markSingleFinerWall for one coarse cell (include/markerFunctions.h:174-220):
+ * 1 when some fine cell of the down^3 block is inside a solid interval. */
+int oray_block_has_wall(const oraymap* m, int ic, int jc, int kc, int down) {
+    const int kFirst = kc * down, kLast = kFirst + down - 1;
+    for (int ja = 0; ja < down; ++ja)
+        for (int ia = 0; ia < down; ++ia) {
+            const size_t ray = (size_t)m->nx * (jc * down + ja) + (ic * down + ia);
+            for (long long s = m->scan[ray]; s < m->scan[ray + 1]; s += 2) {
+                const int kStart = m->map[s];
+                if (kStart > kLast) break;
+                if (kStart >= kFirst) return 1;
+                if (m->map[s + 1] <= kFirst) continue;
+                return 1;
+            }
+        }
+    return 0;
+}
+
 /* intersectRayTriangle (interpolatedBouncebackFunctions.h:400-469): the ray
  * from the origin along e against triangle abc with an edge tolerance;
  * returns 1 and the ray parameter t on a hit (t may be <= 0 or > 1). */

@@ -36,6 +36,7 @@ void oray_empty(oraymap* m, int nx, int ny);
 void oray_free(oraymap* m);
 int oray_solid(const oraymap* m, int i, int j, int k);
 int oray_block_has_fluid(const oraymap* m, int ic, int jc, int kc, int down);
+int oray_block_has_wall(const oraymap* m, int ic, int jc, int kc, int down);
 int oray_triangle(float ax, float ay, float az, float bx, float by, float bz, float cx, float cy, float cz, float ex,
                   float ey, float ez, float edgeTol, float* tOut);
 

@@ -65,7 +65,9 @@ def test_plan_reports_storage_footprint():
 
 
 @pytest.mark.parametrize("mutate,code", [
-    (lambda c: setattr(c, "grid_level_count", 2), A.LBM_ERR_BUILD),
+    (lambda c: setattr(c, "grid_level_count", 5), A.LBM_ERR_BUILD),
+    (lambda c: setattr(c, "grid_level_count", 0), A.LBM_ERR_BUILD),
+    (lambda c: setattr(c, "wall_refinement_count", -1), A.LBM_ERR_BUILD),
     (lambda c: c.bounds.__setitem__(3, c.bounds[0] - 1.0), A.LBM_ERR_BUILD),
     (lambda c: setattr(c.face[0], "kind", 7), A.LBM_ERR_BUILD),
     (lambda c: setattr(c, "res_global", 0.0), A.LBM_ERR_BUILD),
