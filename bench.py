@@ -57,6 +57,18 @@ def make_case(name: str, storage: str):
                 f"D={24.0 * k:g} cells at ({64.0 * k:g},{ny / 2.0:g},{nz / 2.0:g}), IBB, velocity inlet u=0.04, "
                 f"non-reflective pressure outlet, strict-velocity sides, nu=0.0096 (Re 100)")
         return s.case, desc, s
+    if name.startswith("msphere"):
+        # flow around a sphere on three levels: base 128x64x64, refinement
+        # boxes of 96x64x64 level-1 and 112x80x80 level-2 cells around the
+        # sphere (D = 48 finest cells), Re 300, inlet u = 0.04
+        from lbm3_b200.cases import multilevel_sphere
+        dims = name[len("msphere"):] or "128x64x64"
+        nx, ny, nz = (int(v) for v in dims.split("x"))
+        s = multilevel_sphere(nx, ny, nz, storage=st)
+        desc = (f"multilevel sphere: 3 levels (ratio 2), base {nx}x{ny}x{nz}, refinement boxes of 96x64x64 "
+                f"level-1 and 112x80x80 level-2 cells, icosphere of 20480 triangles with D=48 finest cells, "
+                f"wall refinement 2, velocity inlet u=0.04, non-reflective outlet, Re=300")
+        return s.case, desc, s
     if name == "box256x128x128":
         # the 256x128x128 single-level grid of the flow-around-sphere
         # configuration, fully periodic and without the obstacle
@@ -295,11 +307,13 @@ def run_ours(args):
     value = whole_job_rate(updates, args.steps, world, ms_max * 1e-3)
 
     # roofline of the dominant kernel (collide-stream): algorithmic bytes =
-    # 2 x 27 populations per fluid cell update at the storage width
+    # 2 x 27 populations per fluid cell update at the storage width, summed
+    # over the collide launches of a coarse step (one per level substep)
     bpp = BYTES_PER_POP[args.storage]
     alg_bytes = updates * 2 * 27 * bpp
     per_launch_ms = kernel_ms / max(launches, 1)
-    achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
+    per_step_kernel_ms = kernel_ms / kt_steps
+    achieved = alg_bytes / (per_step_kernel_ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
     traffic = None
     tfile = ROOT / "profiles" / "traffic.json"
@@ -311,14 +325,16 @@ def run_ours(args):
     # end to end through the public API: upload the initial state from pinned
     # host memory, then run steps that each read the step's observable back
     e2e_steps = max(10, min(args.steps // 10, 200))
-    f0 = g.populations()
-    pinned = torch.from_numpy(f0).pin_memory()
+    levels = g.level_count()
+    pinned = [torch.from_numpy(g.populations(l)).pin_memory() for l in range(levels)]
     import numpy as np
-    f_np = pinned.numpy()
+    f_np = [t.numpy() for t in pinned]
+    upload_bytes = sum(a.nbytes for a in f_np)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    g.set_populations(f_np)
-    sphere = tgv is not None and hasattr(tgv, "drag_coefficient")
+    for l in range(levels):
+        g.set_populations(f_np[l], l)
+    sphere = tgv is not None and (hasattr(tgv, "drag_coefficient") or hasattr(tgv, "diameter_finest"))
     for _ in range(e2e_steps):
         g.update_all_grids(1)
         if sphere:
@@ -355,10 +371,12 @@ def run_ours(args):
                          "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
                          "kernel": "collidePrefetch (bulk segments + wall-adjacent cells, one persistent launch)",
                          "kernel_ms_per_launch": round(per_launch_ms, 5),
-                         "algorithmic_bytes_per_launch": alg_bytes, "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)"},
+                         "collide_launches_per_step": round(launches / kt_steps, 3),
+                         "algorithmic_bytes_per_launch": int(alg_bytes * kt_steps / max(launches, 1)),
+                         "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)"},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS",
-                    "h2d_bytes_per_step": int(f0.nbytes // e2e_steps), "d2h_bytes_per_step": 48 if sphere else 8,
+                    "h2d_bytes_per_step": int(upload_bytes // e2e_steps), "d2h_bytes_per_step": 48 if sphere else 8,
                     "steps": e2e_steps,
                     "note": "initial populations uploaded from pinned host memory inside the timed "
                             "region; every step reads its tracked observable back (tracker period 1: "
@@ -424,6 +442,24 @@ def storage_comparison(args, f32_value: float, torch) -> dict:
         g.close()
         out["storage_f16"] = {"value": round(v16, 2), "unit": "MLUPS", "ratio_vs_f32": round(v16 / f32_value, 4),
                               "workload": "same workload, FP16-shifted populations, FP32 arithmetic"}
+    # the multilevel configuration: three levels, substep schedule replayed as graphs
+    cm, dm, _ = make_case("msphere128x64x64", args.storage)
+    g = L.build_grids(cm)
+    s = torch.cuda.Stream()
+    g.set_stream(s.cuda_stream)
+    g.update_all_grids(args.warmup)
+    steps = max(2, min(args.steps, 1000))
+    ms = g.time_steps_graph(steps)
+    vm = g.fluid_updates_per_iteration * steps / (ms * 1e-3) / 1e6
+    g.time_steps(min(steps, 200))
+    kms, klaunch = g.last_kernel_time()
+    out["multilevel_sphere"] = {
+        "value": round(vm, 2), "unit": "MLUPS", "ms_per_coarse_step": round(ms / steps, 5),
+        "fluid_updates_per_coarse_step": g.fluid_updates_per_iteration,
+        "cells_per_level": [g.info(l).cell_count for l in range(g.level_count())],
+        "collide_share_of_step": round(kms / min(steps, 200) / (ms / steps), 4),
+        "workload": dm + "; MLUPS counts level-L updates 2^L times per coarse step"}
+    g.close()
     tgv32 = L.tgv_plain_method().case
     g = L.build_grids(tgv32)
     s = torch.cuda.Stream()

@@ -85,10 +85,15 @@ def test_refined_slab_channel_with_leftovers_matches_oracle():
 
 
 def test_refined_sphere_channel_matches_oracle():
-    """Open channel with a sphere refined by its walls: open boundaries on
-    level 0, the body on level 1; fields and the drag force."""
-    c = L.open_channel(48, 24, 24, u_in=0.04, nu_lattice=0.02)
+    """Open channel with a sphere refined by its walls and a refinement box:
+    open boundaries on level 0, the body on level 1; fields and the drag
+    force.  AllOne collision (limiter 0), as the reference's wall drivers
+    use: at this resolution (D = 8 fine cells) K17 with a limiter makes the
+    flow unstable within 20 steps on the GPU and in the oracle alike, and
+    the two then diverge as any two roundings of an unstable run do."""
+    c = L.open_channel(48, 24, 24, u_in=0.04, nu_lattice=0.02, collision_limiter=0.0)
     G.set_bodies(c, [G.icosphere(2, 4.0, (16.0, 12.0, 12.0))])
+    L.set_refine_box(c, 0, (8.0, 4.0, 4.0), (26.0, 20.0, 20.0))
     c.grid_level_count = 2
     c.wall_refinement_count = 2
     c.track_wall_force = 1
@@ -103,6 +108,32 @@ def test_refined_sphere_channel_matches_oracle():
         to_si = c.rho_phys * dx ** 4 / info.dt_phys ** 2
         drag_gpu = g.wall_force(0)[0]
         drag_oracle = d.level(1).wall_force(0)[0] / (2 * steps) * to_si
+        assert drag_gpu == pytest.approx(drag_oracle, rel=1e-4), (drag_gpu, drag_oracle)
+    d.close()
+
+
+def test_multilevel_sphere_configuration_matches_oracle():
+    """The multilevel sphere configuration at its size (base 128x64x64, three
+    levels, D = 48 finest cells, Re 300; AllOne on level 0 and K17 with
+    limiter 0.1 on the finer levels, as the reference's sphere driver):
+    10 coarse steps (40 finest substeps), fields on every level and the drag."""
+    from lbm3_b200.cases import multilevel_sphere
+    s = multilevel_sphere()
+    c = s.case
+    d = O.OracleDomain(c)
+    steps = 10
+    with L.build_grids(c) as g:
+        assert g.level_count() == 3
+        g.update_all_grids(steps)
+        d.step(steps)
+        compare_levels(g, d, near_rest=True)
+        drag_gpu = g.wall_force(0)[0]
+        drag_oracle = 0.0
+        for l in range(3):
+            info = g.info(l)
+            dx = info.res / 1000.0
+            to_si = c.rho_phys * dx ** 4 / info.dt_phys ** 2
+            drag_oracle += d.level(l).wall_force(0)[0] / (steps << l) * to_si
         assert drag_gpu == pytest.approx(drag_oracle, rel=1e-4), (drag_gpu, drag_oracle)
     d.close()
 
