@@ -12,7 +12,8 @@
 //                         velocity); once with wallID -1 for the uniform
 //                         collision limiter, nu multiplier, body force and
 //                         IBB switch the kernels apply everywhere
-//   getRefinementModifier not called: this build has one grid level.
+//   getRefinementModifier every cell of every level but the finest, with the
+//                         marker the walls set (markRefinementCells)
 #pragma once
 
 #include "types.h"
@@ -77,6 +78,12 @@ inline void localBCHook(void*, lbm_bc* bc, int i, int j, int k, const lbm_grid_i
     bcToC(b, bc);
 }
 
+inline void refinementHook(void*, int i, int j, int k, int* mark, const lbm_grid_info* info) {
+    bool m = *mark != 0;
+    ::getRefinementModifier(i, j, k, m, infoFromGridInfo(*info));
+    *mark = m ? 1 : 0;
+}
+
 inline void check(int rc) {
     if (rc < 0) throw std::runtime_error(lbm_last_error());
 }
@@ -119,7 +126,8 @@ struct GridStruct {
 // the fluid cell updates of one coarse iteration.
 inline long long buildGrids(std::vector<GridStruct>& grids, std::vector<STLStruct>& gridStaticSTLs,
                             std::vector<STLStruct>& rotorSTLs, const BoundsStruct& Bounds) {
-    if (GRID_LEVEL_COUNT != 1) throw std::runtime_error("buildGrids: this build has one grid level");
+    if (GRID_LEVEL_COUNT < 1 || GRID_LEVEL_COUNT > LBM_MAX_LEVELS)
+        throw std::runtime_error("buildGrids: GRID_LEVEL_COUNT must be in [1, LBM_MAX_LEVELS]");
     if (gridStaticSTLs.size() > LBM_MAX_BODIES) throw std::runtime_error("buildGrids: too many static STLs");
     if (rotorSTLs.size() > LBM_MAX_ROTORS) throw std::runtime_error("buildGrids: too many rotor STLs");
     lbm_case c;
@@ -172,6 +180,7 @@ inline long long buildGrids(std::vector<GridStruct>& grids, std::vector<STLStruc
     c.open_bc_hook = &lbm3_detail::openBCHook;
     c.initial_condition_hook = &lbm3_detail::initialConditionHook;
     c.local_bc_hook = &lbm3_detail::localBCHook;
+    c.refinement_hook = &lbm3_detail::refinementHook;
     lbm_grids* raw = nullptr;
     long long fluidUpdates = 0;
     lbm3_detail::check(lbm_build_grids(&c, &raw, &fluidUpdates));

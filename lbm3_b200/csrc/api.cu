@@ -109,6 +109,11 @@ struct lbm_grids {
     bool graphsEnabled = true;
     cudaStream_t captureStream = nullptr;
     cudaGraphExec_t pairExec[2] = {nullptr, nullptr};
+    // per level with a finer one: a side stream on which the level's own
+    // update runs while the finer levels' substeps run on the grid stream
+    // (they touch disjoint state until the interface joins them)
+    std::vector<cudaStream_t> sideStreams;
+    std::vector<cudaEvent_t> forkEvents, joinEvents;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double* scratch = nullptr;
     int* errorFlag = nullptr;  // device word the kernels set when a bounded wait gives up
@@ -131,6 +136,9 @@ struct lbm_grids {
         for (cudaGraphExec_t e : pairExec)
             if (e) cudaGraphExecDestroy(e);
         if (captureStream) cudaStreamDestroy(captureStream);
+        for (cudaStream_t t : sideStreams) cudaStreamDestroy(t);
+        for (cudaEvent_t e : forkEvents) cudaEventDestroy(e);
+        for (cudaEvent_t e : joinEvents) cudaEventDestroy(e);
     }
 };
 
@@ -235,21 +243,21 @@ void advanceRotors(LevelState& L) {
     }
 }
 
-void updateSingleGrid(lbm_grids* g, LevelState& L) {
+void updateSingleGrid(lbm_grids* g, LevelState& L, cudaStream_t stream) {
     if (!L.rotors.empty()) advanceRotors(L);
     const bool flip = L.info.esotwistFlipper;
     if (g->timingKernels) {
         const size_t k = static_cast<size_t>(g->kernelEventsUsed);
-        ck(cudaEventRecord(g->kernelEvents[k], g->stream), "event");
-        lbm::launchCollideStream(L.dev, flip, g->stream);
-        ck(cudaEventRecord(g->kernelEvents[k + 1], g->stream), "event");
+        ck(cudaEventRecord(g->kernelEvents[k], stream), "event");
+        lbm::launchCollideStream(L.dev, flip, stream);
+        ck(cudaEventRecord(g->kernelEvents[k + 1], stream), "event");
         g->kernelEventsUsed += 2;
     } else {
-        lbm::launchCollideStream(L.dev, flip, g->stream);
+        lbm::launchCollideStream(L.dev, flip, stream);
     }
     L.info.esotwistFlipper = !flip;  // applyStreaming
-    lbm::launchOpenBoundary(L.dev, L.info.esotwistFlipper, g->stream);
-    lbm::launchPeriodic(L.dev, L.info.esotwistFlipper, g->stream);
+    lbm::launchOpenBoundary(L.dev, L.info.esotwistFlipper, stream);
+    lbm::launchPeriodic(L.dev, L.info.esotwistFlipper, stream);
     L.info.iterationsFinished++;
     L.iterationsSinceTrackerReset++;
 }
@@ -263,14 +271,41 @@ void advanceHostState(LevelState& L) {
 
 // updateAllGrids (include/updateGrid.h:388-396): a level steps once, the
 // next finer level twice (recursively), then the interface between them.
+// The level's own update and the finer substeps read and write disjoint
+// state (the interface of the previous coarse step is their only link), so
+// the level's update runs on a side stream forked from the grid stream and
+// joined before the interface; kernel timing keeps everything on one stream.
 void updateAllGrids(lbm_grids* g, int level) {
-    updateSingleGrid(g, g->levels[level]);
-    if (level + 1 < static_cast<int>(g->levels.size())) {
-        for (int i = 0; i < 2; ++i) updateAllGrids(g, level + 1);
-        LevelState& C = g->levels[level];
-        LevelState& F = g->levels[level + 1];
-        lbm::launchInterface(C.dev, F.dev, C.itf, C.info.esotwistFlipper, F.info.esotwistFlipper, g->stream);
+    const bool finer = level + 1 < static_cast<int>(g->levels.size());
+    if (!finer) {
+        updateSingleGrid(g, g->levels[level], g->stream);
+        return;
     }
+    const bool fork = !g->timingKernels;
+    if (fork) {
+        if (g->sideStreams.size() < g->levels.size()) {
+            g->sideStreams.resize(g->levels.size(), nullptr);
+            g->forkEvents.resize(g->levels.size(), nullptr);
+            g->joinEvents.resize(g->levels.size(), nullptr);
+        }
+        if (!g->sideStreams[level]) {
+            ck(cudaStreamCreateWithFlags(&g->sideStreams[level], cudaStreamNonBlocking), "side stream");
+            ck(cudaEventCreateWithFlags(&g->forkEvents[level], cudaEventDisableTiming), "fork event");
+            ck(cudaEventCreateWithFlags(&g->joinEvents[level], cudaEventDisableTiming), "join event");
+        }
+        cudaStream_t side = g->sideStreams[level];
+        ck(cudaEventRecord(g->forkEvents[level], g->stream), "fork");
+        ck(cudaStreamWaitEvent(side, g->forkEvents[level], 0), "fork wait");
+        updateSingleGrid(g, g->levels[level], side);
+        ck(cudaEventRecord(g->joinEvents[level], side), "join");
+    } else {
+        updateSingleGrid(g, g->levels[level], g->stream);
+    }
+    for (int i = 0; i < 2; ++i) updateAllGrids(g, level + 1);
+    if (fork) ck(cudaStreamWaitEvent(g->stream, g->joinEvents[level], 0), "join wait");
+    LevelState& C = g->levels[level];
+    LevelState& F = g->levels[level + 1];
+    lbm::launchInterface(C.dev, F.dev, C.itf, C.info.esotwistFlipper, F.info.esotwistFlipper, g->stream);
 }
 
 // Host bookkeeping of one coarse step whose kernels ran inside a replayed

@@ -9,8 +9,11 @@
 // row per unknown population u:
 //   f_u = sum_m E[u][m] m_eq[m] + sum_d C[u][d] f_d,
 // E = (S Mfu)^-1 grouped by equilibrium moment and C = -(S Mfu)^-1 S Mfk,
-// formed in double and rounded once, so the kernel runs one short loop over
-// the unknowns (equal to the generated code to rounding).  Populations are
+// formed in double and rounded once (equal to the generated code to
+// rounding).  The tables are stored transposed, column m (or d) holding the
+// weights of every unknown row, padded to kMbbcRowPad, so that a kernel
+// forms all rows at once: one 16-byte shared-memory load feeds four FMAs,
+// and the columns of unknown populations (zero weights) are skipped.  Populations are
 // full (weight-compensated) f, as at the reference's call site
 // (include/updateGrid.h:223-240); restoreRho and restoreUxUyUz keep the
 // generated sums in ascending direction order.
@@ -25,9 +28,11 @@ namespace lbm {
 // coefficients, the generated float values, widened to double).
 constexpr int kMbbcMoments = 23;  // equilibrium moments of the closure, in table order
 
-template <class T> struct MbbcDirT {
-    T E[LBM_MBBC_MAX_UNKNOWN][kMbbcMoments];  // unknown row r: weights of the equilibrium moments
-    T C[LBM_MBBC_MAX_UNKNOWN][27];            // unknown row r: weights of the known populations
+constexpr int kMbbcRowPad = 20;   // LBM_MBBC_MAX_UNKNOWN rounded up to a multiple of 4
+
+template <class T> struct alignas(16) MbbcDirT {
+    T ET[kMbbcMoments][kMbbcRowPad];  // column m: weight of equilibrium moment m in every unknown row
+    T CT[27][kMbbcRowPad];            // column d: weight of known population d in every unknown row
     T rhoMfk[27];                     // restoreRho numerator weights
     T uMfk[3][27];                    // restoreUxUyUz (edges, corners)
     T uInv[3][3];
@@ -67,8 +72,8 @@ template <class V = float> inline MbbcDirT<V> mbbcDirFromTable(const LbmMbbcTabl
             e[T.moment[j]] += double(T.inv[r][j]);
             for (int k = 0; k < T.nk; ++k) c[T.known[k]] -= double(T.inv[r][j]) * double(T.smfk[j][k]);
         }
-        for (int m = 0; m < kMbbcMoments; ++m) D.E[r][m] = V(e[m]);
-        for (int d = 0; d < 27; ++d) D.C[r][d] = V(c[d]);
+        for (int m = 0; m < kMbbcMoments; ++m) D.ET[m][r] = V(e[m]);
+        for (int d = 0; d < 27; ++d) D.CT[d][r] = V(c[d]);
     }
     for (int k = 0; k < T.nk; ++k) {
         D.rhoMfk[T.known[k]] = T.rhoMfk[k];
@@ -111,15 +116,56 @@ template <class V> LBM_HD void mbbcMomentsEq(V rho, V ux, V uy, V uz, V (&m)[kMb
     m[22] = t * rho * ux * uy;
 }
 
-// applyMBBC for unknown row r: the closed (full) population T.unknownDir[r].
+// Four consecutive table entries (16 bytes for float, two 16-byte loads for double).
+LBM_HD void mbbcLoad4(const float* p, float (&o)[4]) {
+#ifdef __CUDA_ARCH__
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+#else
+    for (int k = 0; k < 4; ++k) o[k] = p[k];
+#endif
+}
+LBM_HD void mbbcLoad4(const double* p, double (&o)[4]) {
+#ifdef __CUDA_ARCH__
+    const double2 a = *reinterpret_cast<const double2*>(p), b = *reinterpret_cast<const double2*>(p + 2);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+#else
+    for (int k = 0; k < 4; ++k) o[k] = p[k];
+#endif
+}
+
+// applyMBBC for every unknown row at once: out[r] is the closed (full)
+// population T.unknownDir[r] for r < T.nu.  `unknown` is T.unknownMask (the
+// skipped columns) and `groups` = (T.nu + 3) / 4, both uniform over a CTA.
 template <class V>
-LBM_HD V mbbcUnknown(const MbbcDirT<V>& T, int r, const V (&meq)[kMbbcMoments], const V (&f)[27]) {
-    V v = V(0);
+LBM_HD void mbbcClose(const MbbcDirT<V>& T, unsigned unknown, int groups, const V (&meq)[kMbbcMoments],
+                      const V (&f)[27], V (&out)[kMbbcRowPad]) {
 #pragma unroll
-    for (int m = 0; m < kMbbcMoments; ++m) v = mfma(T.E[r][m], meq[m], v);
+    for (int r = 0; r < kMbbcRowPad; ++r) out[r] = V(0);
 #pragma unroll
-    for (int d = 0; d < 27; ++d) v = mfma(T.C[r][d], f[d], v);
-    return v;
+    for (int m = 0; m < kMbbcMoments; ++m) {
+        if (m == 10) continue;  // the moment is zero at equilibrium
+#pragma unroll
+        for (int q = 0; q < kMbbcRowPad / 4; ++q) {
+            if (q >= groups) break;
+            V w[4];
+            mbbcLoad4(&T.ET[m][4 * q], w);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) out[4 * q + k] = mfma(w[k], meq[m], out[4 * q + k]);
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        if ((unknown >> d) & 1u) continue;
+#pragma unroll
+        for (int q = 0; q < kMbbcRowPad / 4; ++q) {
+            if (q >= groups) break;
+            V w[4];
+            mbbcLoad4(&T.CT[d][4 * q], w);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) out[4 * q + k] = mfma(w[k], f[d], out[4 * q + k]);
+        }
+    }
 }
 
 // restoreRho: density from the known populations and the velocity.

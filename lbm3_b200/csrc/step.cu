@@ -1042,6 +1042,133 @@ __device__ __forceinline__ void openBoundaryDone(const DevLevel& g) {
     }
 }
 
+// One open cell's inputs: its records and its known populations after streaming.
+template <class V> struct OpenCell {
+    int idx, info;
+    int4 rows;
+    float dRhoRef, uNormalRef, beta;
+    float4 target;
+    V f[27];
+};
+
+// Issue the loads of open cell `idx` (records and the known populations of a
+// chunk with unknown-direction mask `unknown`); nothing waits on them here.
+template <bool F, class S>
+__device__ __forceinline__ void openLoad(const DevLevel& g, int idx, unsigned unknown, bool active,
+                                         OpenCell<Real<S>>& c) {
+    using V = Real<S>;
+    c.idx = idx;
+    c.info = __ldg(g.obInfo + idx);
+    c.rows = __ldg(g.obNbr + idx);
+    c.dRhoRef = g.obRhoRef[idx];
+    c.uNormalRef = g.obUnRef[idx];
+    c.target = __ldg(g.obTarget + idx);
+    c.beta = __ldg(g.obBeta + idx);
+    const int n = g.cellCount;
+    int nb[8];
+    nb[0] = c.rows.x;
+    nb[1] = c.rows.x + 1 < n ? c.rows.x + 1 : 0;
+    nb[2] = c.rows.y;
+    nb[3] = c.rows.y + 1 < n ? c.rows.y + 1 : 0;
+    nb[4] = c.rows.z;
+    nb[5] = c.rows.z + 1 < n ? c.rows.z + 1 : 0;
+    nb[6] = c.rows.w;
+    nb[7] = c.rows.w + 1 < n ? c.rows.w + 1 : 0;
+    const S* base = static_cast<const S*>(g.f);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        c.f[d] = V(0);
+        if (active && !(unknown >> d & 1u))
+            c.f[d] = Store<S>::ld(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
+    }
+}
+
+// Close one open cell with the table T of its outer normal: restore the
+// missing macroscopic quantity, write the unknown populations, update the
+// reference averages and the flow sums.
+template <bool F, class S>
+__device__ __forceinline__ void openClose(const DevLevel& g, const MbbcDirT<Real<S>>& T, unsigned unknown,
+                                          int iterationsFinished, OpenCell<Real<S>>& c) {
+    using V = Real<S>;
+    const int info = c.info;
+    const int nx = ((info >> 3) & 3) - 1, ny = ((info >> 5) & 3) - 1, nz = ((info >> 7) & 3) - 1;
+    const int n = g.cellCount;
+    S* base = static_cast<S*>(g.f);
+    V dRhoZ = V(0);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        if (unknown >> d & 1u) continue;
+        if (nx * cx(d) + ny * cy(d) + nz * cz(d) == 0) dRhoZ += c.f[d];
+        else dRhoZ += V(2) * c.f[d];
+        c.f[d] += weightT<V>(d);  // the closure is ill-conditioned on shifted populations
+    }
+    V dRho = c.target.x, ux = c.target.y, uy = c.target.z, uz = c.target.w;
+    const bool nonReflective = info & 4;
+    if ((info & 3) == 2) {  // pressure: density given, velocity restored
+        if (nonReflective) {
+            const V uNormal = nonReflectiveUNormal<V>(c.uNormalRef, dRhoZ, dRho);
+            dRho = (dRhoZ - uNormal) / (V(1) + uNormal);
+        }
+        mbbcRestoreU(T, dRho + V(1), c.f, ux, uy, uz);
+    } else if ((info & 3) == 1) {  // velocity: velocity given, density restored
+        if (nonReflective) {
+            V uTarget = V(0);
+            if (nx != 0) uTarget = nx > 0 ? ux : -ux;
+            if (ny != 0) uTarget = ny > 0 ? uy : -uy;
+            if (nz != 0) uTarget = nz > 0 ? uz : -uz;
+            const V uNormal = nonReflectiveUNormal<V>(uTarget, dRhoZ, c.dRhoRef);
+            if (nx != 0) ux = nx > 0 ? uNormal : -uNormal;
+            if (ny != 0) uy = ny > 0 ? uNormal : -uNormal;
+            if (nz != 0) uz = nz > 0 ? uNormal : -uNormal;
+        }
+        dRho = mbbcRestoreRho(T, ux, uy, uz, c.f) - V(1);
+    }
+    // closure: all unknown rows at once, each written to its pre-collision
+    // slot (F ? inv(d) : d) in the neighbour offset by max(0, -c_d)
+    V closed[kMbbcRowPad];
+    {
+        V meq[kMbbcMoments];
+        mbbcMomentsEq(dRho + V(1), ux, uy, uz, meq);
+        mbbcClose(T, unknown, (T.nu + 3) >> 2, meq, c.f, closed);
+    }
+#pragma unroll
+    for (int r = 0; r < kMbbcRowPad; ++r) {
+        if (r >= T.nu) break;
+        const int k = T.unknownNbr[r];
+        const int sel = k >> 1;
+        int cell = sel == 0 ? c.rows.x : sel == 1 ? c.rows.y : sel == 2 ? c.rows.z : c.rows.w;
+        if (k & 1) cell = cell + 1 < n ? cell + 1 : 0;
+        const int slot = F ? T.unknownInv[r] : T.unknownDir[r];
+        Store<S>::st(base + (long long)slot * g.stride + cell, closed[r] - T.unknownW[r]);
+    }
+    // reference values: exponential average whose weight decays with the
+    // iteration count; below 1e-5 the weight is tripled and the update runs
+    // every 3^k iterations instead (include/updateGrid.h:325-347)
+    const float uNormal = float(V(nx) * ux + V(ny) * uy + V(nz) * uz);
+    float alpha = c.beta / ((float)iterationsFinished + c.beta + 10.f);
+    int updateEvery = 1;
+    while (alpha < 1.e-5f) {
+        alpha *= 3.f;
+        updateEvery *= 3;
+    }
+    if (iterationsFinished % updateEvery == 0) {
+        g.obRhoRef[c.idx] = fmaf(alpha, float(dRho) - c.dRhoRef, c.dRhoRef);
+        g.obUnRef[c.idx] = fmaf(alpha, uNormal - c.uNormalRef, c.uNormalRef);
+    }
+    if (g.trackOpen && (info & 512)) {
+        g.obRhoCum[c.idx] += float(dRho);
+        g.obUnCum[c.idx] += uNormal;
+    }
+}
+
+// Stage the closure tables of normal row `row` in shared memory.
+template <class V> __device__ __forceinline__ void openStageTable(const DevLevel& g, int row, MbbcDirT<V>& T) {
+    const int4* src = reinterpret_cast<const int4*>(static_cast<const MbbcDirT<V>*>(g.obTables) + row);
+    int4* dst = reinterpret_cast<int4*>(&T);
+    for (int q = threadIdx.x; q < int(sizeof(MbbcDirT<V>) / 16); q += blockDim.x) dst[q] = __ldg(src + q);
+}
+
+// One chunk per CTA: the table staging overlaps the gathers.
 template <bool F, class S>
 __global__ void __launch_bounds__(kOpenChunk, LBM3_OPEN_MIN_BLOCKS) openBoundary(DevLevel g) {
     using V = Real<S>;
@@ -1051,105 +1178,12 @@ __global__ void __launch_bounds__(kOpenChunk, LBM3_OPEN_MIN_BLOCKS) openBoundary
     const int iterationsFinished = __ldcg(g.obCounter);
     __shared__ MbbcDirT<V> T;
     const int4 chunk = __ldg(g.obChunk + blockIdx.x);  // {first, count, normal row, unknown mask}
-    {
-        const int* src = reinterpret_cast<const int*>(static_cast<const MbbcDirT<V>*>(g.obTables) + chunk.z);
-        int* dst = reinterpret_cast<int*>(&T);
-        for (int q = threadIdx.x; q < int(sizeof(MbbcDirT<V>) / 4); q += kOpenChunk) dst[q] = __ldg(src + q);
-    }
-    // everything that does not need the tables is loaded before the barrier,
-    // so the population gathers overlap the table staging
+    openStageTable(g, chunk.z, T);
     const bool active = int(threadIdx.x) < chunk.y;
-    const int idx = chunk.x + (active ? int(threadIdx.x) : 0);
-    const int info = __ldg(g.obInfo + idx);
-    const int4 rows = __ldg(g.obNbr + idx);
-    // per-cell records: one round of independent loads with the gathers
-    const float dRhoRef = g.obRhoRef[idx];
-    const float uNormalRef = g.obUnRef[idx];
-    const float4 target = __ldg(g.obTarget + idx);
-    const float beta = __ldg(g.obBeta + idx);
-    const int nx = ((info >> 3) & 3) - 1, ny = ((info >> 5) & 3) - 1, nz = ((info >> 7) & 3) - 1;
-    const unsigned unknown = static_cast<unsigned>(chunk.w);
-    const int n = g.cellCount;
-    int nb[8];
-    nb[0] = rows.x;
-    nb[1] = rows.x + 1 < n ? rows.x + 1 : 0;
-    nb[2] = rows.y;
-    nb[3] = rows.y + 1 < n ? rows.y + 1 : 0;
-    nb[4] = rows.z;
-    nb[5] = rows.z + 1 < n ? rows.z + 1 : 0;
-    nb[6] = rows.w;
-    nb[7] = rows.w + 1 < n ? rows.w + 1 : 0;
-    S* base = static_cast<S*>(g.f);
-    V f[27];
-#pragma unroll
-    for (int d = 0; d < 27; ++d) {
-        f[d] = V(0);
-        if (active && !(unknown >> d & 1u))
-            f[d] = Store<S>::ld(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
-    }
+    OpenCell<V> c;
+    openLoad<F, S>(g, chunk.x + (active ? int(threadIdx.x) : 0), static_cast<unsigned>(chunk.w), active, c);
     __syncthreads();
-    if (!active) return;
-    V dRhoZ = V(0);
-#pragma unroll
-    for (int d = 0; d < 27; ++d) {
-        if (unknown >> d & 1u) continue;
-        if (nx * cx(d) + ny * cy(d) + nz * cz(d) == 0) dRhoZ += f[d];
-        else dRhoZ += V(2) * f[d];
-        f[d] += weightT<V>(d);  // the closure is ill-conditioned on shifted populations
-    }
-    V dRho = target.x, ux = target.y, uy = target.z, uz = target.w;
-    const bool nonReflective = info & 4;
-    if ((info & 3) == 2) {  // pressure: density given, velocity restored
-        if (nonReflective) {
-            const V uNormal = nonReflectiveUNormal<V>(uNormalRef, dRhoZ, dRho);
-            dRho = (dRhoZ - uNormal) / (V(1) + uNormal);
-        }
-        mbbcRestoreU(T, dRho + V(1), f, ux, uy, uz);
-    } else if ((info & 3) == 1) {  // velocity: velocity given, density restored
-        if (nonReflective) {
-            V uTarget = V(0);
-            if (nx != 0) uTarget = nx > 0 ? ux : -ux;
-            if (ny != 0) uTarget = ny > 0 ? uy : -uy;
-            if (nz != 0) uTarget = nz > 0 ? uz : -uz;
-            const V uNormal = nonReflectiveUNormal<V>(uTarget, dRhoZ, dRhoRef);
-            if (nx != 0) ux = nx > 0 ? uNormal : -uNormal;
-            if (ny != 0) uy = ny > 0 ? uNormal : -uNormal;
-            if (nz != 0) uz = nz > 0 ? uNormal : -uNormal;
-        }
-        dRho = mbbcRestoreRho(T, ux, uy, uz, f) - V(1);
-    }
-    // closure: one row per unknown population, written to its pre-collision
-    // slot (F ? inv(d) : d) in the neighbour offset by max(0, -c_d)
-    V meq[kMbbcMoments];
-    mbbcMomentsEq(dRho + V(1), ux, uy, uz, meq);
-#pragma unroll 1
-    for (int r = 0; r < T.nu; ++r) {
-        const V v = mbbcUnknown(T, r, meq, f);
-        const int k = T.unknownNbr[r];
-        const int sel = k >> 1;
-        int c = sel == 0 ? rows.x : sel == 1 ? rows.y : sel == 2 ? rows.z : rows.w;
-        if (k & 1) c = c + 1 < n ? c + 1 : 0;
-        const int slot = F ? T.unknownInv[r] : T.unknownDir[r];
-        Store<S>::st(base + (long long)slot * g.stride + c, v - T.unknownW[r]);
-    }
-    // reference values: exponential average whose weight decays with the
-    // iteration count; below 1e-5 the weight is tripled and the update runs
-    // every 3^k iterations instead (include/updateGrid.h:325-347)
-    const float uNormal = float(V(nx) * ux + V(ny) * uy + V(nz) * uz);
-    float alpha = beta / ((float)iterationsFinished + beta + 10.f);
-    int updateEvery = 1;
-    while (alpha < 1.e-5f) {
-        alpha *= 3.f;
-        updateEvery *= 3;
-    }
-    if (iterationsFinished % updateEvery == 0) {
-        g.obRhoRef[idx] = fmaf(alpha, float(dRho) - dRhoRef, dRhoRef);
-        g.obUnRef[idx] = fmaf(alpha, uNormal - uNormalRef, uNormalRef);
-    }
-    if (g.trackOpen && (info & 512)) {
-        g.obRhoCum[idx] += float(dRho);
-        g.obUnCum[idx] += uNormal;
-    }
+    if (active) openClose<F, S>(g, T, static_cast<unsigned>(chunk.w), iterationsFinished, c);
     openBoundaryDone(g);  // thread 0 is always active
 }
 

@@ -8,7 +8,12 @@
 
 constexpr float PI = 3.14159265358979323846f;
 constexpr int cellsPerDomain = 32;
-constexpr int GRID_LEVEL_COUNT = 1;
+#ifndef TGV_LEVELS
+#define TGV_LEVELS 1
+#endif
+// one level, or the central cube refined on a second level (the reference's
+// refined run, cases/taylorGreenVortex/taylorGreenVortexMain.cu:8-12)
+constexpr int GRID_LEVEL_COUNT = TGV_LEVELS;
 constexpr float reynoldsNumber = 1600.f;
 constexpr float machNumber = 0.1f;
 constexpr float referenceLengthPhys = 1000.f;  // mm
@@ -29,6 +34,11 @@ constexpr bool TRACK_OPEN_BOUNDARIES = false;
 __cuda_callable__ void getRefinementModifier(const int& iCell, const int& jCell, const int& kCell,
                                              bool& refinementMarker, const InfoStruct& Info) {
     refinementMarker = false;
+    if (GRID_LEVEL_COUNT == 1 || Info.gridID != 0) return;
+    float x, y, z;
+    getXYZFromIJKCellIndex(iCell, jCell, kCell, x, y, z, Info);
+    const float half = 0.25f * domainSizePhys;
+    refinementMarker = x > -half && x < half && y > -half && y < half && z > -half && z < half;
 }
 
 __cuda_callable__ void getInitialCondition(BCStruct& BC, const int& iCell, const int& jCell, const int& kCell,

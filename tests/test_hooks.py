@@ -138,16 +138,17 @@ def nvcc():
     return str(cand) if cand.exists() else "nvcc"
 
 
-def build_driver(out: Path) -> Path:
+def build_driver(out: Path, levels: int = 1) -> Path:
     lib = ROOT / "lbm3_b200" / "_lib"
-    exe = out / "tgv_driver"
-    subprocess.run([nvcc(), "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+    exe = out / f"tgv_driver_{levels}"
+    subprocess.run([nvcc(), "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", f"-DTGV_LEVELS={levels}",
                     "-I", str(ROOT / "include"), str(ROOT / "tests" / "drivers" / "tgv_driver.cu"),
                     "-L", str(lib), "-llbm3_b200", "-Xlinker", "-rpath", "-Xlinker", str(lib), "-o", str(exe)],
                    check=True)
     return exe
 
 
-def test_reference_style_driver_compiles(tmp_path):
-    exe = build_driver(tmp_path)
+@pytest.mark.parametrize("levels", [1, 2])
+def test_reference_style_driver_compiles(tmp_path, levels):
+    exe = build_driver(tmp_path, levels)
     assert exe.exists()
