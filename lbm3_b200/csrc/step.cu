@@ -1079,7 +1079,7 @@ __device__ __forceinline__ void openLoad(const DevLevel& g, int idx, unsigned un
     for (int d = 0; d < 27; ++d) {
         c.f[d] = V(0);
         if (active && !(unknown >> d & 1u))
-            c.f[d] = Store<S>::ld(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
+            c.f[d] = Store<S>::ldL2(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
     }
 }
 

@@ -157,7 +157,9 @@ __device__ __forceinline__ void decodeNbr(const DevLevel& g, int cell, int (&nb)
 }
 
 // Typed population storage.  Half and bfloat16 hold the shifted value
-// f_i - w_i directly (the reference already stores shifted FP32).  Arithmetic
+// f_i - w_i directly (the reference already stores shifted FP32).  ldL2
+// reads through L2 only (no L1 line allocation): scattered single-value
+// gathers then move one 32-byte sector instead of a whole 128-byte line.  Arithmetic
 // is FP32 for every storage type except double, which is the FP64 build of
 // the kernels (FP64 storage and arithmetic).
 template <class S> struct Compute { using type = float; };
@@ -167,18 +169,22 @@ template <class S> using Real = typename Compute<S>::type;
 template <class S> struct Store;
 template <> struct Store<double> {
     static __device__ __forceinline__ double ld(const double* p) { return *p; }
+    static __device__ __forceinline__ double ldL2(const double* p) { return __ldcg(p); }
     static __device__ __forceinline__ void st(double* p, double v) { *p = v; }
 };
 template <> struct Store<float> {
     static __device__ __forceinline__ float ld(const float* p) { return *p; }
+    static __device__ __forceinline__ float ldL2(const float* p) { return __ldcg(p); }
     static __device__ __forceinline__ void st(float* p, float v) { *p = v; }
 };
 template <> struct Store<__half> {
     static __device__ __forceinline__ float ld(const __half* p) { return __half2float(*p); }
+    static __device__ __forceinline__ float ldL2(const __half* p) { return __half2float(__ldcg(p)); }
     static __device__ __forceinline__ void st(__half* p, float v) { *p = __float2half_rn(v); }
 };
 template <> struct Store<__nv_bfloat16> {
     static __device__ __forceinline__ float ld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+    static __device__ __forceinline__ float ldL2(const __nv_bfloat16* p) { return __bfloat162float(__ldcg(p)); }
     static __device__ __forceinline__ void st(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
 };
 
