@@ -69,6 +69,22 @@ def make_case(name: str, storage: str):
                 f"level-1 and 112x80x80 level-2 cells, icosphere of 20480 triangles with D=48 finest cells, "
                 f"wall refinement 2, velocity inlet u=0.04, non-reflective outlet, Re=300")
         return s.case, desc, s
+    if name.startswith("xchannel") or name.startswith("yzchannel"):
+        # the sphere configuration's channel without the body, with only the x
+        # faces open (periodic sides) or only the y/z faces open (periodic x):
+        # the open-boundary cost per face kind
+        xonly = name.startswith("xchannel")
+        dims = name[len("xchannel" if xonly else "yzchannel"):] or "256x128x128"
+        nx, ny, nz = (int(v) for v in dims.split("x"))
+        c = L.open_channel(nx, ny, nz, u_in=0.04, nu_lattice=0.0096, sides="periodic" if xonly else "velocity",
+                           storage=st)
+        if not xonly:
+            for f in (A.FACE_XMIN, A.FACE_XMAX):
+                c.face[f] = A.LbmFaceBC(A.LBM_BC_PERIODIC, 0, 0, 0, 7.0, 0.0, 0.0, 0.0, 0.0)
+        desc = (f"channel {nx}x{ny}x{nz} without a body, " +
+                ("velocity inlet and non-reflective outlet on x, periodic y and z" if xonly
+                 else "periodic x, velocity boundaries on the y and z faces") + ", nu=0.0096")
+        return c, desc, None
     if name == "box256x128x128":
         # the 256x128x128 single-level grid of the flow-around-sphere
         # configuration, fully periodic and without the obstacle
@@ -423,6 +439,24 @@ def time_batch(cases, steps: int, warmup: int, torch) -> float:
     return updates * steps / (ms * 1e-3) / 1e6
 
 
+def time_packed(cases, steps: int, warmup: int) -> tuple:
+    """MLUPS of independent single-level domains advanced as one packed batch
+    (one persistent collide-stream launch over the packed block table of all
+    of them, one open-boundary and one periodic launch per step, step pairs
+    replayed as a CUDA graph), device-timed on the batch stream; and the
+    batch's kernel launches per step."""
+    import lbm3_b200 as L
+    grids = [L.build_grids(c) for c in cases]
+    with L.PackedBatch(grids) as b:
+        b.update(warmup + (warmup & 1))
+        ms = b.time_steps(steps)
+        launches = b.info().launches_per_step
+    updates = sum(g.fluid_updates_per_iteration for g in grids)
+    for g in grids:
+        g.close()
+    return updates * steps / (ms * 1e-3) / 1e6, launches
+
+
 def storage_comparison(args, f32_value: float, torch) -> dict:
     """The metric's comparison: the same workload with FP16-shifted storage,
     and the FP16-shifted batched form (8 Taylor-Green 64^3 domains, the plain
@@ -468,22 +502,30 @@ def storage_comparison(args, f32_value: float, torch) -> dict:
     ms = g.time_steps_graph(1000)
     plain = g.fluid_updates_per_iteration * 1000 / (ms * 1e-3) / 1e6
     g.close()
-    batched = time_batch([L.tgv_plain_method(storage=A_STORE["f16"]).case for _ in range(8)], 500, args.warmup, torch)
+    tgv16 = [L.tgv_plain_method(storage=A_STORE["f16"]).case for _ in range(8)]
+    batched, launches = time_packed(tgv16, 500, args.warmup)
+    streams = time_batch(tgv16, 500, args.warmup, torch)
     out["batched_f16"] = {
         "value": round(batched, 2), "unit": "MLUPS",
-        "workload": "8 Taylor-Green 64^3 domains (66^3 with ghosts), FP16-shifted, one stream each, step pairs "
-                    "replayed as CUDA graphs",
+        "workload": "8 Taylor-Green 64^3 domains (66^3 with ghosts), FP16-shifted, one packed batch: one "
+                    "persistent collide-stream launch over all domains' work items and one periodic-ghost "
+                    "launch per step, step pairs replayed as CUDA graphs",
+        "launches_per_step": launches,
         "plain_f32_single_domain": round(plain, 2),
         "ratio_vs_plain_f32_same_configuration": round(batched / plain, 4),
-        "ratio_vs_plain_f32_this_workload": round(batched / f32_value, 4)}
+        "ratio_vs_plain_f32_this_workload": round(batched / f32_value, 4),
+        "one_stream_per_domain": round(streams, 2)}
     return out
 
 
 def run_batch(args, copies: int, base: str):
-    """Many-domain batch: `copies` independent domains of workload `base`, each
-    on its own stream, advanced together by update_batch.  Device-timed: a
-    start event on the launching stream, every domain stream waits on it, and
-    the end event waits for every domain stream."""
+    """Many-domain batch: `copies` independent domains of workload `base`.
+    Single-level domains without rotors advance as one packed batch (one
+    persistent collide-stream launch over all domains' work items per step,
+    graph replay), device-timed on the batch stream; otherwise each domain
+    runs on its own stream, advanced together by update_batch, timed from a
+    start event every domain stream waits on to an end event that waits on
+    all of them."""
     import torch
     import lbm3_b200 as L
     if int(os.environ.get("WORLD_SIZE", "1")) > 1:
@@ -495,11 +537,18 @@ def run_batch(args, copies: int, base: str):
     streams = [torch.cuda.Stream() for _ in grids]
     for g, s in zip(grids, streams):
         g.set_stream(s.cuda_stream)
+    packed = None
+    if args.storage != "f64" and all(g.level_count() == 1 and g.case.rotor_count == 0 for g in grids):
+        packed = L.PackedBatch(grids)
     per_step_launches = 0
-    for g in grids:
-        g.time_steps(1)
-        per_step_launches += g.last_launch_count()
-    L.update_batch(grids, args.warmup)
+    if packed is not None:
+        per_step_launches = packed.info().launches_per_step
+    else:
+        for g in grids:
+            g.time_steps(1)
+            per_step_launches += g.last_launch_count()
+    advance = packed.update if packed is not None else (lambda n: L.update_batch(grids, n))
+    advance(args.warmup + (args.warmup & 1))
     torch.cuda.synchronize()
     updates = sum(g.fluid_updates_per_iteration for g in grids)
     main_stream = torch.cuda.current_stream()
@@ -512,18 +561,21 @@ def run_batch(args, copies: int, base: str):
         pass
     with ClockSampler(uuid) as clk:
         clk.start()
-        start.record(main_stream)
-        for s in streams:
-            s.wait_event(start)
-        L.update_batch(grids, args.steps)
-        for s in streams:
-            ev = torch.cuda.Event()
-            ev.record(s)
-            main_stream.wait_event(ev)
-        end.record(main_stream)
-        end.synchronize()
+        if packed is not None:
+            ms = packed.time_steps(args.steps)
+        else:
+            start.record(main_stream)
+            for s in streams:
+                s.wait_event(start)
+            L.update_batch(grids, args.steps)
+            for s in streams:
+                ev = torch.cuda.Event()
+                ev.record(s)
+                main_stream.wait_event(ev)
+            end.record(main_stream)
+            end.synchronize()
+            ms = start.elapsed_time(end)
         clk.stop()
-    ms = start.elapsed_time(end)
     value = whole_job_rate(updates, args.steps, 1, ms * 1e-3)
     bpp = BYTES_PER_POP[args.storage]
     alg_bytes = updates * 2 * 27 * bpp
@@ -539,12 +591,14 @@ def run_batch(args, copies: int, base: str):
     for g, f0 in zip(grids, states):
         g.set_populations(f0)
     for _ in range(e2e_steps):
-        L.update_batch(grids, 1)
+        advance(1)
         for g, (_, _, tg) in zip(grids, made):
             g.kinetic_energy(tg.u_initial_phys, tg.domain_length) if tg is not None else g.kinetic_energy(1.0, 1000.0)
     e2e_s = time.perf_counter() - t0
     clocks = clk.summary()
     h2d = sum(f.nbytes for f in states)
+    if packed is not None:
+        packed.close()
     for g in grids:
         g.close()
     del np
@@ -554,11 +608,12 @@ def run_batch(args, copies: int, base: str):
         "scaling": "weak", "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
         "config": {"workload": f"batch of {copies} independent domains, each: {desc}", "domains": copies,
                    "fluid_updates_per_step": updates, "storage": args.storage, "compute": "f32",
-                   "l2": "all domains' populations %.0f MB" % (alg_bytes / 2 / 1e6), "parallelism": "one stream per domain"},
+                   "l2": "all domains' populations %.0f MB" % (alg_bytes / 2 / 1e6),
+                   "parallelism": "packed batch" if packed is not None else "one stream per domain"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": None,
                      "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
-                     "kernel": "whole batch step (all kernels of all domains, overlapped)",
+                     "kernel": "whole batch step (all kernels of all domains)",
                      "algorithmic_bytes_per_step": alg_bytes},
         "cpu_baseline": None,
         "e2e": {"value": round(whole_job_rate(updates, e2e_steps, 1, e2e_s), 2), "unit": "MLUPS",

@@ -58,6 +58,9 @@ extern "C" {
 #define LBM_STORE_F32  0
 #define LBM_STORE_F16  1      /* shifted populations f_i - w_i as IEEE half     */
 #define LBM_STORE_BF16 2      /* shifted populations f_i - w_i as bfloat16      */
+                              /* (16-bit stores of collided, boundary and
+                                 interface values round stochastically; see
+                                 lbm_build_grids)                               */
 #define LBM_STORE_F64  3      /* FP64 populations and FP64 arithmetic: the
                                  double-precision build of the same kernels,
                                  the reference of the storage-precision study */
@@ -308,7 +311,14 @@ int lbm_plan_read_array(lbm_plan* p, int level, int which, void* host, size_t by
  * Replaces buildGrids (include/gridBuilderFunctions.h:1577-1670) together with
  * applyInitialCondition (include/boundaryConditions/applyInitialCondition.h:8-84).
  * `fluid_updates_per_iteration` receives Σ_level (cells − wall cells)·2^level
- * (include/gridBuilderFunctions.h:1601-1608); it may be NULL. */
+ * (include/gridBuilderFunctions.h:1601-1608); it may be NULL.
+ * With LBM_STORE_F16 / LBM_STORE_BF16, every store of a collided, boundary
+ * or interpolated population rounds stochastically (up with probability equal
+ * to the distance from the lower representable neighbour, so the rounding
+ * error has zero mean and does not repeat step after step in a steady state);
+ * the random bits are a hash of a per-level step seed, the cell and the
+ * direction, so a run is deterministic and reproducible.  The initial
+ * condition, periodic ghost copies and lbm_write_f round to nearest. */
 int lbm_build_grids(const lbm_case* c, lbm_grids** out,
                     long long* fluid_updates_per_iteration);
 
@@ -333,6 +343,36 @@ int lbm_update_all_grids(lbm_grids* g, int coarse_steps);
  * domain's result is the one it gets when stepped alone.
  * No counterpart in the reference (one domain per driver process). */
 int lbm_update_batch(lbm_grids* const* grids, int count, int coarse_steps);
+
+/* Packed batch: single-level domains (without rotors, of one storage type,
+ * FP32, FP16 or BF16) advanced by ONE persistent collide-stream launch over a
+ * packed table of all domains' work items ({domain, item}: listed-cell chunks
+ * and 128-cell bulk tiles), one open-boundary launch over all domains' chunks
+ * and one periodic-ghost launch, instead of a launch set per domain; step
+ * pairs replay as a CUDA graph.  A member's result is bit-identical to
+ * stepping it alone.  The batch runs on its own stream, ordered after the
+ * work already queued on the members' streams and before what they get
+ * next.  Members keep their own state (trackers, readbacks, lbm_update_all_grids
+ * between batch updates); all members must be at the same esotwist parity
+ * when lbm_batch_update is called (a domain that has made an odd number of
+ * steps more than the others steps once on its own first).  Free the batch
+ * before its members.  No counterpart in the reference (one domain per
+ * driver process). */
+typedef struct lbm_batch lbm_batch;
+typedef struct lbm_batch_info {
+    int domain_count;
+    long long cells;          /* sum of the members' cells (ghosts included) */
+    int collide_items;        /* rows of the packed collide-stream table      */
+    int open_chunks;          /* open-boundary CTAs per step                  */
+    int periodic_cells;       /* periodic ghost cells per step                */
+    int launches_per_step;    /* kernels one packed step launches (<= 3)      */
+} lbm_batch_info;
+int lbm_batch_create(lbm_grids* const* grids, int count, lbm_batch** out);
+int lbm_batch_update(lbm_batch* b, int coarse_steps);
+/* Device time of `coarse_steps` packed steps (graphs captured first). */
+int lbm_batch_time_steps(lbm_batch* b, int coarse_steps, float* ms);
+int lbm_batch_get_info(lbm_batch* b, lbm_batch_info* out);
+void lbm_batch_free(lbm_batch* b);
 
 /* Graph replay of the step schedule.  lbm_update_all_grids and
  * lbm_update_batch advance step pairs by launching a CUDA graph of two steps

@@ -8,11 +8,11 @@ from . import _abi
 from ._abi import LbmCase, LbmError, LbmFaceBC, LbmGridInfo, lib
 from .cases import (flow_around_sphere, open_channel, periodic_box, set_hooks, set_refine_box, taylor_green,
                     taylor_green_refined, tgv_plain_method)
-from .grids import Grids, Plan, apply_collision_batch, build_grids, update_batch
+from .grids import Grids, PackedBatch, Plan, apply_collision_batch, build_grids, update_batch
 
 __all__ = [
     "LbmCase", "LbmError", "LbmFaceBC", "LbmGridInfo", "lib", "Grids", "Plan",
-    "build_grids", "update_batch", "apply_collision_batch", "taylor_green", "tgv_plain_method",
+    "build_grids", "update_batch", "PackedBatch", "apply_collision_batch", "taylor_green", "tgv_plain_method",
     "periodic_box", "open_channel", "flow_around_sphere", "_abi", "set_refine_box", "taylor_green_refined",
     "set_hooks",
 ]

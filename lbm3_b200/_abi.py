@@ -134,6 +134,13 @@ class LbmCase(C.Structure):
     ]
 
 
+class LbmBatchInfo(C.Structure):
+    _fields_ = [
+        ("domain_count", C.c_int), ("cells", C.c_longlong), ("collide_items", C.c_int),
+        ("open_chunks", C.c_int), ("periodic_cells", C.c_int), ("launches_per_step", C.c_int),
+    ]
+
+
 class LbmBC(C.Structure):
     """lbm_bc: BCStruct as a per-cell hook fills it."""
     _fields_ = [
@@ -184,6 +191,11 @@ SIGNATURES = [
     ("lbm_set_stream", C.c_int, [_P, _P]),
     ("lbm_update_all_grids", C.c_int, [_P, C.c_int]),
     ("lbm_update_batch", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int]),
+    ("lbm_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(_P)]),
+    ("lbm_batch_update", C.c_int, [_P, C.c_int]),
+    ("lbm_batch_time_steps", C.c_int, [_P, C.c_int, C.POINTER(C.c_float)]),
+    ("lbm_batch_get_info", C.c_int, [_P, C.POINTER(LbmBatchInfo)]),
+    ("lbm_batch_free", None, [_P]),
     ("lbm_synchronize", C.c_int, [_P]),
     ("lbm_set_graphs", C.c_int, [_P, C.c_int]),
     ("lbm_time_steps_graph", C.c_int, [_P, C.c_int, C.POINTER(C.c_float)]),

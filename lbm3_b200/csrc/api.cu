@@ -136,9 +136,14 @@ struct lbm_grids {
         for (cudaGraphExec_t e : pairExec)
             if (e) cudaGraphExecDestroy(e);
         if (captureStream) cudaStreamDestroy(captureStream);
-        for (cudaStream_t t : sideStreams) cudaStreamDestroy(t);
-        for (cudaEvent_t e : forkEvents) cudaEventDestroy(e);
-        for (cudaEvent_t e : joinEvents) cudaEventDestroy(e);
+        // levels without a finer one have no side stream (null entries): a
+        // destroy of a null handle would leave an error for the next check
+        for (cudaStream_t t : sideStreams)
+            if (t) cudaStreamDestroy(t);
+        for (cudaEvent_t e : forkEvents)
+            if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : joinEvents)
+            if (e) cudaEventDestroy(e);
     }
 };
 
@@ -418,6 +423,78 @@ int guarded(const char* where, const std::function<void()>& body) {
 }
 }  // namespace
 
+// ---- packed batch --------------------------------------------------------------
+
+struct lbm_batch {
+    std::vector<lbm_grids*> members;
+    int storage = LBM_STORE_F32;
+    lbm::DevBatch dev{};
+    lbm_batch_info info{};
+    std::vector<void*> owned;
+    cudaStream_t stream = nullptr;         // the batch's launches
+    cudaStream_t captureStream = nullptr;  // graph capture
+    cudaEvent_t sync = nullptr;            // orders the batch after / before its members
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaGraphExec_t pairExec[2] = {nullptr, nullptr};
+    ~lbm_batch() {
+        for (cudaGraphExec_t e : pairExec)
+            if (e) cudaGraphExecDestroy(e);
+        if (stream) cudaStreamSynchronize(stream);
+        for (void* p : owned) cudaFree(p);
+        if (sync) cudaEventDestroy(sync);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (captureStream) cudaStreamDestroy(captureStream);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+void batchStep(lbm_batch* b, bool flip, cudaStream_t s) { lbm::launchPackedStep(b->dev, b->storage, flip, s); }
+
+// Graph of two packed steps starting at esotwist parity `parity`.
+cudaGraphExec_t batchPairGraph(lbm_batch* b, int parity) {
+    if (b->pairExec[parity]) return b->pairExec[parity];
+    cudaGraph_t graph = nullptr;
+    ck(cudaStreamBeginCapture(b->captureStream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    batchStep(b, parity != 0, b->captureStream);
+    batchStep(b, parity == 0, b->captureStream);
+    const cudaError_t e = cudaStreamEndCapture(b->captureStream, &graph);
+    ck(e, "end capture");
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    ck(ei, "graph instantiate");
+    b->pairExec[parity] = exec;
+    return exec;
+}
+
+// Advance `steps` packed steps on the batch stream (members already waited for).
+void batchAdvance(lbm_batch* b, int steps) {
+    bool flip = b->members[0]->levels[0].info.esotwistFlipper;
+    int s = 0;
+    if (graphable(b->members[0]))
+        for (; s + 2 <= steps; s += 2) ck(cudaGraphLaunch(batchPairGraph(b, flip ? 1 : 0), b->stream), "graph launch");
+    for (; s < steps; ++s) {
+        batchStep(b, flip, b->stream);
+        flip = !flip;
+    }
+    ck(cudaGetLastError(), "batch launch");
+    for (lbm_grids* g : b->members)
+        for (int k = 0; k < steps; ++k) advanceHostState(g->levels[0]);
+}
+
+void batchCheckParity(const lbm_batch* b) {
+    const bool flip = b->members[0]->levels[0].info.esotwistFlipper;
+    for (const lbm_grids* g : b->members)
+        if (g->levels[0].info.esotwistFlipper != flip)
+            throw std::invalid_argument(
+                "members are at different esotwist parities (step the odd ones once on their own)");
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* lbm_last_error(void) { return gLastError.c_str(); }
@@ -592,6 +669,13 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
             d.errorFlag = g->errorFlag;
             d.work = own(devAlloc<int>(2));
             ck(cudaMemsetAsync(d.work, 0, 2 * sizeof(int), s), "memset");
+            d.seed = nullptr;
+            if (c->storage == LBM_STORE_F16 || c->storage == LBM_STORE_BF16) {
+                // the two parities' first step seeds, distinct per level
+                const std::vector<unsigned> seeds = {0x243F6A88u + 0x9E3779B9u * unsigned(l),
+                                                     0x85A308D3u + 0x7F4A7C15u * unsigned(l)};
+                d.seed = own(upload(seeds, s));
+            }
             d.shifter = own(upload(H.shifter, s));
             d.rowI = own(upload(H.rowI, s));
             d.rowJ = own(upload(H.rowJ, s));
@@ -826,6 +910,114 @@ int lbm_update_batch(lbm_grids* const* grids, int count, int steps) {
         ck(cudaGetLastError(), "step launch");
     });
 }
+
+int lbm_batch_create(lbm_grids* const* grids, int count, lbm_batch** out) {
+    if (!grids || count <= 0 || !out) return fail(LBM_ERR_INVALID, "lbm_batch_create: bad argument");
+    *out = nullptr;
+    for (int q = 0; q < count; ++q) {
+        if (!grids[q]) return fail(LBM_ERR_INVALID, "lbm_batch_create: null grids in the batch");
+        for (int r = 0; r < q; ++r)
+            if (grids[r] == grids[q]) return fail(LBM_ERR_INVALID, "lbm_batch_create: a domain is listed twice");
+    }
+    lbm_batch* b = new lbm_batch();
+    const int rc = guarded("lbm_batch_create", [&] {
+        b->members.assign(grids, grids + count);
+        b->storage = grids[0]->c.storage;
+        for (lbm_grids* g : b->members) {
+            if (g->levels.size() != 1) throw std::invalid_argument("a packed batch holds single-level domains");
+            const LevelState& L = g->levels[0];
+            if (!L.rotors.empty()) throw std::invalid_argument("a packed batch holds domains without rotors");
+            if (g->c.storage != b->storage) throw std::invalid_argument("members have different storage types");
+            if (b->storage == LBM_STORE_F64) throw std::invalid_argument("FP64 domains are not packed");
+            if (!lbm::pairFits(L.dev)) throw std::invalid_argument("a member is too large for 32-bit offsets");
+        }
+        // packed tables: every member's items, member by member
+        std::vector<lbm::DevLevel> levels;
+        std::vector<int2> collide, open;
+        std::vector<int> perStart{0};
+        long long cells = 0;
+        for (int q = 0; q < count; ++q) {
+            const lbm::DevLevel& d = b->members[q]->levels[0].dev;
+            levels.push_back(d);
+            const int items = d.segCount + (d.specialCount + 127) / 128;
+            for (int i = 0; i < items; ++i) collide.push_back(make_int2(q, i));
+            for (int i = 0; i < d.obChunkCount; ++i) open.push_back(make_int2(q, i));
+            perStart.push_back(perStart.back() + d.perCount);
+            cells += d.cellCount;
+        }
+        ck(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream");
+        ck(cudaStreamCreateWithFlags(&b->captureStream, cudaStreamNonBlocking), "stream");
+        ck(cudaEventCreateWithFlags(&b->sync, cudaEventDisableTiming), "event");
+        ck(cudaEventCreate(&b->ev0), "event");
+        ck(cudaEventCreate(&b->ev1), "event");
+        auto own = [&](auto* p) { if (p) b->owned.push_back(p); return p; };
+        lbm::DevBatch& D = b->dev;
+        D.levels = own(upload(levels, b->stream));
+        D.domainCount = count;
+        D.collideItems = own(upload(collide, b->stream));
+        D.collideCount = static_cast<int>(collide.size());
+        D.work = own(devAlloc<int>(2));
+        ck(cudaMemsetAsync(D.work, 0, 2 * sizeof(int), b->stream), "memset");
+        D.openItems = open.empty() ? nullptr : own(upload(open, b->stream));
+        D.openCount = static_cast<int>(open.size());
+        D.periodicStart = own(upload(perStart, b->stream));
+        D.periodicCount = perStart.back();
+        ck(cudaStreamSynchronize(b->stream), "batch upload");
+        b->info.domain_count = count;
+        b->info.cells = cells;
+        b->info.collide_items = D.collideCount;
+        b->info.open_chunks = D.openCount;
+        b->info.periodic_cells = D.periodicCount;
+        b->info.launches_per_step = (D.collideCount > 0) + (D.openCount > 0) + (D.periodicCount > 0);
+    });
+    if (rc != LBM_OK) {
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return LBM_OK;
+}
+
+int lbm_batch_update(lbm_batch* b, int coarse_steps) {
+    if (!b || coarse_steps < 0) return fail(LBM_ERR_INVALID, "lbm_batch_update: bad argument");
+    return guarded("lbm_batch_update", [&] {
+        if (coarse_steps == 0) return;
+        batchCheckParity(b);
+        // after whatever the members' streams hold, and before what they get next
+        for (lbm_grids* g : b->members) {
+            ck(cudaEventRecord(b->sync, g->stream), "event");
+            ck(cudaStreamWaitEvent(b->stream, b->sync, 0), "wait");
+        }
+        batchAdvance(b, coarse_steps);
+        ck(cudaEventRecord(b->sync, b->stream), "event");
+        for (lbm_grids* g : b->members) ck(cudaStreamWaitEvent(g->stream, b->sync, 0), "wait");
+    });
+}
+
+int lbm_batch_time_steps(lbm_batch* b, int coarse_steps, float* ms) {
+    if (!b || !ms || coarse_steps < 0) return fail(LBM_ERR_INVALID, "lbm_batch_time_steps: bad argument");
+    return guarded("lbm_batch_time_steps", [&] {
+        batchCheckParity(b);
+        for (lbm_grids* g : b->members) ck(cudaStreamSynchronize(g->stream), "sync");
+        if (graphable(b->members[0])) {  // capture outside the timed region
+            batchPairGraph(b, 0);
+            batchPairGraph(b, 1);
+        }
+        ck(cudaEventRecord(b->ev0, b->stream), "event");
+        batchAdvance(b, coarse_steps);
+        ck(cudaEventRecord(b->ev1, b->stream), "event");
+        ck(cudaEventSynchronize(b->ev1), "event sync");
+        ck(cudaEventElapsedTime(ms, b->ev0, b->ev1), "elapsed");
+    });
+}
+
+int lbm_batch_get_info(lbm_batch* b, lbm_batch_info* out) {
+    if (!b || !out) return fail(LBM_ERR_INVALID, "lbm_batch_get_info: bad argument");
+    *out = b->info;
+    return LBM_OK;
+}
+
+void lbm_batch_free(lbm_batch* b) { delete b; }
 
 int lbm_set_graphs(lbm_grids* g, int enabled) {
     if (!g) return fail(LBM_ERR_INVALID, "lbm_set_graphs: null grids");

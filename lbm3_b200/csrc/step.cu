@@ -27,14 +27,27 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <map>
+#include <mutex>
 #include <string>
 #include <type_traits>
+#include <utility>
 
-// One storage type per translation unit (compiled three times), so the
-// kernels of the three population formats build in parallel.
+// One storage type and one kernel family per translation unit, so the
+// kernel sets build in parallel.  LBM3_STEP_PART selects the family:
+// 1 the paired persistent collide-stream, 2 the other collide-stream
+// variants, 3 open boundary, periodic ghosts, interface and initial
+// condition, 4 reductions and field transfers (with the storage-independent
+// launchers in the FP32 unit), 0 everything.  Templates a part does not
+// launch are never instantiated in its unit.
 #ifndef LBM3_STEP_STORAGE
 #define LBM3_STEP_STORAGE 0
 #endif
+#ifndef LBM3_STEP_PART
+#define LBM3_STEP_PART 0
+#endif
+#define LBM3_PART(n) (LBM3_STEP_PART == 0 || LBM3_STEP_PART == (n))
+#define LBM3_SHARED_UNIT (LBM3_PART(4) && LBM3_STEP_STORAGE == 0)
 #if LBM3_STEP_STORAGE == 1
 #define LBM3_STEP_SUFFIX F16
 #elif LBM3_STEP_STORAGE == 2
@@ -171,6 +184,7 @@ __device__ __forceinline__ void cellRotorForcing(const DevLevel& g, const int (&
 
 template <bool F, class S>
 __global__ void __launch_bounds__(kBlock) collideStream(DevLevel g) {
+    advanceDither<F, S>(g);
     const int cell = blockIdx.x * kBlock + threadIdx.x;
     if (cell >= g.cellCount) return;
     const int wm = __ldg(g.wallMap + cell);
@@ -183,7 +197,7 @@ __global__ void __launch_bounds__(kBlock) collideStream(DevLevel g) {
     T gx = g.gx, gy = g.gy, gz = g.gz, lambda = collConsts<T>(g).lambda;
     if (g.rotorCount > 0) cellRotorForcing<F, S>(g, ijk, wm, f, gx, gy, gz, lambda);
     collideCumulantT(f, collConsts<T>(g), lambda, gx, gy, gz);
-    writePost<F, S>(g, nb, f);
+    writePost<F, S>(g, nb, f, stepDither<F, S>(g, kSaltCollide));
 }
 
 // Rotor volume fraction at (x, y, z) of one rotor (getRotorFraction,
@@ -419,6 +433,8 @@ __global__ void __launch_bounds__(kTile, LBM3_TMA_MIN_BLOCKS) collideBulkTma(Dev
     const int T = g.segCount;
     const int G = gridDim.x;
     const int t = threadIdx.x;
+    advanceDither<F, S>(g);
+    const Dither D = stepDither<F, S>(g, kSaltCollide);
     if (t == 0) {
 #pragma unroll
         for (int k = 0; k < kStages; ++k) mbarInit(&bar[k], 1);
@@ -480,7 +496,7 @@ __global__ void __launch_bounds__(kTile, LBM3_TMA_MIN_BLOCKS) collideBulkTma(Dev
                 }
                 collideCumulantT(f, collConsts<Real<S>>(g), collConsts<Real<S>>(g).lambda, Real<S>(g.gx),
                                  Real<S>(g.gy), Real<S>(g.gz));
-                writePost<F, S>(g, nb, f);
+                writePost<F, S>(g, nb, f, D);
             }
         }
         if (stop) break;
@@ -514,8 +530,9 @@ __device__ __forceinline__ void collideSpecialCell(const DevLevel& g, int cell) 
     T gx = g.gx, gy = g.gy, gz = g.gz, lambda = collConsts<T>(g).lambda;
     if (kRotors) cellRotorForcing<F, S>(g, ijk, wm, f, gx, gy, gz, lambda);
     collideCumulantT(f, collConsts<T>(g), lambda, gx, gy, gz);
+    const Dither D = stepDither<F, S>(g, kSaltCollide);
     if (wm < 0) {
-        writePost<F, S>(g, nb, f);
+        writePost<F, S>(g, nb, f, D);
         return;
     }
     const unsigned wallData = __ldg(g.wallData + wm);
@@ -557,11 +574,12 @@ __device__ __forceinline__ void collideSpecialCell(const DevLevel& g, int cell) 
     // writes: a linked direction goes to the next pre-collision slot of its
     // inverse (inside the wall cell), the others stream as usual
     S* wbase = static_cast<S*>(g.f);
+    const unsigned cb = D.cell(cell);
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         const bool linked = d != 0 && ((wallData >> d) & 1u);
         const int slot = linked ? (F ? inv(d) : d) : postSlot<F>(d);
-        Store<S>::st(wbase + (long long)slot * g.stride + nb[postNbr(d)], out[d]);
+        stD(wbase + (long long)slot * g.stride + nb[postNbr(d)], out[d], D, cb, d);
     }
     if (g.trackWallForce && !(wallData & 1u)) {
         g.wallForce[wm] += double(fx);
@@ -572,6 +590,7 @@ __device__ __forceinline__ void collideSpecialCell(const DevLevel& g, int cell) 
 
 template <bool F, class S>
 __global__ void __launch_bounds__(kBlock) collideList(DevLevel g) {
+    advanceDither<F, S>(g);
     const int idx = blockIdx.x * kBlock + threadIdx.x;
     if (idx >= g.specialCount) return;
     collideSpecialCell<F, S>(g, __ldg(g.special + idx));
@@ -581,6 +600,7 @@ __global__ void __launch_bounds__(kBlock) collideList(DevLevel g) {
 // update with the rotor forcing before the collision.
 template <bool F, class S>
 __global__ void __launch_bounds__(kBlock) collideRotorList(DevLevel g) {
+    advanceDither<F, S>(g);
     const int idx = blockIdx.x * kBlock + threadIdx.x;
     if (idx >= g.rotorCellCount) return;
     collideSpecialCell<F, S, true>(g, __ldg(g.rotorCells + idx));
@@ -598,6 +618,8 @@ __global__ void __launch_bounds__(kTile, LBM3_PREFETCH_MIN_BLOCKS) collidePrefet
     const int nSpecial = (g.specialCount + kTile - 1) / kTile;
     const int t = threadIdx.x;
     int parity = 0;
+    advanceDither<F, S>(g);
+    const Dither D = stepDither<F, S>(g, kSaltCollide);
     auto fetch = [&]() {
         if (t == 0) slot[parity] = atomicAdd(g.work, 1);
         __syncthreads();
@@ -633,7 +655,7 @@ __global__ void __launch_bounds__(kTile, LBM3_PREFETCH_MIN_BLOCKS) collidePrefet
         if (t < lNext) readPre<F, S>(g, nbn, fn);
         if (t < lCur) {
             collideCumulantT(f, P, P.lambda, T(g.gx), T(g.gy), T(g.gz));
-            writePost<F, S>(g, nb, f);
+            writePost<F, S>(g, nb, f, D);
         }
 #pragma unroll
         for (int q = 0; q < 8; ++q) nb[q] = nbn[q];
@@ -697,15 +719,27 @@ __device__ __forceinline__ void loadPair(const DevLevel& g, const int4& d, int t
     }
 }
 
+// For 16-bit storage one stochastic conversion rounds both lanes' values (cells
+// d.x + t and d.x + t + kHalf) from one 32-bit draw.
 template <bool F, class S>
-__device__ __forceinline__ void storePair(const DevLevel& g, const int4& d, int t, int len, const Pair (&f)[27]) {
+__device__ __forceinline__ void storePair(const DevLevel& g, const int4& d, int t, int len, const Pair (&f)[27],
+                                          const Dither& D) {
     S* base = static_cast<S*>(g.f);
     const bool okA = t < len, okB = t + kHalf < len;
+    if constexpr (sizeof(S) == 2) {
+        const unsigned cb = D.cell(d.x + t);
 #pragma unroll
-    for (int q = 0; q < 27; ++q) {
-        S* p = base + (runOffset32<F, false>(g, d, q) + t);
-        if (okA) Store<S>::st(p, f[q].v.x);
-        if (okB) Store<S>::st(p + kHalf, f[q].v.y);
+        for (int q = 0; q < 27; ++q) {
+            S* p = base + (runOffset32<F, false>(g, d, q) + t);
+            Store<S>::st2R(p, p + kHalf, f[q].v.x, f[q].v.y, Dither::dir(cb, q), okA, okB);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+            S* p = base + (runOffset32<F, false>(g, d, q) + t);
+            if (okA) Store<S>::st(p, f[q].v.x);
+            if (okB) Store<S>::st(p + kHalf, f[q].v.y);
+        }
     }
 }
 
@@ -721,6 +755,8 @@ __global__ void __launch_bounds__(kHalf, LBM3_PAIR_MIN_BLOCKS) collidePair(DevLe
     const int nSpecial = (g.specialCount + kTile - 1) / kTile;
     const int t = threadIdx.x;
     int parity = 0;
+    advanceDither<F, S>(g);
+    const Dither D = stepDither<F, S>(g, kSaltCollide);
     auto fetch = [&]() {
         if (t == 0) slot[parity] = atomicAdd(g.work, 1);
         __syncthreads();
@@ -759,7 +795,7 @@ __global__ void __launch_bounds__(kHalf, LBM3_PAIR_MIN_BLOCKS) collidePair(DevLe
         loadTilePair<F, S>(g, dNext, t, lNext, fn);
 #endif
         collideCumulantT(f, g.coll, g.coll.lambda, g.gx, g.gy, g.gz);
-        storePair<F, S>(g, dCur, t, lCur, f);
+        storePair<F, S>(g, dCur, t, lCur, f, D);
         dCur = dNext;
         lCur = lNext;
     }
@@ -773,6 +809,7 @@ __global__ void __launch_bounds__(kHalf, LBM3_PAIR_MIN_BLOCKS) collidePair(DevLe
     }
 }
 
+#if LBM3_SHARED_UNIT
 // FP64 force and torque about the origin of the cells of one wall ID
 // (updateTracker wall branch, include/trackerFunctions.h:386-428).
 __global__ void __launch_bounds__(kBlock) wallForceSum(DevLevel g, int wallID, double* out) {
@@ -883,12 +920,11 @@ __global__ void __launch_bounds__(kBlock) openFlowSum(DevLevel g, int openBCID, 
         atomicAdd(out + threadIdx.x, a);
     }
 }
+#endif
 
 // F is the flipper after streaming, i.e. the state the ghosts are read in.
 template <bool F, class S>
-__global__ void __launch_bounds__(kBlock) periodicCopy(DevLevel g) {
-    const int idx = blockIdx.x * kBlock + threadIdx.x;
-    if (idx >= g.perCount) return;
+__device__ __forceinline__ void periodicCell(const DevLevel& g, int idx) {
     const int cell = __ldg(g.perIndex + idx);
     const int src = __ldg(g.perSource + idx);
     int nb[8];
@@ -897,6 +933,12 @@ __global__ void __launch_bounds__(kBlock) periodicCopy(DevLevel g) {
     readPre<F, S>(g, nb, f);
     decodeNbr(g, cell, nb, nullptr);
     writePre<F, S>(g, nb, f);
+}
+
+template <bool F, class S>
+__global__ void __launch_bounds__(kBlock) periodicCopy(DevLevel g) {
+    const int idx = blockIdx.x * kBlock + threadIdx.x;
+    if (idx < g.perCount) periodicCell<F, S>(g, idx);
 }
 
 // K4-K6 (updateInterface, include/updateInterface.h:155-891): the interface
@@ -924,11 +966,14 @@ __global__ void __launch_bounds__(kBlock) interfaceExchange(DevLevel C, DevLevel
         const itf::Fit<T> fit = itf::fitStencil(itf::cellMoments(f, omegaF), lane, mask, false);
         T out[27];
         itf::populationsFromGradient(out, fit.d0, fit.c0[0], fit.c0[1], fit.c0[2], fit.g, T(2) / omegaC);
-        decodeNbr(C, __ldg(I.f2cIndex + unit), nb, nullptr);
+        const int coarse = __ldg(I.f2cIndex + unit);
+        decodeNbr(C, coarse, nb, nullptr);
         S* base = static_cast<S*>(C.f);
+        const Dither D = stepDither<FC, S>(C, kSaltInterface);
+        const unsigned cb = D.cell(coarse);
 #pragma unroll
         for (int d = 0; d < 27; ++d)
-            if ((d & 7) == lane) Store<S>::st(base + (long long)preSlot<FC>(d) * C.stride + nb[preNbr(d)], out[d]);
+            if ((d & 7) == lane) stD(base + (long long)preSlot<FC>(d) * C.stride + nb[preNbr(d)], out[d], D, cb, d);
         return;
     }
     if (unit < I.f2cCount + I.c2fCount) {
@@ -948,7 +993,7 @@ __global__ void __launch_bounds__(kBlock) interfaceExchange(DevLevel C, DevLevel
         itf::populationsFromGradient(out, dRho, uv[0], uv[1], uv[2], G, T(0.5) / omegaF);
         decodeNbr(Fn, __ldg(I.c2fChild + u), nb, nullptr);
         decodeNbr(Fn, nb[lane], nr, nullptr);
-        writePre<FF, S>(Fn, nr, out);
+        writePreD<FF, S>(Fn, nr, out, stepDither<FF, S>(Fn, kSaltInterface));
         return;
     }
     // leftovers: the parent plus one coarse neighbour per axis, linear
@@ -999,7 +1044,7 @@ __global__ void __launch_bounds__(kBlock) interfaceExchange(DevLevel C, DevLevel
     T out[27];
     itf::populationsFromGradient(out, r[0], r[1], r[2], r[3], G, T(0.5) / omegaF);
     decodeNbr(Fn, __ldg(I.leftIndex + idx), nb, nullptr);
-    writePre<FF, S>(Fn, nb, out);
+    writePreD<FF, S>(Fn, nb, out, stepDither<FF, S>(Fn, kSaltInterface));
 }
 
 // Characteristic (non-reflective) normal velocity of a face cell: the
@@ -1034,7 +1079,7 @@ __device__ __forceinline__ V nonReflectiveUNormal(V uTarget, V dRhoZ, V dRhoRef)
 __device__ __forceinline__ void openBoundaryDone(const DevLevel& g) {
     if (threadIdx.x == 0) {
         __threadfence();
-        if (atomicAdd(g.obCounter + 1, 1) == int(gridDim.x) - 1) {
+        if (atomicAdd(g.obCounter + 1, 1) == g.obChunkCount - 1) {
             g.obCounter[1] = 0;
             g.obCounter[0] += 1;
             __threadfence();
@@ -1131,6 +1176,8 @@ __device__ __forceinline__ void openClose(const DevLevel& g, const MbbcDirT<Real
         mbbcMomentsEq(dRho + V(1), ux, uy, uz, meq);
         mbbcClose(T, unknown, (T.nu + 3) >> 2, meq, c.f, closed);
     }
+    const Dither D = stepDither<F, S>(g, kSaltOpen);
+    const unsigned cb = D.cell(c.rows.x);
 #pragma unroll
     for (int r = 0; r < kMbbcRowPad; ++r) {
         if (r >= T.nu) break;
@@ -1139,7 +1186,7 @@ __device__ __forceinline__ void openClose(const DevLevel& g, const MbbcDirT<Real
         int cell = sel == 0 ? c.rows.x : sel == 1 ? c.rows.y : sel == 2 ? c.rows.z : c.rows.w;
         if (k & 1) cell = cell + 1 < n ? cell + 1 : 0;
         const int slot = F ? T.unknownInv[r] : T.unknownDir[r];
-        Store<S>::st(base + (long long)slot * g.stride + cell, closed[r] - T.unknownW[r]);
+        stD(base + (long long)slot * g.stride + cell, closed[r] - T.unknownW[r], D, cb, r);
     }
     // reference values: exponential average whose weight decays with the
     // iteration count; below 1e-5 the weight is tripled and the update runs
@@ -1168,16 +1215,15 @@ template <class V> __device__ __forceinline__ void openStageTable(const DevLevel
     for (int q = threadIdx.x; q < int(sizeof(MbbcDirT<V>) / 16); q += blockDim.x) dst[q] = __ldg(src + q);
 }
 
-// One chunk per CTA: the table staging overlaps the gathers.
+// One chunk of open cells on one CTA: the table staging overlaps the gathers.
 template <bool F, class S>
-__global__ void __launch_bounds__(kOpenChunk, LBM3_OPEN_MIN_BLOCKS) openBoundary(DevLevel g) {
+__device__ __forceinline__ void openBoundaryChunk(const DevLevel& g, int chunkIndex, MbbcDirT<Real<S>>& T) {
     using V = Real<S>;
     // the level's finished iterations live on the device (obCounter[0]), so
     // a captured step graph replays with the right count; the last CTA of the
-    // launch advances it once every CTA has read it
+    // level's chunks advances it once every CTA has read it
     const int iterationsFinished = __ldcg(g.obCounter);
-    __shared__ MbbcDirT<V> T;
-    const int4 chunk = __ldg(g.obChunk + blockIdx.x);  // {first, count, normal row, unknown mask}
+    const int4 chunk = __ldg(g.obChunk + chunkIndex);  // {first, count, normal row, unknown mask}
     openStageTable(g, chunk.z, T);
     const bool active = int(threadIdx.x) < chunk.y;
     OpenCell<V> c;
@@ -1185,6 +1231,13 @@ __global__ void __launch_bounds__(kOpenChunk, LBM3_OPEN_MIN_BLOCKS) openBoundary
     __syncthreads();
     if (active) openClose<F, S>(g, T, static_cast<unsigned>(chunk.w), iterationsFinished, c);
     openBoundaryDone(g);  // thread 0 is always active
+}
+
+// One chunk per CTA.
+template <bool F, class S>
+__global__ void __launch_bounds__(kOpenChunk, LBM3_OPEN_MIN_BLOCKS) openBoundary(DevLevel g) {
+    __shared__ MbbcDirT<Real<S>> T;
+    openBoundaryChunk<F, S>(g, blockIdx.x, T);
 }
 
 
@@ -1378,6 +1431,7 @@ __global__ void __launch_bounds__(kBlock) scatterF(DevLevel g, const float* in) 
     Store<S>::st(static_cast<S*>(g.f) + slot * g.stride + cell, in[i]);
 }
 
+#if LBM3_SHARED_UNIT
 __global__ void __launch_bounds__(kBlock) collideBatch(float* f, int n, CollisionConsts P,
                                                        float gx, float gy, float gz) {
     const int c = blockIdx.x * kBlock + threadIdx.x;
@@ -1388,6 +1442,111 @@ __global__ void __launch_bounds__(kBlock) collideBatch(float* f, int n, Collisio
     collideCumulant(v, P, P.lambda, gx, gy, gz);
 #pragma unroll
     for (int d = 0; d < 27; ++d) f[(long long)d * n + c] = v[d];
+}
+#endif
+
+// ---- packed batch ------------------------------------------------------------
+// Domains of a batch advance together: one persistent collide-stream launch
+// takes work items from the packed table of all domains (listed-cell chunks
+// and bulk tiles of domain 0, then of domain 1, ...), so small domains fill
+// the GPU together instead of one underfilled launch each, and the open
+// boundary and periodic ghosts of all domains take one launch each.  A CTA
+// stages the level descriptor of its item's domain in shared memory when the
+// domain changes (a domain's items are contiguous, so that happens a few
+// times per CTA and launch); the work per item is the paired kernel's, so a
+// domain's result is bit-identical to stepping it alone.
+
+// Copy a level descriptor into shared memory (all threads of the CTA).
+__device__ __forceinline__ void stageLevel(const DevLevel* src, DevLevel& dst) {
+    static_assert(sizeof(DevLevel) % 8 == 0, "descriptor copied in 8-byte words");
+    const long long* s = reinterpret_cast<const long long*>(src);
+    long long* d = reinterpret_cast<long long*>(&dst);
+    for (int q = threadIdx.x; q < int(sizeof(DevLevel) / 8); q += blockDim.x) d[q] = __ldg(s + q);
+}
+
+template <bool F, class S>
+__global__ void __launch_bounds__(kHalf, LBM3_PAIR_MIN_BLOCKS) collidePacked(DevBatch b) {
+    __shared__ int slot[2];
+    __shared__ DevLevel sg;
+    const int t = threadIdx.x;
+    if constexpr (sizeof(S) == 2) {
+        // every domain's next step seed (advanceDither of the single-domain launch)
+        if (blockIdx.x == 0)
+            for (int q = t; q < b.domainCount; q += kHalf) {
+                unsigned* seed = b.levels[q].seed;
+                seed[F ? 0 : 1] = mix32(seed[F ? 1 : 0] + 0x6D2B79F5u);
+            }
+    }
+    int parity = 0;
+    auto fetch = [&]() {
+        if (t == 0) slot[parity] = atomicAdd(b.work, 1);
+        __syncthreads();
+        const int v = slot[parity];
+        parity ^= 1;
+        return v;
+    };
+    int dom = -1;
+    int item = fetch();
+    while (item < b.collideCount) {  // CTA-uniform: items come through shared memory
+        const int2 it = __ldg(b.collideItems + item);
+        if (it.x != dom) {
+            __syncthreads();  // every thread is done with the previous domain's descriptor
+            stageLevel(b.levels + it.x, sg);
+            __syncthreads();
+            dom = it.x;
+        }
+        const int next = fetch();  // the atomic's latency overlaps this item's loads
+        const int nSpecial = (sg.specialCount + kTile - 1) / kTile;
+        if (it.y < nSpecial) {
+            const int q = it.y * kTile + t;
+            if (q < sg.specialCount) collideSpecialCell<F, S>(sg, __ldg(sg.special + q));
+            if (q + kHalf < sg.specialCount) collideSpecialCell<F, S>(sg, __ldg(sg.special + q + kHalf));
+        } else {
+            int4 d;
+            int l;
+            loadDesc(sg, it.y - nSpecial, d, l);
+            Pair f[27];
+            loadTilePair<F, S>(sg, d, t, l, f);
+            collideCumulantT(f, sg.coll, sg.coll.lambda, sg.gx, sg.gy, sg.gz);
+            storePair<F, S>(sg, d, t, l, f, stepDither<F, S>(sg, kSaltCollide));
+        }
+        item = next;
+    }
+    if (t == 0) {
+        __threadfence();
+        if (atomicAdd(b.work + 1, 1) == int(gridDim.x) - 1) {
+            b.work[0] = 0;
+            b.work[1] = 0;
+            __threadfence();
+        }
+    }
+}
+
+// One open-boundary chunk of one domain per CTA.
+template <bool F, class S>
+__global__ void __launch_bounds__(kOpenChunk, LBM3_OPEN_MIN_BLOCKS) openPacked(DevBatch b) {
+    __shared__ MbbcDirT<Real<S>> T;
+    __shared__ DevLevel sg;
+    const int2 it = __ldg(b.openItems + blockIdx.x);
+    stageLevel(b.levels + it.x, sg);
+    __syncthreads();
+    openBoundaryChunk<F, S>(sg, it.y, T);
+}
+
+// Periodic ghosts of all domains, one thread per ghost.
+template <bool F, class S>
+__global__ void __launch_bounds__(kBlock) periodicPacked(DevBatch b) {
+    const int idx = blockIdx.x * kBlock + threadIdx.x;
+    if (idx >= b.periodicCount) return;
+    // the last domain whose first ghost is at or before idx (domains without
+    // ghosts share their start with the next one)
+    int lo = 0, hi = b.domainCount - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(b.periodicStart + mid) <= idx) lo = mid;
+        else hi = mid - 1;
+    }
+    periodicCell<F, S>(b.levels[lo], idx - __ldg(b.periodicStart + lo));
 }
 
 inline unsigned blocksFor(long long n) { return static_cast<unsigned>((n + kBlock - 1) / kBlock); }
@@ -1400,70 +1559,64 @@ void dispatch(const DevLevel& g, bool flip, A&&... args) {
 }
 
 // Persistent grid size of a kernel on the current device: SMs x resident
-// CTAs.  Cached per device and kernel (devices may differ in SM count).
+// CTAs.  Cached per device and kernel (devices may differ in SM count); a
+// kernel that needs more than the default dynamic shared memory gets the
+// attribute set before its occupancy is queried.
 template <class K> int persistentGrid(K kernel, int block, int smem) {
-    constexpr int kMaxDevices = 64;
-    static int cache[kMaxDevices] = {};
+    static std::mutex m;
+    static std::map<std::pair<int, const void*>, int> cache;
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev >= 0 && dev < kMaxDevices && cache[dev] > 0) return cache[dev];
+    const std::pair<int, const void*> key(dev, reinterpret_cast<const void*>(kernel));
+    std::lock_guard<std::mutex> lock(m);
+    const auto hit = cache.find(key);
+    if (hit != cache.end()) return hit->second;
     int sms = 0, perSm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (smem > 0) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, block, smem);
     const int grid = (sms > 0 ? sms : 1) * (perSm > 0 ? perSm : 1);
-    if (dev >= 0 && dev < kMaxDevices) cache[dev] = grid;
+    cache[key] = grid;
     return grid;
 }
 
-enum class CollideVariant { Tma, Prefetch, Simple, Pair };
-
-CollideVariant collideVariant() {
-    static int v = -1;
-    if (v < 0) {
-        const char* e = std::getenv("LBM3_COLLIDE_KERNEL");
-        const std::string s = e ? e : "";
-        v = s == "simple" ? 2 : s == "tma" ? 0 : s == "prefetch" ? 1 : 3;
-    }
-    return static_cast<CollideVariant>(v);
-}
-
-// The paired kernel indexes populations with 32-bit element offsets.
-bool pairFits(const DevLevel& g) { return 27LL * g.stride + kTile < (1LL << 31); }
-
-template <bool F, class S> struct RunCollide {
+// The paired persistent kernel: listed cells and bulk tiles in one launch
+// (FP32 arithmetic on two cells per thread), then the rotor cells.
+template <bool F, class S> struct RunCollidePair {
     static void run(const DevLevel& g, cudaStream_t s) {
-        const CollideVariant v = collideVariant();
+        if constexpr (!std::is_same<S, double>::value) {
+            const int items = g.segCount + (g.specialCount + kTile - 1) / kTile;
+            if (items > 0) {
+                const int grid = persistentGrid(collidePair<F, S>, kHalf, 0);
+                collidePair<F, S><<<std::min(grid, items), kHalf, 0, s>>>(g);
+            }
+            if (g.rotorCellCount > 0) collideRotorList<F, S><<<blocksFor(g.rotorCellCount), kBlock, 0, s>>>(g);
+        }
+    }
+};
+
+// The other collide-stream variants (LBM3_COLLIDE_KERNEL), the FP64 build
+// and grids too large for the paired kernel's 32-bit offsets.
+template <bool F, class S> struct RunCollideOther {
+    static void run(const DevLevel& g, cudaStream_t s, CollideVariant v) {
         if (v == CollideVariant::Simple) {
             collideStream<F, S><<<blocksFor(g.cellCount), kBlock, 0, s>>>(g);
             return;
         }
-        if (g.segCount > 0) {
-            if (v == CollideVariant::Tma) {
+        if (v == CollideVariant::Tma) {
+            if (g.segCount > 0) {
                 const int grid = persistentGrid(collideBulkTma<F, S>, kTile, tmaSmemBytes<S>());
                 persistentGrid(collideBulkTma<!F, S>, kTile, tmaSmemBytes<S>());
                 collideBulkTma<F, S><<<std::min(grid, g.segCount), kTile, tmaSmemBytes<S>(), s>>>(g);
             }
-        }
-        // the paired kernel packs two FP32 cells; the FP64 build collides one cell per thread
-        const bool pair = v == CollideVariant::Pair && pairFits(g) && !std::is_same<S, double>::value;
-        if (v == CollideVariant::Prefetch || (v == CollideVariant::Pair && !pair)) {
+            if (g.specialCount > 0) collideList<F, S><<<blocksFor(g.specialCount), kBlock, 0, s>>>(g);
+        } else {
             // bulk segments and listed cells in one persistent launch
             const int items = g.segCount + (g.specialCount + kTile - 1) / kTile;
             if (items > 0) {
                 const int grid = persistentGrid(collidePrefetch<F, S>, kTile, 0);
                 collidePrefetch<F, S><<<std::min(grid, items), kTile, 0, s>>>(g);
             }
-        } else if (pair) {
-            if constexpr (!std::is_same<S, double>::value) {
-                const int items = g.segCount + (g.specialCount + kTile - 1) / kTile;
-                if (items > 0) {
-                    const int grid = persistentGrid(collidePair<F, S>, kHalf, 0);
-                    collidePair<F, S><<<std::min(grid, items), kHalf, 0, s>>>(g);
-                }
-            }
-        } else if (g.specialCount > 0) {
-            collideList<F, S><<<blocksFor(g.specialCount), kBlock, 0, s>>>(g);
         }
         if (g.rotorCellCount > 0) collideRotorList<F, S><<<blocksFor(g.rotorCellCount), kBlock, 0, s>>>(g);
     }
@@ -1538,7 +1691,15 @@ template <bool F, class S> struct RunScatter {
 
 #define LBM3_FN(name) LBM3_STEP_JOIN(name, LBM3_STEP_SUFFIX)
 
-void LBM3_FN(launchCollideStream)(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunCollide>(g, flip, s); }
+#if LBM3_PART(1)
+void LBM3_FN(launchCollidePair)(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunCollidePair>(g, flip, s); }
+#endif
+#if LBM3_PART(2)
+void LBM3_FN(launchCollideOther)(const DevLevel& g, bool flip, cudaStream_t s, CollideVariant v) {
+    dispatch<RunCollideOther>(g, flip, s, v);
+}
+#endif
+#if LBM3_PART(3)
 void LBM3_FN(launchPeriodic)(const DevLevel& g, bool flip, cudaStream_t s) { dispatch<RunPeriodic>(g, flip, s); }
 void LBM3_FN(launchInterface)(const DevLevel& coarse, const DevLevel& fine, const DevInterface& I, bool flipCoarse,
                               bool flipFine, cudaStream_t s) {
@@ -1551,6 +1712,8 @@ void LBM3_FN(launchOpenBoundaryInit)(const DevLevel& g, bool flip, cudaStream_t 
 void LBM3_FN(launchInit)(const DevLevel& g, bool flip, cudaStream_t s, const float4* macro, float4 uniform) {
     dispatch<RunInit>(g, flip, s, macro, uniform);
 }
+#endif
+#if LBM3_PART(4)
 void LBM3_FN(launchKineticEnergy)(const DevLevel& g, bool flip, cudaStream_t s, double* out) {
     dispatch<RunEnergy>(g, flip, s, out);
 }
@@ -1564,9 +1727,30 @@ void LBM3_FN(launchFlowReport)(const DevLevel& g, bool flip, cudaStream_t s, int
                                int v0, int v1, double* out) {
     dispatch<RunFlowReport>(g, flip, s, plane, layer, h0, h1, v0, v1, out);
 }
+#endif
 
-#if LBM3_STEP_STORAGE == 0
-// storage-independent launchers live in the FP32 unit
+#if LBM3_PART(5)
+// One step of a packed batch: collide-stream at flipper F, then the open
+// boundary and periodic ghosts on the streamed state (!F).
+template <bool F, class S> struct RunPackedStep {
+    static void run(const DevBatch& b, cudaStream_t s) {
+        if constexpr (!std::is_same<S, double>::value) {
+            if (b.collideCount > 0) {
+                const int grid = persistentGrid(collidePacked<F, S>, kHalf, 0);
+                collidePacked<F, S><<<std::min(grid, b.collideCount), kHalf, 0, s>>>(b);
+            }
+            if (b.openCount > 0) openPacked<!F, S><<<b.openCount, kOpenChunk, 0, s>>>(b);
+            if (b.periodicCount > 0) periodicPacked<!F, S><<<blocksFor(b.periodicCount), kBlock, 0, s>>>(b);
+        }
+    }
+};
+void LBM3_FN(launchPackedStep)(const DevBatch& b, bool flip, cudaStream_t s) {
+    flip ? RunPackedStep<true, StepStore>::run(b, s) : RunPackedStep<false, StepStore>::run(b, s);
+}
+#endif
+
+#if LBM3_SHARED_UNIT
+// storage-independent launchers live in the FP32 unit of part 4
 int stepLaunchCount(const DevLevel& g) {
     int n = 0;
     const CollideVariant v = collideVariant();

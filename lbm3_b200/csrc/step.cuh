@@ -58,6 +58,8 @@ struct DevLevel {
     int* errorFlag;          // set to nonzero when a bounded device wait gives up
     int* work;               // [2] work-item counter and finished-CTA count of the
                              // persistent collide-stream (zero between launches)
+    unsigned* seed;          // [2] step seeds of the stochastic rounding of 16-bit
+                             // storage, by esotwist parity (null for FP32 / FP64)
     // wall-adjacent cells (WallStruct)
     const unsigned* wallData;      // [wallCount]
     const unsigned* linkLength;    // [7][wallCount] packed 8-bit link codes
@@ -96,6 +98,22 @@ struct DevLevel {
     const int* rotorCells;         // cells inside a rotor's swept cylinder
     int rotorCellCount;
     int trackRotorForce;
+};
+
+// A packed batch of single-level domains advanced together (one launch per
+// kernel kind for all of them): the domains' level descriptors on the device
+// and the packed tables of work items.
+struct DevBatch {
+    const DevLevel* levels;    // [domainCount] device copies
+    int domainCount;
+    const int2* collideItems;  // {domain, item}: items of the paired collide-stream
+                               // (listed-cell chunks first, then bulk tiles), by domain
+    int collideCount;
+    int* work;                 // [2] item counter and finished-CTA count (zero between launches)
+    const int2* openItems;     // {domain, chunk} of the open-boundary kernel
+    int openCount;
+    const int* periodicStart;  // [domainCount + 1] prefix sums of the ghost counts
+    int periodicCount;
 };
 
 // Interface lists between a coarse level and the next finer one
@@ -177,16 +195,97 @@ template <> struct Store<float> {
     static __device__ __forceinline__ float ldL2(const float* p) { return __ldcg(p); }
     static __device__ __forceinline__ void st(float* p, float v) { *p = v; }
 };
+// stR / st2R round stochastically with the random bits r: cvt.rs adds random
+// bits below the kept mantissa and truncates, so a value rounds up with
+// probability equal to its distance from the lower neighbour in units of the
+// spacing.  st2R converts two values with one instruction (a to *pa, b to *pb).
 template <> struct Store<__half> {
     static __device__ __forceinline__ float ld(const __half* p) { return __half2float(*p); }
     static __device__ __forceinline__ float ldL2(const __half* p) { return __half2float(__ldcg(p)); }
     static __device__ __forceinline__ void st(__half* p, float v) { *p = __float2half_rn(v); }
+    static __device__ __forceinline__ void stR(__half* p, float v, unsigned r) {
+        unsigned d;
+        asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(0.f), "f"(v), "r"(r));
+        *reinterpret_cast<unsigned short*>(p) = static_cast<unsigned short>(d & 0xFFFFu);
+    }
+    static __device__ __forceinline__ void st2R(__half* pa, __half* pb, float a, float b, unsigned r, bool okA,
+                                                bool okB) {
+        unsigned d;
+        asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(b), "f"(a), "r"(r));
+        if (okA) *reinterpret_cast<unsigned short*>(pa) = static_cast<unsigned short>(d & 0xFFFFu);
+        if (okB) *reinterpret_cast<unsigned short*>(pb) = static_cast<unsigned short>(d >> 16);
+    }
 };
 template <> struct Store<__nv_bfloat16> {
     static __device__ __forceinline__ float ld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
     static __device__ __forceinline__ float ldL2(const __nv_bfloat16* p) { return __bfloat162float(__ldcg(p)); }
     static __device__ __forceinline__ void st(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+    static __device__ __forceinline__ void stR(__nv_bfloat16* p, float v, unsigned r) {
+        unsigned d;
+        asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(0.f), "f"(v), "r"(r));
+        *reinterpret_cast<unsigned short*>(p) = static_cast<unsigned short>(d & 0xFFFFu);
+    }
+    static __device__ __forceinline__ void st2R(__nv_bfloat16* pa, __nv_bfloat16* pb, float a, float b, unsigned r,
+                                                bool okA, bool okB) {
+        unsigned d;
+        asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(b), "f"(a), "r"(r));
+        if (okA) *reinterpret_cast<unsigned short*>(pa) = static_cast<unsigned short>(d & 0xFFFFu);
+        if (okB) *reinterpret_cast<unsigned short*>(pb) = static_cast<unsigned short>(d >> 16);
+    }
 };
+
+// Stochastic rounding of 16-bit storage.  With round-to-nearest, a steady
+// state rounds every population the same way step after step, and that fixed
+// error is a constant forcing that the slowly relaxing hydrodynamic modes add
+// up; with random rounding the error has zero mean and averages out.  The bits
+// are a counter-based hash of (step seed, kernel salt, cell, direction) with
+// the lowbias32 finaliser (C. Wellons, "Prospecting for hash functions",
+// 2018), so results are deterministic: a replayed graph, a domain stepped
+// alone or inside a batch draw the same bits.  Kernels of esotwist parity F
+// read seed[F]; every collide-stream launch of the step writes the next value
+// into seed[!F], which no kernel of that step reads.
+__device__ __forceinline__ unsigned mix32(unsigned x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+struct Dither {
+    unsigned seed;
+    // bits of one cell; dir() then gives one 32-bit draw per direction
+    __device__ __forceinline__ unsigned cell(int c) const { return seed ^ (static_cast<unsigned>(c) * 0x9E3779B1u); }
+    static __device__ __forceinline__ unsigned dir(unsigned cellBits, int q) {
+        return mix32(cellBits + static_cast<unsigned>(q) * 0x632BE5ABu);
+    }
+};
+
+enum : unsigned { kSaltCollide = 0u, kSaltOpen = 0x51ED270Bu, kSaltInterface = 0xA3C59AC3u };
+
+// The rounding is fixed per storage type at compile time: a run-time choice
+// between the two roundings in every store multiplies the code the
+// assembler has to schedule.
+template <bool F, class S>
+__device__ __forceinline__ Dither stepDither(const DevLevel& g, unsigned salt) {
+    if constexpr (sizeof(S) == 2) return Dither{g.seed[F ? 1 : 0] ^ salt};
+    else return Dither{0u};
+}
+
+template <bool F, class S>
+__device__ __forceinline__ void advanceDither(const DevLevel& g) {
+    if constexpr (sizeof(S) == 2) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) g.seed[F ? 0 : 1] = mix32(g.seed[F ? 1 : 0] + 0x6D2B79F5u);
+    }
+}
+
+// Store one collided value: stochastic for 16-bit storage, as is otherwise.
+template <class S, class T>
+__device__ __forceinline__ void stD(S* p, T v, const Dither& D, unsigned cellBits, int q) {
+    if constexpr (sizeof(S) == 2) Store<S>::stR(p, v, Dither::dir(cellBits, q));
+    else Store<S>::st(p, v);
+}
 
 // Esotwist: with flipper F, direction d is read from the cell offset by
 // max(0,-c_d) in slot (F ? inv(d) : d) and written after collision to the
@@ -204,11 +303,11 @@ __device__ __forceinline__ void readPre(const DevLevel& g, const int (&nb)[8], T
 }
 
 template <bool F, class S, class T>
-__device__ __forceinline__ void writePost(const DevLevel& g, const int (&nb)[8], const T (&f)[27]) {
+__device__ __forceinline__ void writePost(const DevLevel& g, const int (&nb)[8], const T (&f)[27], const Dither& D) {
     S* base = static_cast<S*>(g.f);
+    const unsigned cb = D.cell(nb[0]);
 #pragma unroll
-    for (int d = 0; d < 27; ++d)
-        Store<S>::st(base + (long long)postSlot<F>(d) * g.stride + nb[postNbr(d)], f[d]);
+    for (int d = 0; d < 27; ++d) stD(base + (long long)postSlot<F>(d) * g.stride + nb[postNbr(d)], f[d], D, cb, d);
 }
 
 // Write f as pre-collision values of the cell (used by initial condition and
@@ -219,6 +318,15 @@ __device__ __forceinline__ void writePre(const DevLevel& g, const int (&nb)[8], 
 #pragma unroll
     for (int d = 0; d < 27; ++d)
         Store<S>::st(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)], f[d]);
+}
+
+// writePre of interpolated values (interface), rounded like collided ones.
+template <bool F, class S, class T>
+__device__ __forceinline__ void writePreD(const DevLevel& g, const int (&nb)[8], const T (&f)[27], const Dither& D) {
+    S* base = static_cast<S*>(g.f);
+    const unsigned cb = D.cell(nb[0]);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) stD(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)], f[d], D, cb, d);
 }
 
 }  // namespace lbm

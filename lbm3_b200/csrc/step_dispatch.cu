@@ -2,6 +2,9 @@
 // population storage type, and these entry points forward to its unit.
 #include "step_launch.h"
 
+#include <cstdlib>
+#include <string>
+
 namespace lbm {
 
 #define LBM3_BY_STORAGE(name, ...)                                          \
@@ -12,7 +15,28 @@ namespace lbm {
         default: name##F32(__VA_ARGS__);                                    \
     }
 
-void launchCollideStream(const DevLevel& g, bool flip, cudaStream_t s) { LBM3_BY_STORAGE(launchCollideStream, g, flip, s) }
+CollideVariant collideVariant() {
+    static const CollideVariant v = [] {
+        const char* e = std::getenv("LBM3_COLLIDE_KERNEL");
+        const std::string s = e ? e : "";
+        return s == "simple" ? CollideVariant::Simple
+               : s == "tma"  ? CollideVariant::Tma
+               : s == "prefetch" ? CollideVariant::Prefetch
+                                 : CollideVariant::Pair;
+    }();
+    return v;
+}
+
+// The paired kernel packs two FP32 cells per thread; the FP64 build collides
+// one cell per thread in the prefetching kernel.
+void launchCollideStream(const DevLevel& g, bool flip, cudaStream_t s) {
+    const CollideVariant v = collideVariant();
+    if (v == CollideVariant::Pair && pairFits(g) && g.storage != LBM_STORE_F64) {
+        LBM3_BY_STORAGE(launchCollidePair, g, flip, s)
+    } else {
+        LBM3_BY_STORAGE(launchCollideOther, g, flip, s, v == CollideVariant::Pair ? CollideVariant::Prefetch : v)
+    }
+}
 void launchPeriodic(const DevLevel& g, bool flip, cudaStream_t s) { LBM3_BY_STORAGE(launchPeriodic, g, flip, s) }
 void launchInterface(const DevLevel& coarse, const DevLevel& fine, const DevInterface& I, bool flipCoarse,
                      bool flipFine, cudaStream_t s) {
@@ -40,6 +64,15 @@ void launchScatterF(const DevLevel& g, cudaStream_t s, const float* in) { LBM3_B
 void launchFlowReport(const DevLevel& g, bool flip, cudaStream_t s, int plane, int layer, int h0, int h1, int v0,
                       int v1, double* out) {
     LBM3_BY_STORAGE(launchFlowReport, g, flip, s, plane, layer, h0, h1, v0, v1, out)
+}
+
+void launchPackedStep(const DevBatch& b, int storage, bool flip, cudaStream_t s) {
+    switch (storage) {
+        case LBM_STORE_F16: launchPackedStepF16(b, flip, s); break;
+        case LBM_STORE_BF16: launchPackedStepBF16(b, flip, s); break;
+        case LBM_STORE_F32: launchPackedStepF32(b, flip, s); break;
+        default: break;  // FP64 domains are not packed
+    }
 }
 
 #undef LBM3_BY_STORAGE

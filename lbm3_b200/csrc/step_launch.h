@@ -10,6 +10,13 @@
 
 namespace lbm {
 
+// Collide-stream kernel choice (LBM3_COLLIDE_KERNEL = simple | tma | prefetch;
+// default: the paired persistent kernel)
+enum class CollideVariant { Tma, Prefetch, Simple, Pair };
+CollideVariant collideVariant();
+// The paired kernel indexes populations with 32-bit element offsets.
+inline bool pairFits(const DevLevel& g) { return 27LL * g.stride + 128 < (1LL << 31); }  // 128: one tile
+
 void launchCollideStream(const DevLevel& g, bool flip, cudaStream_t s);
 // kernels one updateSingleGrid launches for this level
 int stepLaunchCount(const DevLevel& g);
@@ -36,10 +43,14 @@ void launchRotorForce(const DevRotor& R, const int* index, cudaStream_t s, doubl
 void launchOpenFlow(const DevLevel& g, int openBCID, float invSpan, cudaStream_t s, double* out);
 void launchCollideBatch(float* f, int n, const CollisionConsts& P, float gx, float gy, float gz,
                         cudaStream_t s);
+// One step of a packed batch of single-level domains of one storage type
+// (FP32, FP16 or BF16), all at esotwist flipper `flip`.
+void launchPackedStep(const DevBatch& b, int storage, bool flip, cudaStream_t s);
 
 // per-storage launchers (one set per step.cu unit)
 #define LBM3_DECLARE_STORAGE_LAUNCHERS(SUF)                                                                      \
-    void launchCollideStream##SUF(const DevLevel& g, bool flip, cudaStream_t s);                               \
+    void launchCollidePair##SUF(const DevLevel& g, bool flip, cudaStream_t s);                                 \
+    void launchCollideOther##SUF(const DevLevel& g, bool flip, cudaStream_t s, CollideVariant v);              \
     void launchPeriodic##SUF(const DevLevel& g, bool flip, cudaStream_t s);                                    \
     void launchInterface##SUF(const DevLevel& coarse, const DevLevel& fine, const DevInterface& I, bool flipC,  \
                               bool flipF, cudaStream_t s);                                                     \
@@ -52,7 +63,8 @@ void launchCollideBatch(float* f, int n, const CollisionConsts& P, float gx, flo
     void launchGatherF##SUF(const DevLevel& g, cudaStream_t s, float* out);                                    \
     void launchScatterF##SUF(const DevLevel& g, cudaStream_t s, const float* in);                              \
     void launchFlowReport##SUF(const DevLevel& g, bool flip, cudaStream_t s, int plane, int layer, int h0,     \
-                               int h1, int v0, int v1, double* out);
+                               int h1, int v0, int v1, double* out);                                           \
+    void launchPackedStep##SUF(const DevBatch& b, bool flip, cudaStream_t s);
 LBM3_DECLARE_STORAGE_LAUNCHERS(F32)
 LBM3_DECLARE_STORAGE_LAUNCHERS(F16)
 LBM3_DECLARE_STORAGE_LAUNCHERS(BF16)

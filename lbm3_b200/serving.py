@@ -6,11 +6,16 @@ grid_memory_bytes, every device array the build allocates) fits the
 remaining HBM budget.  Its grids are then built on a builder thread (host
 voxelization and tables, upload, initial condition) while the domains
 already resident keep stepping; once built, a domain joins the active set.
-Active domains keep their populations and tables resident and advance
-together with update_batch, one stream each, in chunks of steps, so that
-work of requests that arrived at different times overlaps on the GPU.  A
-finished domain reads its result, frees its memory and its slot, and the
-next waiting request is admitted.
+Active domains keep their populations and tables resident and advance in
+chunks of steps.  Single-level domains without rotors advance in a packed
+batch per storage type: one persistent collide-stream launch over the packed
+block table of all of them, one open-boundary and one periodic launch per
+step, replayed as a CUDA graph (PackedBatch); the batch is rebuilt whenever
+a domain joins or leaves.  A domain that joins at the other esotwist parity
+than the batch steps once on its own first.  Other domains (several levels,
+rotors, FP64) advance with update_batch on their own streams.  A finished
+domain reads its result, frees its memory and its slot, and the next
+waiting request is admitted.
 
 Each result is the one the request gets when run alone: batched stepping is
 bit-identical to stepping a domain by itself.
@@ -24,7 +29,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _abi as A
-from .grids import Grids, Plan, update_batch
+from .grids import Grids, PackedBatch, Plan, update_batch
 
 
 @dataclass
@@ -66,6 +71,16 @@ class _Active:
     admitted: float
     updates: int
     build: object = None        # future of the grid build while it runs
+    packable: bool = False      # single level, no rotors, FP32 / FP16 / BF16
+
+    @property
+    def parity(self) -> int:
+        return (self.req.steps - self.remaining) & 1
+
+
+def _packable(g: Grids) -> bool:
+    c = g.case
+    return g.level_count() == 1 and c.rotor_count == 0 and c.storage != A.LBM_STORE_F64
 
 
 def _footprint(req: Request):
@@ -88,7 +103,33 @@ class Server:
     chunk_steps: int = 100
     keep_fields: bool = False
     builders: int = 2
+    pack: bool = True           # packed batches (False: every domain on its own stream)
     results: list = field(default_factory=list)
+    _batches: dict = field(default_factory=dict)   # storage -> (member rids, PackedBatch)
+
+    def _close_batches(self, rids=None):
+        """Close the packed batches holding any of `rids` (all with None)."""
+        for st in list(self._batches):
+            key, b = self._batches[st]
+            if rids is None or any(r in key for r in rids):
+                b.close()
+                del self._batches[st]
+
+    def _advance(self, ready, chunk):
+        groups, loose = {}, []
+        for a in ready:
+            (groups.setdefault(a.req.case.storage, []) if self.pack and a.packable else loose).append(a)
+        for st, members in groups.items():
+            if len(members) == 1:
+                loose.extend(members)
+                continue
+            key = tuple(a.req.rid for a in members)
+            if st not in self._batches or self._batches[st][0] != key:
+                self._close_batches([r for r in (self._batches.get(st) or ((), None))[0]])
+                self._batches[st] = (key, PackedBatch([a.grids for a in members]))
+            self._batches[st][1].update(chunk)
+        if loose:
+            update_batch([a.grids for a in loose], chunk)
 
     def run(self, requests) -> list:
         import torch
@@ -125,17 +166,28 @@ class Server:
                         a.build = None
                         a.stream = torch.cuda.Stream()
                         a.grids.set_stream(a.stream.cuda_stream)
-                ready = [a for a in active if a.grids is not None]
-                if not ready:
+                        a.packable = _packable(a.grids)
+                        # join the packed batch of its storage type at the batch's parity
+                        mates = [b for b in active if b is not a and b.grids is not None and b.packable
+                                 and b.req.case.storage == a.req.case.storage and b.remaining > 0]
+                        if self.pack and a.packable and mates and mates[0].parity != a.parity:
+                            a.grids.update_all_grids(1)
+                            a.remaining -= 1
+                ready = [a for a in active if a.grids is not None and a.remaining > 0]
+                finished = any(a.grids is not None and a.remaining == 0 for a in active)
+                if not ready and not finished:
                     # idle until the next arrival or build completion
                     wait = 0.002 if active else max(0.0, pending[0].arrival - (time.perf_counter() - t0))
                     time.sleep(min(0.01, wait))
                     continue
-                chunk = min(self.chunk_steps, min(a.remaining for a in ready))
-                update_batch([a.grids for a in ready], chunk)
-                for a in ready:
-                    a.remaining -= chunk
-                done = [a for a in ready if a.remaining == 0]
+                if ready:
+                    chunk = min(self.chunk_steps, min(a.remaining for a in ready))
+                    self._advance(ready, chunk)
+                    for a in ready:
+                        a.remaining -= chunk
+                done = [a for a in active if a.grids is not None and a.remaining == 0]
+                if done:
+                    self._close_batches([a.req.rid for a in done])
                 for a in done:
                     g = a.grids
                     g.synchronize()
@@ -154,6 +206,7 @@ class Server:
                 active = [a for a in active if a.remaining > 0]
         finally:
             # on an error, release everything admitted so far
+            self._close_batches()
             for a in active:
                 if a.build is not None:
                     try:

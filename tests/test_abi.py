@@ -30,9 +30,10 @@ def test_every_declared_symbol_is_exported():
 def test_struct_layouts_match_the_header(tmp_path):
     src = tmp_path / "sizes.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "lbm3_b200.h"\n'
-                   'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(lbm_case), sizeof(lbm_face_bc),'
+                   'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(lbm_case), sizeof(lbm_face_bc),'
                    ' sizeof(lbm_grid_info), offsetof(lbm_case, storage), offsetof(lbm_grid_info, grid_memory_bytes),'
-                   ' offsetof(lbm_case, track_rotor_force), sizeof(lbm_rotor), sizeof(lbm_rotor_info));'
+                   ' offsetof(lbm_case, track_rotor_force), sizeof(lbm_rotor), sizeof(lbm_rotor_info),'
+                   ' sizeof(lbm_batch_info), offsetof(lbm_batch_info, collide_items));'
                    'return 0;}\n')
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
@@ -45,6 +46,8 @@ def test_struct_layouts_match_the_header(tmp_path):
     assert int(out[5]) == A.LbmCase.track_rotor_force.offset
     assert int(out[6]) == C.sizeof(A.LbmRotor)
     assert int(out[7]) == C.sizeof(A.LbmRotorInfo)
+    assert int(out[8]) == C.sizeof(A.LbmBatchInfo)
+    assert int(out[9]) == A.LbmBatchInfo.collide_items.offset
 
 
 def test_null_arguments_are_rejected_without_a_device():
@@ -64,6 +67,16 @@ def test_null_arguments_are_rejected_without_a_device():
     assert lib.lbm_save_state(None, None, 0) == A.LBM_ERR_INVALID
     assert lib.lbm_load_state(None, None, 0) == A.LBM_ERR_INVALID
     assert lib.lbm_kinetic_energy_noalloc(None, 1.0, 1.0, out) == A.LBM_ERR_INVALID
+    h = C.c_void_p()
+    assert lib.lbm_batch_create(None, 1, C.byref(h)) == A.LBM_ERR_INVALID
+    arr = (C.c_void_p * 2)(None, None)
+    assert lib.lbm_batch_create(arr, 2, C.byref(h)) == A.LBM_ERR_INVALID and not h.value
+    assert lib.lbm_batch_update(None, 1) == A.LBM_ERR_INVALID
+    ms = C.c_float()
+    assert lib.lbm_batch_time_steps(None, 1, C.byref(ms)) == A.LBM_ERR_INVALID
+    info = A.LbmBatchInfo()
+    assert lib.lbm_batch_get_info(None, C.byref(info)) == A.LBM_ERR_INVALID
+    lib.lbm_batch_free(None)
 
 
 def test_plan_rotor_queries_on_the_host():

@@ -46,3 +46,74 @@ def test_batch_rejects_null_entries():
     import ctypes as C
     arr = (C.c_void_p * 2)(None, None)
     assert A.lib().lbm_update_batch(arr, 2, 1) == A.LBM_ERR_INVALID
+
+
+def packed_cases(storage):
+    """Three single-level domains of one storage type: Taylor-Green 32^3 with
+    periodic ghosts, a channel around a sphere (open boundaries, walls) and a
+    stirred periodic box with a body force."""
+    c1 = L.taylor_green(32, storage=storage).case
+    c2 = L.open_channel(40, 20, 18, u_in=0.04, nu_lattice=0.02, storage=storage)
+    G.set_bodies(c2, [G.icosphere(2, 3.5, (14.0, 10.0, 9.0))])
+    c2.track_wall_force = 1
+    c3 = L.periodic_box(20, 28, 24, nu_lattice=0.03, storage=storage)
+    c3.gx = 1e-5
+    return [c1, c2, c3]
+
+
+@pytest.mark.parametrize("storage", [A.LBM_STORE_F32, A.LBM_STORE_F16, A.LBM_STORE_BF16])
+def test_packed_batch_matches_domains_stepped_alone(storage):
+    """One packed launch set for all members: every member's populations and
+    wall force equal those of the member stepped alone, bit for bit (graph
+    pairs, a trailing odd step, and member steps between batch updates)."""
+    alone = []
+    for c in packed_cases(storage):
+        with L.build_grids(c) as g:
+            g.update_all_grids(13)
+            alone.append((g.populations(), g.wall_force(0) if c.track_wall_force else None))
+    grids = [L.build_grids(c) for c in packed_cases(storage)]
+    try:
+        with L.PackedBatch(grids) as b:
+            info = b.info()
+            assert info.domain_count == 3 and info.launches_per_step == 3
+            assert info.cells == sum(g.info(0).cell_count for g in grids)
+            b.update(4)
+            b.update(5)
+            for g in grids:  # members keep their own stepping between batch updates
+                g.update_all_grids(2)
+            b.update(2)
+        for g, (f, force) in zip(grids, alone):
+            g.synchronize()
+            np.testing.assert_array_equal(g.populations(), f)
+            if force is not None:
+                np.testing.assert_array_equal(g.wall_force(0), force)
+    finally:
+        for g in grids:
+            g.close()
+
+
+def test_packed_batch_requires_one_parity_and_plain_members():
+    c = packed_cases(A.LBM_STORE_F32)
+    grids = [L.build_grids(c[0]), L.build_grids(c[2])]
+    try:
+        grids[1].update_all_grids(1)
+        with L.PackedBatch(grids) as b:
+            with pytest.raises(A.LbmError):
+                b.update(2)
+            grids[0].update_all_grids(1)
+            b.update(2)
+        f16 = L.build_grids(packed_cases(A.LBM_STORE_F16)[2])
+        with pytest.raises(A.LbmError):
+            L.PackedBatch([grids[0], f16])
+        f16.close()
+        r = L.periodic_box(24, 24, 24, nu_lattice=0.02)
+        G.set_rotors(r, [(G.rotor(hub_radius=2, tip_radius=7, chord=3, thickness=1.0, hub_length=4),
+                          dict(axis=2, origin=(0, 0, 0), radians_per_second=2.0))])
+        with L.build_grids(r) as rg:
+            with pytest.raises(A.LbmError):
+                L.PackedBatch([grids[0], rg])
+        with pytest.raises(A.LbmError):
+            L.PackedBatch([grids[0], grids[0]])
+    finally:
+        for g in grids:
+            g.close()
