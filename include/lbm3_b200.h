@@ -164,6 +164,15 @@ typedef struct lbm_face_bc {
 
 #define LBM_MAX_LEVELS 4      /* grid levels of one domain, refinement ratio 2  */
 
+/* non-reflective open-boundary scheme (lbm_case.open_bc_scheme) */
+#define LBM_OPEN_CHARACTERISTIC 0  /* outgoing characteristic against exponentially
+                                      averaged reference values (include/updateGrid.h:250-347) */
+#define LBM_OPEN_IMPEDANCE      1  /* impedance scheme: the given density / normal
+                                      velocity is clamped to within a density tolerance
+                                      of the non-reflecting state computed from the
+                                      previous completed boundary state
+                                      (cases/nonReflectiveTest/updateGrid_SCHLAFFER_IMPEDANCE_SCHEME.h) */
+
 /* One static body: a triangle soup in mm (the reference's gridStaticSTLs
  * entry; its index is the body's wallID). */
 typedef struct lbm_body {
@@ -258,6 +267,12 @@ typedef struct lbm_case {
      * refinement_hook, if set, then sees the marker and may change it. */
     float refine_box[LBM_MAX_LEVELS][6];
     lbm_refinement_hook refinement_hook;
+
+    /* Non-reflective open boundaries (cells whose BC sets nonReflective):
+     * LBM_OPEN_*; rho_reflection_tolerance is the impedance scheme's
+     * RHO_REFLECTION_TOLERANCE (>= 0; 1 or more turns the scheme off). */
+    int   open_bc_scheme;
+    float rho_reflection_tolerance;
 } lbm_case;
 
 /* The reference's BCStruct defaults (include/types.h:131-136). */

@@ -38,6 +38,8 @@ LBM_STORE_F32 = 0
 LBM_STORE_F16 = 1
 LBM_STORE_BF16 = 2
 LBM_STORE_F64 = 3
+LBM_OPEN_CHARACTERISTIC = 0
+LBM_OPEN_IMPEDANCE = 1
 STORAGE_NAMES = {LBM_STORE_F32: "f32", LBM_STORE_F16: "f16", LBM_STORE_BF16: "bf16", LBM_STORE_F64: "f64"}
 
 # arrays
@@ -131,6 +133,7 @@ class LbmCase(C.Structure):
         ("open_bc_hook", C.c_void_p), ("initial_condition_hook", C.c_void_p), ("local_bc_hook", C.c_void_p),
         ("hook_user", C.c_void_p),
         ("refine_box", (C.c_float * 6) * LBM_MAX_LEVELS), ("refinement_hook", C.c_void_p),
+        ("open_bc_scheme", C.c_int), ("rho_reflection_tolerance", C.c_float),
     ]
 
 

@@ -199,6 +199,96 @@ def open_channel(nx: int, ny: int, nz: int, u_in: float = 0.04, nu_lattice: floa
 
 
 @dataclass
+class PipeSetup:
+    """The non-reflective boundary study: the case and the inlet profile."""
+    case: A.LbmCase
+    u_mean: float             # lattice mean inlet velocity
+    radius_mm: float
+    dt: float                 # s per step
+
+    def inlet_target(self, i: int, j: int, info) -> float:
+        """Lattice uz the inlet prescribes at cell (i, j), as getOpenBC forms it."""
+        return _pipe_profile(i, j, info, self.u_mean, self.radius_mm)
+
+
+def _pipe_profile(i, j, info, u_mean, radius):
+    # getXYZFromIJKCellIndex and the radius as device code forms them, with
+    # contracted multiply-adds: x = fma(i, res, ox), r2 = fma(x, x, y * y)
+    # (the products are exact in FP64, so one FP32 rounding of the sum is the fma)
+    x = f32(float(i) * float(f32(info.res)) + float(f32(info.ox)))
+    y = f32(float(j) * float(f32(info.res)) + float(f32(info.oy)))
+    r2 = f32(float(x) * float(x) + float(f32(y * y)))
+    return f32(f32(2.0) * f32(u_mean) * max(f32(0.0), f32(f32(1.0) - f32(r2 / f32(f32(radius) * f32(radius))))))
+
+
+def non_reflective_pipe(scheme: str = "characteristic", tolerance: float = 2e-5, cells_per_mm: int = 5,
+                        storage: int = A.LBM_STORE_F32) -> PipeSetup:
+    """The reference's non-reflective boundary study
+    (cases/nonReflectiveTest/nonReflectiveTestMain.cu): a pipe of 20 mm
+    diameter, the bore of a 25 mm square block (a 90-sided polygon, vertices
+    every 4 degrees), cut to 100 mm along z at 0.2 mm cells, Re 1000 on the
+    mean velocity 0.03 (air: nu 1.5e-5 m^2/s, rho 1.225 kg/m^3), fluid at
+    rest initially.  The inlet (k = 0, openBCID 0) prescribes the parabolic
+    profile 2 u (1 - r^2 / R^2); the outlet (last k, openBCID 1) dRho = 0.
+    `scheme`: "dirichlet" (plain inlet), "characteristic" (the stock
+    non-reflective inlet) or "impedance" (the impedance scheme with
+    RHO_REFLECTION_TOLERANCE = `tolerance`).  Walls without interpolation,
+    AllOne collision (collision limiter 0)."""
+    from .geometry import bored_block, set_bodies
+    u_mean = f32(0.03)
+    reynolds = f32(1000.0)
+    diameter = f32(20.0)
+    length = f32(100.0)
+    radius = f32(f32(0.5) * diameter)
+    nu_phys = f32(1.5e-5)
+    res = f32(f32(1.0) / f32(cells_per_mm))
+    u_phys = f32(reynolds * nu_phys / f32(diameter / f32(1000.0)))
+    dt = f32(f32(u_mean / u_phys) * f32(res / f32(1000.0)))
+    c = _blank_case()
+    c.res_global = res
+    c.nu_phys = nu_phys
+    c.rho_phys = f32(1.225)
+    c.dt_phys_global = dt
+    tris = bored_block(12.5, float(radius), -100.0, 100.0, segments=90)
+    set_bodies(c, [tris])
+    lo, hi = tris.reshape(-1, 3).min(axis=0), tris.reshape(-1, 3).max(axis=0)
+    c.bounds[0], c.bounds[1], c.bounds[3], c.bounds[4] = lo[0], lo[1], hi[0], hi[1]
+    c.bounds[2], c.bounds[5] = -f32(length * f32(0.5)), f32(length * f32(0.5))
+    c.collision_limiter = 0.0
+    c.use_ibb = 0
+    c.track_open_boundaries = 1
+    c.storage = storage
+    if scheme == "impedance":
+        c.open_bc_scheme = A.LBM_OPEN_IMPEDANCE
+        c.rho_reflection_tolerance = tolerance
+    elif scheme not in ("characteristic", "dirichlet"):
+        raise ValueError("scheme must be 'dirichlet', 'characteristic' or 'impedance'")
+    non_reflective = scheme != "dirichlet"
+
+    def open_bc(bc, i, j, k, info):
+        if k == 0:
+            bc.dirichletU = 1
+            bc.ux, bc.uy = 0.0, 0.0
+            bc.uz = _pipe_profile(i, j, info, u_mean, radius)
+            bc.nonReflective = int(non_reflective)
+            bc.openBCID = 0
+        elif k == info.cell_count_z - 1:
+            bc.dirichletRho = 1
+            bc.dRho = 0.0
+            bc.nonReflective = 0
+            bc.openBCID = 1
+
+    def local_bc(bc, i, j, k, info):
+        bc.collisionLimiter = 0.0
+        if bc.wallID >= 0:
+            bc.ux = bc.uy = bc.uz = 0.0
+        bc.useIBB = 0
+
+    set_hooks(c, open_bc=open_bc, local_bc=local_bc)
+    return PipeSetup(c, float(u_mean), float(radius), float(dt))
+
+
+@dataclass
 class SphereSetup:
     """Flow around a sphere: the case and what the drag coefficient needs."""
     case: A.LbmCase

@@ -777,6 +777,8 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
                 d.obUnCum = d.obRhoCum ? d.obRhoCum + m : nullptr;
                 if (m) ck(cudaMemsetAsync(d.obRhoCum, 0, 2 * m * sizeof(float), s), "memset");
                 d.trackOpen = c->track_open_boundaries ? 1 : 0;
+                d.obImpedance = c->open_bc_scheme == LBM_OPEN_IMPEDANCE ? 1 : 0;
+                d.obTolerance = c->rho_reflection_tolerance;
                 d.obChunk = own(upload(chunks, s));
                 d.obCounter = m ? own(devAlloc<int>(2)) : nullptr;
                 if (m) ck(cudaMemsetAsync(d.obCounter, 0, 2 * sizeof(int), s), "memset");

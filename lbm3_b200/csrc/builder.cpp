@@ -174,6 +174,10 @@ void validateCase(const lbm_case& c) {
     if (c.storage != LBM_STORE_F32 && c.storage != LBM_STORE_F16 && c.storage != LBM_STORE_BF16 &&
         c.storage != LBM_STORE_F64)
         throw std::runtime_error("unknown storage precision");
+    if (c.open_bc_scheme != LBM_OPEN_CHARACTERISTIC && c.open_bc_scheme != LBM_OPEN_IMPEDANCE)
+        throw std::runtime_error("unknown open-boundary scheme");
+    if (c.open_bc_scheme == LBM_OPEN_IMPEDANCE && !(c.rho_reflection_tolerance >= 0.f))
+        throw std::runtime_error("RHO_REFLECTION_TOLERANCE must be non-negative");
     if (c.body_count < 0 || c.body_count > LBM_MAX_BODIES)
         throw std::runtime_error("body_count must be in [0, LBM_MAX_BODIES]");
     for (int b = 0; b < c.body_count; ++b) {

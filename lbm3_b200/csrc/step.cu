@@ -1050,6 +1050,24 @@ __global__ void __launch_bounds__(kBlock) interfaceExchange(DevLevel C, DevLevel
 // Characteristic (non-reflective) normal velocity of a face cell: the
 // outgoing Riemann invariant of the streamed state against the reference
 // values (include/updateGrid.h:268-308).
+// Non-reflecting density of the impedance scheme from the previous completed
+// boundary state (dRhoPrev, uNormalPrev) and the streamed partial density
+// sum dRhoZ: the root of the characteristic quadratic in dRho, written as
+// H / (B + sqrt(B^2 + D H)) so that it stays well conditioned
+// (cases/nonReflectiveTest/updateGrid_SCHLAFFER_IMPEDANCE_SCHEME.h:268-280).
+template <class V>
+__device__ __forceinline__ V impedanceDRho(V dRhoPrev, V uNormalPrev, V dRhoZ) {
+    const V cs = V(0.57735026918962576f);  // INVSQRT3 of the FP32 build
+    const V cs2 = cs * cs;
+    const V bracket = uNormalPrev + cs + V(1);
+    const V t = uNormalPrev - dRhoZ;
+    const V Dq = fma(bracket, bracket, cs2);
+    const V B = fma(bracket, cs + t, -cs2 * dRhoPrev);
+    const V H = fma(-t, V(2) * cs + t, V(2) * cs2 * dRhoPrev);
+    const V disc = fma(Dq, H, B * B);
+    return H / (B + sqrt(disc));
+}
+
 template <class V>
 __device__ __forceinline__ V nonReflectiveUNormal(V uTarget, V dRhoZ, V dRhoRef) {
     const V cs = V(0.57735026918962576);  // 1/sqrt(3)
@@ -1148,14 +1166,32 @@ __device__ __forceinline__ void openClose(const DevLevel& g, const MbbcDirT<Real
         c.f[d] += weightT<V>(d);  // the closure is ill-conditioned on shifted populations
     }
     V dRho = c.target.x, ux = c.target.y, uy = c.target.z, uz = c.target.w;
-    const bool nonReflective = info & 4;
+    // face cells only (the host clears the flag on edges and corners)
+    const bool nonReflective = (info & 4) && !g.obImpedance;
+    // impedance scheme: clamp the given value to within the tolerance of the
+    // non-reflecting state of the previous completed boundary state, which
+    // the reference arrays hold under this scheme
+    const bool impedance = (info & 4) && g.obImpedance && g.obTolerance < 1.f;
+    const V tol = V(g.obTolerance);
+    const V dRhoNR = impedance ? impedanceDRho<V>(V(c.dRhoRef), V(c.uNormalRef), dRhoZ) : V(0);
     if ((info & 3) == 2) {  // pressure: density given, velocity restored
         if (nonReflective) {
             const V uNormal = nonReflectiveUNormal<V>(c.uNormalRef, dRhoZ, dRho);
             dRho = (dRhoZ - uNormal) / (V(1) + uNormal);
         }
+        if (impedance) dRho = fmin(fmax(dRho, dRhoNR - tol), dRhoNR + tol);
         mbbcRestoreU(T, dRho + V(1), c.f, ux, uy, uz);
     } else if ((info & 3) == 1) {  // velocity: velocity given, density restored
+        if (impedance) {
+            const V uMin = (dRhoZ - dRhoNR - tol) / (dRhoNR + V(1) + tol);
+            const V uMax = (dRhoZ - dRhoNR + tol) / (dRhoNR + V(1) - tol);
+            if (nx > 0) ux = fmin(fmax(ux, uMin), uMax);
+            if (nx < 0) ux = fmin(fmax(ux, -uMax), -uMin);
+            if (ny > 0) uy = fmin(fmax(uy, uMin), uMax);
+            if (ny < 0) uy = fmin(fmax(uy, -uMax), -uMin);
+            if (nz > 0) uz = fmin(fmax(uz, uMin), uMax);
+            if (nz < 0) uz = fmin(fmax(uz, -uMax), -uMin);
+        }
         if (nonReflective) {
             V uTarget = V(0);
             if (nx != 0) uTarget = nx > 0 ? ux : -ux;
@@ -1192,15 +1228,21 @@ __device__ __forceinline__ void openClose(const DevLevel& g, const MbbcDirT<Real
     // iteration count; below 1e-5 the weight is tripled and the update runs
     // every 3^k iterations instead (include/updateGrid.h:325-347)
     const float uNormal = float(V(nx) * ux + V(ny) * uy + V(nz) * uz);
-    float alpha = c.beta / ((float)iterationsFinished + c.beta + 10.f);
-    int updateEvery = 1;
-    while (alpha < 1.e-5f) {
-        alpha *= 3.f;
-        updateEvery *= 3;
-    }
-    if (iterationsFinished % updateEvery == 0) {
-        g.obRhoRef[c.idx] = fmaf(alpha, float(dRho) - c.dRhoRef, c.dRhoRef);
-        g.obUnRef[c.idx] = fmaf(alpha, uNormal - c.uNormalRef, c.uNormalRef);
+    if (g.obImpedance) {
+        // the completed state, for the next step's non-reflecting state
+        g.obRhoRef[c.idx] = float(dRho);
+        g.obUnRef[c.idx] = uNormal;
+    } else {
+        float alpha = c.beta / ((float)iterationsFinished + c.beta + 10.f);
+        int updateEvery = 1;
+        while (alpha < 1.e-5f) {
+            alpha *= 3.f;
+            updateEvery *= 3;
+        }
+        if (iterationsFinished % updateEvery == 0) {
+            g.obRhoRef[c.idx] = fmaf(alpha, float(dRho) - c.dRhoRef, c.dRhoRef);
+            g.obUnRef[c.idx] = fmaf(alpha, uNormal - c.uNormalRef, c.uNormalRef);
+        }
     }
     if (g.trackOpen && (info & 512)) {
         g.obRhoCum[c.idx] += float(dRho);

@@ -82,6 +82,8 @@ struct DevLevel {
     float* obUnCum;                // uNormalCumulativeArray
     int obCount;
     int trackOpen;
+    int obImpedance;               // LBM_OPEN_IMPEDANCE scheme for non-reflective cells
+    float obTolerance;             // its RHO_REFLECTION_TOLERANCE
     // cells are grouped by outer normal; each chunk {first, count, normal row,
     // unknown-direction mask} is one CTA of the boundary kernel
     const int4* obChunk;

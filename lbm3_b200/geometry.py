@@ -148,15 +148,16 @@ def cylinder(radius: float, z0: float, z1: float, center=(0.0, 0.0), segments: i
     return np.array([np.concatenate(t) for t in np.array(tris, dtype=np.float64)], dtype=np.float32)
 
 
-def bored_block(half: float, radius: float, z0: float, z1: float, center=(0.0, 0.0), segments: int = 128) -> np.ndarray:
+def bored_block(half: float, radius: float, z0: float, z1: float, center=(0.0, 0.0), segments: int = 128,
+                phase_deg: float = 0.0) -> np.ndarray:
     """Closed solid: the square prism |x|, |y| <= half (about `center`) along z
-    with a cylindrical bore of `radius`, i.e. the fixed outer wall of a
-    Taylor-Couette cell.  `segments` must be a multiple of 8 so that the
-    square's corners are vertices of the outer polygon."""
-    if segments % 8:
-        raise ValueError("segments must be a multiple of 8")
+    with a cylindrical bore of `radius` whose `segments` polygon vertices sit
+    at phase_deg + 360 q / segments degrees (the fixed outer wall of a
+    Taylor-Couette cell, or a pipe in a square block).  The outer boundary
+    follows each bore vertex's ray out to the square, with the square's
+    corners inserted where they fall between two rays."""
     cx, cy = float(center[0]), float(center[1])
-    a = np.linspace(0.0, 2.0 * np.pi, segments, endpoint=False)
+    a = np.radians(phase_deg) + np.linspace(0.0, 2.0 * np.pi, segments, endpoint=False)
     c, s = np.cos(a), np.sin(a)
     inner = np.stack([cx + radius * c, cy + radius * s], axis=1)
     scale = half / np.maximum(np.abs(c), np.abs(s))   # ray from the axis to the square
@@ -164,12 +165,25 @@ def bored_block(half: float, radius: float, z0: float, z1: float, center=(0.0, 0
     tris = []
     for q in range(segments):
         r = (q + 1) % segments
-        i0, i1, o0, o1 = inner[q], inner[r], outer[q], outer[r]
-        # bore (normal towards the axis), outer sides, end caps (annular strips)
+        i0, i1 = inner[q], inner[r]
+        # outer path from ray q to ray q+1: a square corner strictly between
+        # the two rays is a vertex of it
+        path = [outer[q]]
+        a0, a1 = a[q], a[q] + 2.0 * np.pi / segments
+        for k in range(-1, 9):
+            ac = np.pi / 4.0 + k * np.pi / 2.0
+            if a0 + 1e-12 < ac < a1 - 1e-12:
+                path.append(np.array([cx + half * np.sign(np.cos(ac)), cy + half * np.sign(np.sin(ac))]))
+        path.append(outer[r])
+        # bore (normal towards the axis)
         tris += [((*i0, z0), (*i1, z1), (*i1, z0)), ((*i0, z0), (*i0, z1), (*i1, z1))]
-        tris += [((*o0, z0), (*o1, z0), (*o1, z1)), ((*o0, z0), (*o1, z1), (*o0, z1))]
-        tris += [((*i0, z0), (*i1, z0), (*o1, z0)), ((*i0, z0), (*o1, z0), (*o0, z0))]
-        tris += [((*i0, z1), (*o1, z1), (*i1, z1)), ((*i0, z1), (*o0, z1), (*o1, z1))]
+        for o0, o1 in zip(path[:-1], path[1:]):
+            # outer sides
+            tris += [((*o0, z0), (*o1, z0), (*o1, z1)), ((*o0, z0), (*o1, z1), (*o0, z1))]
+        # end caps: the strip between the bore edge and the outer path, fanned from i0
+        tris += [((*i0, z0), (*i1, z0), (*path[-1], z0)), ((*i0, z1), (*path[-1], z1), (*i1, z1))]
+        for o0, o1 in zip(path[:-1], path[1:]):
+            tris += [((*i0, z0), (*o1, z0), (*o0, z0)), ((*i0, z1), (*o0, z1), (*o1, z1))]
     return np.array([np.concatenate(t) for t in np.array(tris, dtype=np.float64)], dtype=np.float32)
 
 

@@ -57,7 +57,7 @@ class OGrid(C.Structure):
         ("linkLength", C.POINTER(C.c_uint)), ("wallVel", C.POINTER(C.c_float)),
         ("wallForce", C.POINTER(C.c_float)), ("trackWallForce", C.c_int),
         ("face", FaceBC * 6), ("openCount", C.c_int), ("openIndex", _IP),
-        ("openRef", C.POINTER(C.c_float)), ("openCum", C.POINTER(C.c_float)), ("trackOpen", C.c_int),
+        ("openRef", C.POINTER(C.c_float)), ("openCum", C.POINTER(C.c_float)), ("trackOpen", C.c_int), ("openImpedance", C.c_int), ("openTolerance", C.c_float),
         ("rotorCount", C.c_int), ("rotors", C.c_void_p), ("trackRotorForce", C.c_int),
         ("openHook", C.c_void_p), ("hookUser", C.c_void_p),
     ]

@@ -1176,6 +1176,8 @@ static void init_info(const lbm_case* c, ogrid* g) {
     g->useIBB = c->use_ibb;
     g->trackWallForce = c->track_wall_force;
     g->trackOpen = c->track_open_boundaries;
+    g->openImpedance = c->open_bc_scheme == LBM_OPEN_IMPEDANCE;
+    g->openTolerance = c->rho_reflection_tolerance;
     g->trackRotorForce = c->track_rotor_force;
     memcpy(g->face, c->face, sizeof(g->face));
     g->openHook = c->open_bc_hook;
@@ -1386,6 +1388,42 @@ static void open_boundary(ogrid* g) {
         if (abs(on[0]) + abs(on[1]) + abs(on[2]) != 1) bc.nonReflective = 0;
         const float cs = 0.57735026918962576f;
         const int code = (on[0] + 5) * 100 + (on[1] + 5) * 10 + (on[2] + 5);
+        /* the impedance scheme (cases/nonReflectiveTest/
+         * updateGrid_SCHLAFFER_IMPEDANCE_SCHEME.h:250-310): the reference
+         * arrays hold the previous completed boundary state; the given density
+         * or normal velocity is clamped to within the tolerance of the
+         * non-reflecting state computed from it */
+        const int impedance = g->openImpedance && bc.nonReflective && g->openTolerance < 1.f;
+        const float tol = g->openTolerance;
+        float dRhoNR = 0.f;
+        if (g->openImpedance) {
+            if (impedance) {
+                const float cs2 = cs * cs;
+                const float bracket = uNormalRef + cs + 1.f;
+                const float t = uNormalRef - dRhoZ;
+                const float Dq = fmaf(bracket, bracket, cs2);
+                const float B = fmaf(bracket, cs + t, -cs2 * dRhoRef);
+                const float H = fmaf(-t, 2.f * cs + t, 2.f * cs2 * dRhoRef);
+                const float disc = fmaf(Dq, H, B * B);
+                dRhoNR = H / (B + sqrtf(disc));
+            }
+            bc.nonReflective = 0;
+        }
+        if (bc.dirichletRho && impedance) {
+            if (bc.dRho < dRhoNR - tol) bc.dRho = dRhoNR - tol;
+            if (bc.dRho > dRhoNR + tol) bc.dRho = dRhoNR + tol;
+        }
+        if (bc.dirichletU && impedance) {
+            const float uMin = (dRhoZ - dRhoNR - tol) / (dRhoNR + 1.f + tol);
+            const float uMax = (dRhoZ - dRhoNR + tol) / (dRhoNR + 1.f - tol);
+            float* comp[3] = {&bc.ux, &bc.uy, &bc.uz};
+            for (int a = 0; a < 3; ++a) {
+                if (on[a] == 0) continue;
+                const float lo = on[a] > 0 ? uMin : -uMax, hi = on[a] > 0 ? uMax : -uMin;
+                if (*comp[a] < lo) *comp[a] = lo;
+                if (*comp[a] > hi) *comp[a] = hi;
+            }
+        }
         if (bc.dirichletRho) {
             if (bc.nonReflective) {
                 const float dRhoTarget = bc.dRho;
@@ -1434,13 +1472,18 @@ static void open_boundary(ogrid* g) {
             g->f[(size_t)(g->flip ? INV[d] : d) * n + nb[pre_nbr(d)]] = f[d];
         }
         const float uNormal = (float)on[0] * bc.ux + (float)on[1] * bc.uy + (float)on[2] * bc.uz;
-        const float beta = bc.nonReflectiveBeta;
-        float alpha = beta / (g->iterationsFinished + beta + 10.f);
-        int updateEvery = 1;
-        while (alpha < 1.e-5f) { alpha *= 3.f; updateEvery *= 3; }
-        if (g->iterationsFinished % updateEvery == 0) {
-            g->openRef[q] = fmaf(alpha, bc.dRho - dRhoRef, dRhoRef);
-            g->openRef[m + q] = fmaf(alpha, uNormal - uNormalRef, uNormalRef);
+        if (g->openImpedance) {
+            g->openRef[q] = bc.dRho;  /* the completed state */
+            g->openRef[m + q] = uNormal;
+        } else {
+            const float beta = bc.nonReflectiveBeta;
+            float alpha = beta / (g->iterationsFinished + beta + 10.f);
+            int updateEvery = 1;
+            while (alpha < 1.e-5f) { alpha *= 3.f; updateEvery *= 3; }
+            if (g->iterationsFinished % updateEvery == 0) {
+                g->openRef[q] = fmaf(alpha, bc.dRho - dRhoRef, dRhoRef);
+                g->openRef[m + q] = fmaf(alpha, uNormal - uNormalRef, uNormalRef);
+            }
         }
         if (!g->trackOpen || !trackFlow) continue;
         g->openCum[q] += bc.dRho;

@@ -82,6 +82,8 @@ typedef struct ogrid {
     float* openRef;                  /* [2][openCount] dRhoRef, uNormalRef */
     float* openCum;                  /* [2][openCount] dRho, uNormal sums */
     int trackOpen;
+    int openImpedance;       /* LBM_OPEN_IMPEDANCE for non-reflective face cells */
+    float openTolerance;     /* its RHO_REFLECTION_TOLERANCE */
     /* forcing rotors (RotorStruct), set with oracle_set_rotor */
     int rotorCount;
     void* rotors;                    /* orotor[4], private to lbm_oracle.c */

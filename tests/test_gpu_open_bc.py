@@ -102,3 +102,25 @@ def test_open_channel_low_precision_storage(storage):
         ma, mb = a.macro(), b.macro()
     tol = 2e-3 if storage == A.LBM_STORE_F16 else 2e-2
     assert rel_l2(mb[1:4].reshape(-1), ma[1:4].reshape(-1)) < tol
+
+
+@pytest.mark.parametrize("tolerance", [2e-5, 2e-3])
+@pytest.mark.parametrize("steps", [1, 30])
+def test_impedance_scheme_matches_oracle(tolerance, steps):
+    """The impedance open-boundary scheme (non-reflective velocity inlet and
+    pressure outlet clamped to within the density tolerance of the
+    non-reflecting state): fields, and the reference arrays, which under this
+    scheme hold the previous completed boundary state."""
+    c = L.open_channel(32, 16, 12, u_in=0.04, nu_lattice=0.02, inlet_non_reflective=True)
+    c.open_bc_scheme = A.LBM_OPEN_IMPEDANCE
+    c.rho_reflection_tolerance = tolerance
+    p, o, g = _perturbed(c, seed=11)
+    with g:
+        g.update_all_grids(steps)
+        o.step(steps)
+        e_rho, e_u, d_rho = density_velocity_errors(g.macro(), o.macro())
+        assert e_rho < FIELD_REL_L2 and e_u < FIELD_REL_L2 and d_rho < 1e-6, (e_rho, e_u, d_rho)
+        ref_g, ref_o = g.open_reference(), o.open_reference()
+        assert np.abs(ref_g[0] - ref_o[0]).max() < 1e-6
+        assert rel_l2(ref_g[1], ref_o[1]) < FIELD_REL_L2
+    o.close()

@@ -72,6 +72,9 @@ def test_plan_reports_storage_footprint():
     (lambda c: setattr(c.face[0], "kind", 7), A.LBM_ERR_BUILD),
     (lambda c: setattr(c, "res_global", 0.0), A.LBM_ERR_BUILD),
     (lambda c: setattr(c, "storage", 9), A.LBM_ERR_BUILD),
+    (lambda c: setattr(c, "open_bc_scheme", 2), A.LBM_ERR_BUILD),
+    (lambda c: (setattr(c, "open_bc_scheme", A.LBM_OPEN_IMPEDANCE),
+                setattr(c, "rho_reflection_tolerance", -1e-5)), A.LBM_ERR_BUILD),
 ])
 def test_plan_rejects_invalid_cases(mutate, code):
     c = L.tgv_plain_method().case
