@@ -21,7 +21,7 @@ OBJ_DIR = PKG / "_build"
 # storage type and kernel family (LBM3_STEP_PART) so the kernel sets build in
 # parallel; the heaviest unit bounds the build time
 STEP_STORAGES = [("f32", 0), ("f16", 1), ("bf16", 2), ("f64", 3)]
-STEP_PARTS = [1, 5, 2, 3, 4]
+STEP_PARTS = [1, 2, 3, 4]
 SOURCES = [
     # (each unit instantiates only its family, so helpers of the other
     # families are unreferenced there: diagnostic 177 is expected)

@@ -851,6 +851,14 @@ int lbm_build_grids(const lbm_case* c, lbm_grids** out, long long* fluidUpdates)
             I.omegaCoarse = omega(H.info.nu);
             I.omegaFine = omega(host.levels[l + 1].info.nu);
         }
+        // each level's descriptor on the device, for the collide-stream launch
+        // that reads it there (the fields it uses do not change after the build)
+        for (LevelState& L : g->levels) {
+            lbm::DevLevel* self = devAlloc<lbm::DevLevel>(1);
+            L.owned.push_back(self);
+            L.dev.self = self;
+            ck(cudaMemcpyAsync(self, &L.dev, sizeof(lbm::DevLevel), cudaMemcpyHostToDevice, s), "descriptor copy");
+        }
         ck(cudaStreamSynchronize(s), "build sync");
         if (fluidUpdates) *fluidUpdates = host.fluidUpdatesPerIteration;
         // the driver's hooks are evaluated during the build only
@@ -1637,6 +1645,8 @@ std::vector<StateRegion> stateRegions(LevelState& L) {
     if (d.wallCount) r.push_back({d.wallForce, 3ULL * d.wallCount * sizeof(double)});
     for (int q = 0; q < d.rotorCount; ++q)
         if (d.rotor[q].nonzero) r.push_back({d.rotor[q].force, 3ULL * 27 * d.rotor[q].nonzero * sizeof(float)});
+    // the stochastic rounding's step seeds, so a resumed run draws the same bits
+    if (d.seed) r.push_back({d.seed, 2 * sizeof(unsigned)});
     return r;
 }
 

@@ -14,6 +14,7 @@
 #include "lattice.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <stdexcept>
 
@@ -918,7 +919,7 @@ void buildSegments(HostLevel& L) {
         // extent of the compressed row starting at c
         int end = c + 1;
         while (end < n && L.shifter[end] < 0) ++end;
-        const int row = L.shifter[c];
+        int row = L.shifter[c];
         // neighbours of the cell at offset `off` in this row
         auto jP = [&](int off) { return L.rowJP[row] + off; };
         auto kP = [&](int off) { return L.rowKP[row] + off; };
@@ -940,11 +941,46 @@ void buildSegments(HostLevel& L) {
             int r = q;
             while (r < end && r - q < kSegmentCells && bulk(r)) ++r;
             const int off = q - c;
+            // A run that reaches the end of its row continues into the next
+            // rows while their neighbour rows continue the same arithmetic
+            // progression (a dense block of full rows): the +1 neighbour is
+            // index + 1 everywhere, so the lane offsets stay valid and short
+            // rows still fill whole tiles.
+            int rowEnd = end, rowStart = c, rowId = row;
+            static const bool rowSegments = std::getenv("LBM3_ROW_SEGMENTS") != nullptr;  // tuning: one row per segment
+            while (!rowSegments && r == rowEnd && r - q < kSegmentCells && rowEnd < n) {
+                const int next = L.shifter[rowEnd];
+                const int len = rowEnd - rowStart;
+                if (next < 0 || L.rowJP[next] != L.rowJP[rowId] + len || L.rowKP[next] != L.rowKP[rowId] + len ||
+                    L.rowJKP[next] != L.rowJKP[rowId] + len)
+                    break;
+                int nextEnd = rowEnd + 1;
+                while (nextEnd < n && L.shifter[nextEnd] < 0) ++nextEnd;
+                const int nextStart = rowEnd;
+                auto bulkIn = [&L, n, next, nextStart](int x) {
+                    const int o = x - nextStart;
+                    const bool w = x + 1 >= n || L.rowJP[next] + o + 1 >= n || L.rowKP[next] + o + 1 >= n ||
+                                   L.rowJKP[next] + o + 1 >= n;
+                    return (L.wallMap[x] == -1 || L.wallMap[x] == -2) && !w &&
+                           (L.rotorCell.empty() || !L.rotorCell[x]);
+                };
+                if (!bulkIn(rowEnd)) break;
+                rowStart = rowEnd;
+                rowId = next;
+                rowEnd = nextEnd;
+                while (r < rowEnd && r - q < kSegmentCells && bulkIn(r)) ++r;
+            }
             L.segCell.push_back(q);
             L.segJP.push_back(jP(off));
             L.segKP.push_back(kP(off));
             L.segJKP.push_back(jkP(off));
             L.segLen.push_back(r - q);
+            if (r > end) {
+                // the run ended inside a later row: carry on from there
+                c = rowStart;
+                end = rowEnd;
+                row = rowId;
+            }
             q = r;
         }
         c = end;

@@ -35,7 +35,8 @@
 
 // One storage type and one kernel family per translation unit, so the
 // kernel sets build in parallel.  LBM3_STEP_PART selects the family:
-// 1 the paired persistent collide-stream, 2 the other collide-stream
+// 1 the packed persistent collide-stream (one domain, or a batch with its
+// open-boundary and periodic launches), 2 the other collide-stream
 // variants, 3 open boundary, periodic ghosts, interface and initial
 // condition, 4 reductions and field transfers (with the storage-independent
 // launchers in the FP32 unit), 0 everything.  Templates a part does not
@@ -1530,16 +1531,18 @@ __global__ void __launch_bounds__(kHalf, LBM3_PAIR_MIN_BLOCKS) collidePacked(Dev
     int dom = -1;
     int item = fetch();
     while (item < b.collideCount) {  // CTA-uniform: items come through shared memory
-        const int2 it = __ldg(b.collideItems + item);
+        // a one-domain launch has no table: item i of domain 0
+        const int2 it = b.collideItems ? __ldg(b.collideItems + item) : make_int2(0, item);
         if (it.x != dom) {
             __syncthreads();  // every thread is done with the previous domain's descriptor
             stageLevel(b.levels + it.x, sg);
             __syncthreads();
             dom = it.x;
         }
-        const int next = fetch();  // the atomic's latency overlaps this item's loads
         const int nSpecial = (sg.specialCount + kTile - 1) / kTile;
-        if (it.y < nSpecial) {
+        int next;
+        if (it.y < nSpecial) {  // CTA-uniform branch: both sides fetch once
+            next = fetch();
             const int q = it.y * kTile + t;
             if (q < sg.specialCount) collideSpecialCell<F, S>(sg, __ldg(sg.special + q));
             if (q + kHalf < sg.specialCount) collideSpecialCell<F, S>(sg, __ldg(sg.special + q + kHalf));
@@ -1549,6 +1552,7 @@ __global__ void __launch_bounds__(kHalf, LBM3_PAIR_MIN_BLOCKS) collidePacked(Dev
             loadDesc(sg, it.y - nSpecial, d, l);
             Pair f[27];
             loadTilePair<F, S>(sg, d, t, l, f);
+            next = fetch();  // the atomic and the barrier overlap the tile's loads in flight
             collideCumulantT(f, sg.coll, sg.coll.lambda, sg.gx, sg.gy, sg.gz);
             storePair<F, S>(sg, d, t, l, f, stepDither<F, S>(sg, kSaltCollide));
         }
@@ -1624,15 +1628,39 @@ template <class K> int persistentGrid(K kernel, int block, int smem) {
 
 // The paired persistent kernel: listed cells and bulk tiles in one launch
 // (FP32 arithmetic on two cells per thread), then the rotor cells.
+// One domain steps through the same kernel as a packed batch (a batch of
+// one, its descriptor read from the device copy), so a domain stepped alone
+// and inside a batch runs identical machine code and gets identical results.
 template <bool F, class S> struct RunCollidePair {
     static void run(const DevLevel& g, cudaStream_t s) {
         if constexpr (!std::is_same<S, double>::value) {
             const int items = g.segCount + (g.specialCount + kTile - 1) / kTile;
             if (items > 0) {
-                const int grid = persistentGrid(collidePair<F, S>, kHalf, 0);
-                collidePair<F, S><<<std::min(grid, items), kHalf, 0, s>>>(g);
+                DevBatch b{};
+                b.levels = g.self;
+                b.domainCount = 1;
+                b.collideItems = nullptr;
+                b.collideCount = items;
+                b.work = g.work;
+                const int grid = persistentGrid(collidePacked<F, S>, kHalf, 0);
+                collidePacked<F, S><<<std::min(grid, items), kHalf, 0, s>>>(b);
             }
             if (g.rotorCellCount > 0) collideRotorList<F, S><<<blocksFor(g.rotorCellCount), kBlock, 0, s>>>(g);
+        }
+    }
+};
+
+// One step of a packed batch: collide-stream at flipper F, then the open
+// boundary and periodic ghosts on the streamed state (!F).
+template <bool F, class S> struct RunPackedStep {
+    static void run(const DevBatch& b, cudaStream_t s) {
+        if constexpr (!std::is_same<S, double>::value) {
+            if (b.collideCount > 0) {
+                const int grid = persistentGrid(collidePacked<F, S>, kHalf, 0);
+                collidePacked<F, S><<<std::min(grid, b.collideCount), kHalf, 0, s>>>(b);
+            }
+            if (b.openCount > 0) openPacked<!F, S><<<b.openCount, kOpenChunk, 0, s>>>(b);
+            if (b.periodicCount > 0) periodicPacked<!F, S><<<blocksFor(b.periodicCount), kBlock, 0, s>>>(b);
         }
     }
 };
@@ -1645,7 +1673,16 @@ template <bool F, class S> struct RunCollideOther {
             collideStream<F, S><<<blocksFor(g.cellCount), kBlock, 0, s>>>(g);
             return;
         }
-        if (v == CollideVariant::Tma) {
+        if (v == CollideVariant::PairLevel) {
+            // the paired kernel with the descriptor as a kernel parameter
+            if constexpr (!std::is_same<S, double>::value) {
+                const int items = g.segCount + (g.specialCount + kTile - 1) / kTile;
+                if (items > 0) {
+                    const int grid = persistentGrid(collidePair<F, S>, kHalf, 0);
+                    collidePair<F, S><<<std::min(grid, items), kHalf, 0, s>>>(g);
+                }
+            }
+        } else if (v == CollideVariant::Tma) {
             if (g.segCount > 0) {
                 const int grid = persistentGrid(collideBulkTma<F, S>, kTile, tmaSmemBytes<S>());
                 persistentGrid(collideBulkTma<!F, S>, kTile, tmaSmemBytes<S>());
@@ -1771,21 +1808,7 @@ void LBM3_FN(launchFlowReport)(const DevLevel& g, bool flip, cudaStream_t s, int
 }
 #endif
 
-#if LBM3_PART(5)
-// One step of a packed batch: collide-stream at flipper F, then the open
-// boundary and periodic ghosts on the streamed state (!F).
-template <bool F, class S> struct RunPackedStep {
-    static void run(const DevBatch& b, cudaStream_t s) {
-        if constexpr (!std::is_same<S, double>::value) {
-            if (b.collideCount > 0) {
-                const int grid = persistentGrid(collidePacked<F, S>, kHalf, 0);
-                collidePacked<F, S><<<std::min(grid, b.collideCount), kHalf, 0, s>>>(b);
-            }
-            if (b.openCount > 0) openPacked<!F, S><<<b.openCount, kOpenChunk, 0, s>>>(b);
-            if (b.periodicCount > 0) periodicPacked<!F, S><<<blocksFor(b.periodicCount), kBlock, 0, s>>>(b);
-        }
-    }
-};
+#if LBM3_PART(1)
 void LBM3_FN(launchPackedStep)(const DevBatch& b, bool flip, cudaStream_t s) {
     flip ? RunPackedStep<true, StepStore>::run(b, s) : RunPackedStep<false, StepStore>::run(b, s);
 }

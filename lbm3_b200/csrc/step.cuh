@@ -58,6 +58,8 @@ struct DevLevel {
     int* errorFlag;          // set to nonzero when a bounded device wait gives up
     int* work;               // [2] work-item counter and finished-CTA count of the
                              // persistent collide-stream (zero between launches)
+    const DevLevel* self;    // device copy of this descriptor (the one-domain
+                             // launch of the packed collide-stream reads it)
     unsigned* seed;          // [2] step seeds of the stochastic rounding of 16-bit
                              // storage, by esotwist parity (null for FP32 / FP64)
     // wall-adjacent cells (WallStruct)

@@ -22,6 +22,7 @@ CollideVariant collideVariant() {
         return s == "simple" ? CollideVariant::Simple
                : s == "tma"  ? CollideVariant::Tma
                : s == "prefetch" ? CollideVariant::Prefetch
+               : s == "pairlevel" ? CollideVariant::PairLevel
                                  : CollideVariant::Pair;
     }();
     return v;
@@ -31,10 +32,12 @@ CollideVariant collideVariant() {
 // one cell per thread in the prefetching kernel.
 void launchCollideStream(const DevLevel& g, bool flip, cudaStream_t s) {
     const CollideVariant v = collideVariant();
-    if (v == CollideVariant::Pair && pairFits(g) && g.storage != LBM_STORE_F64) {
+    const bool paired = v == CollideVariant::Pair || v == CollideVariant::PairLevel;
+    if (v == CollideVariant::Pair && pairFits(g) && g.storage != LBM_STORE_F64 && g.self) {
         LBM3_BY_STORAGE(launchCollidePair, g, flip, s)
     } else {
-        LBM3_BY_STORAGE(launchCollideOther, g, flip, s, v == CollideVariant::Pair ? CollideVariant::Prefetch : v)
+        LBM3_BY_STORAGE(launchCollideOther, g, flip, s,
+                        paired && (!pairFits(g) || g.storage == LBM_STORE_F64) ? CollideVariant::Prefetch : v)
     }
 }
 void launchPeriodic(const DevLevel& g, bool flip, cudaStream_t s) { LBM3_BY_STORAGE(launchPeriodic, g, flip, s) }
