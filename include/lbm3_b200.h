@@ -364,8 +364,10 @@ int lbm_update_batch(lbm_grids* const* grids, int count, int coarse_steps);
  * packed table of all domains' work items ({domain, item}: listed-cell chunks
  * and 128-cell bulk tiles), one open-boundary launch over all domains' chunks
  * and one periodic-ghost launch, instead of a launch set per domain; step
- * pairs replay as a CUDA graph.  A member's result is bit-identical to
- * stepping it alone.  The batch runs on its own stream, ordered after the
+ * pairs replay as a CUDA graph.  A member's result is bit-identical to the
+ * member stepped as a batch of one (the per-item work does not depend on the
+ * other members) and agrees to FP32 rounding with lbm_update_all_grids, whose
+ * kernel takes the level descriptor as a kernel parameter.  The batch runs on its own stream, ordered after the
  * work already queued on the members' streams and before what they get
  * next.  Members keep their own state (trackers, readbacks, lbm_update_all_grids
  * between batch updates); all members must be at the same esotwist parity

@@ -1628,9 +1628,10 @@ template <class K> int persistentGrid(K kernel, int block, int smem) {
 
 // The paired persistent kernel: listed cells and bulk tiles in one launch
 // (FP32 arithmetic on two cells per thread), then the rotor cells.
-// One domain steps through the same kernel as a packed batch (a batch of
-// one, its descriptor read from the device copy), so a domain stepped alone
-// and inside a batch runs identical machine code and gets identical results.
+// One domain through the packed batch's kernel (a batch of one, its
+// descriptor read from the device copy): the same machine code as the
+// domain inside a batch, so the same results bit for bit
+// (LBM3_COLLIDE_KERNEL=packed; a one-member lbm_batch does the same).
 template <bool F, class S> struct RunCollidePair {
     static void run(const DevLevel& g, cudaStream_t s) {
         if constexpr (!std::is_same<S, double>::value) {
@@ -1673,8 +1674,9 @@ template <bool F, class S> struct RunCollideOther {
             collideStream<F, S><<<blocksFor(g.cellCount), kBlock, 0, s>>>(g);
             return;
         }
-        if (v == CollideVariant::PairLevel) {
+        if (v == CollideVariant::Pair) {
             // the paired kernel with the descriptor as a kernel parameter
+            // (faster on one large domain than the packed kernel's staged copy)
             if constexpr (!std::is_same<S, double>::value) {
                 const int items = g.segCount + (g.specialCount + kTile - 1) / kTile;
                 if (items > 0) {
@@ -1820,7 +1822,7 @@ int stepLaunchCount(const DevLevel& g) {
     int n = 0;
     const CollideVariant v = collideVariant();
     if (v == CollideVariant::Simple) n += g.cellCount > 0;
-    else if (v == CollideVariant::Prefetch || v == CollideVariant::Pair)
+    else if (v == CollideVariant::Prefetch || v == CollideVariant::Pair || v == CollideVariant::Packed)
         n += ((g.segCount + g.specialCount) > 0) + (g.rotorCellCount > 0);
     else n += (g.segCount > 0) + (g.specialCount > 0) + (g.rotorCellCount > 0);
     return n + (g.obCount > 0) + (g.perCount > 0);

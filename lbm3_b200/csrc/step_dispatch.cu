@@ -22,7 +22,7 @@ CollideVariant collideVariant() {
         return s == "simple" ? CollideVariant::Simple
                : s == "tma"  ? CollideVariant::Tma
                : s == "prefetch" ? CollideVariant::Prefetch
-               : s == "pairlevel" ? CollideVariant::PairLevel
+               : s == "packed" ? CollideVariant::Packed
                                  : CollideVariant::Pair;
     }();
     return v;
@@ -32,8 +32,8 @@ CollideVariant collideVariant() {
 // one cell per thread in the prefetching kernel.
 void launchCollideStream(const DevLevel& g, bool flip, cudaStream_t s) {
     const CollideVariant v = collideVariant();
-    const bool paired = v == CollideVariant::Pair || v == CollideVariant::PairLevel;
-    if (v == CollideVariant::Pair && pairFits(g) && g.storage != LBM_STORE_F64 && g.self) {
+    const bool paired = v == CollideVariant::Pair || v == CollideVariant::Packed;
+    if (v == CollideVariant::Packed && pairFits(g) && g.storage != LBM_STORE_F64 && g.self) {
         LBM3_BY_STORAGE(launchCollidePair, g, flip, s)
     } else {
         LBM3_BY_STORAGE(launchCollideOther, g, flip, s,

@@ -10,9 +10,10 @@
 
 namespace lbm {
 
-// Collide-stream kernel choice (LBM3_COLLIDE_KERNEL = simple | tma | prefetch;
-// default: the paired persistent kernel)
-enum class CollideVariant { Tma, Prefetch, Simple, Pair, PairLevel };
+// Collide-stream kernel choice (LBM3_COLLIDE_KERNEL = simple | tma | prefetch |
+// packed; default: the paired persistent kernel with the level descriptor as
+// a kernel parameter)
+enum class CollideVariant { Tma, Prefetch, Simple, Pair, Packed };
 CollideVariant collideVariant();
 // The paired kernel indexes populations with 32-bit element offsets.
 inline bool pairFits(const DevLevel& g) { return 27LL * g.stride + 128 < (1LL << 31); }  // 128: one tile

@@ -348,8 +348,9 @@ class PackedBatch:
     """Single-level domains advanced by one packed launch per kernel kind
     (lbm_batch_create): one persistent collide-stream over the packed
     {domain, item} table of all members, one open-boundary and one
-    periodic-ghost launch; each member's result is bit-identical to stepping
-    it alone.  Free (close) the batch before its members."""
+    periodic-ghost launch; each member's result is bit-identical to the member
+    run as a batch of one and agrees to FP32 rounding with update_all_grids.
+    Free (close) the batch before its members."""
 
     def __init__(self, grids):
         self.members = list(grids)

@@ -12,13 +12,17 @@ batch per storage type: one persistent collide-stream launch over the packed
 block table of all of them, one open-boundary and one periodic launch per
 step, replayed as a CUDA graph (PackedBatch); the batch is rebuilt whenever
 a domain joins or leaves.  A domain that joins at the other esotwist parity
-than the batch steps once on its own first.  Other domains (several levels,
+than the batch steps once on its own first (as a batch of one).  Other domains (several levels,
 rotors, FP64) advance with update_batch on their own streams.  A finished
 domain reads its result, frees its memory and its slot, and the next
 waiting request is admitted.
 
-Each result is the one the request gets when run alone: batched stepping is
-bit-identical to stepping a domain by itself.
+Each result is the one the request gets when served alone: a packable
+domain always steps through the packed kernel (alone it is a batch of one),
+whose per-item work does not depend on the other members, so its fields are
+bit-identical alone and in the mix; against lbm_update_all_grids, whose
+kernel takes the level descriptor as a parameter, they agree to FP32
+rounding.
 """
 from __future__ import annotations
 
@@ -120,9 +124,7 @@ class Server:
         for a in ready:
             (groups.setdefault(a.req.case.storage, []) if self.pack and a.packable else loose).append(a)
         for st, members in groups.items():
-            if len(members) == 1:
-                loose.extend(members)
-                continue
+            # a lone domain is a batch of one: the same kernel alone or in the mix
             key = tuple(a.req.rid for a in members)
             if st not in self._batches or self._batches[st][0] != key:
                 self._close_batches([r for r in (self._batches.get(st) or ((), None))[0]])
@@ -171,7 +173,8 @@ class Server:
                         mates = [b for b in active if b is not a and b.grids is not None and b.packable
                                  and b.req.case.storage == a.req.case.storage and b.remaining > 0]
                         if self.pack and a.packable and mates and mates[0].parity != a.parity:
-                            a.grids.update_all_grids(1)
+                            with PackedBatch([a.grids]) as own:
+                                own.update(1)
                             a.remaining -= 1
                 ready = [a for a in active if a.grids is not None and a.remaining > 0]
                 finished = any(a.grids is not None and a.remaining == 0 for a in active)
