@@ -361,8 +361,10 @@ int lbm_update_batch(lbm_grids* const* grids, int count, int coarse_steps);
 
 /* Packed batch: single-level domains (without rotors, of one storage type,
  * FP32, FP16 or BF16) advanced by ONE persistent collide-stream launch over a
- * packed table of all domains' work items ({domain, item}: listed-cell chunks
- * and 128-cell bulk tiles), one open-boundary launch over all domains' chunks
+ * packed table of all domains' work items (per domain its listed-cell chunks
+ * and 128-cell bulk tiles, with an item counter each: a CTA works through its
+ * home domain, then helps the others), one open-boundary launch over all
+ * domains' chunks
  * and one periodic-ghost launch, instead of a launch set per domain; step
  * pairs replay as a CUDA graph.  A member's result is bit-identical to the
  * member stepped as a batch of one (the per-item work does not depend on the
@@ -379,7 +381,7 @@ typedef struct lbm_batch lbm_batch;
 typedef struct lbm_batch_info {
     int domain_count;
     long long cells;          /* sum of the members' cells (ghosts included) */
-    int collide_items;        /* rows of the packed collide-stream table      */
+    int collide_items;        /* collide-stream work items of all members     */
     int open_chunks;          /* open-boundary CTAs per step                  */
     int periodic_cells;       /* periodic ghost cells per step                */
     int launches_per_step;    /* kernels one packed step launches (<= 3)      */

@@ -943,14 +943,15 @@ int lbm_batch_create(lbm_grids* const* grids, int count, lbm_batch** out) {
         }
         // packed tables: every member's items, member by member
         std::vector<lbm::DevLevel> levels;
-        std::vector<int2> collide, open;
+        std::vector<int2> open;
+        std::vector<int> itemStart{0};
         std::vector<int> perStart{0};
         long long cells = 0;
         for (int q = 0; q < count; ++q) {
             const lbm::DevLevel& d = b->members[q]->levels[0].dev;
             levels.push_back(d);
             const int items = d.segCount + (d.specialCount + 127) / 128;
-            for (int i = 0; i < items; ++i) collide.push_back(make_int2(q, i));
+            itemStart.push_back(itemStart.back() + items);
             for (int i = 0; i < d.obChunkCount; ++i) open.push_back(make_int2(q, i));
             perStart.push_back(perStart.back() + d.perCount);
             cells += d.cellCount;
@@ -964,10 +965,10 @@ int lbm_batch_create(lbm_grids* const* grids, int count, lbm_batch** out) {
         lbm::DevBatch& D = b->dev;
         D.levels = own(upload(levels, b->stream));
         D.domainCount = count;
-        D.collideItems = own(upload(collide, b->stream));
-        D.collideCount = static_cast<int>(collide.size());
-        D.work = own(devAlloc<int>(2));
-        ck(cudaMemsetAsync(D.work, 0, 2 * sizeof(int), b->stream), "memset");
+        D.itemStart = own(upload(itemStart, b->stream));
+        D.collideCount = itemStart.back();
+        D.work = own(devAlloc<int>(count + 1));
+        ck(cudaMemsetAsync(D.work, 0, (count + 1) * sizeof(int), b->stream), "memset");
         D.openItems = open.empty() ? nullptr : own(upload(open, b->stream));
         D.openCount = static_cast<int>(open.size());
         D.periodicStart = own(upload(perStart, b->stream));

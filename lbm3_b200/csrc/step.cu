@@ -1521,48 +1521,51 @@ __global__ void __launch_bounds__(kHalf, LBM3_PAIR_MIN_BLOCKS) collidePacked(Dev
             }
     }
     int parity = 0;
-    auto fetch = [&]() {
-        if (t == 0) slot[parity] = atomicAdd(b.work, 1);
+    auto fetch = [&](int domain) {
+        if (t == 0) slot[parity] = atomicAdd(b.work + domain, 1);
         __syncthreads();
         const int v = slot[parity];
         parity ^= 1;
         return v;
     };
-    int dom = -1;
-    int item = fetch();
-    while (item < b.collideCount) {  // CTA-uniform: items come through shared memory
-        // a one-domain launch has no table: item i of domain 0
-        const int2 it = b.collideItems ? __ldg(b.collideItems + item) : make_int2(0, item);
-        if (it.x != dom) {
-            __syncthreads();  // every thread is done with the previous domain's descriptor
-            stageLevel(b.levels + it.x, sg);
-            __syncthreads();
-            dom = it.x;
-        }
+    // Each domain has its own item counter.  A CTA starts on its home domain
+    // (blockIdx modulo the domain count) and moves on to the next domain when
+    // that one runs out, so it stages a descriptor at most once per domain.
+    const int D = b.domainCount;
+    int dom = static_cast<int>(blockIdx.x % unsigned(D));
+    for (int visited = 0; visited < D; ++visited, dom = dom + 1 == D ? 0 : dom + 1) {
+        const int count = b.itemStart ? __ldg(b.itemStart + dom + 1) - __ldg(b.itemStart + dom) : b.collideCount;
+        if (count <= 0) continue;
+        int item = fetch(dom);
+        if (item >= count) continue;  // CTA-uniform
+        __syncthreads();              // every thread is done with the previous descriptor
+        stageLevel(b.levels + dom, sg);
+        __syncthreads();
         const int nSpecial = (sg.specialCount + kTile - 1) / kTile;
-        int next;
-        if (it.y < nSpecial) {  // CTA-uniform branch: both sides fetch once
-            next = fetch();
-            const int q = it.y * kTile + t;
-            if (q < sg.specialCount) collideSpecialCell<F, S>(sg, __ldg(sg.special + q));
-            if (q + kHalf < sg.specialCount) collideSpecialCell<F, S>(sg, __ldg(sg.special + q + kHalf));
-        } else {
-            int4 d;
-            int l;
-            loadDesc(sg, it.y - nSpecial, d, l);
-            Pair f[27];
-            loadTilePair<F, S>(sg, d, t, l, f);
-            next = fetch();  // the atomic and the barrier overlap the tile's loads in flight
-            collideCumulantT(f, sg.coll, sg.coll.lambda, sg.gx, sg.gy, sg.gz);
-            storePair<F, S>(sg, d, t, l, f, stepDither<F, S>(sg, kSaltCollide));
+        while (item < count) {  // CTA-uniform: items come through shared memory
+            int next;
+            if (item < nSpecial) {  // CTA-uniform branch: both sides fetch once
+                next = fetch(dom);
+                const int q = item * kTile + t;
+                if (q < sg.specialCount) collideSpecialCell<F, S>(sg, __ldg(sg.special + q));
+                if (q + kHalf < sg.specialCount) collideSpecialCell<F, S>(sg, __ldg(sg.special + q + kHalf));
+            } else {
+                int4 d;
+                int l;
+                loadDesc(sg, item - nSpecial, d, l);
+                Pair f[27];
+                loadTilePair<F, S>(sg, d, t, l, f);
+                next = fetch(dom);  // the atomic and the barrier overlap the tile's loads in flight
+                collideCumulantT(f, sg.coll, sg.coll.lambda, sg.gx, sg.gy, sg.gz);
+                storePair<F, S>(sg, d, t, l, f, stepDither<F, S>(sg, kSaltCollide));
+            }
+            item = next;
         }
-        item = next;
     }
     if (t == 0) {
         __threadfence();
-        if (atomicAdd(b.work + 1, 1) == int(gridDim.x) - 1) {
-            b.work[0] = 0;
-            b.work[1] = 0;
+        if (atomicAdd(b.work + D, 1) == int(gridDim.x) - 1) {
+            for (int q = 0; q <= D; ++q) b.work[q] = 0;
             __threadfence();
         }
     }
@@ -1640,7 +1643,7 @@ template <bool F, class S> struct RunCollidePair {
                 DevBatch b{};
                 b.levels = g.self;
                 b.domainCount = 1;
-                b.collideItems = nullptr;
+                b.itemStart = nullptr;
                 b.collideCount = items;
                 b.work = g.work;
                 const int grid = persistentGrid(collidePacked<F, S>, kHalf, 0);

@@ -110,10 +110,12 @@ struct DevLevel {
 struct DevBatch {
     const DevLevel* levels;    // [domainCount] device copies
     int domainCount;
-    const int2* collideItems;  // {domain, item}: items of the paired collide-stream
-                               // (listed-cell chunks first, then bulk tiles), by domain
+    const int* itemStart;      // [domainCount + 1] prefix sums of the domains' collide-stream
+                               // items (listed-cell chunks first, then bulk tiles); null:
+                               // one domain with collideCount items
     int collideCount;
-    int* work;                 // [2] item counter and finished-CTA count (zero between launches)
+    int* work;                 // [domainCount + 1] per-domain item counters, then the
+                               // finished-CTA count (zero between launches)
     const int2* openItems;     // {domain, chunk} of the open-boundary kernel
     int openCount;
     const int* periodicStart;  // [domainCount + 1] prefix sums of the ghost counts
