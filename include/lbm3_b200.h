@@ -517,9 +517,12 @@ int lbm_rotor_force(lbm_grids* g, int rotor, int reset, double* out);
  * mostly rotor volume are left out.  out = {area-averaged normal velocity
  * [m/s], mass flow [kg/s], momentum thrust [N], area-averaged pressure [Pa],
  * pressure power [W], normal kinetic power [W], fluid area [mm^2]}; sums in
- * FP64 on the device.  A cut outside the grid is LBM_ERR_INVALID.
- * Replaces getFlowReportXY/ZY/ZX (include/flowReportFunctions.h:11-373) for a
- * single-level grid. */
+ * FP64 on the device.  A cut outside the grid is LBM_ERR_INVALID.  With
+ * several levels the cut is the finest level's layer and the report is taken
+ * on a section image at the finest level whose pixel count fits 16,000,000,
+ * filled level by level (finer levels overwrite coarser ones; a coarser level
+ * whose layers bracket the cut blends the two); areas are that level's pixels.
+ * Replaces getFlowReportXY/ZY/ZX (include/flowReportFunctions.h:11-373). */
 int lbm_flow_report(lbm_grids* g, int plane, float cut, const float* bounds, double* out);
 
 /* Write every cell of every level to a legacy ASCII VTK file (POLYDATA, one

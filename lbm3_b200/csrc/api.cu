@@ -173,6 +173,9 @@ unsigned long long levelBytes(const lbm::HostLevel& H, int storage) {
     const size_t n = static_cast<size_t>(H.info.cellCount);
     ull b = 27ULL * planeStride(static_cast<long long>(n), storage) * storageBytes(storage) + 256;  // populations
     b += bytes(2, sizeof(int));                                     // work counter
+    b += bytes(1, sizeof(lbm::DevLevel));                           // device copy of the descriptor
+    if (storage == LBM_STORE_F16 || storage == LBM_STORE_BF16)
+        b += bytes(2, sizeof(unsigned));                            // stochastic-rounding seeds
     b += bytes(n, sizeof(int)) * 2;                                 // shifter, wallMap
     b += bytes(H.rowI.size(), sizeof(int)) * 6;                     // compressed rows
     b += bytes(H.perIndex.size(), sizeof(int)) * 2;                 // periodic index, source
@@ -491,6 +494,96 @@ void batchCheckParity(const lbm_batch* b) {
         if (g->levels[0].info.esotwistFlipper != flip)
             throw std::invalid_argument(
                 "members are at different esotwist parities (step the odd ones once on their own)");
+}
+
+}  // namespace
+
+namespace {
+
+// Flow report of a domain with several levels (getFlowReportGeneral,
+// include/flowReportFunctions.h:11-352): a section image at the finest level
+// whose pixel count fits FLOW_REPORT_PIXEL_LIMIT, filled level by level (a
+// finer level overwrites a coarser one; a coarser level's cut between two
+// layers blends them), then summed over its fluid pixels.
+int flowReportLevels(lbm_grids* g, int plane, float cut, const float* bounds, double* out) {
+    constexpr long long kPixelLimit = 16000000;  // FLOW_REPORT_PIXEL_LIMIT
+    const int levels = static_cast<int>(g->levels.size());
+    const lbm::Info& fin = g->levels[levels - 1].info;
+    const int n[3] = {fin.nx, fin.ny, fin.nz};
+    const float o[3] = {fin.ox, fin.oy, fin.oz};
+    const int axis = plane == LBM_PLANE_XY ? 2 : plane == LBM_PLANE_ZY ? 0 : 1;
+    // getIJKCellIndexFromXYZ on the finest level (include/flowReportFunctions.h:355-372)
+    const int cutIndex = static_cast<int>((cut - o[axis]) / fin.res + 0.5f);
+    if (cutIndex < 0 || cutIndex >= n[axis]) return fail(LBM_ERR_INVALID, "lbm_flow_report: cut outside the grid");
+    const double cutPosition = double(o[axis]) + double(cutIndex) * fin.res;
+    int lo[3] = {0, 0, 0}, hi[3] = {n[0], n[1], n[2]};
+    if (bounds && (bounds[0] != 0.f || bounds[1] != 0.f || bounds[2] != 0.f || bounds[3] != 0.f ||
+                   bounds[4] != 0.f || bounds[5] != 0.f))
+        for (int a = 0; a < 3; ++a) {
+            const float tMin = o[a] - 0.5f * fin.res;
+            const float tMax = o[a] + fin.res * (n[a] - 0.5f);
+            lo[a] = std::max(0, static_cast<int>(std::ceil((bounds[a] - tMin) / fin.res)));
+            hi[a] = std::min(n[a], n[a] - static_cast<int>(std::ceil((tMax - bounds[a + 3]) / fin.res)));
+        }
+    const int hAxis = plane == LBM_PLANE_XY ? 0 : 2, vAxis = plane == LBM_PLANE_ZX ? 0 : 1;
+    int pixelsH = hi[hAxis] - lo[hAxis], pixelsV = hi[vAxis] - lo[vAxis];
+    int startH = lo[hAxis], startV = lo[vAxis];
+    int imageLevel = levels - 1;
+    long long pixels = (long long)pixelsH * pixelsV;
+    while (pixels > kPixelLimit && imageLevel > 0) {
+        --imageLevel;
+        pixelsH /= 2; startH /= 2;
+        pixelsV /= 2; startV /= 2;
+        pixels = (long long)pixelsH * pixelsV;
+    }
+    if (pixelsH <= 0 || pixelsV <= 0 || pixels > kPixelLimit)
+        return fail(LBM_ERR_INVALID, "lbm_flow_report: empty crop or image above the pixel limit");
+    return guarded("lbm_flow_report", [&] {
+        float* img = devAlloc<float>(3 * size_t(pixels));
+        struct Free { float* p; ~Free() { cudaFree(p); } } keep{img};
+        lbm::launchFlowImageClear(img, pixels, g->stream);
+        for (int l = 0; l < levels; ++l) {
+            LevelState& L = g->levels[l];
+            const lbm::Info& in = L.info;
+            const int count = plane == LBM_PLANE_XY ? in.nz : plane == LBM_PLANE_ZY ? in.nx : in.ny;
+            if (in.cellCount <= 0 || count <= 0) continue;
+            const double origin = plane == LBM_PLANE_XY ? in.oz : plane == LBM_PLANE_ZY ? in.ox : in.oy;
+            const double index = std::clamp((cutPosition - origin) / double(in.res), 0.0, double(count - 1));
+            lbm::FlowImagePass a{};
+            a.plane = plane;
+            a.lowerNormal = static_cast<int>(std::floor(index));
+            a.alpha = static_cast<float>(index - a.lowerNormal);
+            a.interpolate = a.alpha > 0.f;
+            a.downsample = l > imageLevel ? 1 << (l - imageLevel) : 1;
+            a.upsample = l < imageLevel ? 1 << (imageLevel - l) : 1;
+            a.startH = startH;
+            a.startV = startV;
+            a.pixelsH = pixelsH;
+            a.pixelsV = pixelsV;
+            lbm::launchFlowImage(L.dev, in.esotwistFlipper, g->stream, a, img);
+        }
+        ck(cudaMemsetAsync(g->scratch, 0, 6 * sizeof(double), g->stream), "memset");
+        lbm::launchFlowImageSum(img, pixels, g->stream, g->scratch);
+        ck(cudaGetLastError(), "flow report launch");
+        double t[6];
+        ck(cudaMemcpyAsync(t, g->scratch, sizeof(t), cudaMemcpyDeviceToHost, g->stream), "copy");
+        ck(cudaStreamSynchronize(g->stream), "sync");
+        for (int q = 0; q < 7; ++q) out[q] = 0.0;
+        if (t[5] == 0.0) return;
+        // unit conversion with the pixel size of the image level
+        // (include/flowReportFunctions.h:322-351)
+        const lbm::Info& in = g->levels[imageLevel].info;
+        const double px = double(in.res) / 1000.0, area = px * px, vs = px / double(in.dtPhys);
+        const double ps = double(g->c.rho_phys) * vs * vs / 3.0;
+        const double mfs = double(g->c.rho_phys) * area * vs;
+        out[0] = t[0] / t[5] * vs;
+        out[1] = (t[0] + t[1]) * mfs;
+        out[2] = t[2] * mfs * vs;
+        out[3] = t[3] / t[5] * ps;
+        out[4] = t[1] * area * ps * vs;
+        out[5] = t[4] * mfs * vs * vs;
+        out[6] = t[5] * double(in.res) * in.res;
+    });
 }
 
 }  // namespace
@@ -1581,7 +1674,7 @@ int lbm_export_vtk(lbm_grids* g, const char* filename) {
 
 int lbm_flow_report(lbm_grids* g, int plane, float cut, const float* bounds, double* out) {
     if (!g || !out || plane < 0 || plane > 2) return fail(LBM_ERR_INVALID, "lbm_flow_report: bad argument");
-    if (g->levels.size() != 1) return fail(LBM_ERR_UNSUPPORTED, "lbm_flow_report: single-level grids only");
+    if (g->levels.size() != 1) return flowReportLevels(g, plane, cut, bounds, out);
     LevelState& L = g->levels[0];
     const lbm::Info& in = L.info;
     const int n[3] = {in.nx, in.ny, in.nz};

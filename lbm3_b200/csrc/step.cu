@@ -237,6 +237,84 @@ __device__ __forceinline__ float rotorFractionAt(const DevRotor& R, float x, flo
     return (v0 + zw * (v1 - v0)) * 0.125f;
 }
 
+// Solid fraction of all rotors at (x, y, z), clamped to [0, 1].
+__device__ __forceinline__ float rotorMarkerAt(const DevLevel& g, float x, float y, float z) {
+    float m = 0.f;
+    for (int r = 0; r < g.rotorCount; ++r) m += rotorFractionAt(g.rotor[r], x, y, z);
+    return fminf(fmaxf(m, 0.f), 1.f);
+}
+
+// One level's cells written into the section image img[3][pixelsV][pixelsH]
+// (dRho, normal velocity, solid marker); finer levels run later and
+// overwrite (include/flowReportFunctions.h:133-262).
+template <bool F, class S>
+__global__ void __launch_bounds__(kBlock) flowImageLevel(DevLevel g, FlowImagePass a, float* img) {
+    const int cell = blockIdx.x * kBlock + threadIdx.x;
+    if (cell >= g.cellCount) return;
+    int nb[8], ijk[3];
+    decodeNbr(g, cell, nb, ijk);
+    const int normal = a.plane == LBM_PLANE_XY ? ijk[2] : a.plane == LBM_PLANE_ZY ? ijk[0] : ijk[1];
+    if (normal != a.lowerNormal) return;
+    const int ch = a.plane == LBM_PLANE_XY ? ijk[0] : ijk[2];
+    const int cv = a.plane == LBM_PLANE_ZX ? ijk[0] : ijk[1];
+    if (ch % a.downsample != 0 || cv % a.downsample != 0) return;
+    const int ih = (ch / a.downsample) * a.upsample, iv = (cv / a.downsample) * a.upsample;
+    if (ih + a.upsample <= a.startH || ih >= a.startH + a.pixelsH) return;
+    if (iv + a.upsample <= a.startV || iv >= a.startV + a.pixelsV) return;
+    // the next layer along the normal: an actual adjacent centre, or no sample
+    int upper = cell, nu[8], uijk[3];
+    if (a.interpolate) {
+        upper = a.plane == LBM_PLANE_XY ? nb[4] : a.plane == LBM_PLANE_ZY ? nb[1] : nb[2];
+        if (upper < 0 || upper >= g.cellCount) return;
+        decodeNbr(g, upper, nu, uijk);
+        if (uijk[0] != ijk[0] + (a.plane == LBM_PLANE_ZY) || uijk[1] != ijk[1] + (a.plane == LBM_PLANE_ZX) ||
+            uijk[2] != ijk[2] + (a.plane == LBM_PLANE_XY))
+            return;
+    } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) nu[q] = nb[q];
+    }
+    const bool lowerSolid = __ldg(g.wallMap + cell) == -3, upperSolid = __ldg(g.wallMap + upper) == -3;
+    const bool solid = a.alpha <= 0.5f ? lowerSolid : upperSolid;
+    float marker = solid ? 1.f : 0.f;
+    float dRho = 0.f, ux = 0.f, uy = 0.f, uz = 0.f;
+    if (!solid) {
+        const bool blend = a.interpolate && !lowerSolid && !upperSolid;
+        float f[27];
+        if (lowerSolid) readPre<F, S>(g, nu, f);
+        else readPre<F, S>(g, nb, f);
+        macroFromF(f, dRho, ux, uy, uz);
+        marker = rotorMarkerAt(g, ijk[0] * g.res + g.ox, ijk[1] * g.res + g.oy, ijk[2] * g.res + g.oz);
+        if (blend) {
+            readPre<F, S>(g, nu, f);
+            float dU, xU, yU, zU;
+            macroFromF(f, dU, xU, yU, zU);
+            dRho += a.alpha * (dU - dRho);
+            ux += a.alpha * (xU - ux);
+            uy += a.alpha * (yU - uy);
+            uz += a.alpha * (zU - uz);
+            const int pi = ijk[0] + (a.plane == LBM_PLANE_ZY), pj = ijk[1] + (a.plane == LBM_PLANE_ZX),
+                      pk = ijk[2] + (a.plane == LBM_PLANE_XY);
+            const float mU = rotorMarkerAt(g, pi * g.res + g.ox, pj * g.res + g.oy, pk * g.res + g.oz);
+            marker += a.alpha * (mU - marker);
+        }
+    }
+    const float un = a.plane == LBM_PLANE_XY ? uz : a.plane == LBM_PLANE_ZY ? ux : uy;
+    const long long plane = (long long)a.pixelsH * a.pixelsV;
+    for (int sv = 0; sv < a.upsample; ++sv) {
+        const int y = iv + sv - a.startV;
+        if (y < 0 || y >= a.pixelsV) continue;
+        for (int sh = 0; sh < a.upsample; ++sh) {
+            const int x = ih + sh - a.startH;
+            if (x < 0 || x >= a.pixelsH) continue;
+            const long long p = (long long)y * a.pixelsH + x;
+            img[p] = dRho;
+            img[plane + p] = un;
+            img[2 * plane + p] = marker;
+        }
+    }
+}
+
 // Section-plane flow sums (getFlowReportGeneral, include/flowReportFunctions.h:11-352)
 // on one level: cells of layer `layer` along the plane normal inside the
 // in-plane index ranges [h0, h1) x [v0, v1); walls and pixels that are at
@@ -811,6 +889,47 @@ __global__ void __launch_bounds__(kHalf, LBM3_PAIR_MIN_BLOCKS) collidePair(DevLe
 }
 
 #if LBM3_SHARED_UNIT
+// Section image cleared to solid (marker 1, values 0).
+__global__ void __launch_bounds__(kBlock) flowImageClear(float* img, long long pixels) {
+    const long long p = blockIdx.x * (long long)kBlock + threadIdx.x;
+    if (p >= pixels) return;
+    img[p] = 0.f;
+    img[pixels + p] = 0.f;
+    img[2 * pixels + p] = 1.f;
+}
+
+// Flow sums over the fluid pixels of a section image
+// (include/flowReportFunctions.h:263-318): {u, dRho u, (1+dRho) u |u|, dRho,
+// (1+dRho) u^3 / 2, pixels}, each pixel's terms in FP32, summed in FP64.
+__global__ void __launch_bounds__(kBlock) flowImageSum(const float* img, long long pixels, double* out) {
+    const long long p = blockIdx.x * (long long)kBlock + threadIdx.x;
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    if (p < pixels && img[2 * pixels + p] < 0.5f) {
+        const float dRho = img[p], u = img[pixels + p];
+        const float rhoU = fmaf(dRho, u, u);
+        v[0] = u;
+        v[1] = dRho * u;
+        v[2] = rhoU * fabsf(u);
+        v[3] = dRho;
+        v[4] = 0.5f * rhoU * u * u;
+        v[5] = 1.0;
+    }
+    __shared__ double part[6][kBlock / 32];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        double x = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0) part[q][threadIdx.x >> 5] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double x = 0.0;
+        for (int k = 0; k < kBlock / 32; ++k) x += part[threadIdx.x][k];
+        atomicAdd(out + threadIdx.x, x);
+    }
+}
+
 // FP64 force and torque about the origin of the cells of one wall ID
 // (updateTracker wall branch, include/trackerFunctions.h:386-428).
 __global__ void __launch_bounds__(kBlock) wallForceSum(DevLevel g, int wallID, double* out) {
@@ -1740,6 +1859,11 @@ template <bool F, class S> struct RunFlowReport {
         flowReportSum<F, S><<<blocksFor(g.cellCount), kBlock, 0, s>>>(g, plane, layer, h0, h1, v0, v1, out);
     }
 };
+template <bool F, class S> struct RunFlowImage {
+    static void run(const DevLevel& g, cudaStream_t s, const FlowImagePass& a, float* img) {
+        flowImageLevel<F, S><<<blocksFor(g.cellCount), kBlock, 0, s>>>(g, a, img);
+    }
+};
 template <bool F, class S> struct RunInit {
     static void run(const DevLevel& g, cudaStream_t s, const float4* macro, float4 u) {
         initFeq<F, S><<<blocksFor(g.cellCount), kBlock, 0, s>>>(g, macro, u);
@@ -1807,6 +1931,9 @@ void LBM3_FN(launchGlobalSums)(const DevLevel& g, bool flip, cudaStream_t s, dou
 }
 void LBM3_FN(launchGatherF)(const DevLevel& g, cudaStream_t s, float* out) { dispatch<RunGather>(g, false, s, out); }
 void LBM3_FN(launchScatterF)(const DevLevel& g, cudaStream_t s, const float* in) { dispatch<RunScatter>(g, false, s, in); }
+void LBM3_FN(launchFlowImage)(const DevLevel& g, bool flip, cudaStream_t s, const FlowImagePass& a, float* img) {
+    dispatch<RunFlowImage>(g, flip, s, a, img);
+}
 void LBM3_FN(launchFlowReport)(const DevLevel& g, bool flip, cudaStream_t s, int plane, int layer, int h0, int h1,
                                int v0, int v1, double* out) {
     dispatch<RunFlowReport>(g, flip, s, plane, layer, h0, h1, v0, v1, out);
@@ -1842,6 +1969,12 @@ void launchOpenFlow(const DevLevel& g, int openBCID, float invSpan, cudaStream_t
 void launchCollideBatch(float* f, int n, const CollisionConsts& P, float gx, float gy, float gz,
                         cudaStream_t s) {
     collideBatch<<<blocksFor(n), kBlock, 0, s>>>(f, n, P, gx, gy, gz);
+}
+void launchFlowImageClear(float* img, long long pixels, cudaStream_t s) {
+    flowImageClear<<<blocksFor(pixels), kBlock, 0, s>>>(img, pixels);
+}
+void launchFlowImageSum(const float* img, long long pixels, cudaStream_t s, double* out) {
+    flowImageSum<<<blocksFor(pixels), kBlock, 0, s>>>(img, pixels, out);
 }
 #endif
 

@@ -122,6 +122,18 @@ struct DevBatch {
     int periodicCount;
 };
 
+// One level's pass over the section image of a flow report
+// (getFlowReportGeneral, include/flowReportFunctions.h:96-262): the cells of
+// layer `lowerNormal` (blended with the next layer by `alpha` when
+// `interpolate`), sampled every `downsample` cells in plane and written over
+// upsample x upsample pixels of the image of pixelsH x pixelsV starting at
+// (startH, startV) in image-level cell units.
+struct FlowImagePass {
+    int plane, lowerNormal, interpolate;
+    float alpha;
+    int downsample, upsample, startH, startV, pixelsH, pixelsV;
+};
+
 // Interface lists between a coarse level and the next finer one
 // (InterfaceStruct, include/types.h:198-200) and the two levels' omega1.
 struct DevInterface {

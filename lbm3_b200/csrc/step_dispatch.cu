@@ -69,6 +69,10 @@ void launchFlowReport(const DevLevel& g, bool flip, cudaStream_t s, int plane, i
     LBM3_BY_STORAGE(launchFlowReport, g, flip, s, plane, layer, h0, h1, v0, v1, out)
 }
 
+void launchFlowImage(const DevLevel& g, bool flip, cudaStream_t s, const FlowImagePass& a, float* img) {
+    LBM3_BY_STORAGE(launchFlowImage, g, flip, s, a, img)
+}
+
 void launchPackedStep(const DevBatch& b, int storage, bool flip, cudaStream_t s) {
     switch (storage) {
         case LBM_STORE_F16: launchPackedStepF16(b, flip, s); break;

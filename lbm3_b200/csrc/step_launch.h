@@ -44,6 +44,11 @@ void launchRotorForce(const DevRotor& R, const int* index, cudaStream_t s, doubl
 void launchOpenFlow(const DevLevel& g, int openBCID, float invSpan, cudaStream_t s, double* out);
 void launchCollideBatch(float* f, int n, const CollisionConsts& P, float gx, float gy, float gz,
                         cudaStream_t s);
+// Section image of a flow report over several levels: clear, one pass per
+// level (finer levels later), then the sums over the fluid pixels.
+void launchFlowImageClear(float* img, long long pixels, cudaStream_t s);
+void launchFlowImage(const DevLevel& g, bool flip, cudaStream_t s, const FlowImagePass& a, float* img);
+void launchFlowImageSum(const float* img, long long pixels, cudaStream_t s, double* out);
 // One step of a packed batch of single-level domains of one storage type
 // (FP32, FP16 or BF16), all at esotwist flipper `flip`.
 void launchPackedStep(const DevBatch& b, int storage, bool flip, cudaStream_t s);
@@ -65,7 +70,8 @@ void launchPackedStep(const DevBatch& b, int storage, bool flip, cudaStream_t s)
     void launchScatterF##SUF(const DevLevel& g, cudaStream_t s, const float* in);                              \
     void launchFlowReport##SUF(const DevLevel& g, bool flip, cudaStream_t s, int plane, int layer, int h0,     \
                                int h1, int v0, int v1, double* out);                                           \
-    void launchPackedStep##SUF(const DevBatch& b, bool flip, cudaStream_t s);
+    void launchPackedStep##SUF(const DevBatch& b, bool flip, cudaStream_t s);                                   \
+    void launchFlowImage##SUF(const DevLevel& g, bool flip, cudaStream_t s, const FlowImagePass& a, float* img);
 LBM3_DECLARE_STORAGE_LAUNCHERS(F32)
 LBM3_DECLARE_STORAGE_LAUNCHERS(F16)
 LBM3_DECLARE_STORAGE_LAUNCHERS(BF16)

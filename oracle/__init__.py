@@ -126,6 +126,9 @@ def lib() -> C.CDLL:
         h.oracle_mbbc_restore_u.argtypes = [C.c_int, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
         h.oracle_domain_build.argtypes = [C.c_void_p, C.POINTER(ODomain)]
         h.oracle_domain_build.restype = C.c_int
+        h.oracle_flow_image.argtypes = [C.POINTER(ODomain), C.c_int, C.c_float, C.POINTER(C.c_float),
+                                        C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        h.oracle_flow_image.restype = C.c_int
         h.oracle_domain_free.argtypes = [C.POINTER(ODomain)]
         h.oracle_domain_step.argtypes = [C.POINTER(ODomain), C.c_int]
         h.oracle_domain_kinetic_energy.argtypes = [C.POINTER(ODomain), C.c_float, C.c_float]
@@ -414,6 +417,16 @@ class OracleDomain:
 
     def kinetic_energy(self, u_ref_phys: float, domain_length: float) -> float:
         return lib().oracle_domain_kinetic_energy(C.byref(self.d), u_ref_phys, domain_length)
+
+    def flow_image(self, plane: int, cut: float, bounds=None):
+        """Raw section-image sums of every level and the image's level."""
+        out = (C.c_double * 6)()
+        lvl = C.c_int()
+        b = (C.c_float * 6)(*bounds) if bounds is not None else None
+        rc = lib().oracle_flow_image(C.byref(self.d), int(plane), float(cut), b, out, C.byref(lvl))
+        if rc != 0:
+            raise ValueError(f"oracle_flow_image failed with status {rc}")
+        return np.array(out[:]), lvl.value
 
     def macro(self, l: int = 0) -> np.ndarray:
         return self.levels[l].macro()

@@ -1735,6 +1735,134 @@ static float rotor_fraction(const orotor* R, float x, float y, float z) {
     return (v0 + zw * (v1 - v0)) * 0.125f;
 }
 
+/* Section image of getFlowReportGeneral over every level of a domain
+ * (include/flowReportFunctions.h:11-318); see oracle_flow_image in the header. */
+static float rotor_marker(const ogrid* g, float x, float y, float z) {
+    float m = 0.f;
+    for (int r = 0; r < g->rotorCount; ++r) m += rotor_fraction((const orotor*)g->rotors + r, x, y, z);
+    return m < 0.f ? 0.f : (m > 1.f ? 1.f : m);
+}
+
+static void read_macro(const ogrid* g, int cell, float m[4]) {
+    const size_t n = (size_t)g->cellCount;
+    int nb[8];
+    get_nbr(g, cell, nb);
+    float f[27];
+    for (int d = 0; d < 27; ++d) f[d] = g->f[(size_t)(g->flip ? INV[d] : d) * n + nb[pre_nbr(d)]];
+    oracle_get_drho_u(f, m);
+}
+
+int oracle_flow_image(const odomain* dom, int plane, float cut, const float* bounds, double* out, int* imageLevelOut) {
+    const long long limit = 16000000;
+    const int levels = dom->levelCount;
+    const ogrid* fin = &dom->level[levels - 1];
+    const int n[3] = {fin->nx, fin->ny, fin->nz};
+    const float o[3] = {fin->ox, fin->oy, fin->oz};
+    const int axis = plane == 0 ? 2 : (plane == 1 ? 0 : 1);
+    const int cutIndex = (int)((cut - o[axis]) / fin->res + 0.5f);
+    if (cutIndex < 0 || cutIndex >= n[axis]) return -1;
+    const double cutPosition = (double)o[axis] + (double)cutIndex * fin->res;
+    int lo[3] = {0, 0, 0}, hi[3] = {n[0], n[1], n[2]};
+    if (bounds && (bounds[0] != 0.f || bounds[1] != 0.f || bounds[2] != 0.f || bounds[3] != 0.f || bounds[4] != 0.f ||
+                   bounds[5] != 0.f))
+        for (int a = 0; a < 3; ++a) {
+            const float tMin = o[a] - 0.5f * fin->res, tMax = o[a] + fin->res * (n[a] - 0.5f);
+            const int l0 = (int)ceilf((bounds[a] - tMin) / fin->res);
+            const int h0 = n[a] - (int)ceilf((tMax - bounds[a + 3]) / fin->res);
+            lo[a] = l0 > 0 ? l0 : 0;
+            hi[a] = h0 < n[a] ? h0 : n[a];
+        }
+    const int hA = plane == 0 ? 0 : 2, vA = plane == 2 ? 0 : 1;
+    int pH = hi[hA] - lo[hA], pV = hi[vA] - lo[vA], sH = lo[hA], sV = lo[vA];
+    int imageLevel = levels - 1;
+    long long pixels = (long long)pH * pV;
+    while (pixels > limit && imageLevel > 0) {
+        --imageLevel;
+        pH /= 2; sH /= 2; pV /= 2; sV /= 2;
+        pixels = (long long)pH * pV;
+    }
+    if (pH <= 0 || pV <= 0 || pixels > limit) return -2;
+    float* img = (float*)malloc(3 * (size_t)pixels * sizeof(float));
+    if (!img) return -3;
+    for (long long p = 0; p < pixels; ++p) { img[p] = 0.f; img[pixels + p] = 0.f; img[2 * pixels + p] = 1.f; }
+    for (int l = 0; l < levels; ++l) {
+        const ogrid* g = &dom->level[l];
+        const int count = plane == 0 ? g->nz : (plane == 1 ? g->nx : g->ny);
+        if (g->cellCount <= 0 || count <= 0) continue;
+        const double origin = plane == 0 ? g->oz : (plane == 1 ? g->ox : g->oy);
+        double index = (cutPosition - origin) / (double)g->res;
+        if (index < 0.0) index = 0.0;
+        if (index > count - 1) index = count - 1;
+        const int lower = (int)floor(index);
+        const float alpha = (float)(index - lower);
+        const int interpolate = alpha > 0.f;
+        const int down = l > imageLevel ? 1 << (l - imageLevel) : 1, up = l < imageLevel ? 1 << (imageLevel - l) : 1;
+        for (int cell = 0; cell < g->cellCount; ++cell) {
+            int ci, cj, ck;
+            get_ijk(g, cell, &ci, &cj, &ck);
+            if ((plane == 0 ? ck : (plane == 1 ? ci : cj)) != lower) continue;
+            const int ch = plane == 0 ? ci : ck, cv = plane == 2 ? ci : cj;
+            if (ch % down || cv % down) continue;
+            const int ih = (ch / down) * up, iv = (cv / down) * up;
+            if (ih + up <= sH || ih >= sH + pH || iv + up <= sV || iv >= sV + pV) continue;
+            int upper = cell;
+            if (interpolate) {
+                int nb[8];
+                get_nbr(g, cell, nb);
+                upper = plane == 0 ? nb[4] : (plane == 1 ? nb[1] : nb[2]);
+                if (upper < 0 || upper >= g->cellCount) continue;
+                int ui, uj, uk;
+                get_ijk(g, upper, &ui, &uj, &uk);
+                if (ui != ci + (plane == 1) || uj != cj + (plane == 2) || uk != ck + (plane == 0)) continue;
+            }
+            const int lowerSolid = g->wallMap[cell] == -3, upperSolid = g->wallMap[upper] == -3;
+            const int solid = alpha <= 0.5f ? lowerSolid : upperSolid;
+            float marker = solid ? 1.f : 0.f, m[4] = {0.f, 0.f, 0.f, 0.f};
+            if (!solid) {
+                read_macro(g, lowerSolid ? upper : cell, m);
+                marker = rotor_marker(g, ci * g->res + g->ox, cj * g->res + g->oy, ck * g->res + g->oz);
+                if (interpolate && !lowerSolid && !upperSolid) {
+                    float mu[4];
+                    read_macro(g, upper, mu);
+                    for (int q = 0; q < 4; ++q) m[q] += alpha * (mu[q] - m[q]);
+                    const float mk = rotor_marker(g, (ci + (plane == 1)) * g->res + g->ox,
+                                                  (cj + (plane == 2)) * g->res + g->oy,
+                                                  (ck + (plane == 0)) * g->res + g->oz);
+                    marker += alpha * (mk - marker);
+                }
+            }
+            const float un = plane == 0 ? m[3] : (plane == 1 ? m[1] : m[2]);
+            for (int yv = 0; yv < up; ++yv) {
+                const int y = iv + yv - sV;
+                if (y < 0 || y >= pV) continue;
+                for (int xh = 0; xh < up; ++xh) {
+                    const int x = ih + xh - sH;
+                    if (x < 0 || x >= pH) continue;
+                    const long long p = (long long)y * pH + x;
+                    img[p] = m[0];
+                    img[pixels + p] = un;
+                    img[2 * pixels + p] = marker;
+                }
+            }
+        }
+    }
+    for (int q = 0; q < 6; ++q) out[q] = 0.0;
+    for (long long p = 0; p < pixels; ++p) {
+        if (!(img[2 * pixels + p] < 0.5f)) continue;
+        const float dRho = img[p], u = img[pixels + p];
+        const float rhoU = fmaf(dRho, u, u);
+        out[0] += u;
+        out[1] += dRho * u;
+        out[2] += rhoU * fabsf(u);
+        out[3] += dRho;
+        out[4] += 0.5f * rhoU * u * u;
+        out[5] += 1.0;
+    }
+    free(img);
+    *imageLevelOut = imageLevel;
+    return 0;
+}
+
 void oracle_flow_sums(const ogrid* g, int plane, int layer, int h0, int h1, int v0, int v1, double* out) {
     for (int q = 0; q < 6; ++q) out[q] = 0.0;
     const size_t n = (size_t)g->cellCount;

@@ -183,6 +183,16 @@ typedef struct odomain {
  * single-level case builds exactly as oracle_build.  Returns 0 or a negative
  * LBM_ERR_* code. */
 int oracle_domain_build(const lbm_case* c, odomain* d);
+
+/* getFlowReportGeneral over every level of a domain
+ * (include/flowReportFunctions.h:11-318): the finest level's layer nearest
+ * to `cut` (mm), a section image at the finest level within 16,000,000
+ * pixels (cropped to `bounds`, NULL or all zero: none), filled level by
+ * level (finer overwrite coarser, a coarser level whose layers bracket the
+ * cut blends them); out[6] as oracle_flow_sums over the fluid pixels and
+ * *imageLevel the image's level.  Returns 0, or < 0 for a cut outside the
+ * grid or an empty / oversized image. */
+int oracle_flow_image(const odomain* d, int plane, float cut, const float* bounds, double* out, int* imageLevel);
 void oracle_domain_free(odomain* d);
 /* updateAllGrids(grids, 0) `coarseSteps` times (include/updateGrid.h:388-396):
  * level L steps 2^L times per coarse step, each finer pair followed by

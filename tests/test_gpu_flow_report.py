@@ -71,3 +71,30 @@ def test_uniform_stream_through_a_cropped_plane():
         assert rep["mass_flow"] == pytest.approx(1.0 * 100e-6, rel=1e-4)
         with pytest.raises(A.LbmError):
             g.flow_report(A.PLANE_ZY, 500.0)
+
+
+@pytest.mark.parametrize("plane,frac", [(A.PLANE_XY, 0.013), (A.PLANE_ZY, -0.31), (A.PLANE_ZX, 0.07)])
+def test_flow_report_on_two_levels_matches_oracle(plane, frac):
+    """A refined Taylor-Green domain: the section image at the finest level,
+    filled by both levels (the coarse level's layers bracket the cut and are
+    blended), against the oracle's restatement of the same image."""
+    s = L.taylor_green(32)
+    c = s.case
+    c.grid_level_count = 2
+    q = float(s.domain_length)
+    c.refine_box[0][:] = (-0.2 * q, -0.25 * q, -0.2 * q, 0.22 * q, 0.25 * q, 0.2 * q)
+    d = O.OracleDomain(c)
+    cut = frac * q
+    with L.build_grids(c) as g:
+        g.update_all_grids(3)
+        d.step(3)
+        rep = g.flow_report(plane, cut)
+        t, level = d.flow_image(plane, cut)
+        info = g.info(level)
+        want = converted(t, info)
+        got = np.array(list(rep.values()))
+        assert got[6] == pytest.approx(want[6])  # same fluid pixels, areas of the image level
+        area = got[6] * 1e-6
+        ps = (info.res / 1000.0 / info.dt_phys) ** 2 / 3.0
+        unit = np.array([1.0, area, area, ps, area * ps, area])
+        assert np.all(np.abs(got[:6] - want[:6]) <= 1e-4 * np.abs(want[:6]) + 1e-6 * unit), (got, want)

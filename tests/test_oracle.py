@@ -80,3 +80,35 @@ def test_oracle_uniform_flow_stays_uniform():
     m1 = g.macro()
     assert np.max(np.abs(m1 - m0)) < 1e-6
     g.close()
+
+
+def test_section_image_of_one_level_equals_the_layer_sums():
+    """On one level the section image holds exactly the cut layer's cells, so
+    its sums equal the direct layer sums (crop included)."""
+    import lbm3_b200 as L
+    from lbm3_b200 import _abi as A
+    c = L.open_channel(24, 12, 10, u_in=0.04, nu_lattice=0.02)
+    d = O.OracleDomain(c)
+    o = O.OracleGrid(c)
+    d.step(3)
+    o.step(3)
+    p = L.Plan(c)
+    info = p.info()
+    bounds = (0.3, 2.8, 1.8, 23.7, 9.2, 7.2)
+    for plane, cut in ((A.PLANE_ZY, 8.5), (A.PLANE_XY, 4.5), (A.PLANE_ZX, 6.5)):
+        t, level = d.flow_image(plane, cut, bounds)
+        assert level == 0
+        axis = {A.PLANE_XY: 2, A.PLANE_ZY: 0, A.PLANE_ZX: 1}[plane]
+        o_ = (info.ox, info.oy, info.oz)
+        n = (info.cell_count_x, info.cell_count_y, info.cell_count_z)
+        layer = int(np.float32((cut - o_[axis]) / info.res + 0.5))
+        lo, hi = [], []
+        for a in range(3):
+            t_min = np.float32(o_[a] - 0.5 * info.res)
+            t_max = np.float32(o_[a] + info.res * (n[a] - 0.5))
+            lo.append(max(0, int(np.ceil(np.float32((bounds[a] - t_min) / info.res)))))
+            hi.append(min(n[a], n[a] - int(np.ceil(np.float32((t_max - bounds[a + 3]) / info.res)))))
+        ha, va = (0 if plane == A.PLANE_XY else 2), (0 if plane == A.PLANE_ZX else 1)
+        ref = o.flow_sums(plane, layer, lo[ha], hi[ha], lo[va], hi[va])
+        np.testing.assert_allclose(t, ref, rtol=1e-12, atol=1e-12)
+    o.close()
