@@ -806,11 +806,16 @@ __device__ __forceinline__ void storePair(const DevLevel& g, const int4& d, int 
     S* base = static_cast<S*>(g.f);
     const bool okA = t < len, okB = t + kHalf < len;
     if constexpr (sizeof(S) == 2) {
-        const unsigned cb = D.cell(d.x + t);
+        // one full hash per lane, then a 32-bit linear congruential step per
+        // direction (Numerical Recipes' constants) with its high half folded
+        // into the low half: three instructions per draw instead of a full
+        // finaliser in the hottest store loop
+        unsigned x = mix32(D.cell(d.x + t));
 #pragma unroll
         for (int q = 0; q < 27; ++q) {
             S* p = base + (runOffset32<F, false>(g, d, q) + t);
-            Store<S>::st2R(p, p + kHalf, f[q].v.x, f[q].v.y, Dither::dir(cb, q), okA, okB);
+            x = x * 1664525u + 1013904223u;
+            Store<S>::st2R(p, p + kHalf, f[q].v.x, f[q].v.y, x ^ (x >> 16), okA, okB);
         }
     } else {
 #pragma unroll
