@@ -385,7 +385,10 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
-                         "kernel": "collidePrefetch (bulk segments + wall-adjacent cells, one persistent launch)",
+                         "kernel": {"pair": "collidePair", "packed": "collidePacked", "prefetch": "collidePrefetch",
+                                    "tma": "collideBulkTma", "simple": "collideStream"}.get(
+                             os.environ.get("LBM3_COLLIDE_KERNEL", "pair") or "pair", "collidePair")
+                         + " (bulk segments + wall-adjacent cells, one persistent launch)",
                          "kernel_ms_per_launch": round(per_launch_ms, 5),
                          "collide_launches_per_step": round(launches / kt_steps, 3),
                          "algorithmic_bytes_per_launch": int(alg_bytes * kt_steps / max(launches, 1)),
