@@ -773,13 +773,15 @@ constexpr int kHalf = kTile / 2;
 #endif
 
 // Element offset of direction q's pre- (Pre) or post-collision run for the
-// tile with descriptor d: slot x stride + the neighbour row start.
+// tile with descriptor d: slot x stride + the neighbour row start.  The
+// callers read the stride once: a descriptor held in shared memory would
+// otherwise be read again after every store through a generic pointer.
 template <bool F, bool Pre>
-__device__ __forceinline__ int runOffset32(const DevLevel& g, const int4& d, int q) {
+__device__ __forceinline__ int runOffset32(int stride, const int4& d, int q) {
     const int k = Pre ? preNbr(q) : postNbr(q);
     const int b = (k >> 1) == 0 ? d.x : (k >> 1) == 1 ? d.y : (k >> 1) == 2 ? d.z : d.w;
     const int slot = Pre ? preSlot<F>(q) : postSlot<F>(q);
-    return slot * static_cast<int>(g.stride) + b + (k & 1);
+    return slot * stride + b + (k & 1);
 }
 
 // Load the 27 pre-collision values of lanes t and t + kHalf.  A partial tile
@@ -787,11 +789,12 @@ __device__ __forceinline__ int runOffset32(const DevLevel& g, const int4& d, int
 template <bool F, class S, bool kFull>
 __device__ __forceinline__ void loadPair(const DevLevel& g, const int4& d, int t, int len, Pair (&f)[27]) {
     const S* base = static_cast<const S*>(g.f);
+    const int stride = static_cast<int>(g.stride);
     const int tA = kFull ? t : min(t, len - 1);
     const bool okB = kFull || t + kHalf < len;
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
-        const S* p = base + (runOffset32<F, true>(g, d, q) + tA);
+        const S* p = base + (runOffset32<F, true>(stride, d, q) + tA);
         const float a = Store<S>::ld(p);
         const float b = okB ? Store<S>::ld(p + kHalf) : 0.f;
         f[q] = mkPair(a, b);
@@ -804,6 +807,7 @@ template <bool F, class S>
 __device__ __forceinline__ void storePair(const DevLevel& g, const int4& d, int t, int len, const Pair (&f)[27],
                                           const Dither& D) {
     S* base = static_cast<S*>(g.f);
+    const int stride = static_cast<int>(g.stride);
     const bool okA = t < len, okB = t + kHalf < len;
     if constexpr (sizeof(S) == 2) {
         // one full hash per lane, then a 32-bit linear congruential step per
@@ -813,14 +817,14 @@ __device__ __forceinline__ void storePair(const DevLevel& g, const int4& d, int 
         unsigned x = mix32(D.cell(d.x + t));
 #pragma unroll
         for (int q = 0; q < 27; ++q) {
-            S* p = base + (runOffset32<F, false>(g, d, q) + t);
+            S* p = base + (runOffset32<F, false>(stride, d, q) + t);
             x = x * 1664525u + 1013904223u;
             Store<S>::st2R(p, p + kHalf, f[q].v.x, f[q].v.y, x ^ (x >> 16), okA, okB);
         }
     } else {
 #pragma unroll
         for (int q = 0; q < 27; ++q) {
-            S* p = base + (runOffset32<F, false>(g, d, q) + t);
+            S* p = base + (runOffset32<F, false>(stride, d, q) + t);
             if (okA) Store<S>::st(p, f[q].v.x);
             if (okB) Store<S>::st(p + kHalf, f[q].v.y);
         }
