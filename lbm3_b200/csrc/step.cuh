@@ -315,17 +315,19 @@ template <bool F> __device__ __forceinline__ constexpr int postSlot(int d) { ret
 template <bool F, class S, class T>
 __device__ __forceinline__ void readPre(const DevLevel& g, const int (&nb)[8], T (&f)[27]) {
     const S* base = static_cast<const S*>(g.f);
+    const long long stride = g.stride;
 #pragma unroll
     for (int d = 0; d < 27; ++d)
-        f[d] = Store<S>::ld(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)]);
+        f[d] = Store<S>::ld(base + (long long)preSlot<F>(d) * stride + nb[preNbr(d)]);
 }
 
 template <bool F, class S, class T>
 __device__ __forceinline__ void writePost(const DevLevel& g, const int (&nb)[8], const T (&f)[27], const Dither& D) {
     S* base = static_cast<S*>(g.f);
+    const long long stride = g.stride;  // once: stores may alias a descriptor in memory
     const unsigned cb = D.cell(nb[0]);
 #pragma unroll
-    for (int d = 0; d < 27; ++d) stD(base + (long long)postSlot<F>(d) * g.stride + nb[postNbr(d)], f[d], D, cb, d);
+    for (int d = 0; d < 27; ++d) stD(base + (long long)postSlot<F>(d) * stride + nb[postNbr(d)], f[d], D, cb, d);
 }
 
 // Write f as pre-collision values of the cell (used by initial condition and
@@ -333,18 +335,20 @@ __device__ __forceinline__ void writePost(const DevLevel& g, const int (&nb)[8],
 template <bool F, class S, class T>
 __device__ __forceinline__ void writePre(const DevLevel& g, const int (&nb)[8], const T (&f)[27]) {
     S* base = static_cast<S*>(g.f);
+    const long long stride = g.stride;  // once: stores may alias a descriptor in memory
 #pragma unroll
     for (int d = 0; d < 27; ++d)
-        Store<S>::st(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)], f[d]);
+        Store<S>::st(base + (long long)preSlot<F>(d) * stride + nb[preNbr(d)], f[d]);
 }
 
 // writePre of interpolated values (interface), rounded like collided ones.
 template <bool F, class S, class T>
 __device__ __forceinline__ void writePreD(const DevLevel& g, const int (&nb)[8], const T (&f)[27], const Dither& D) {
     S* base = static_cast<S*>(g.f);
+    const long long stride = g.stride;  // once: stores may alias a descriptor in memory
     const unsigned cb = D.cell(nb[0]);
 #pragma unroll
-    for (int d = 0; d < 27; ++d) stD(base + (long long)preSlot<F>(d) * g.stride + nb[preNbr(d)], f[d], D, cb, d);
+    for (int d = 0; d < 27; ++d) stD(base + (long long)preSlot<F>(d) * stride + nb[preNbr(d)], f[d], D, cb, d);
 }
 
 }  // namespace lbm
