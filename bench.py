@@ -690,7 +690,9 @@ def run_serving(args):
                    f"{cal_wall:.1f} s", "offered_load_fraction": load,
                    "arrival_rate_per_s": round(rate, 4),
                    "offered_mlups": round(offered, 1) if offered else None,
-                   "parallelism": "continuous batching, one stream per domain, grids built on 2 host threads"},
+                   "parallelism": "continuous batching: the resident domains of each storage type advance as one "
+                                  "packed batch (one persistent collide-stream launch per step), rebuilt as "
+                                  "requests join and leave; grids built on 2 host threads"},
         "serving": {"requests": summ["requests"], "p50_s": round(summ["p50_s"], 4), "p99_s": round(summ["p99_s"], 4),
                     "wall_s": round(wall, 3)},
     }
